@@ -1,0 +1,150 @@
+/*
+ * metad_b200.h -- C ABI of libmetad_b200.so, the sm_100a implementation of
+ * Metad-toy's metadynamics hot path (STEINH Steinhardt CVs, structure factor,
+ * Gaussian-hill bias grid) behind the `fix metad` argument grammar.
+ *
+ * Every entry point takes plain pointers and sizes.  Each one names the
+ * reference interface it replaces (paths inside the Metad-toy project).
+ *
+ * Threading: one host thread per context; calls on one context are not
+ * thread-safe.  Each context owns one CUDA stream and all of its device
+ * memory.  Caller arrays are borrowed for the duration of a call only.
+ */
+#ifndef METAD_B200_H
+#define METAD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MTD_ABI_VERSION 1
+
+/* Status codes.  The reference stops the run through error->all() / exit(1)
+ * (include/utils/zqc_debug.h:59-78); this library returns a code and keeps a
+ * message for mtd_last_error(). */
+typedef enum {
+    MTD_OK = 0,
+    MTD_ERR_INVALID_ARG = 1,
+    MTD_ERR_PARSE = 2,
+    MTD_ERR_CUDA = 3,
+    MTD_ERR_OOM = 4,
+    MTD_ERR_NEIGH_OVERFLOW = 5,
+    MTD_ERR_TIMEOUT = 6,
+    MTD_ERR_NAN = 7,
+    MTD_ERR_IO = 8,
+    MTD_ERR_UNSUPPORTED = 9
+} mtd_status;
+
+/* Per-atom arithmetic.  MIXED: FP32 per-atom/per-pair work, FP64 global sums,
+ * grid and well-tempered height.  FP64: everything in double. */
+typedef enum { MTD_PREC_MIXED = 0, MTD_PREC_FP64 = 1 } mtd_precision;
+
+typedef struct mtd_ctx mtd_ctx;
+
+typedef struct {
+    int precision;                    /* mtd_precision */
+    int device;                       /* CUDA device ordinal */
+    double boltz;                     /* force->boltz (metal units: 8.617343e-5 eV/K) */
+    int n_groups;                     /* LAMMPS group table: name -> bitmask, used by CAL ... <group> */
+    const char *const *group_names;
+    const int *group_bits;
+    const char *hills_path;           /* HILLS file; NULL -> "HILLS"; "" -> no file */
+    const char *work_dir;             /* directory for rec.log and relative paths; NULL -> CWD */
+} mtd_options;
+
+/* Fills defaults: MIXED, device 0, boltz 8.617343e-5, group "all" -> bit 1. */
+void mtd_options_default(mtd_options *opt);
+
+/* Parse the `fix ID group metad ...` arguments (the tokens after the style
+ * name, i.e. the reference's arg[3..]) and build a context.
+ * Replaces FixMetadynamics::FixMetadynamics (src/core/fix_crystallize.cu:32-302),
+ * CVFactory::create (src/core/CVFactory.cu:17-29), Steinhardt::create
+ * (src/cvs/CVs_Steinhardt.cu:33-161), Stru_factor::create
+ * (src/cvs/CVs_Strufactor.cu:34-237) and SwitchFunction::create
+ * (include/utils/zqc_switch_function.h:81-161). */
+mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, mtd_ctx **out);
+
+/* Replaces FixMetadynamics::~FixMetadynamics (src/core/fix_crystallize.cu:304-337).
+ * mtd_create leaves a context in *out even when it fails, so that
+ * mtd_last_error() can report why; destroy it either way. */
+void mtd_destroy(mtd_ctx *ctx);
+
+/* Host-only check of the same argument grammar, no GPU touched: returns the
+ * status mtd_create would return for a parse error and copies the message
+ * into err (errlen bytes).  Same reference lines as mtd_create. */
+mtd_status mtd_parse_args(int narg, const char *const *arg, const mtd_options *opt, char *err, int errlen);
+
+/* Host-only evaluation of a DIM expression over named symbol values, with the
+ * exact partial derivatives d expr / d symbol (grad, nsym values).  The device
+ * evaluates the same bytecode every step.  Replaces the exprtk expression and
+ * exprtk::derivative of MetaDimensionManager (src/grids/DimSet.cu:54-97). */
+mtd_status mtd_eval_expression(const char *expr, int nsym, const char *const *names, const double *values,
+                               double *value, double *grad);
+
+/* Box geometry (domain->boxlo/boxhi, x/y/zperiodic); orthogonal boxes.
+ * Replaces the box read in Steinhardt_env::get_env (src/cvs/CVs_Steinhardt.cu:443-446). */
+mtd_status mtd_set_box(mtd_ctx *ctx, const double lo[3], const double hi[3], const int periodic[3]);
+
+/* First-run initialisation: allocates the bias grid, replays HILLS when
+ * METAD_RESTART 1, opens HILLS for writing/appending.
+ * Replaces FixMetadynamics::init (src/core/fix_crystallize.cu:343-378),
+ * GH_t0_uniformGrid::init_set_mode/init_hills (src/grids/GH_t0_uniformGrid.cu:74-192). */
+mtd_status mtd_init(mtd_ctx *ctx);
+
+/* One MD step on host arrays: computes every CAL, the DIM values, deposits a
+ * hill when step % PACE == 0, evaluates V(s) and dV/ds, and subtracts the bias
+ * force from f (AoS n*3, in place).  mask: LAMMPS atom->mask (NULL = every
+ * atom in every group).  image: LAMMPS packed imageint (default 10-bit layout)
+ * used to unwrap x for the virial; NULL = x taken as unwrapped.  virial (6,
+ * may be NULL) receives sum over atoms of r (x) delta_f as
+ * (xx, yy, zz, xy, xz, yz).
+ * Replaces FixMetadynamics::post_force (src/core/fix_crystallize.cu:386-472). */
+mtd_status mtd_post_force(mtd_ctx *ctx, int64_t step, int n, const double *x, const int *mask,
+                          const int *image, double *f, double virial[6]);
+
+/* Same step on device-resident arrays, enqueued on the context stream without
+ * a host synchronisation.  f_in and f_out may alias.  Completion and device
+ * error flags are collected by mtd_sync(). */
+mtd_status mtd_post_force_device(mtd_ctx *ctx, int64_t step, int n, const double *d_x, const int *d_mask,
+                                 const int *d_image, const double *d_f_in, double *d_f_out);
+
+/* Waits for the context stream and reports device-side errors (neighbour
+ * overflow, NaN forces, timeouts) raised by earlier asynchronous calls. */
+mtd_status mtd_sync(mtd_ctx *ctx);
+
+/* Thermo output.  Replaces FixMetadynamics::compute_scalar / compute_vector
+ * (src/core/fix_crystallize.cu:484-494): bias energy V_b(s) and CV k (0-based). */
+double mtd_compute_scalar(const mtd_ctx *ctx);
+double mtd_compute_vector(const mtd_ctx *ctx, int k);
+int mtd_cv_dim(const mtd_ctx *ctx);
+
+/* Per-atom export for `compute metad/atom` / Fix::extract
+ * ("colvar_peratom:<CAL>.<prop>", props stein_q, dcvdx_x/y/z, stru_f).
+ * Copies n values (caller order) into out.
+ * Replaces FixMetadynamics::extract (src/core/fix_crystallize.cu:592-613),
+ * STEIN_QL::get_peratom_ptr (src/cvs/CVs_Steinhardt.cu:1278-1322),
+ * Stru_factor::get_peratom_ptr (src/cvs/CVs_Strufactor.cu:974-979). */
+mtd_status mtd_extract_peratom(mtd_ctx *ctx, const char *key, double *out, int n);
+
+/* Replays a HILLS file into the grid (rows `step cv[D] height sigma`).
+ * Replaces GH_t0_uniformGrid::init_hills (src/grids/GH_t0_uniformGrid.cu:101-192). */
+mtd_status mtd_hills_replay(mtd_ctx *ctx, const char *path);
+
+/* Copies the bias grid (FP64, row-major, dimension 0 slowest) to host. */
+mtd_status mtd_get_grid(mtd_ctx *ctx, double *out, int64_t count);
+
+/* Number of device kernels the last step launched (diagnostics). */
+int mtd_last_launch_count(const mtd_ctx *ctx);
+
+/* Largest neighbour count seen by the last step for CAL `name` (cap reporting). */
+int mtd_max_neighbors(mtd_ctx *ctx, const char *name);
+
+const char *mtd_last_error(const mtd_ctx *ctx);
+int mtd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

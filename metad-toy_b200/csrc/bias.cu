@@ -1,0 +1,363 @@
+// bias.cu -- the per-step bias kernel: global CV reductions, DIM expressions,
+// well-tempered hill deposit on the FP64 grid, Catmull-Rom V(s) and dV/ds, and
+// the chain-rule coefficients handed to the force kernels.  One block; the
+// step number is a kernel argument so no host round trip is needed.
+//
+// Replaces, on the device:
+//   KahanAverager / compute_sw reductions   src/utils/CVs_tools.cu:6-55
+//   MetaDimensionManager::compute_*          src/grids/DimSet.cu:68-97
+//   GH_t0_uniformGrid::add_hill/add_to_grid  src/grids/GH_t0_uniformGrid.cu:195-282
+//   GH_t0_uniformGrid::get_dVdcv/get_bias_energy  :313-461
+// Built with -fmad=false so the deposit's bin-centre and Gaussian arithmetic
+// rounds like the FP64 oracle.
+#include "kernels.h"
+
+namespace mtd {
+
+namespace {
+
+__device__ __forceinline__ double cr_value(double p0, double p1, double p2, double p3, double x) {
+    return p1 + 0.5 * x * ((p2 - p0) + x * (2.0 * p0 - 5.0 * p1 + 4.0 * p2 - p3) + x * x * (-p0 + 3.0 * p1 - 3.0 * p2 + p3));
+}
+__device__ __forceinline__ double cr_deriv(double p0, double p1, double p2, double p3, double x) {
+    return 0.5 * ((p2 - p0) + 2.0 * x * (2.0 * p0 - 5.0 * p1 + 4.0 * p2 - p3) + 3.0 * x * x * (-p0 + 3.0 * p1 - 3.0 * p2 + p3));
+}
+__device__ __forceinline__ void center_frac_clamp(double cv, double lo, double h, int nb, int &i, double &f) {
+    double u = (cv - lo) / h - 0.5;
+    i = (int)floor(u);
+    f = u - i;
+    if (i < 1) { i = 1; f = 0.0; }
+    if (i > nb - 3) { i = nb - 3; f = 1.0; }
+}
+
+// Catmull-Rom value and gradient on the bin-centred grid (dimension 0 slowest).
+__device__ double grid_value(const BiasPlan &P, const double *s, double *dV) {
+    int ix[3];
+    double fx[3];
+    for (int k = 0; k < P.D; ++k) center_frac_clamp(s[k], P.lo[k], P.dcv[k], P.nbin[k], ix[k], fx[k]);
+    const double *G = P.grid;
+    double V;
+    if (P.D == 1) {
+        const double *p = G + ix[0] - 1;
+        V = cr_value(p[0], p[1], p[2], p[3], fx[0]);
+        dV[0] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]) / P.dcv[0];
+        if (isnan(dV[0])) dV[0] = 0.0;
+    } else if (P.D == 2) {
+        double col[4], dcol[4];
+        const int n1 = P.nbin[1];
+        for (int t = 0; t < 4; ++t) {
+            const int jj = ix[1] - 1 + t;
+            double p0 = G[(ix[0] - 1) * n1 + jj], p1 = G[ix[0] * n1 + jj];
+            double p2 = G[(ix[0] + 1) * n1 + jj], p3 = G[(ix[0] + 2) * n1 + jj];
+            col[t] = cr_value(p0, p1, p2, p3, fx[0]);
+            dcol[t] = cr_deriv(p0, p1, p2, p3, fx[0]);
+        }
+        V = cr_value(col[0], col[1], col[2], col[3], fx[1]);
+        dV[0] = cr_value(dcol[0], dcol[1], dcol[2], dcol[3], fx[1]) / P.dcv[0];
+        dV[1] = cr_deriv(col[0], col[1], col[2], col[3], fx[1]) / P.dcv[1];
+        if (isnan(dV[0]) || isnan(dV[1])) { dV[0] = 0.0; dV[1] = 0.0; }
+    } else {
+        const int n1 = P.nbin[1], n2 = P.nbin[2];
+        double a[4], da[4], b0[4];
+        for (int u = 0; u < 4; ++u) {
+            const int kk = ix[2] - 1 + u;
+            double c[4], dc[4];
+            for (int t = 0; t < 4; ++t) {
+                const int jj = ix[1] - 1 + t;
+                double p[4];
+                for (int q = 0; q < 4; ++q) p[q] = G[((ix[0] - 1 + q) * n1 + jj) * n2 + kk];
+                c[t] = cr_value(p[0], p[1], p[2], p[3], fx[0]);
+                dc[t] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]);
+            }
+            a[u] = cr_value(c[0], c[1], c[2], c[3], fx[1]);
+            da[u] = cr_deriv(c[0], c[1], c[2], c[3], fx[1]);
+            b0[u] = cr_value(dc[0], dc[1], dc[2], dc[3], fx[1]);
+        }
+        V = cr_value(a[0], a[1], a[2], a[3], fx[2]);
+        dV[0] = cr_value(b0[0], b0[1], b0[2], b0[3], fx[2]) / P.dcv[0];
+        dV[1] = cr_value(da[0], da[1], da[2], da[3], fx[2]) / P.dcv[1];
+        dV[2] = cr_deriv(a[0], a[1], a[2], a[3], fx[2]) / P.dcv[2];
+        if (isnan(dV[0]) || isnan(dV[1]) || isnan(dV[2])) dV[0] = dV[1] = dV[2] = 0.0;
+    }
+    return V;
+}
+
+// Band of a hill: [c - R, c + R] clipped to the grid, c = (int)((s - lo)/dcv)
+// (C truncation as in add_to_grid), R from the fix's sigma.
+__device__ __forceinline__ void hill_band(const BiasPlan &P, const double *s, int *lo, int *hi) {
+    for (int k = 0; k < P.D; ++k) {
+        const int c = (int)((s[k] - P.lo[k]) / P.dcv[k]);
+        lo[k] = max(0, c - P.band[k]);
+        hi[k] = min(P.nbin[k] - 1, c + P.band[k]);
+    }
+}
+
+__device__ __forceinline__ double hill_gauss(const BiasPlan &P, const double *s, const int *idx, double sigma) {
+    double r2 = 0.0;
+    for (int k = 0; k < P.D; ++k) {
+        const double c = P.lo[k] + (idx[k] + 0.5) * (P.hi[k] - P.lo[k]) / P.nbin[k];
+        const double dx = s[k] - c;
+        r2 = r2 + dx * dx;
+    }
+    return exp(-0.5 * r2 / (sigma * sigma));
+}
+
+struct Dual {
+    double v;
+    double g[kMaxSymbols];
+};
+
+__device__ double eval_code(const ExprInstr *code, int n, const double *sym, int nsym, double *grad) {
+    Dual st[kMaxExprStack];
+    int sp = 0;
+    for (int p = 0; p < n; ++p) {
+        const ExprInstr c = code[p];
+        if (c.op == EOP_CONST || c.op == EOP_SYM) {
+            st[sp].v = (c.op == EOP_CONST) ? c.val : sym[c.arg];
+            for (int k = 0; k < nsym; ++k) st[sp].g[k] = (c.op == EOP_SYM && k == c.arg) ? 1.0 : 0.0;
+            ++sp;
+            continue;
+        }
+        if (c.op == EOP_ADD || c.op == EOP_SUB || c.op == EOP_MUL || c.op == EOP_DIV || c.op == EOP_POW ||
+            c.op == EOP_MIN || c.op == EOP_MAX || c.op == EOP_ATAN2) {
+            Dual &a = st[sp - 2];
+            const Dual &b = st[sp - 1];
+            double v, da, db;
+            switch (c.op) {
+            case EOP_ADD: v = a.v + b.v; da = 1; db = 1; break;
+            case EOP_SUB: v = a.v - b.v; da = 1; db = -1; break;
+            case EOP_MUL: v = a.v * b.v; da = b.v; db = a.v; break;
+            case EOP_DIV: v = a.v / b.v; da = 1.0 / b.v; db = -a.v / (b.v * b.v); break;
+            case EOP_POW: v = pow(a.v, b.v); da = b.v * pow(a.v, b.v - 1.0); db = (a.v > 0) ? v * log(a.v) : 0.0; break;
+            case EOP_MIN: v = a.v <= b.v ? a.v : b.v; da = a.v <= b.v; db = !(a.v <= b.v); break;
+            case EOP_MAX: v = a.v >= b.v ? a.v : b.v; da = a.v >= b.v; db = !(a.v >= b.v); break;
+            default: { double r2 = a.v * a.v + b.v * b.v; v = atan2(a.v, b.v); da = b.v / r2; db = -a.v / r2; }
+            }
+            for (int k = 0; k < nsym; ++k) a.g[k] = da * a.g[k] + db * b.g[k];
+            a.v = v;
+            --sp;
+            continue;
+        }
+        Dual &a = st[sp - 1];
+        const double x = a.v;
+        double v = 0, dv = 0;
+        switch (c.op) {
+        case EOP_NEG: v = -x; dv = -1; break;
+        case EOP_SIN: v = sin(x); dv = cos(x); break;
+        case EOP_COS: v = cos(x); dv = -sin(x); break;
+        case EOP_TAN: v = tan(x); dv = 1.0 + v * v; break;
+        case EOP_ASIN: v = asin(x); dv = 1.0 / sqrt(1.0 - x * x); break;
+        case EOP_ACOS: v = acos(x); dv = -1.0 / sqrt(1.0 - x * x); break;
+        case EOP_ATAN: v = atan(x); dv = 1.0 / (1.0 + x * x); break;
+        case EOP_EXP: v = exp(x); dv = v; break;
+        case EOP_LOG: v = log(x); dv = 1.0 / x; break;
+        case EOP_LOG10: v = log10(x); dv = 1.0 / (x * 2.30258509299404568402); break;
+        case EOP_SQRT: v = sqrt(x); dv = 0.5 / v; break;
+        case EOP_ABS: v = fabs(x); dv = (x > 0) - (x < 0); break;
+        case EOP_TANH: v = tanh(x); dv = 1.0 - v * v; break;
+        case EOP_SINH: v = sinh(x); dv = cosh(x); break;
+        case EOP_COSH: v = cosh(x); dv = sinh(x); break;
+        }
+        for (int k = 0; k < nsym; ++k) a.g[k] *= dv;
+        a.v = v;
+    }
+    for (int k = 0; k < nsym; ++k) grad[k] = st[0].g[k];
+    return st[0].v;
+}
+
+__global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
+    const BiasPlan &P = *Pp;
+    __shared__ double smem[8 * 32];
+    __shared__ double usum[kMaxUnits][8];
+    __shared__ double sv[kMaxDim];
+    __shared__ double hill_w;
+    __shared__ int do_dep;
+    // 1. deterministic reductions of every unit's block partials
+    for (int u = 0; u < P.nunit; ++u) {
+        const UnitPlan &U = P.unit[u];
+        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (U.partials) {
+            for (int b = threadIdx.x; b < U.nparts; b += blockDim.x)
+                for (int t = 0; t < U.nvals && t < 8; ++t) v[t] += U.partials[(size_t)b * U.pstride + t];
+        }
+        block_sum<8>(v, smem);
+        if (threadIdx.x == 0)
+            for (int t = 0; t < 8; ++t) usum[u][t] = v[t];
+        __syncthreads();
+    }
+    double jac[kMaxDim][kMaxSymbols];
+    if (threadIdx.x == 0) {
+        // 2. symbol values
+        double sym[kMaxSymbols];
+        for (int q = 0; q < P.nsym; ++q) {
+            const SymPlan &S = P.sym[q];
+            const double *us = usum[S.unit];
+            double v = 0.0;
+            switch (S.kind) {
+            case SYM_Q_AVE: v = us[3] > 0 ? us[0] / us[3] : 0.0; break;
+            case SYM_Q_SW: v = us[1 + S.slot]; break;
+            case SYM_L_MEAN: v = us[2 * S.slot + 1] != 0.0 ? us[2 * S.slot] / us[2 * S.slot + 1] : 0.0; break;
+            case SYM_L_NSOLID: v = us[2 * S.slot + 1]; break;
+            case SYM_L_FRAC: v = us[4] > 0 ? us[2 * S.slot + 1] / us[4] : 0.0; break;
+            case SYM_SF_AVE: v = us[2] > 0 ? us[0] / us[2] : 0.0; break;
+            case SYM_SF_COUNT: v = us[1]; break;
+            case SYM_SK_AVE: {
+                const UnitPlan &U = P.unit[S.unit];
+                const double N = *U.sk_n;
+                double acc = 0.0;
+                for (int k = 0; k < U.K; ++k) acc += U.rho[2 * k] * U.rho[2 * k] + U.rho[2 * k + 1] * U.rho[2 * k + 1];
+                v = (N > 0 && U.K > 0) ? acc / N / U.K : 0.0;
+                break;
+            }
+            }
+            sym[q] = v;
+            P.out[kOutSymOffset + q] = v;
+        }
+        // 3. DIM expressions with exact chain factors
+        for (int dd = 0; dd < P.D; ++dd) sv[dd] = eval_code(P.code[dd], P.ncode[dd], sym, P.nsym, jac[dd]);
+        // 4. well-tempered height from V(s) before the deposit
+        do_dep = (P.pace != 0) && (step % P.pace == 0);
+        if (do_dep) {
+            double dV[kMaxDim];
+            double Vb = P.wt ? grid_value(P, sv, dV) : 0.0;
+            hill_w = P.h0 * exp(-(Vb) / (P.temp * P.kb * (P.biasf - 1.0)));
+        }
+    }
+    __syncthreads();
+    // 5. banded deposit, one thread per band bin
+    if (do_dep) {
+        int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
+        hill_band(P, sv, lo, hi);
+        int total = 1;
+        for (int k = 0; k < P.D; ++k) {
+            ext[k] = hi[k] - lo[k] + 1;
+            total *= ext[k];
+        }
+        for (int t = threadIdx.x; t < total; t += blockDim.x) {
+            int idx[3] = {0, 0, 0}, rem = t;
+            for (int k = P.D - 1; k >= 0; --k) {
+                idx[k] = lo[k] + rem % ext[k];
+                rem /= ext[k];
+            }
+            size_t g = idx[0];
+            for (int k = 1; k < P.D; ++k) g = g * P.nbin[k] + idx[k];
+            P.grid[g] += hill_w * hill_gauss(P, sv, idx, P.sigma);
+        }
+        if (threadIdx.x == 0) {
+            unsigned long long h = *P.nhills;
+            HillRec r;
+            r.step = step;
+            for (int k = 0; k < 3; ++k) r.s[k] = k < P.D ? sv[k] : 0.0;
+            r.w = hill_w;
+            r.sigma = P.sigma;
+            P.hills[h % (unsigned long long)P.hill_cap] = r;
+            *P.nhills = h + 1;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // 6. V and dV/ds at s after the deposit, chain rule to every symbol
+        double dV[kMaxDim] = {0, 0, 0, 0};
+        const double V = grid_value(P, sv, dV);
+        double alpha[kMaxSymbols];
+        for (int q = 0; q < P.nsym; ++q) {
+            double a = 0.0;
+            for (int dd = 0; dd < P.D; ++dd) a += dV[dd] * jac[dd][q];
+            alpha[q] = a;
+        }
+        for (int dd = 0; dd < P.D; ++dd) P.out[dd] = sv[dd];
+        P.out[P.D] = V;
+        P.out[P.D + 1] = do_dep ? 1.0 : 0.0;
+        // 7. per-unit force coefficients
+        for (int u = 0; u < P.nunit; ++u) {
+            const UnitPlan &U = P.unit[u];
+            const double *us = usum[u];
+            double c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            if (U.kind == 1) {   // STEINH L: c1 = aM/W, c2 = -aM cv/W + aN + aF/max(N,1) per order
+                for (int slot = 0; slot < 2; ++slot) {
+                    double aM = 0, aN = 0, aF = 0;
+                    for (int q = 0; q < P.nsym; ++q) {
+                        if (P.sym[q].unit != u || P.sym[q].slot != slot) continue;
+                        if (P.sym[q].kind == SYM_L_MEAN) aM += alpha[q];
+                        if (P.sym[q].kind == SYM_L_NSOLID) aN += alpha[q];
+                        if (P.sym[q].kind == SYM_L_FRAC) aF += alpha[q];
+                    }
+                    const double S1 = us[2 * slot], S0 = us[2 * slot + 1], N = us[4];
+                    const double W = fmax(S0, 1e-300);
+                    const double cv = S0 != 0.0 ? S1 / S0 : 0.0;
+                    c[2 * slot] = aM / W;
+                    c[2 * slot + 1] = -aM * cv / W + aN + aF / fmax(N, 1.0);
+                }
+            } else if (U.kind == 0) {   // STEINH Q: c_ave = a/N, c_sw = a
+                for (int q = 0; q < P.nsym; ++q) {
+                    if (P.sym[q].unit != u) continue;
+                    if (P.sym[q].kind == SYM_Q_AVE) c[0] += us[3] > 0 ? alpha[q] / us[3] : 0.0;
+                    if (P.sym[q].kind == SYM_Q_SW) c[1 + P.sym[q].slot] += alpha[q];
+                }
+            } else if (U.kind == 2) {   // STRU_FACTOR: c_ave = a/N, c_count = a
+                for (int q = 0; q < P.nsym; ++q) {
+                    if (P.sym[q].unit != u) continue;
+                    if (P.sym[q].kind == SYM_SF_AVE) c[0] += us[2] > 0 ? alpha[q] / us[2] : 0.0;
+                    if (P.sym[q].kind == SYM_SF_COUNT) c[1] += alpha[q];
+                }
+            } else {   // S(k): 2 a / (N K)
+                const double N = U.sk_n ? *U.sk_n : 0.0;
+                for (int q = 0; q < P.nsym; ++q)
+                    if (P.sym[q].unit == u && P.sym[q].kind == SYM_SK_AVE && N > 0 && U.K > 0)
+                        c[0] += 2.0 * alpha[q] / (N * U.K);
+            }
+            for (int t = 0; t < 8; ++t) U.coef[t] = c[t];
+        }
+    }
+}
+
+// HILLS replay: every thread owns grid bins and adds the hills in file order,
+// so the FP64 sum order per bin is the file order.
+__global__ void k_hills_replay(const BiasPlan *__restrict__ Pp, const HillRec *__restrict__ h, int nh, int ncell) {
+    const BiasPlan &P = *Pp;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ncell; g += gridDim.x * blockDim.x) {
+        int idx[3] = {0, 0, 0}, rem = g;
+        for (int k = P.D - 1; k >= 0; --k) {
+            idx[k] = rem % P.nbin[k];
+            rem /= P.nbin[k];
+        }
+        double acc = P.grid[g];
+        for (int q = 0; q < nh; ++q) {
+            int lo[3], hi[3];
+            hill_band(P, h[q].s, lo, hi);
+            bool in = true;
+            for (int k = 0; k < P.D; ++k) in = in && idx[k] >= lo[k] && idx[k] <= hi[k];
+            if (in) acc += h[q].w * hill_gauss(P, h[q].s, idx, h[q].sigma);
+        }
+        P.grid[g] = acc;
+    }
+}
+
+__global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, double *out6) {
+    __shared__ double smem[6 * 32];
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+        for (int t = 0; t < 6; ++t) v[t] += vpart[(size_t)b * 8 + t];
+    block_sum<6>(v, smem);
+    if (threadIdx.x == 0)
+        for (int t = 0; t < 6; ++t) out6[t] = v[t];
+}
+
+}  // namespace
+
+void launch_bias_step(const BiasPlan *d_plan, long long step, int, cudaStream_t st) {
+    k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
+}
+
+void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st) {
+    if (nh <= 0 || ncell <= 0) return;
+    int blocks = (ncell + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    k_hills_replay<<<blocks, 256, 0, st>>>(d_plan, h, nh, ncell);
+}
+
+void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st) {
+    k_virial_finalize<<<1, 256, 0, st>>>(vpart, nparts, out6);
+}
+
+}  // namespace mtd

@@ -1,0 +1,166 @@
+// common.cuh -- shared types, switching functions and small device helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <type_traits>
+
+namespace mtd {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kBlock = 256;          // threads per block for per-atom kernels
+constexpr int kMaxSymbols = 16;      // SYMBOL entries per context
+constexpr int kMaxDim = 4;           // CV_dim handled by the device grid kernel
+constexpr int kFlagBit = 30;         // pair.j bit: neighbour kept by the centre (STEINH Q cap)
+
+enum SwType { SW_LINE = 0, SW_STEP = 1, SW_FERMI = 2, SW_TANH = 3, SW_RATIONAL = 4 };
+
+// Switching-function parameters passed by value to kernels; the same fields as
+// SwitchFunctionRequest (include/utils/zqc_switch_function.h:24-31).
+struct SwParams {
+    int type;
+    double r0, d0, alpha;
+    int n, m;
+};
+
+template <typename T> __host__ __device__ __forceinline__ T ipow_t(T x, int n) {
+    T r = T(1);
+    T b = x;
+    int e = n < 0 ? -n : n;
+    while (e) {
+        if (e & 1) r *= b;
+        b *= b;
+        e >>= 1;
+    }
+    return n < 0 ? T(1) / r : r;
+}
+
+template <typename T> __host__ __device__ __forceinline__ T t_exp(T x);
+template <> __host__ __device__ __forceinline__ double t_exp<double>(double x) { return exp(x); }
+template <> __host__ __device__ __forceinline__ float t_exp<float>(float x) { return expf(x); }
+template <typename T> __host__ __device__ __forceinline__ T t_tanh(T x);
+template <> __host__ __device__ __forceinline__ double t_tanh<double>(double x) { return tanh(x); }
+template <> __host__ __device__ __forceinline__ float t_tanh<float>(float x) { return tanhf(x); }
+template <typename T> __host__ __device__ __forceinline__ T t_sqrt(T x);
+template <> __host__ __device__ __forceinline__ double t_sqrt<double>(double x) { return sqrt(x); }
+template <> __host__ __device__ __forceinline__ float t_sqrt<float>(float x) { return sqrtf(x); }
+
+// f and df of the switching functions, following
+// include/utils/zqc_switch_function.h:163-313 case by case (the RATIONAL n == 2m
+// branch returns 1 + x^m exactly as the reference does).
+template <typename T> __host__ __device__ __forceinline__ T sw_f(const SwParams &p, T x) {
+    switch (p.type) {
+    case SW_LINE: return T(1);
+    case SW_STEP: return (x < T(p.r0)) ? T(1) : T(0);
+    case SW_FERMI: return T(1) / (T(1) + t_exp<T>(-T(p.alpha) * (x - T(p.r0))));
+    case SW_TANH: return T(0.5) * (T(1) + t_tanh<T>(T(p.alpha) * (x - T(p.r0))));
+    case SW_RATIONAL: {
+        const int n = p.n, m = p.m;
+        T y = (x - T(p.d0)) / T(p.r0);
+        if (n == 6 && m == 12) { T y2 = y * y; T y6 = y2 * y2 * y2; return T(1) / (T(1) + y6); }
+        if (n == 4 && m == 8) { T y2 = y * y; T y4 = y2 * y2; return T(1) / (T(1) + y4); }
+        if (2 * n == m) return T(1) / (T(1) + ipow_t(y, n));
+        if (n == 2 * m) return T(1) + ipow_t(y, m);
+        return (T(1) - ipow_t(y, n)) / (T(1) - ipow_t(y, m));
+    }
+    default: return T(1);
+    }
+}
+
+template <typename T> __host__ __device__ __forceinline__ T sw_df(const SwParams &p, T x) {
+    switch (p.type) {
+    case SW_LINE: return T(0);
+    case SW_STEP: return T(0);
+    case SW_FERMI: {
+        T e = t_exp<T>(-T(p.alpha) * (x - T(p.r0)));
+        T den = T(1) + e;
+        return (T(p.alpha) * e) / (den * den);
+    }
+    case SW_TANH: {
+        T t = t_tanh<T>(T(p.alpha) * (x - T(p.r0)));
+        return T(0.5) * T(p.alpha) * (T(1) - t * t);
+    }
+    case SW_RATIONAL: {
+        const int n = p.n, m = p.m;
+        T y = (x - T(p.d0)) / T(p.r0);
+        if (n == 6 && m == 12) {
+            T y2 = y * y, y5 = y2 * y2 * y, y6 = y2 * y2 * y2;
+            return -T(n) * y5 / ((T(1) + y6) * (T(1) + y6)) / T(p.r0);
+        }
+        if (n == 4 && m == 8) {
+            T y2 = y * y, y3 = y2 * y, y4 = y2 * y2;
+            return -T(n) * y3 / ((T(1) + y4) * (T(1) + y4)) / T(p.r0);
+        }
+        if (2 * n == m) {
+            T a = ipow_t(y, n - 1), b = ipow_t(y, n);
+            return -T(n) * a / ((T(1) + b) * (T(1) + b)) / T(p.r0);
+        }
+        if (n == 2 * m) return T(m) * ipow_t(y, m - 1) / T(p.r0);
+        T ymm1 = ipow_t(y, m - 1), ym = ymm1 * y;
+        T one_m = T(1) - ym;
+        if ((one_m < T(0) ? -one_m : one_m) < T(1e-12)) return T(-0.5) * T(n * (n - m)) / T(m) / T(p.r0);
+        T ynm1 = ipow_t(y, n - 1);
+        return (T(n - m) * ynm1 * ym + T(m) * ymm1 - T(n) * ynm1) / (one_m * one_m) / T(p.r0);
+    }
+    default: return T(0);
+    }
+}
+
+// Pair record of the neighbour lists: displacement x_j - x_i (minimum image,
+// computed in FP64 and rounded to T) and the sorted index of j (bit kFlagBit
+// marks a neighbour kept by the centre's cap).
+template <typename T> struct alignas(16) Pair;
+template <> struct alignas(16) Pair<float> { float x, y, z; int j; };
+template <> struct alignas(16) Pair<double> { double x, y, z; int j; int pad; };
+
+// Device-side error word shared by the kernels of one context.
+struct DevStatus {
+    unsigned int overflow;        // max neighbour count seen when above capacity
+    unsigned int nan_force;       // a force component was not finite
+    unsigned int timeout;         // a bounded wait gave up
+    unsigned int pad;
+};
+
+// Deterministic block sum of up to NV doubles per thread (fixed shuffle tree,
+// then warp 0 over the warp partials).  Result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /* NV * 32 */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int t = 0; t < NV; ++t) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[t] += __shfl_down_sync(0xffffffffu, v[t], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int t = 0; t < NV; ++t) smem[t * 32 + warp] = v[t];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int t = 0; t < NV; ++t) {
+            double s = lane < nw ? smem[t * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            v[t] = s;
+        }
+    }
+}
+
+}  // namespace mtd
+
+namespace mtd {
+template <typename T> __device__ __forceinline__ T t_rsqrt(T x);
+template <> __device__ __forceinline__ float t_rsqrt<float>(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ double t_rsqrt<double>(double x) { return rsqrt(x); }
+
+constexpr int pad4(int v) { return (v + 3) & ~3; }
+
+// LAMMPS packed image flags (default 10-bit layout: IMGBITS 10, IMGMAX 512).
+__device__ __forceinline__ void unpack_image(int img, int &ix, int &iy, int &iz) {
+    ix = (img & 1023) - 512;
+    iy = ((img >> 10) & 1023) - 512;
+    iz = (img >> 20) - 512;
+}
+}  // namespace mtd

@@ -1,0 +1,1152 @@
+// context.cu -- the C ABI of libmetad_b200.so: context set-up from the
+// `fix metad` arguments, device memory, the per-step launch sequence and the
+// HILLS / rec.log files.
+//
+// Per step (one CUDA stream, no host synchronisation inside the step):
+//   cells -> neighbour lists (one per distinct environment) -> CV value
+//   kernels -> bias kernel (reductions, DIM, deposit, V, dV/ds) -> force
+//   kernels (f_out = f_in - dV/dx) -> virial reduction.
+// This is FixMetadynamics::post_force (src/core/fix_crystallize.cu:386-472)
+// without its host loops, PCIe round trips and per-call synchronisations.
+#include "../../include/metad_b200.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "args.h"
+#include "expr.h"
+#include "kernels.h"
+
+using namespace mtd;
+
+namespace {
+
+enum EnvKind { ENV_Q = 0, ENV_L = 1, ENV_R = 2 };
+
+struct Env {
+    int kind = ENV_R;
+    double rc = 0;
+    int cap = 0;
+    SwParams sw{};
+    double eps = 0;
+    int M = 0;
+    int cap_n = 0;
+    void *pairs = nullptr;
+    int *count = nullptr;
+    double *key_r2 = nullptr;
+    int *key_id = nullptr;
+    int *nkept = nullptr;
+    std::vector<int> cals;
+};
+
+struct Unit {
+    int kind = 0;                 // CalKind
+    std::vector<std::string> calnames;
+    int env = -1;
+    int LA = 0, LB = 0;
+    int groupbit = 1;
+    SwParams sw_r{}, sw_cvA{}, sw_cvB{};
+    std::vector<SwParams> qsw;
+    std::vector<std::string> qswnames;
+    double rc = 0, qf = 0;
+    SwParams sf_sw{};
+    bool dsig = false;
+    bool used = false;
+    int cap_n = 0;
+    void *q = nullptr, *nf = nullptr, *lq = nullptr, *lqs = nullptr, *e12 = nullptr, *lam = nullptr, *g = nullptr,
+         *tu = nullptr, *Q = nullptr, *S = nullptr;
+    double *partials = nullptr;
+    int nblocks = 0;
+    double *coef = nullptr;
+    int K = 0;
+    double *kvec = nullptr, *rho = nullptr, *skn = nullptr;
+};
+
+template <typename P> cudaError_t dalloc(P **p, size_t bytes) {
+    *p = nullptr;
+    return cudaMalloc((void **)p, bytes < 16 ? 16 : bytes);
+}
+template <typename P> void dfree(P *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+}  // namespace
+
+struct mtd_ctx {
+    int fp64 = 0;
+    int device = 0;
+    double boltz = 8.617343e-5;
+    GroupTable groups;
+    std::string hills_path = "HILLS";
+    std::string work_dir;
+    Config cfg;
+    std::vector<std::string> symnames;
+    std::vector<std::vector<ExprInstr>> code;
+    cudaStream_t st = nullptr;
+    bool box_set = false;
+    double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+    int periodic[3] = {1, 1, 1};
+    bool initialized = false;
+    int n = 0, npad = 0, cap_n = 0, n_plan = -1;
+    double *d_x = nullptr, *d_fin = nullptr, *d_fout = nullptr;
+    int *d_mask = nullptr, *d_image = nullptr;
+    int *cellof = nullptr, *slot = nullptr, *perm = nullptr, *scell = nullptr, *smask = nullptr;
+    double *xs = nullptr;
+    float4 *pf = nullptr;
+    int *count = nullptr, *start = nullptr;
+    int cap_cell = 0;
+    std::vector<Env> envs;
+    std::vector<Unit> units;
+    BiasPlan plan{};
+    BiasPlan *d_plan = nullptr;
+    bool plan_dirty = true;
+    double *d_grid = nullptr;
+    long long grid_size = 0;
+    HillRec *d_hills = nullptr;
+    unsigned long long *d_nhills = nullptr;
+    double *d_out = nullptr;
+    DevStatus *d_status = nullptr;
+    double *d_vpart = nullptr;
+    int cap_vpart = 0;
+    double *d_vir = nullptr;
+    double *h_out = nullptr;
+    DevStatus *h_status = nullptr;
+    double *h_vir = nullptr;
+    HillRec *h_hills = nullptr;
+    unsigned long long *h_nhills = nullptr;
+    unsigned long long hills_written = 0;
+    std::vector<double> cv;
+    double bias = 0.0;
+    double virial[6] = {0, 0, 0, 0, 0, 0};
+    FILE *f_hills = nullptr;
+    FILE *f_rec = nullptr;
+    std::string err;
+    int launches = 0;
+    bool want_virial = false;
+    bool pending = false;
+    long long pending_step = 0;
+    CellGrid last_grid{};
+};
+
+namespace {
+
+constexpr int kHillCap = 4096;
+
+mtd_status fail(mtd_ctx *c, mtd_status s, const std::string &m) {
+    if (c) c->err = m;
+    return s;
+}
+
+mtd_status cuda_check(mtd_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return MTD_OK;
+    if (e == cudaErrorMemoryAllocation) return fail(c, MTD_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(c, MTD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define MTD_CU(expr, what)                                        \
+    do {                                                          \
+        mtd_status _s = cuda_check(c, (expr), what);              \
+        if (_s != MTD_OK) return _s;                              \
+    } while (0)
+
+size_t real_size(const mtd_ctx *c) { return c->fp64 ? sizeof(double) : sizeof(float); }
+size_t pair_size(const mtd_ctx *c) { return c->fp64 ? sizeof(Pair<double>) : sizeof(Pair<float>); }
+
+int record_stride(const Unit &u) {
+    if (u.kind == CAL_STEINH_L) return pad4(2 * (u.LA + 1) + (u.LB ? 2 * (u.LB + 1) : 0));
+    if (u.kind == CAL_STEINH_Q) return pad4(2 * (u.LA + 1));
+    return 0;
+}
+
+double env_cutoff(const Env &e) { return e.rc; }
+
+CellGrid make_grid(const mtd_ctx *c) {
+    CellGrid g{};
+    double rmax = 0.0;
+    for (const Env &e : c->envs) rmax = std::fmax(rmax, env_cutoff(e));
+    double Lmax = 0.0;
+    for (int d = 0; d < 3; ++d) Lmax = std::fmax(Lmax, c->hi[d] - c->lo[d]);
+    const double guard = 1e-6 * Lmax + 1e-6;
+    long long ncell = 1;
+    for (int d = 0; d < 3; ++d) {
+        double L = c->hi[d] - c->lo[d];
+        if (!(L > 0)) L = 1.0;
+        int nc = rmax > 0 ? (int)std::floor(L / (rmax + guard)) : 1;
+        if (nc < 1) nc = 1;
+        if (nc > 512) nc = 512;
+        g.nc[d] = nc;
+        g.periodic[d] = c->periodic[d];
+        g.L[d] = L;
+        g.lo[d] = c->lo[d];
+        g.inv_h[d] = nc / L;
+        g.Lf[d] = (float)L;
+        g.invLf[d] = 1.0f / (float)L;
+        ncell *= nc;
+    }
+    g.ncell = (int)ncell;
+    return g;
+}
+
+float prefilter(const mtd_ctx *c, double rc) {
+    double Lmax = 0.0;
+    for (int d = 0; d < 3; ++d) Lmax = std::fmax(Lmax, c->hi[d] - c->lo[d]);
+    const double r = rc + 1e-6 * Lmax + 1e-6;
+    return (float)(r * r);
+}
+
+int estimate_M(const mtd_ctx *c, double rc, int n) {
+    double V = 1.0;
+    for (int d = 0; d < 3; ++d) V *= std::fmax(c->hi[d] - c->lo[d], 1e-9);
+    const double rho = n / V;
+    const double expect = 4.0 / 3.0 * kPi * rc * rc * rc * rho;
+    int M = (int)std::ceil(1.6 * expect + 8.0);
+    M = (M + 3) & ~3;
+    return M < 8 ? 8 : M;
+}
+
+mtd_status alloc_env(mtd_ctx *c, Env &e, int npad) {
+    dfree(e.pairs);
+    dfree(e.count);
+    dfree(e.key_r2);
+    dfree(e.key_id);
+    dfree(e.nkept);
+    MTD_CU(dalloc(&e.pairs, pair_size(c) * (size_t)e.M * npad), "neighbour list");
+    MTD_CU(dalloc(&e.count, sizeof(int) * (size_t)npad), "neighbour counts");
+    if (e.kind == ENV_Q) {
+        MTD_CU(dalloc(&e.key_r2, sizeof(double) * (size_t)npad), "cap keys");
+        MTD_CU(dalloc(&e.key_id, sizeof(int) * (size_t)npad), "cap keys");
+        MTD_CU(dalloc(&e.nkept, sizeof(int) * (size_t)npad), "cap counts");
+    }
+    e.cap_n = npad;
+    return MTD_OK;
+}
+
+mtd_status alloc_unit(mtd_ctx *c, Unit &u, int npad) {
+    const size_t R = real_size(c);
+    const int SQ = record_stride(u);
+    const int nb = (npad + kBlock - 1) / kBlock;
+    void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S};
+    for (void **a : arrs) dfree(*a);
+    dfree(u.partials);
+    if (u.kind == CAL_STEINH_L) {
+        MTD_CU(dalloc(&u.q, R * SQ * (size_t)npad), "q_lm");
+        MTD_CU(dalloc(&u.lq, R * SQ * (size_t)npad), "LQ_lm");
+        MTD_CU(dalloc(&u.lam, R * SQ * (size_t)npad), "adjoint");
+        MTD_CU(dalloc(&u.nf, R * (size_t)npad), "NF");
+        MTD_CU(dalloc(&u.lqs, R * 2 * (size_t)npad), "LQ");
+        MTD_CU(dalloc(&u.e12, R * 4 * (size_t)npad), "weights");
+        if (u.dsig) {
+            MTD_CU(dalloc(&u.g, R * SQ * (size_t)npad), "G");
+            MTD_CU(dalloc(&u.tu, R * 4 * (size_t)npad), "t,u");
+        }
+        u.nblocks = nb;
+        MTD_CU(dalloc(&u.partials, sizeof(double) * 8 * (size_t)nb), "partials");
+    } else if (u.kind == CAL_STEINH_Q) {
+        MTD_CU(dalloc(&u.q, R * SQ * (size_t)npad), "q_lm");
+        MTD_CU(dalloc(&u.Q, R * (size_t)npad), "Q");
+        u.nblocks = nb;
+        MTD_CU(dalloc(&u.partials, sizeof(double) * 8 * (size_t)nb), "partials");
+    } else if (u.kind == CAL_STRU_FACTOR) {
+        MTD_CU(dalloc(&u.S, R * (size_t)npad), "S");
+        u.nblocks = nb;
+        MTD_CU(dalloc(&u.partials, sizeof(double) * 8 * (size_t)nb), "partials");
+    } else {
+        u.nblocks = sk_blocks(npad);
+        MTD_CU(dalloc(&u.partials, sizeof(double) * (size_t)u.nblocks * (2 * u.K + 2)), "S(k) partials");
+    }
+    u.cap_n = npad;
+    return MTD_OK;
+}
+
+mtd_status ensure_capacity(mtd_ctx *c, int n) {
+    const int npad = ((n + kBlock - 1) / kBlock) * kBlock + kBlock;
+    c->n = n;
+    c->npad = npad;
+    if (n != c->n_plan) {   // the bias kernel reads ceil(n / block) partials per unit
+        c->plan_dirty = true;
+        c->n_plan = n;
+    }
+    if (npad > c->cap_n) {
+        const int cap = npad + npad / 4;
+        dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
+        dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->scell); dfree(c->smask);
+        dfree(c->xs); dfree(c->pf); dfree(c->d_vpart);
+        MTD_CU(dalloc(&c->d_x, sizeof(double) * 3 * (size_t)cap), "x");
+        MTD_CU(dalloc(&c->d_fin, sizeof(double) * 3 * (size_t)cap), "f");
+        MTD_CU(dalloc(&c->d_fout, sizeof(double) * 3 * (size_t)cap), "f");
+        MTD_CU(dalloc(&c->d_mask, sizeof(int) * (size_t)cap), "mask");
+        MTD_CU(dalloc(&c->d_image, sizeof(int) * (size_t)cap), "image");
+        MTD_CU(dalloc(&c->cellof, sizeof(int) * (size_t)cap), "cells");
+        MTD_CU(dalloc(&c->slot, sizeof(int) * (size_t)cap), "cells");
+        MTD_CU(dalloc(&c->perm, sizeof(int) * (size_t)cap), "perm");
+        MTD_CU(dalloc(&c->scell, sizeof(int) * (size_t)cap), "cells");
+        MTD_CU(dalloc(&c->smask, sizeof(int) * (size_t)cap), "mask");
+        MTD_CU(dalloc(&c->xs, sizeof(double) * 3 * (size_t)cap), "x sorted");
+        MTD_CU(dalloc(&c->pf, sizeof(float4) * (size_t)cap), "x float");
+        c->cap_vpart = 8 * ((cap + 255) / 256) * (int)(c->units.size() + 1);
+        MTD_CU(dalloc(&c->d_vpart, sizeof(double) * 8 * (size_t)c->cap_vpart), "virial partials");
+        c->cap_n = cap;
+        for (Env &e : c->envs) {
+            if (e.M == 0) e.M = estimate_M(c, e.rc, n);
+            if (e.kind == ENV_Q && e.M > 64) e.M = 64;
+            mtd_status s = alloc_env(c, e, cap);
+            if (s != MTD_OK) return s;
+        }
+        for (Unit &u : c->units) {
+            mtd_status s = alloc_unit(c, u, cap);
+            if (s != MTD_OK) return s;
+        }
+        c->plan_dirty = true;
+    }
+    return MTD_OK;
+}
+
+mtd_status ensure_cells(mtd_ctx *c, int ncell) {
+    if (ncell + 1 > c->cap_cell) {
+        dfree(c->count);
+        dfree(c->start);
+        const int cap = ncell + 1 + ncell / 4;
+        MTD_CU(dalloc(&c->count, sizeof(int) * (size_t)cap), "cell counts");
+        MTD_CU(dalloc(&c->start, sizeof(int) * (size_t)(cap + 1)), "cell starts");
+        c->cap_cell = cap;
+    }
+    return MTD_OK;
+}
+
+void build_plan(mtd_ctx *c) {
+    BiasPlan &P = c->plan;
+    const Config &cfg = c->cfg;
+    P.D = cfg.cv_dim;
+    for (int d = 0; d < 3; ++d) {
+        if (d < P.D) {
+            P.nbin[d] = cfg.dims[d].nbins;
+            P.lo[d] = cfg.dims[d].lo;
+            P.hi[d] = cfg.dims[d].hi;
+            P.dcv[d] = (P.hi[d] - P.lo[d]) / P.nbin[d];
+            P.band[d] = (int)std::ceil(4.0 * cfg.sigma / P.dcv[d]) + 1;   // GH_t0_uniformGrid.cu:87
+        } else {
+            P.nbin[d] = 1; P.lo[d] = 0; P.hi[d] = 1; P.dcv[d] = 1; P.band[d] = 0;
+        }
+    }
+    P.sigma = cfg.sigma;
+    P.h0 = cfg.height0;
+    P.biasf = cfg.biasf;
+    P.temp = cfg.temp;
+    P.kb = c->boltz;
+    P.wt = cfg.wt ? 1 : 0;
+    P.pace = cfg.pace;
+    P.nunit = (int)c->units.size();
+    for (int u = 0; u < P.nunit; ++u) {
+        const Unit &U = c->units[u];
+        UnitPlan &Q = P.unit[u];
+        Q.kind = U.kind;
+        Q.coef = U.coef;
+        if (U.kind == CAL_STRU_FACTOR_K) {
+            Q.partials = nullptr;
+            Q.nparts = 0;
+            Q.pstride = 0;
+            Q.nvals = 0;
+            Q.rho = U.rho;
+            Q.K = U.K;
+            Q.sk_n = U.skn;
+        } else {
+            Q.partials = U.partials;
+            Q.nparts = (c->n + kBlock - 1) / kBlock;
+            Q.pstride = 8;
+            Q.nvals = U.kind == CAL_STEINH_L ? 5 : 4;
+            Q.rho = nullptr;
+            Q.K = 0;
+            Q.sk_n = nullptr;
+        }
+    }
+    P.grid = c->d_grid;
+    P.hills = c->d_hills;
+    P.hill_cap = kHillCap;
+    P.nhills = c->d_nhills;
+    P.out = c->d_out;
+}
+
+// Neighbour-list and CV-unit layout from the parsed CAL table (env pooling as in
+// Steinhardt_env::get_or_create, src/cvs/CVs_Steinhardt.cu:191-220).
+mtd_status plan_units(mtd_ctx *c) {
+    Config &cfg = c->cfg;
+    auto same_sw = [](const SwParams &a, const SwParams &b) {
+        return a.type == b.type && a.r0 == b.r0 && a.d0 == b.d0 && a.alpha == b.alpha && a.n == b.n && a.m == b.m;
+    };
+    std::map<std::string, int> unit_of;   // CAL name -> unit
+    std::map<std::string, int> slot_of;   // CAL name -> slot in unit
+    for (auto &kv : cfg.cals) {
+        const CalDef &d = kv.second;
+        bool used = false;
+        for (auto &s : cfg.symbols) used = used || (s.cal == d.name);
+        if (d.kind == CAL_STRU_FACTOR_K) {
+            Unit u;
+            u.kind = d.kind;
+            u.calnames = {d.name};
+            u.groupbit = d.groupbit;
+            u.K = d.nk;
+            u.used = used;
+            unit_of[d.name] = (int)c->units.size();
+            slot_of[d.name] = 0;
+            c->units.push_back(u);
+            continue;
+        }
+        int ek = d.kind == CAL_STEINH_Q ? ENV_Q : (d.kind == CAL_STEINH_L ? ENV_L : ENV_R);
+        int env = -1;
+        for (size_t e = 0; e < c->envs.size(); ++e) {
+            const Env &E = c->envs[e];
+            if (E.kind != ek || E.rc != d.cutoff_r) continue;
+            if (ek == ENV_Q && E.cap != d.cutoff_natoms) continue;
+            if (ek == ENV_L && (!same_sw(E.sw, d.sw_r) || E.eps != d.cutoff_eps)) continue;
+            env = (int)e;
+        }
+        if (env < 0) {
+            Env E;
+            E.kind = ek;
+            E.rc = d.cutoff_r;
+            E.cap = ek == ENV_Q ? d.cutoff_natoms : 0;
+            E.sw = d.sw_r;
+            E.eps = d.cutoff_eps;
+            env = (int)c->envs.size();
+            c->envs.push_back(E);
+        }
+        // fuse a second STEINH L order into an open unit of the same environment
+        if (d.kind == CAL_STEINH_L) {
+            bool fused = false;
+            for (size_t u = 0; u < c->units.size(); ++u) {
+                Unit &U = c->units[u];
+                if (U.kind != CAL_STEINH_L || U.env != env || U.LB != 0 || U.groupbit != d.groupbit) continue;
+                const int key = U.LA * 16 + d.l;
+                if (key != 4 * 16 + 6 && key != 6 * 16 + 4 && key != 3 * 16 + 4 && key != 3 * 16 + 6) continue;
+                U.LB = d.l;
+                U.sw_cvB = d.sw_cv;
+                U.calnames.push_back(d.name);
+                U.used = U.used || used;
+                unit_of[d.name] = (int)u;
+                slot_of[d.name] = 1;
+                fused = true;
+                break;
+            }
+            if (fused) continue;
+        }
+        Unit u;
+        u.kind = d.kind;
+        u.calnames = {d.name};
+        u.env = env;
+        u.groupbit = d.groupbit;
+        u.LA = d.l;
+        u.LB = 0;
+        u.sw_r = d.sw_r;
+        u.sw_cvA = d.sw_cv;
+        u.sw_cvB = d.sw_cv;
+        u.dsig = (d.kind == CAL_STEINH_L) && d.sw_r.type != SW_STEP;
+        u.rc = d.cutoff_r;
+        u.qf = d.q_factor;
+        u.sf_sw = d.sf_sw;
+        u.used = used;
+        unit_of[d.name] = (int)c->units.size();
+        slot_of[d.name] = 0;
+        c->units.push_back(u);
+    }
+    if ((int)c->units.size() > kMaxUnits) return fail(c, MTD_ERR_UNSUPPORTED, "too many CAL units");
+    // symbols
+    BiasPlan &P = c->plan;
+    P.nsym = (int)cfg.symbols.size();
+    for (int q = 0; q < P.nsym; ++q) {
+        const SymbolDef &s = cfg.symbols[q];
+        const CalDef &d = cfg.cals[s.cal];
+        SymPlan sp{};
+        sp.unit = unit_of[s.cal];
+        sp.slot = slot_of[s.cal];
+        Unit &U = c->units[sp.unit];
+        if (d.kind == CAL_STEINH_Q) {
+            if (s.func == "AVE") sp.kind = SYM_Q_AVE;
+            else {
+                sp.kind = SYM_Q_SW;
+                int slot = -1;
+                for (size_t t = 0; t < U.qswnames.size(); ++t)
+                    if (U.qswnames[t] == s.sub) slot = (int)t;
+                if (slot < 0) {
+                    if (U.qsw.size() >= 2) return fail(c, MTD_ERR_UNSUPPORTED, "at most two SW_FUNC symbols per STEINH Q CAL");
+                    U.qsw.push_back(cfg.sws[s.sub]);
+                    U.qswnames.push_back(s.sub);
+                    slot = (int)U.qsw.size() - 1;
+                }
+                sp.slot = slot;
+            }
+        } else if (d.kind == CAL_STEINH_L) {
+            if (s.func == "MEAN_SOLID" || s.func == "AVE") sp.kind = SYM_L_MEAN;
+            else if (s.func == "NSOLID" || s.func == "SW_FUNC") sp.kind = SYM_L_NSOLID;
+            else sp.kind = SYM_L_FRAC;
+            if (sp.slot == 0) U.sw_cvA = d.sw_cv;
+            else U.sw_cvB = d.sw_cv;
+        } else if (d.kind == CAL_STRU_FACTOR) {
+            sp.kind = s.func == "AVE" ? SYM_SF_AVE : SYM_SF_COUNT;
+        } else {
+            sp.kind = SYM_SK_AVE;
+        }
+        P.sym[q] = sp;
+        c->symnames.push_back(s.name);
+    }
+    for (int dd = 0; dd < cfg.cv_dim; ++dd) {
+        std::vector<ExprInstr> code;
+        std::string e = compile_expr(cfg.dims[dd].expr, c->symnames, code);
+        if (!e.empty()) return fail(c, MTD_ERR_PARSE, e);
+        P.ncode[dd] = (int)code.size();
+        for (size_t t = 0; t < code.size(); ++t) P.code[dd][t] = code[t];
+        c->code.push_back(code);
+    }
+    // per-unit small device blocks
+    for (Unit &u : c->units) {
+        MTD_CU(dalloc(&u.coef, sizeof(double) * 8), "coefficients");
+        MTD_CU(cudaMemset(u.coef, 0, sizeof(double) * 8), "coefficients");
+        if (u.kind == CAL_STRU_FACTOR_K) {
+            const CalDef &d = cfg.cals[u.calnames[0]];
+            MTD_CU(dalloc(&u.kvec, sizeof(double) * 3 * u.K), "k vectors");
+            MTD_CU(dalloc(&u.rho, sizeof(double) * 2 * u.K), "rho");
+            MTD_CU(dalloc(&u.skn, sizeof(double)), "rho");
+            MTD_CU(cudaMemcpy(u.kvec, d.kvecs.data(), sizeof(double) * 3 * u.K, cudaMemcpyHostToDevice), "k vectors");
+        }
+    }
+    return MTD_OK;
+}
+
+template <typename T> NeighDev<T> env_dev(const Env &e) {
+    NeighDev<T> nd;
+    nd.pairs = (Pair<T> *)e.pairs;
+    nd.count = e.count;
+    nd.key_r2 = e.key_r2;
+    nd.key_id = e.key_id;
+    nd.nkept = e.nkept;
+    nd.M = e.M;
+    return nd;
+}
+
+SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
+    SysDev s;
+    s.n = c->n;
+    s.npad = c->cap_n;
+    s.x = x;
+    s.mask = mask;
+    s.image = image;
+    s.cellof = c->cellof;
+    s.slot = c->slot;
+    s.count = c->count;
+    s.start = c->start;
+    s.perm = c->perm;
+    s.scell = c->scell;
+    s.smask = c->smask;
+    s.xs = c->xs;
+    s.pf = c->pf;
+    return s;
+}
+
+template <typename T>
+void run_units(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, const int *mask, long long step,
+               const double *fin, double *fout, bool virial) {
+    cudaStream_t st = c->st;
+    // CV values
+    for (Unit &u : c->units) {
+        if (u.kind == CAL_STEINH_L) {
+            LocalDev<T> d{};
+            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.LA = u.LA; d.LB = u.LB;
+            d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
+            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]);
+            d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
+            d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
+            launch_local_values<T>(d, st);
+            c->launches += 2;
+        } else if (u.kind == CAL_STEINH_Q) {
+            GlobalDev<T> d{};
+            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.L = u.LA; d.groupbit = u.groupbit;
+            d.nsw = (int)u.qsw.size();
+            for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
+            d.smask = c->smask; d.perm = c->perm; d.xs = c->xs; d.grid = g; d.nb = env_dev<T>(c->envs[u.env]);
+            d.q = (T *)u.q; d.Q = (T *)u.Q; d.partials = u.partials; d.coef = u.coef;
+            launch_global_values<T>(d, st);
+            c->launches += 1;
+        } else if (u.kind == CAL_STRU_FACTOR) {
+            DebyeDev<T> d{};
+            d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
+            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]); d.S = (T *)u.S;
+            d.partials = u.partials; d.coef = u.coef;
+            launch_debye_values<T>(d, st);
+            c->launches += 1;
+        } else {
+            SkDev d{};
+            d.n = c->n; d.K = u.K; d.groupbit = u.groupbit; d.x = x; d.mask = mask; d.k = u.kvec;
+            d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
+            d.fp64 = c->fp64;
+            launch_sk_values(d, st);
+            c->launches += 2;
+        }
+    }
+    launch_bias_step(c->d_plan, step, 0, st);
+    c->launches += 1;
+    // forces
+    bool first = true;
+    int voff = 0;
+    for (Unit &u : c->units) {
+        if (!u.used) continue;
+        const double *src = first ? fin : fout;
+        double *vp = virial ? c->d_vpart + (size_t)voff * 8 : nullptr;
+        int nb = (c->n + kBlock - 1) / kBlock;
+        if (u.kind == CAL_STEINH_L) {
+            LocalDev<T> d{};
+            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.LA = u.LA; d.LB = u.LB;
+            d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
+            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]);
+            d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
+            d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
+            launch_local_forces<T>(d, src, fout, s, g, vp, c->d_status, st);
+            c->launches += 2;
+        } else if (u.kind == CAL_STEINH_Q) {
+            GlobalDev<T> d{};
+            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.L = u.LA; d.groupbit = u.groupbit;
+            d.nsw = (int)u.qsw.size();
+            for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
+            d.smask = c->smask; d.perm = c->perm; d.xs = c->xs; d.grid = g; d.nb = env_dev<T>(c->envs[u.env]);
+            d.q = (T *)u.q; d.Q = (T *)u.Q; d.partials = u.partials; d.coef = u.coef;
+            launch_global_forces<T>(d, src, fout, s, g, vp, c->d_status, st);
+            c->launches += 1;
+        } else if (u.kind == CAL_STRU_FACTOR) {
+            DebyeDev<T> d{};
+            d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
+            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]); d.S = (T *)u.S;
+            d.partials = u.partials; d.coef = u.coef;
+            launch_debye_forces<T>(d, src, fout, s, g, vp, c->d_status, st);
+            c->launches += 1;
+        } else {
+            SkDev d{};
+            d.n = c->n; d.K = u.K; d.groupbit = u.groupbit; d.x = x; d.mask = mask; d.k = u.kvec;
+            d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
+            d.fp64 = c->fp64;
+            launch_sk_forces(d, src, fout, s, g, vp, st);
+            c->launches += 1;
+        }
+        voff += nb;
+        first = false;
+    }
+    if (first && fin != fout) cudaMemcpyAsync(fout, fin, sizeof(double) * 3 * (size_t)c->n, cudaMemcpyDeviceToDevice, st);
+    if (virial) {
+        launch_virial_finalize(c->d_vpart, voff, c->d_vir, st);
+        c->launches += 1;
+    }
+}
+
+mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, const int *mask, const int *image,
+                        const double *fin, double *fout, bool virial) {
+    if (!c->box_set) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_box must be called before the first step");
+    mtd_status s0 = ensure_capacity(c, n);
+    if (s0 != MTD_OK) return s0;
+    CellGrid g = make_grid(c);
+    c->last_grid = g;
+    if (c->plan_dirty) {
+        build_plan(c);
+        MTD_CU(cudaMemcpyAsync(c->d_plan, &c->plan, sizeof(BiasPlan), cudaMemcpyHostToDevice, c->st), "plan");
+        MTD_CU(cudaStreamSynchronize(c->st), "plan");
+        c->plan_dirty = false;
+    }
+    c->launches = 0;
+    SysDev s = sys_dev(c, x, mask, image);
+    if (!c->envs.empty()) {
+        mtd_status sc = ensure_cells(c, g.ncell);
+        if (sc != MTD_OK) return sc;
+        s.count = c->count;
+        s.start = c->start;
+        launch_build_cells(g, s, c->st);
+        c->launches += 4;
+        for (Env &e : c->envs) {
+            NeighSpec ns{};
+            ns.kind = e.kind == ENV_L ? NK_SWITCH : NK_RANGE;
+            ns.rc2 = e.rc * e.rc;
+            ns.rcf2 = prefilter(c, e.rc);
+            ns.eps = e.eps;
+            ns.sw = e.sw;
+            ns.cap = e.kind == ENV_Q ? e.cap : 0;
+            if (c->fp64) launch_neighbors<double>(g, s, ns, env_dev<double>(e), c->d_status, c->st);
+            else launch_neighbors<float>(g, s, ns, env_dev<float>(e), c->d_status, c->st);
+            c->launches += ns.cap > 0 ? 2 : 1;
+        }
+    }
+    if (c->fp64) run_units<double>(c, s, g, x, mask, step, fin, fout, virial);
+    else run_units<float>(c, s, g, x, mask, step, fin, fout, virial);
+    MTD_CU(cudaGetLastError(), "kernel launch");
+    // outputs of this step into pinned host memory
+    MTD_CU(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(double) * 64, cudaMemcpyDeviceToHost, c->st), "outputs");
+    MTD_CU(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->st), "status");
+    MTD_CU(cudaMemcpyAsync(c->h_nhills, c->d_nhills, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st), "hills");
+    if (virial) MTD_CU(cudaMemcpyAsync(c->h_vir, c->d_vir, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->st), "virial");
+    c->want_virial = virial;
+    c->pending = true;
+    c->pending_step = step;
+    return MTD_OK;
+}
+
+void write_hill_line(mtd_ctx *c, const HillRec &h) {
+    if (!c->f_hills) return;
+    std::fprintf(c->f_hills, "%lld", h.step);   // GH_t0_uniformGrid.cu:211-220
+    for (int d = 0; d < c->cfg.cv_dim; ++d) std::fprintf(c->f_hills, " %.16g", h.s[d]);
+    std::fprintf(c->f_hills, " %.16g %.16g\n", h.w, h.sigma);
+    std::fflush(c->f_hills);
+}
+
+// Collects the outputs of the last enqueued step (stream already synchronised).
+mtd_status collect(mtd_ctx *c) {
+    if (!c->pending) return MTD_OK;
+    c->pending = false;
+    const int D = c->cfg.cv_dim;
+    for (int d = 0; d < D; ++d) c->cv[d] = c->h_out[d];
+    c->bias = c->h_out[D];
+    if (c->want_virial)
+        for (int t = 0; t < 6; ++t) c->virial[t] = c->h_vir[t];
+    const unsigned long long nh = *c->h_nhills;
+    if (nh > c->hills_written) {
+        unsigned long long from = c->hills_written;
+        if (nh - from > (unsigned long long)kHillCap) from = nh - kHillCap;
+        for (unsigned long long h = from; h < nh; ++h) {
+            HillRec r;
+            MTD_CU(cudaMemcpy(&r, c->d_hills + (h % kHillCap), sizeof(HillRec), cudaMemcpyDeviceToHost), "hill record");
+            write_hill_line(c, r);
+        }
+        c->hills_written = nh;
+    }
+    if (c->f_rec && c->cfg.rec_pace > 0 && c->pending_step % c->cfg.rec_pace == 0) {
+        std::fprintf(c->f_rec, "%lld", c->pending_step);
+        for (int d = 0; d < D; ++d) std::fprintf(c->f_rec, " %.16g", c->cv[d]);
+        std::fprintf(c->f_rec, " %.16g\n", c->bias);
+        std::fflush(c->f_rec);
+    }
+    if (c->h_status->nan_force) return fail(c, MTD_ERR_NAN, "STEIN_QL CV error: force is infinity, check your system or cv_value.");
+    return MTD_OK;
+}
+
+std::string path_in(const mtd_ctx *c, const std::string &p) {
+    if (p.empty() || p[0] == '/' || c->work_dir.empty()) return p;
+    return c->work_dir + "/" + p;
+}
+
+mtd_status replay_records(mtd_ctx *c, const std::vector<HillRec> &recs) {
+    if (recs.empty()) return MTD_OK;
+    HillRec *d = nullptr;
+    MTD_CU(dalloc(&d, sizeof(HillRec) * recs.size()), "replay");
+    cudaMemcpy(d, recs.data(), sizeof(HillRec) * recs.size(), cudaMemcpyHostToDevice);
+    if (c->plan_dirty) {
+        build_plan(c);
+        cudaMemcpy(c->d_plan, &c->plan, sizeof(BiasPlan), cudaMemcpyHostToDevice);
+        c->plan_dirty = false;
+    }
+    launch_hills_replay(c->d_plan, d, (int)recs.size(), (int)c->grid_size, c->st);
+    cudaError_t e = cudaStreamSynchronize(c->st);
+    cudaFree(d);
+    return cuda_check(c, e, "HILLS replay");
+}
+
+// HILLS rows `step cv[D] height sigma`; '#' and blank lines skipped
+// (GH_t0_uniformGrid.cu:101-192 on one rank).
+mtd_status read_hills(mtd_ctx *c, const std::string &path, std::vector<HillRec> &recs, bool *exists) {
+    FILE *f = std::fopen(path.c_str(), "r");
+    if (exists) *exists = f != nullptr;
+    if (!f) return MTD_OK;
+    char line[1024];
+    const int D = c->cfg.cv_dim;
+    while (std::fgets(line, sizeof(line), f)) {
+        if (line[0] == '#' || line[0] == '\n' || line[0] == '\r') continue;
+        char *p = line, *e = nullptr;
+        HillRec r{};
+        r.step = std::strtoll(p, &e, 10);
+        if (e == p) continue;
+        p = e;
+        bool ok = true;
+        for (int d = 0; d < D; ++d) {
+            r.s[d] = std::strtod(p, &e);
+            ok = ok && e != p;
+            p = e;
+        }
+        r.w = std::strtod(p, &e);
+        ok = ok && e != p;
+        p = e;
+        r.sigma = std::strtod(p, &e);
+        ok = ok && e != p;
+        if (!ok) {
+            std::fclose(f);
+            return fail(c, MTD_ERR_IO, "malformed HILLS line: " + std::string(line));
+        }
+        recs.push_back(r);
+    }
+    std::fclose(f);
+    return MTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mtd_options_default(mtd_options *o) {
+    static const char *names[] = {"all"};
+    static const int bits[] = {1};
+    o->precision = MTD_PREC_MIXED;
+    o->device = 0;
+    o->boltz = 8.617343e-5;
+    o->n_groups = 1;
+    o->group_names = names;
+    o->group_bits = bits;
+    o->hills_path = nullptr;
+    o->work_dir = nullptr;
+}
+
+int mtd_abi_version(void) { return MTD_ABI_VERSION; }
+
+mtd_status mtd_parse_args(int narg, const char *const *arg, const mtd_options *opt, char *err, int errlen) {
+    mtd_options def;
+    mtd_options_default(&def);
+    if (!opt) opt = &def;
+    GroupTable groups;
+    for (int i = 0; i < opt->n_groups; ++i) {
+        groups.names.push_back(opt->group_names[i]);
+        groups.bits.push_back(opt->group_bits[i]);
+    }
+    Config cfg;
+    std::string e = parse_fix_args(narg, arg, groups, cfg);
+    std::vector<std::string> names;
+    for (auto &s : cfg.symbols) names.push_back(s.name);
+    for (int d = 0; e.empty() && d < cfg.cv_dim; ++d) {
+        std::vector<ExprInstr> code;
+        e = compile_expr(cfg.dims[d].expr, names, code);
+    }
+    if (err && errlen > 0) {
+        std::strncpy(err, e.c_str(), (size_t)errlen - 1);
+        err[errlen - 1] = '\0';
+    }
+    return e.empty() ? MTD_OK : MTD_ERR_PARSE;
+}
+
+mtd_status mtd_eval_expression(const char *expr, int nsym, const char *const *names, const double *values,
+                               double *value, double *grad) {
+    if (!expr || nsym < 0 || nsym > kMaxSymbols || (nsym > 0 && (!names || !values)) || !value) return MTD_ERR_INVALID_ARG;
+    std::vector<std::string> sym(names, names + nsym);
+    std::vector<ExprInstr> code;
+    if (!compile_expr(expr, sym, code).empty()) return MTD_ERR_PARSE;
+    double g[kMaxSymbols];
+    *value = eval_expr_host(code, values, nsym, g);
+    if (grad)
+        for (int k = 0; k < nsym; ++k) grad[k] = g[k];
+    return MTD_OK;
+}
+
+mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, mtd_ctx **out) {
+    if (!out) return MTD_ERR_INVALID_ARG;
+    *out = nullptr;
+    mtd_options def;
+    mtd_options_default(&def);
+    if (!opt) opt = &def;
+    mtd_ctx *c = new mtd_ctx();
+    c->fp64 = opt->precision == MTD_PREC_FP64;
+    c->device = opt->device;
+    c->boltz = opt->boltz;
+    for (int i = 0; i < opt->n_groups; ++i) {
+        c->groups.names.push_back(opt->group_names[i]);
+        c->groups.bits.push_back(opt->group_bits[i]);
+    }
+    if (opt->hills_path) c->hills_path = opt->hills_path;
+    if (opt->work_dir) c->work_dir = opt->work_dir;
+    std::string e = parse_fix_args(narg, arg, c->groups, c->cfg);
+    if (!e.empty()) {
+        // a parse error leaves a context only to report the message
+        c->err = e;
+        *out = c;
+        return MTD_ERR_PARSE;
+    }
+    for (auto &kv : c->cfg.cals)
+        if (kv.second.kind == CAL_STRU_FACTOR_K && kv.second.nk > 1024) {
+            c->err = "Error: STRU_FACTOR_K supports at most 1024 k-vectors.";
+            *out = c;
+            return MTD_ERR_UNSUPPORTED;
+        }
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        c->err = "cudaSetDevice failed";
+        *out = c;
+        return MTD_ERR_CUDA;
+    }
+    cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    c->cv.assign(c->cfg.cv_dim, 0.0);
+    mtd_status s = plan_units(c);
+    if (s == MTD_OK) {
+        cudaError_t ce = cudaSuccess;
+        ce = dalloc(&c->d_plan, sizeof(BiasPlan));
+        if (ce == cudaSuccess) ce = dalloc(&c->d_out, sizeof(double) * 64);
+        if (ce == cudaSuccess) ce = dalloc(&c->d_status, sizeof(DevStatus));
+        if (ce == cudaSuccess) ce = dalloc(&c->d_hills, sizeof(HillRec) * kHillCap);
+        if (ce == cudaSuccess) ce = dalloc(&c->d_nhills, sizeof(unsigned long long));
+        if (ce == cudaSuccess) ce = dalloc(&c->d_vir, sizeof(double) * 8);
+        if (ce == cudaSuccess) ce = cudaMemset(c->d_out, 0, sizeof(double) * 64);
+        if (ce == cudaSuccess) ce = cudaMemset(c->d_status, 0, sizeof(DevStatus));
+        if (ce == cudaSuccess) ce = cudaMemset(c->d_nhills, 0, sizeof(unsigned long long));
+        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_out, sizeof(double) * 64);
+        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_status, sizeof(DevStatus));
+        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_vir, sizeof(double) * 8);
+        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_nhills, sizeof(unsigned long long));
+        s = cuda_check(c, ce, "context allocation");
+    }
+    *out = c;
+    return s;
+}
+
+void mtd_destroy(mtd_ctx *c) {
+    if (!c) return;
+    if (c->st) cudaStreamSynchronize(c->st);
+    for (Env &e : c->envs) {
+        dfree(e.pairs); dfree(e.count); dfree(e.key_r2); dfree(e.key_id); dfree(e.nkept);
+    }
+    for (Unit &u : c->units) {
+        void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S};
+        for (void **a : arrs) dfree(*a);
+        dfree(u.partials); dfree(u.coef); dfree(u.kvec); dfree(u.rho); dfree(u.skn);
+    }
+    dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
+    dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->scell); dfree(c->smask);
+    dfree(c->xs); dfree(c->pf); dfree(c->count); dfree(c->start); dfree(c->d_vpart);
+    dfree(c->d_plan); dfree(c->d_grid); dfree(c->d_hills); dfree(c->d_nhills); dfree(c->d_out);
+    dfree(c->d_status); dfree(c->d_vir);
+    if (c->h_out) cudaFreeHost(c->h_out);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->h_vir) cudaFreeHost(c->h_vir);
+    if (c->h_nhills) cudaFreeHost(c->h_nhills);
+    if (c->st) cudaStreamDestroy(c->st);
+    if (c->f_hills) std::fclose(c->f_hills);
+    if (c->f_rec) std::fclose(c->f_rec);
+    delete c;
+}
+
+mtd_status mtd_set_box(mtd_ctx *c, const double lo[3], const double hi[3], const int periodic[3]) {
+    if (!c || !lo || !hi || !periodic) return MTD_ERR_INVALID_ARG;
+    for (int d = 0; d < 3; ++d) {
+        if (!(hi[d] > lo[d])) return fail(c, MTD_ERR_INVALID_ARG, "box upper bound must exceed the lower bound");
+        c->lo[d] = lo[d];
+        c->hi[d] = hi[d];
+        c->periodic[d] = periodic[d] ? 1 : 0;
+    }
+    double rmax = 0.0;
+    for (const Env &e : c->envs) rmax = std::fmax(rmax, e.rc);
+    for (int d = 0; d < 3; ++d)
+        if (c->periodic[d] && hi[d] - lo[d] < 2.0 * rmax)
+            return fail(c, MTD_ERR_INVALID_ARG, "Warning: box < cutoff_r, please check your system ! (periodic box must be >= 2 cutoff_r)");
+    c->box_set = true;
+    return MTD_OK;
+}
+
+mtd_status mtd_init(mtd_ctx *c) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    if (c->initialized) return MTD_OK;
+    c->grid_size = 1;
+    for (int d = 0; d < c->cfg.cv_dim; ++d) c->grid_size *= c->cfg.dims[d].nbins;
+    MTD_CU(dalloc(&c->d_grid, sizeof(double) * (size_t)c->grid_size), "bias grid");
+    MTD_CU(cudaMemset(c->d_grid, 0, sizeof(double) * (size_t)c->grid_size), "bias grid");
+    c->plan_dirty = true;
+    build_plan(c);
+    MTD_CU(cudaMemcpy(c->d_plan, &c->plan, sizeof(BiasPlan), cudaMemcpyHostToDevice), "plan");
+    c->plan_dirty = false;
+    const std::string hp = path_in(c, c->hills_path);
+    bool appended = false;
+    if (c->cfg.restart && !hp.empty()) {
+        std::vector<HillRec> recs;
+        bool exists = false;
+        mtd_status s = read_hills(c, hp, recs, &exists);
+        if (s != MTD_OK) return s;
+        if (exists) {
+            s = replay_records(c, recs);
+            if (s != MTD_OK) return s;
+            c->f_hills = std::fopen(hp.c_str(), "a");
+            appended = true;
+        }
+    }
+    if (!hp.empty() && !appended) {
+        c->f_hills = std::fopen(hp.c_str(), "w");
+        if (!c->f_hills) return fail(c, MTD_ERR_IO, "Cannot open HILLS file for writing/appending.");
+        if (c->cfg.cv_dim == 2) std::fprintf(c->f_hills, "# step cv1 cv2 height sigma\n");
+        if (c->cfg.cv_dim == 1) std::fprintf(c->f_hills, "# step cv_values height sigma\n");
+        std::fflush(c->f_hills);
+    }
+    if (!c->cfg.rec_file.empty()) {
+        c->f_rec = std::fopen(path_in(c, c->cfg.rec_file).c_str(), "w+");
+        if (c->f_rec) {
+            std::fprintf(c->f_rec, "# step");
+            for (int d = 0; d < c->cfg.cv_dim; ++d) std::fprintf(c->f_rec, " s%d", d + 1);
+            std::fprintf(c->f_rec, " bias_energy\n");
+            std::fflush(c->f_rec);
+        }
+    }
+    c->initialized = true;
+    return MTD_OK;
+}
+
+mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, const int *mask, const int *image,
+                          double *f, double virial[6]) {
+    if (!c || n < 0 || (n > 0 && (!x || !f))) return MTD_ERR_INVALID_ARG;
+    if (!c->initialized) {
+        mtd_status s = mtd_init(c);
+        if (s != MTD_OK) return s;
+    }
+    mtd_status s = ensure_capacity(c, n);
+    if (s != MTD_OK) return s;
+    const size_t b3 = sizeof(double) * 3 * (size_t)n;
+    MTD_CU(cudaMemcpyAsync(c->d_x, x, b3, cudaMemcpyHostToDevice, c->st), "x upload");
+    MTD_CU(cudaMemcpyAsync(c->d_fin, f, b3, cudaMemcpyHostToDevice, c->st), "f upload");
+    if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
+    if (image && virial) MTD_CU(cudaMemcpyAsync(c->d_image, image, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "image upload");
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
+        s = enqueue_step(c, step, n, c->d_x, mask ? c->d_mask : nullptr, (image && virial) ? c->d_image : nullptr,
+                         c->d_fin, c->d_fout, virial != nullptr);
+        if (s != MTD_OK) return s;
+        MTD_CU(cudaStreamSynchronize(c->st), "step");
+        if (c->h_status->overflow == 0) break;
+        // neighbour capacity too small: grow and run the step again
+        const int need = (int)c->h_status->overflow;
+        for (Env &e : c->envs) {
+            if (e.M >= need) continue;
+            if (e.kind == ENV_Q && need > 64)
+                return fail(c, MTD_ERR_UNSUPPORTED, "STEINH Q: more than 64 atoms within cutoff_r");
+            e.M = ((need + 8) + 3) & ~3;
+            s = alloc_env(c, e, c->cap_n);
+            if (s != MTD_OK) return s;
+        }
+        c->pending = false;
+        if (attempt == 3) return fail(c, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded");
+    }
+    s = collect(c);
+    if (s != MTD_OK) return s;
+    MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
+    MTD_CU(cudaStreamSynchronize(c->st), "f download");
+    if (virial)
+        for (int t = 0; t < 6; ++t) virial[t] = c->virial[t];
+    return MTD_OK;
+}
+
+mtd_status mtd_post_force_device(mtd_ctx *c, int64_t step, int n, const double *d_x, const int *d_mask,
+                                 const int *d_image, const double *d_f_in, double *d_f_out) {
+    if (!c || n < 0 || (n > 0 && (!d_x || !d_f_in || !d_f_out))) return MTD_ERR_INVALID_ARG;
+    if (!c->initialized) {
+        mtd_status s = mtd_init(c);
+        if (s != MTD_OK) return s;
+    }
+    if (c->pending) {   // keep the previous step's outputs
+        MTD_CU(cudaStreamSynchronize(c->st), "step");
+        mtd_status s = collect(c);
+        if (s != MTD_OK) return s;
+    }
+    return enqueue_step(c, step, n, d_x, d_mask, d_image, d_f_in, d_f_out, false);
+}
+
+mtd_status mtd_sync(mtd_ctx *c) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    MTD_CU(cudaStreamSynchronize(c->st), "sync");
+    if (c->h_status && c->h_status->overflow) {
+        const int need = (int)c->h_status->overflow;
+        for (Env &e : c->envs)
+            if (e.M < need) {
+                e.M = ((need + 8) + 3) & ~3;
+                alloc_env(c, e, c->cap_n);
+            }
+        cudaMemset(c->d_status, 0, sizeof(DevStatus));
+        c->h_status->overflow = 0;
+        c->pending = false;
+        return fail(c, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded; capacity grown, repeat the step");
+    }
+    return collect(c);
+}
+
+double mtd_compute_scalar(const mtd_ctx *c) { return c ? c->bias : 0.0; }
+
+double mtd_compute_vector(const mtd_ctx *c, int k) {
+    if (!c || k < 0 || k >= (int)c->cv.size()) return 0.0;
+    return c->cv[k];
+}
+
+int mtd_cv_dim(const mtd_ctx *c) { return c ? c->cfg.cv_dim : 0; }
+
+mtd_status mtd_extract_peratom(mtd_ctx *c, const char *key, double *out, int n) {
+    if (!c || !key || !out) return MTD_ERR_INVALID_ARG;
+    std::string k(key);
+    if (k.rfind("colvar_peratom:", 0) == 0) k = k.substr(15);
+    size_t dot = k.find('.');
+    if (dot == std::string::npos) return fail(c, MTD_ERR_INVALID_ARG, "key must be <CAL>.<prop>");
+    const std::string cal = k.substr(0, dot), prop = k.substr(dot + 1);
+    if (n != c->n) return fail(c, MTD_ERR_INVALID_ARG, "atom count differs from the last step");
+    MTD_CU(cudaStreamSynchronize(c->st), "extract");
+    for (Unit &u : c->units) {
+        for (size_t slot = 0; slot < u.calnames.size(); ++slot) {
+            if (u.calnames[slot] != cal) continue;
+            std::vector<int> perm(n);
+            MTD_CU(cudaMemcpy(perm.data(), c->perm, sizeof(int) * n, cudaMemcpyDeviceToHost), "perm");
+            std::vector<double> v(n, 0.0);
+            const size_t R = real_size(c);
+            std::vector<unsigned char> raw;
+            int stride = 1, off = 0;
+            const void *src = nullptr;
+            if (prop == "stein_q" && u.kind == CAL_STEINH_Q) { src = u.Q; }
+            else if (prop == "stein_q" && u.kind == CAL_STEINH_L) { src = u.lqs; stride = 2; off = (int)slot; }
+            else if (prop == "stru_f" && u.kind == CAL_STRU_FACTOR) { src = u.S; }
+            else return fail(c, MTD_ERR_INVALID_ARG, "unknown per-atom property " + prop + " for CAL " + cal);
+            raw.resize(R * stride * (size_t)n);
+            MTD_CU(cudaMemcpy(raw.data(), src, R * stride * (size_t)n, cudaMemcpyDeviceToHost), "extract");
+            for (int t = 0; t < n; ++t) {
+                double val = c->fp64 ? ((const double *)raw.data())[t * stride + off]
+                                     : (double)((const float *)raw.data())[t * stride + off];
+                out[perm[t]] = val;
+            }
+            return MTD_OK;
+        }
+    }
+    return fail(c, MTD_ERR_INVALID_ARG, "unknown CAL " + cal);
+}
+
+mtd_status mtd_hills_replay(mtd_ctx *c, const char *path) {
+    if (!c || !path) return MTD_ERR_INVALID_ARG;
+    if (!c->initialized) {
+        mtd_status s = mtd_init(c);
+        if (s != MTD_OK) return s;
+    }
+    std::vector<HillRec> recs;
+    bool exists = false;
+    mtd_status s = read_hills(c, path_in(c, path), recs, &exists);
+    if (s != MTD_OK) return s;
+    if (!exists) return fail(c, MTD_ERR_IO, std::string("cannot open ") + path);
+    return replay_records(c, recs);
+}
+
+mtd_status mtd_get_grid(mtd_ctx *c, double *out, int64_t count) {
+    if (!c || !out) return MTD_ERR_INVALID_ARG;
+    if (!c->initialized || count != c->grid_size) return fail(c, MTD_ERR_INVALID_ARG, "grid not allocated or size mismatch");
+    MTD_CU(cudaStreamSynchronize(c->st), "grid");
+    MTD_CU(cudaMemcpy(out, c->d_grid, sizeof(double) * (size_t)count, cudaMemcpyDeviceToHost), "grid");
+    return MTD_OK;
+}
+
+int mtd_last_launch_count(const mtd_ctx *c) { return c ? c->launches : 0; }
+
+int mtd_max_neighbors(mtd_ctx *c, const char *name) {
+    if (!c || !name) return -1;
+    for (Unit &u : c->units)
+        for (auto &cn : u.calnames)
+            if (cn == name && u.env >= 0) {
+                const Env &e = c->envs[u.env];
+                if (c->n == 0) return 0;
+                std::vector<int> cnt(c->n);
+                cudaStreamSynchronize(c->st);
+                if (cudaMemcpy(cnt.data(), e.count, sizeof(int) * c->n, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+                int m = 0;
+                for (int v : cnt) m = v > m ? v : m;
+                return m;
+            }
+    return -1;
+}
+
+const char *mtd_last_error(const mtd_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+// kernels.h -- device data layouts and the host-side launchers of every kernel.
+//
+// Layout in HBM (n atoms, npad = n rounded up to the block size):
+//   caller order : x_in, f_in, f_out (FP64 AoS n*3), mask, image (int n)
+//   sorted order : atoms counting-sorted by cell; perm[k] = caller index of
+//                  sorted atom k; xs (FP64 AoS raw coordinates), pf (FP32
+//                  wrapped position, float4), smask, scell
+//   pair lists   : ELL, slot-major Pair<T>[M][npad] so a warp reads 32
+//                  consecutive records per slot; count[npad]
+//   per-atom CV  : AoS records of SQ reals (q_lm, LQ_lm, lambda ...) so one
+//                  neighbour gather touches one or two 128-byte lines
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "expr.h"
+
+namespace mtd {
+
+struct CellGrid {
+    int nc[3];
+    int ncell;
+    int periodic[3];
+    double L[3], lo[3], inv_h[3];
+    float Lf[3], invLf[3];
+};
+
+struct SysDev {
+    int n, npad;
+    const double *x;      // caller order, AoS n*3
+    const int *mask;      // caller order, may be null (all groups)
+    const int *image;     // caller order, may be null
+    int *cellof, *slot, *count, *start, *perm, *scell, *smask;
+    double *xs;           // sorted raw coordinates AoS npad*3
+    float4 *pf;           // sorted wrapped coordinates
+};
+
+// Neighbour criteria (the reference's per-CV filters).
+enum NeighKind {
+    NK_RANGE = 0,   // 1e-12 <= r2 <= rc2           (STEINH Q :1358, STRU_FACTOR :1048)
+    NK_SWITCH = 1   // r2 <= rc2 and sw(r) >= eps    (STEINH L, Local.cu:1257-1262)
+};
+
+struct NeighSpec {
+    int kind;
+    double rc2;         // exact FP64 bound
+    float rcf2;         // FP32 prefilter bound (rc + guard)^2
+    double eps;
+    SwParams sw;
+    int cap;            // STEINH Q cutoff_Natoms, 0 = none
+};
+
+template <typename T> struct NeighDev {
+    Pair<T> *pairs;     // [M][npad]
+    int *count;         // [npad] neighbours found (may exceed M: overflow)
+    double *key_r2;     // STEINH Q: r2 of the last kept neighbour (inf when cap not binding)
+    int *key_id;        // STEINH Q: caller index of the last kept neighbour
+    int *nkept;         // STEINH Q: min(count, cap)
+    int M;
+};
+
+// ------------------------------------------------------------------ neighbours
+void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st);
+template <typename T>
+void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev<T> nd, DevStatus *status,
+                      cudaStream_t st);
+
+// ------------------------------------------------------------------ STEINH L
+template <typename T> struct LocalDev {
+    int n, npad, SQ;
+    int LA, LB;                 // orders handled by this unit (LB = 0: single)
+    int groupbit;
+    SwParams sw_r, sw_cvA, sw_cvB;
+    const int *smask;
+    const int *perm;
+    NeighDev<T> nb;
+    T *q, *nf, *lq, *lqs, *e12, *lam, *g, *tu;
+    double *partials;           // [nblocks][8]: S1A S0A S1B S0B N
+    const double *coef;         // c1A c2A c1B c2B (written by the bias kernel)
+};
+template <typename T> void launch_local_values(const LocalDev<T> &d, cudaStream_t st);
+template <typename T>
+void launch_local_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                         double *vpart, DevStatus *status, cudaStream_t st);
+
+// ------------------------------------------------------------------ STEINH Q
+template <typename T> struct GlobalDev {
+    int n, npad, SQ, L;
+    int groupbit, nsw;
+    SwParams sw[2];             // SW_FUNC symbols of this CAL
+    const int *smask, *perm;
+    const double *xs;
+    CellGrid grid;
+    NeighDev<T> nb;
+    T *q, *Q;
+    double *partials;           // [nblocks][8]: sumQ, sum f1(Q), sum f2(Q), N
+    const double *coef;         // c_ave, c_sw1, c_sw2
+};
+template <typename T> void launch_global_values(const GlobalDev<T> &d, cudaStream_t st);
+template <typename T>
+void launch_global_forces(const GlobalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s,
+                          const CellGrid &g, double *vpart, DevStatus *status, cudaStream_t st);
+
+// ------------------------------------------------------------------ STRU_FACTOR (Debye) and S(k)
+template <typename T> struct DebyeDev {
+    int n, npad;
+    int groupbit;
+    double rc2, qf;
+    SwParams sw;
+    const int *smask, *perm;
+    NeighDev<T> nb;
+    T *S;
+    double *partials;           // [nblocks][4]: sumS, sum f(S), N
+    const double *coef;         // c_ave, c_count
+};
+template <typename T> void launch_debye_values(const DebyeDev<T> &d, cudaStream_t st);
+template <typename T>
+void launch_debye_forces(const DebyeDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                         double *vpart, DevStatus *status, cudaStream_t st);
+
+struct SkDev {
+    int n, K, groupbit;
+    const double *x;            // caller order AoS
+    const int *mask;
+    const double *k;            // K*3
+    double *partials;           // [nblocks][2K]
+    int nblocks;
+    double *rho;                // 2K (re, im)
+    double *ngroup;             // group count
+    const double *coef;         // alpha
+    int fp64;
+};
+void launch_sk_values(const SkDev &d, cudaStream_t st);
+void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                      double *vpart, cudaStream_t st);
+int sk_blocks(int n);
+
+// ------------------------------------------------------------------ bias grid
+enum SymKind {
+    SYM_Q_AVE = 0, SYM_Q_SW, SYM_L_MEAN, SYM_L_NSOLID, SYM_L_FRAC, SYM_SF_AVE, SYM_SF_COUNT, SYM_SK_AVE
+};
+
+struct SymPlan {
+    int kind;
+    int unit;        // index in the unit table
+    int slot;        // l slot (0/1) for STEINH L, SW slot for STEINH Q
+};
+
+struct UnitPlan {
+    int kind;              // CalKind of the unit
+    const double *partials;
+    int nparts, pstride, nvals;
+    double *coef;          // coefficient block written for the force kernels
+    const double *rho;     // S(k)
+    int K;
+    const double *sk_n;
+};
+
+struct HillRec {
+    long long step;
+    double s[3];
+    double w, sigma;
+};
+
+constexpr int kMaxUnits = 16;
+
+struct BiasPlan {
+    int D;
+    int nbin[3];
+    double lo[3], hi[3], dcv[3];
+    int band[3];
+    double sigma, h0, biasf, temp, kb;
+    int wt, pace;
+    int nsym;
+    SymPlan sym[kMaxSymbols];
+    int nunit;
+    UnitPlan unit[kMaxUnits];
+    int ncode[3];
+    ExprInstr code[3][kMaxExprLen];
+    double *grid;
+    HillRec *hills;
+    int hill_cap;
+    unsigned long long *nhills;
+    double *out;           // [0..D) s, D: V, D+1: deposited flag, D+2.. D+2+nsym: symbol values
+};
+constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
+
+void launch_bias_step(const BiasPlan *d_plan, long long step, int nunit_threads, cudaStream_t st);
+void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
+void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st);
+void launch_scan_status(const double *f, int n, DevStatus *status, cudaStream_t st);
+
+}  // namespace mtd

@@ -1,0 +1,421 @@
+// local_ql.cu -- STEINH L (local-averaged Q_l) values and analytic forces.
+//
+// Replaces steinhardt_Local_cv_get_qlm / _get_LQl
+// (src/cvs/CVs_Steinhardt_Local.cu:1309-1580), the MEAN_SOLID / NSOLID / FRAC
+// reductions (:695-745, src/utils/CVs_tools.cu:20-55) and the ij + jk force
+// kernels with FP64 atomics (:1622-2130).
+//
+// Definitions (sigma = SW_FUNC_r, N(i) = {j : sigma(r_ij) >= eps}):
+//   NF_i = sum_j sigma_ij,  q_i = sum_j sigma_ij Y(d_ij) / NF_i,
+//   LQ_i = (q_i + sum_j sigma_ij q_j) / (NF_i + 1),  LQ_i = |LQ_i|_l.
+// Forces use an adjoint (gather) formulation with no atomics, so FP64 runs are
+// bitwise reproducible.  For each atom
+//   G_i   = dCV/dLQ_i * (4 pi/(2l+1)) / LQ_i * w_m LQ_lm,i / (NF_i + 1)
+//   lam_k = G_k + sum_{i in N(k)} sigma_ki G_i                  (adjoint of q_k)
+// and the gradient on atom a gathers over its neighbours j with
+//   Lam = lam_a/NF_a + (-1)^l lam_j/NF_j,
+//   dCV/dx_a = - sum_j [ sigma grad_d Re(Lam . Y(d_aj))
+//                        + sigma' dhat (c_aj + c_ja + Re(Lam . Y) - t_a - t_j) ]
+// where c_aj = Re G_a.(q_j - LQ_a), t_a = Re lam_a.q_a / NF_a.  Two orders
+// (Q4 and Q6 of one neighbour environment) are fused in one pass.
+#include "kernels.h"
+#include "ylm.cuh"
+
+namespace mtd {
+
+namespace {
+
+template <int LA, int LB> struct LSet {
+    static constexpr int SA = 2 * (LA + 1);
+    static constexpr int SB = LB ? 2 * (LB + 1) : 0;
+    static constexpr int SQ = pad4(SA + SB);
+};
+
+template <typename T, int N> __device__ __forceinline__ void load_rec(const T *__restrict__ p, T (&v)[N]) {
+    static_assert(N % 4 == 0, "record stride");
+    if constexpr (std::is_same<T, float>::value) {
+        const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+        for (int i = 0; i < N / 4; ++i) {
+            float4 t = __ldg(q + i);
+            v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+        }
+    } else {
+        const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+        for (int i = 0; i < N / 2; ++i) {
+            double2 t = __ldg(q + i);
+            v[2 * i] = t.x; v[2 * i + 1] = t.y;
+        }
+    }
+}
+
+template <typename T, int N> __device__ __forceinline__ void store_rec(T *__restrict__ p, const T (&v)[N]) {
+    if constexpr (std::is_same<T, float>::value) {
+        float4 *q = reinterpret_cast<float4 *>(p);
+#pragma unroll
+        for (int i = 0; i < N / 4; ++i) q[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    } else {
+        double2 *q = reinterpret_cast<double2 *>(p);
+#pragma unroll
+        for (int i = 0; i < N / 2; ++i) q[i] = make_double2(v[2 * i], v[2 * i + 1]);
+    }
+}
+
+// sum_m w_m |v_m|^2 with w_0 = 1, w_m = 2 (the reference's Q_l norm).
+template <int L, typename T> __device__ __forceinline__ T qnorm2(const T *v) {
+    T s = v[0] * v[0];
+#pragma unroll
+    for (int m = 1; m <= L; ++m) s += T(2) * (v[2 * m] * v[2 * m] + v[2 * m + 1] * v[2 * m + 1]);
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ void pair_geom(const Pair<T> &pr, const SwParams &sw, bool step, T &ux, T &uy, T &uz, T &rinv,
+                                          T &sg, T &dsg) {
+    const T r2 = pr.x * pr.x + pr.y * pr.y + pr.z * pr.z;
+    rinv = t_rsqrt<T>(r2);
+    const T r = r2 * rinv;
+    ux = pr.x * rinv;
+    uy = pr.y * rinv;
+    uz = pr.z * rinv;
+    if (step) {   // listed pairs of a STEP switch have sigma = 1 by construction
+        sg = T(1);
+        dsg = T(0);
+    } else {
+        sg = sw_f<T>(sw, r);
+        dsg = sw_df<T>(sw, r);
+    }
+}
+
+// Pass 1: q_lm and NF for every atom.
+template <int LA, int LB, typename T> __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
+    using S = LSet<LA, LB>;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const bool step = d.sw_r.type == SW_STEP;
+    const int c = min(d.nb.count[k], d.nb.M);
+    T acc[S::SQ];
+#pragma unroll
+    for (int t = 0; t < S::SQ; ++t) acc[t] = T(0);
+    T nf = T(0);
+    for (int t = 0; t < c; ++t) {
+        const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+        T ux, uy, uz, rinv, sg, dsg;
+        pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
+        nf += sg;
+        ylm_accum<LA, T>(ux, uy, uz, sg, acc);
+        if constexpr (LB > 0) ylm_accum<LB, T>(ux, uy, uz, sg, acc + S::SA);
+    }
+    const bool active = c > 0 && nf >= T(1e-12);
+    const T inv = active ? T(1) / nf : T(0);
+#pragma unroll
+    for (int t = 0; t < S::SQ; ++t) acc[t] *= inv;
+    store_rec(d.q + (size_t)k * S::SQ, acc);
+    d.nf[k] = active ? nf : T(0);
+}
+
+// Pass 2: LQ_lm, LQ, the e1/e2 weights of the adjoint and block partial sums.
+template <int LA, int LB, typename T> __global__ void __launch_bounds__(kBlock) k_local_lq(LocalDev<T> d) {
+    using S = LSet<LA, LB>;
+    __shared__ double smem[5 * 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = k < d.n;
+    const bool step = d.sw_r.type == SW_STEP;
+    double part[5] = {0, 0, 0, 0, 0};
+    if (valid) {
+        const bool ing = (d.smask[k] & d.groupbit) != 0;
+        const T nfk = d.nf[k];
+        T A[S::SQ];
+        T lqA = T(0), lqB = T(0);
+        if (ing && nfk > T(0)) {
+            load_rec(d.q + (size_t)k * S::SQ, A);
+            const int c = min(d.nb.count[k], d.nb.M);
+            for (int t = 0; t < c; ++t) {
+                const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+                T ux, uy, uz, rinv, sg, dsg;
+                pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
+                T qj[S::SQ];
+                load_rec(d.q + (size_t)pr.j * S::SQ, qj);
+#pragma unroll
+                for (int s = 0; s < S::SQ; ++s) A[s] += sg * qj[s];
+            }
+            const T inv = T(1) / (nfk + T(1));
+#pragma unroll
+            for (int s = 0; s < S::SQ; ++s) A[s] *= inv;
+            lqA = t_sqrt<T>(qnorm2<LA, T>(A) * T(4.0 * kPi / (2 * LA + 1)));
+            if constexpr (LB > 0) lqB = t_sqrt<T>(qnorm2<LB, T>(A + S::SA) * T(4.0 * kPi / (2 * LB + 1)));
+        } else {
+#pragma unroll
+            for (int s = 0; s < S::SQ; ++s) A[s] = T(0);
+        }
+        store_rec(d.lq + (size_t)k * S::SQ, A);
+        d.lqs[2 * k] = lqA;
+        d.lqs[2 * k + 1] = lqB;
+        T e[4] = {T(0), T(0), T(0), T(0)};
+        if (ing) {
+            const double fA = sw_f<double>(d.sw_cvA, (double)lqA);
+            part[0] = (double)lqA * fA;
+            part[1] = fA;
+            part[4] = 1.0;
+            if (nfk > T(0)) {
+                const double dfA = sw_df<double>(d.sw_cvA, (double)lqA);
+                const double den = fmax((double)lqA, 1e-12) * ((double)nfk + 1.0);
+                const double C = 4.0 * kPi / (2 * LA + 1);
+                e[0] = (T)((dfA * lqA + fA) * C / den);
+                e[1] = (T)(dfA * C / den);
+            }
+            if constexpr (LB > 0) {
+                const double fB = sw_f<double>(d.sw_cvB, (double)lqB);
+                part[2] = (double)lqB * fB;
+                part[3] = fB;
+                if (nfk > T(0)) {
+                    const double dfB = sw_df<double>(d.sw_cvB, (double)lqB);
+                    const double den = fmax((double)lqB, 1e-12) * ((double)nfk + 1.0);
+                    const double C = 4.0 * kPi / (2 * LB + 1);
+                    e[2] = (T)((dfB * lqB + fB) * C / den);
+                    e[3] = (T)(dfB * C / den);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) d.e12[4 * k + t] = e[t];
+    }
+    block_sum<5>(part, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int t = 0; t < 5; ++t) d.partials[blockIdx.x * 8 + t] = part[t];
+    }
+}
+
+// G = (c1 e1 + c2 e2) w_m LQ_lm for one order, accumulated with weight s.
+template <int L, typename T>
+__device__ __forceinline__ void add_g(T *acc, const T *lq, T w, T s) {
+    const T a = s * w;
+    acc[0] += a * lq[0];
+#pragma unroll
+    for (int m = 1; m <= L; ++m) {
+        acc[2 * m] += T(2) * a * lq[2 * m];
+        acc[2 * m + 1] += T(2) * a * lq[2 * m + 1];
+    }
+}
+
+// Pass 3 (after the bias kernel): lam_k / NF_k, and for smooth switches G_k, t_k, u_k.
+template <int LA, int LB, typename T, bool DSIG>
+__global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
+    using S = LSet<LA, LB>;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const T c1A = (T)d.coef[0], c2A = (T)d.coef[1], c1B = (T)d.coef[2], c2B = (T)d.coef[3];
+    const T nfk = d.nf[k];
+    T lam[S::SQ];
+#pragma unroll
+    for (int s = 0; s < S::SQ; ++s) lam[s] = T(0);
+    if (!(nfk > T(0))) {
+        store_rec(d.lam + (size_t)k * S::SQ, lam);
+        if constexpr (DSIG) {
+            store_rec(d.g + (size_t)k * S::SQ, lam);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) d.tu[4 * k + t] = T(0);
+        }
+        return;
+    }
+    const bool step = d.sw_r.type == SW_STEP;
+    T lqk[S::SQ];
+    load_rec(d.lq + (size_t)k * S::SQ, lqk);
+    const float4 dummy = make_float4(0, 0, 0, 0);
+    (void)dummy;
+    T ek[4] = {d.e12[4 * k], d.e12[4 * k + 1], d.e12[4 * k + 2], d.e12[4 * k + 3]};
+    const T wA = c1A * ek[0] + c2A * ek[1];
+    const T wB = c1B * ek[2] + c2B * ek[3];
+    add_g<LA, T>(lam, lqk, wA, T(1));
+    if constexpr (LB > 0) add_g<LB, T>(lam + S::SA, lqk + S::SA, wB, T(1));
+    T Gk[S::SQ];
+    if constexpr (DSIG) {
+#pragma unroll
+        for (int s = 0; s < S::SQ; ++s) Gk[s] = lam[s];
+    }
+    const int c = min(d.nb.count[k], d.nb.M);
+    for (int t = 0; t < c; ++t) {
+        const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+        T ux, uy, uz, rinv, sg, dsg;
+        pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
+        const int j = pr.j;
+        const T ej0 = d.e12[4 * j], ej1 = d.e12[4 * j + 1], ej2 = d.e12[4 * j + 2], ej3 = d.e12[4 * j + 3];
+        const T wjA = c1A * ej0 + c2A * ej1;
+        const T wjB = c1B * ej2 + c2B * ej3;
+        if (wjA == T(0) && wjB == T(0)) continue;
+        T lqj[S::SQ];
+        load_rec(d.lq + (size_t)j * S::SQ, lqj);
+        add_g<LA, T>(lam, lqj, wjA, sg);
+        if constexpr (LB > 0) add_g<LB, T>(lam + S::SA, lqj + S::SA, wjB, sg);
+    }
+    const T inv = T(1) / nfk;
+    if constexpr (DSIG) {
+        T qk[S::SQ];
+        load_rec(d.q + (size_t)k * S::SQ, qk);
+        T tA = T(0), tB = T(0), uA = T(0), uB = T(0);
+#pragma unroll
+        for (int s = 0; s < S::SA; ++s) { tA += lam[s] * qk[s]; uA += Gk[s] * lqk[s]; }
+#pragma unroll
+        for (int s = S::SA; s < S::SA + S::SB; ++s) { tB += lam[s] * qk[s]; uB += Gk[s] * lqk[s]; }
+        d.tu[4 * k] = tA * inv;
+        d.tu[4 * k + 1] = uA;
+        d.tu[4 * k + 2] = tB * inv;
+        d.tu[4 * k + 3] = uB;
+        store_rec(d.g + (size_t)k * S::SQ, Gk);
+    }
+#pragma unroll
+    for (int s = 0; s < S::SQ; ++s) lam[s] *= inv;
+    store_rec(d.lam + (size_t)k * S::SQ, lam);
+}
+
+// Pass 4: gather forces, f_dst = f_src - dV/dx, plus the virial block partials.
+template <int LA, int LB, typename T, bool DSIG>
+__global__ void __launch_bounds__(kBlock) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
+                                                        double *__restrict__ f_dst, SysDev s, CellGrid g,
+                                                        double *vpart, DevStatus *status) {
+    using S = LSet<LA, LB>;
+    __shared__ double smem[6 * 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = k < d.n;
+    double vir[6] = {0, 0, 0, 0, 0, 0};
+    if (valid) {
+        const bool step = d.sw_r.type == SW_STEP;
+        T la[S::SQ];
+        load_rec(d.lam + (size_t)k * S::SQ, la);
+        T qa[S::SQ], ga[S::SQ];
+        T tua[4] = {T(0), T(0), T(0), T(0)};
+        if constexpr (DSIG) {
+            load_rec(d.q + (size_t)k * S::SQ, qa);
+            load_rec(d.g + (size_t)k * S::SQ, ga);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) tua[t] = d.tu[4 * k + t];
+        }
+        T gx = T(0), gy = T(0), gz = T(0);
+        const int c = min(d.nb.count[k], d.nb.M);
+        constexpr T sgnA = (LA & 1) ? T(-1) : T(1);
+        constexpr T sgnB = (LB & 1) ? T(-1) : T(1);
+        for (int t = 0; t < c; ++t) {
+            const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+            T ux, uy, uz, rinv, sg, dsg;
+            pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
+            const int j = pr.j;
+            T lj[S::SQ];
+            load_rec(d.lam + (size_t)j * S::SQ, lj);
+            T Lm[S::SQ];
+#pragma unroll
+            for (int q = 0; q < S::SA; ++q) Lm[q] = la[q] + sgnA * lj[q];
+#pragma unroll
+            for (int q = S::SA; q < S::SQ; ++q) Lm[q] = la[q] + sgnB * lj[q];
+            T ax, ay, az;
+            const T sA = ylm_dot_grad<LA, T>(ux, uy, uz, rinv, Lm, ax, ay, az);
+            gx -= sg * ax;
+            gy -= sg * ay;
+            gz -= sg * az;
+            T sB = T(0);
+            if constexpr (LB > 0) {
+                T bx, by, bz;
+                sB = ylm_dot_grad<LB, T>(ux, uy, uz, rinv, Lm + S::SA, bx, by, bz);
+                gx -= sg * bx;
+                gy -= sg * by;
+                gz -= sg * bz;
+            }
+            if constexpr (DSIG) {
+                if (dsg != T(0)) {
+                    T qj[S::SQ], gj[S::SQ];
+                    load_rec(d.q + (size_t)j * S::SQ, qj);
+                    load_rec(d.g + (size_t)j * S::SQ, gj);
+                    T cross = sA + sB - tua[0] - tua[1] - tua[2] - tua[3] - d.tu[4 * j] - d.tu[4 * j + 1] -
+                              d.tu[4 * j + 2] - d.tu[4 * j + 3];
+#pragma unroll
+                    for (int q = 0; q < S::SA + S::SB; ++q) cross += ga[q] * qj[q] + gj[q] * qa[q];
+                    gx -= dsg * cross * ux;
+                    gy -= dsg * cross * uy;
+                    gz -= dsg * cross * uz;
+                }
+            }
+        }
+        const int i = d.perm[k];
+        const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;   // delta f = -dV/dx
+        f_dst[3 * i] = f_src[3 * i] + fx;
+        f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
+        f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&status->nan_force, 1u);
+        if (vpart) {
+            double ux_ = s.xs[3 * k], uy_ = s.xs[3 * k + 1], uz_ = s.xs[3 * k + 2];
+            if (s.image) {
+                int ix, iy, iz;
+                unpack_image(s.image[i], ix, iy, iz);
+                ux_ += ix * g.L[0];
+                uy_ += iy * g.L[1];
+                uz_ += iz * g.L[2];
+            }
+            vir[0] = fx * ux_; vir[1] = fy * uy_; vir[2] = fz * uz_;
+            vir[3] = fx * uy_; vir[4] = fx * uz_; vir[5] = fy * uz_;
+        }
+    }
+    if (vpart) {
+        block_sum<6>(vir, smem);
+        if (threadIdx.x == 0)
+            for (int t = 0; t < 6; ++t) vpart[blockIdx.x * 8 + t] = vir[t];
+    }
+}
+
+template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cudaStream_t st) {
+    const int nb = (d.n + kBlock - 1) / kBlock;
+    k_local_q<LA, LB, T><<<nb, kBlock, 0, st>>>(d);
+    k_local_lq<LA, LB, T><<<nb, kBlock, 0, st>>>(d);
+}
+
+template <int LA, int LB, typename T>
+void run_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                double *vpart, DevStatus *status, cudaStream_t st) {
+    const int nb = (d.n + kBlock - 1) / kBlock;
+    const bool dsig = !(d.sw_r.type == SW_STEP);
+    if (dsig) {
+        k_local_lambda<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
+        k_local_force<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+    } else {
+        k_local_lambda<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
+        k_local_force<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+    }
+}
+
+}  // namespace
+
+#define MTD_LOCAL_DISPATCH(FN, ...)                                                          \
+    do {                                                                                     \
+        const int key = d.LA * 16 + d.LB;                                                    \
+        switch (key) {                                                                       \
+        case 3 * 16: FN<3, 0, T>(__VA_ARGS__); break;                                        \
+        case 4 * 16: FN<4, 0, T>(__VA_ARGS__); break;                                        \
+        case 6 * 16: FN<6, 0, T>(__VA_ARGS__); break;                                        \
+        case 4 * 16 + 6: FN<4, 6, T>(__VA_ARGS__); break;                                    \
+        case 6 * 16 + 4: FN<6, 4, T>(__VA_ARGS__); break;                                    \
+        case 3 * 16 + 4: FN<3, 4, T>(__VA_ARGS__); break;                                    \
+        case 3 * 16 + 6: FN<3, 6, T>(__VA_ARGS__); break;                                    \
+        default: break;                                                                      \
+        }                                                                                    \
+    } while (0)
+
+template <typename T> void launch_local_values(const LocalDev<T> &d, cudaStream_t st) {
+    if (d.n == 0) return;
+    MTD_LOCAL_DISPATCH(run_values, d, st);
+}
+
+template <typename T>
+void launch_local_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                         double *vpart, DevStatus *status, cudaStream_t st) {
+    if (d.n == 0) return;
+    MTD_LOCAL_DISPATCH(run_forces, d, f_src, f_dst, s, g, vpart, status, st);
+}
+
+template void launch_local_values<float>(const LocalDev<float> &, cudaStream_t);
+template void launch_local_values<double>(const LocalDev<double> &, cudaStream_t);
+template void launch_local_forces<float>(const LocalDev<float> &, const double *, double *, const SysDev &,
+                                         const CellGrid &, double *, DevStatus *, cudaStream_t);
+template void launch_local_forces<double>(const LocalDev<double> &, const double *, double *, const SysDev &,
+                                          const CellGrid &, double *, DevStatus *, cudaStream_t);
+
+}  // namespace mtd

@@ -1,0 +1,267 @@
+// neigh.cu -- cell list and neighbour lists on the device.
+//
+// Replaces the host CSR flatten of LAMMPS neighbour lists plus the selection
+// kernels get_environment_Steinhardt_Q (src/cvs/CVs_Steinhardt.cu:1324-1406),
+// get_environment_Steinhardt_LocalQ (src/cvs/CVs_Steinhardt_Local.cu:1210-1285)
+// and get_environment_Strufactor (src/cvs/CVs_Strufactor.cu:1014-1080).
+//
+// Pipeline per step: bin atoms to cells (counting sort: histogram, one-block
+// scan, scatter, per-cell sort by caller index for a deterministic order), then
+// one thread per sorted atom scans the 27 neighbour cells.  A candidate passes
+// an FP32 prefilter on wrapped float positions with a guard band, then the
+// neighbour decision is taken in FP64 on the caller's raw coordinates with
+// the same operation order as the FP64 oracle (minimum image, no FMA), so the
+// neighbour sets are exact.
+#include "kernels.h"
+
+#include <math_constants.h>
+
+namespace mtd {
+
+namespace {
+
+__device__ __forceinline__ int wrap_cell(double v, const CellGrid &g, int c, float &wf) {
+    double w = v - g.lo[c];
+    if (g.periodic[c]) {
+        w = w - g.L[c] * floor(w / g.L[c]);
+        if (w >= g.L[c]) w -= g.L[c];
+        if (w < 0.0) w = 0.0;
+    }
+    wf = (float)w;
+    int k = (int)(w * g.inv_h[c]);
+    if (k < 0) k = 0;
+    if (k >= g.nc[c]) k = g.nc[c] - 1;
+    return k;
+}
+
+__global__ void k_bin(CellGrid g, SysDev s) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    float wf;
+    int cx = wrap_cell(s.x[3 * i + 0], g, 0, wf);
+    int cy = wrap_cell(s.x[3 * i + 1], g, 1, wf);
+    int cz = wrap_cell(s.x[3 * i + 2], g, 2, wf);
+    int cell = (cx * g.nc[1] + cy) * g.nc[2] + cz;
+    s.cellof[i] = cell;
+    s.slot[i] = atomicAdd(&s.count[cell], 1);
+}
+
+// Exclusive scan of the cell histogram in one block (ncell up to a few million).
+__global__ void k_scan(const int *__restrict__ count, int *__restrict__ start, int ncell) {
+    __shared__ int warp_tot[32];
+    __shared__ int carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ncell; base += blockDim.x) {
+        int i = base + tid;
+        int v = (i < ncell) ? count[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int t = (lane < (blockDim.x >> 5)) ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;
+        }
+        __syncthreads();
+        int excl = carry + (warp > 0 ? warp_tot[warp - 1] : 0) + x - v;
+        if (i < ncell) start[i] = excl;
+        __syncthreads();
+        if (tid == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (tid == 0) start[ncell] = carry;
+}
+
+__global__ void k_scatter(SysDev s) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    s.perm[s.start[s.cellof[i]] + s.slot[i]] = i;
+}
+
+// Per cell: order members by caller index (removes the atomic arrival order),
+// then write the sorted per-atom arrays.
+__global__ void k_cellsort(CellGrid g, SysDev s) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.ncell) return;
+    const int b = s.start[c], e = s.start[c + 1];
+    for (int a = b + 1; a < e; ++a) {
+        int v = s.perm[a];
+        int t = a - 1;
+        while (t >= b && s.perm[t] > v) {
+            s.perm[t + 1] = s.perm[t];
+            --t;
+        }
+        s.perm[t + 1] = v;
+    }
+    for (int k = b; k < e; ++k) {
+        int i = s.perm[k];
+        double x0 = s.x[3 * i], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
+        s.xs[3 * k] = x0;
+        s.xs[3 * k + 1] = x1;
+        s.xs[3 * k + 2] = x2;
+        float4 p;
+        wrap_cell(x0, g, 0, p.x);
+        wrap_cell(x1, g, 1, p.y);
+        wrap_cell(x2, g, 2, p.z);
+        p.w = 0.f;
+        s.pf[k] = p;
+        s.scell[k] = c;
+        s.smask[k] = s.mask ? s.mask[i] : -1;
+    }
+}
+
+// Minimum-image displacement and r^2 in FP64 with the oracle's operation order.
+__device__ __forceinline__ double exact_disp(const CellGrid &g, const double *xi, const double *xj, double *d) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double t = __dsub_rn(xj[c], xi[c]);
+        if (g.periodic[c]) {
+            double k = rint(__ddiv_rn(t, g.L[c]));
+            t = __dsub_rn(t, __dmul_rn(g.L[c], k));
+        }
+        d[c] = t;
+    }
+    return __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2]));
+}
+
+__device__ __forceinline__ int stencil(const CellGrid &g, int c, int ci, int *out) {
+    const int nc = g.nc[c];
+    if (nc == 1) { out[0] = 0; return 1; }
+    if (g.periodic[c]) {
+        if (nc == 2) { out[0] = 0; out[1] = 1; return 2; }
+        out[0] = ci == 0 ? nc - 1 : ci - 1;
+        out[1] = ci;
+        out[2] = ci == nc - 1 ? 0 : ci + 1;
+        return 3;
+    }
+    int k = 0;
+    if (ci > 0) out[k++] = ci - 1;
+    out[k++] = ci;
+    if (ci < nc - 1) out[k++] = ci + 1;
+    return k;
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, NeighSpec ns, NeighDev<T> nd, DevStatus *status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= s.n) return;
+    const float4 p = s.pf[k];
+    const int c = s.scell[k];
+    const int cz = c % g.nc[2], cy = (c / g.nc[2]) % g.nc[1], cx = c / (g.nc[2] * g.nc[1]);
+    int sx[3], sy[3], sz[3];
+    const int nx = stencil(g, 0, cx, sx), ny = stencil(g, 1, cy, sy), nz = stencil(g, 2, cz, sz);
+    const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
+    int cnt = 0;
+    for (int a = 0; a < nx; ++a)
+        for (int b = 0; b < ny; ++b)
+            for (int e = 0; e < nz; ++e) {
+                const int cc = (sx[a] * g.nc[1] + sy[b]) * g.nc[2] + sz[e];
+                const int jb = s.start[cc], je = s.start[cc + 1];
+                for (int j = jb; j < je; ++j) {
+                    if (j == k) continue;
+                    const float4 q = s.pf[j];
+                    float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+                    if (g.periodic[0]) dx -= g.Lf[0] * rintf(dx * g.invLf[0]);
+                    if (g.periodic[1]) dy -= g.Lf[1] * rintf(dy * g.invLf[1]);
+                    if (g.periodic[2]) dz -= g.Lf[2] * rintf(dz * g.invLf[2]);
+                    if (dx * dx + dy * dy + dz * dz > ns.rcf2) continue;
+                    const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
+                    double d[3];
+                    const double r2 = exact_disp(g, xk, xj, d);
+                    bool ok;
+                    if (KIND == NK_RANGE) ok = (r2 <= ns.rc2) && (r2 >= 1e-12);
+                    else ok = (r2 <= ns.rc2) && (sw_f<double>(ns.sw, __dsqrt_rn(r2)) >= ns.eps);
+                    if (!ok) continue;
+                    if (cnt < nd.M) {
+                        Pair<T> pr;
+                        pr.x = (T)d[0];
+                        pr.y = (T)d[1];
+                        pr.z = (T)d[2];
+                        pr.j = j;
+                        nd.pairs[(size_t)cnt * s.npad + k] = pr;
+                    }
+                    ++cnt;
+                }
+            }
+    nd.count[k] = cnt;
+    if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
+}
+
+constexpr int kMaxCapList = 64;
+
+// STEINH Q cap: keep the `cap` nearest by (r2, caller index), the order of the
+// reference's strict-'>' insertion with ties resolved canonically.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, NeighSpec ns, NeighDev<T> nd) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= s.n) return;
+    const int c = min(nd.count[k], min(nd.M, kMaxCapList));
+    double r2[kMaxCapList];
+    int id[kMaxCapList];
+    const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
+    for (int t = 0; t < c; ++t) {
+        Pair<T> pr = nd.pairs[(size_t)t * s.npad + k];
+        const int j = pr.j;
+        const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
+        double d[3];
+        r2[t] = exact_disp(g, xk, xj, d);
+        id[t] = s.perm[j];
+    }
+    double kr2 = CUDART_INF;
+    int kid = 0x7fffffff;
+    for (int t = 0; t < c; ++t) {
+        int rank = 0;
+        for (int u = 0; u < c; ++u)
+            if (r2[u] < r2[t] || (r2[u] == r2[t] && id[u] < id[t])) ++rank;
+        if (rank < ns.cap) {
+            Pair<T> *pp = &nd.pairs[(size_t)t * s.npad + k];
+            pp->j |= (1 << kFlagBit);
+        }
+        if (c > ns.cap && rank == ns.cap - 1) {
+            kr2 = r2[t];
+            kid = id[t];
+        }
+    }
+    nd.key_r2[k] = kr2;
+    nd.key_id[k] = kid;
+    nd.nkept[k] = c < ns.cap ? c : ns.cap;
+}
+
+}  // namespace
+
+void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
+    cudaMemsetAsync(s.count, 0, sizeof(int) * (size_t)g.ncell, st);
+    const int nb = (s.n + kBlock - 1) / kBlock;
+    if (s.n > 0) k_bin<<<nb, kBlock, 0, st>>>(g, s);
+    k_scan<<<1, 1024, 0, st>>>(s.count, s.start, g.ncell);
+    if (s.n > 0) k_scatter<<<nb, kBlock, 0, st>>>(s);
+    k_cellsort<<<(g.ncell + kBlock - 1) / kBlock, kBlock, 0, st>>>(g, s);
+}
+
+template <typename T>
+void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev<T> nd, DevStatus *status,
+                      cudaStream_t st) {
+    if (s.n == 0) return;
+    const int nb = (s.n + kBlock - 1) / kBlock;
+    if (ns.kind == NK_RANGE) k_neighbors<T, NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    else k_neighbors<T, NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    if (ns.cap > 0) k_select_cap<T><<<nb, kBlock, 0, st>>>(g, s, ns, nd);
+}
+
+template void launch_neighbors<float>(const CellGrid &, const SysDev &, const NeighSpec &, NeighDev<float>, DevStatus *,
+                                      cudaStream_t);
+template void launch_neighbors<double>(const CellGrid &, const SysDev &, const NeighSpec &, NeighDev<double>,
+                                       DevStatus *, cudaStream_t);
+
+}  // namespace mtd

@@ -1,0 +1,284 @@
+// sf.cu -- structure-factor CVs.
+//
+// STRU_FACTOR (Debye form) replaces structure_factor_cv_kernel and the AVE /
+// COUNT gradient kernels (src/cvs/CVs_Strufactor.cu:1082-1271):
+//   S_i = 1 + sum_{j: 1e-12 <= r2 <= rc2} sin(q r)/(q r) s(r),
+//   s = 1 - ((r2 - 0.8 rc2)/(0.2 rc2))^3 above 0.8 rc2,
+//   dCV/dx_a = - sum_j (a_a + a_j) g'(r_aj) dhat_aj,  a_i = dCV/dS_i.
+// STRU_FACTOR_K (no reference counterpart): rho_k = sum_j exp(i k.x_j) over the
+// group, S(k) = |rho_k|^2/N, CV = mean_k S(k),
+//   dCV/dx_j = 2/(N K) sum_k k (-Re rho_k sin(k.x_j) + Im rho_k cos(k.x_j)).
+// Phases are formed in FP64 and reduced to [-pi, pi] before an FP32 sincos;
+// the sums over atoms are FP64 block partials reduced in a fixed order.
+#include "kernels.h"
+
+namespace mtd {
+
+namespace {
+
+template <typename T> __device__ __forceinline__ void t_sincos(T x, T *s, T *c);
+template <> __device__ __forceinline__ void t_sincos<float>(float x, float *s, float *c) { sincosf(x, s, c); }
+template <> __device__ __forceinline__ void t_sincos<double>(double x, double *s, double *c) { sincos(x, s, c); }
+
+template <typename T> __device__ __forceinline__ void debye_g(T r2, T rc2, T qf, T &gv, T &dg) {
+    const T r = t_sqrt<T>(r2), th = qf * r;
+    T s = T(1), ds = T(0);
+    const T r_on = T(0.8) * rc2;
+    if (r2 > r_on) {
+        const T t = (r2 - r_on) / (rc2 - r_on);
+        s = T(1) - t * t * t;
+        ds = T(-3) * t * t * (T(2) * r) / (rc2 - r_on);
+    }
+    T sn, cs;
+    t_sincos<T>(th, &sn, &cs);
+    gv = sn / th * s;
+    dg = (cs / th - sn / (th * th)) * s * qf + ds * sn / th;
+}
+
+template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(DebyeDev<T> d) {
+    __shared__ double smem[4 * 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double part[4] = {0, 0, 0, 0};
+    if (k < d.n) {
+        T S = T(0);
+        if (d.smask[k] & d.groupbit) {
+            const int c = min(d.nb.count[k], d.nb.M);
+            const T rc2 = (T)d.rc2, qf = (T)d.qf;
+            for (int t = 0; t < c; ++t) {
+                const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+                T gv, dg;
+                debye_g<T>(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z, rc2, qf, gv, dg);
+                S += gv;
+            }
+            S += T(1);
+            part[0] = (double)S;
+            part[1] = sw_f<double>(d.sw, (double)S);
+            part[2] = 1.0;
+        }
+        d.S[k] = S;
+    }
+    block_sum<4>(part, smem);
+    if (threadIdx.x == 0)
+        for (int t = 0; t < 4; ++t) d.partials[blockIdx.x * 8 + t] = part[t];
+}
+
+template <typename T>
+__device__ __forceinline__ T debye_a(const DebyeDev<T> &d, int k, double c0, double c1) {
+    if (!(d.smask[k] & d.groupbit)) return T(0);
+    double a = c0;
+    if (c1 != 0.0) a += c1 * sw_df<double>(d.sw, (double)d.S[k]);
+    return (T)a;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const double *__restrict__ f_src,
+                                                        double *__restrict__ f_dst, SysDev s, CellGrid g,
+                                                        double *vpart, DevStatus *status) {
+    __shared__ double smem[6 * 32];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double vir[6] = {0, 0, 0, 0, 0, 0};
+    const double c0 = d.coef[0], c1 = d.coef[1];
+    if (k < d.n) {
+        const T ak = debye_a<T>(d, k, c0, c1);
+        const T rc2 = (T)d.rc2, qf = (T)d.qf;
+        T gx = T(0), gy = T(0), gz = T(0);
+        const int c = min(d.nb.count[k], d.nb.M);
+        for (int t = 0; t < c; ++t) {
+            const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+            const T w = ak + debye_a<T>(d, pr.j, c0, c1);
+            if (w == T(0)) continue;
+            const T r2 = pr.x * pr.x + pr.y * pr.y + pr.z * pr.z;
+            T gv, dg;
+            debye_g<T>(r2, rc2, qf, gv, dg);
+            const T f = w * dg * t_rsqrt<T>(r2);
+            gx -= f * pr.x;
+            gy -= f * pr.y;
+            gz -= f * pr.z;
+        }
+        const int i = d.perm[k];
+        const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;
+        f_dst[3 * i] = f_src[3 * i] + fx;
+        f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
+        f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&status->nan_force, 1u);
+        if (vpart) {
+            double ux = s.xs[3 * k], uy = s.xs[3 * k + 1], uz = s.xs[3 * k + 2];
+            if (s.image) {
+                int ix, iy, iz;
+                unpack_image(s.image[i], ix, iy, iz);
+                ux += ix * g.L[0];
+                uy += iy * g.L[1];
+                uz += iz * g.L[2];
+            }
+            vir[0] = fx * ux; vir[1] = fy * uy; vir[2] = fz * uz;
+            vir[3] = fx * uy; vir[4] = fx * uz; vir[5] = fy * uz;
+        }
+    }
+    if (vpart) {
+        block_sum<6>(vir, smem);
+        if (threadIdx.x == 0)
+            for (int t = 0; t < 6; ++t) vpart[blockIdx.x * 8 + t] = vir[t];
+    }
+}
+
+// ------------------------------------------------------------------ S(k)
+constexpr int kSkChunk = 8;        // k-vectors per register tile
+constexpr int kSkBlocks = 148 * 8;  // grid for the partial sums (8 blocks per SM)
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kInvTwoPi = 0.15915494309189533576888376337251;
+
+template <bool FP64> __device__ __forceinline__ void phase_sincos(double ph, double &s, double &c) {
+    if (FP64) {
+        sincos(ph, &s, &c);
+    } else {
+        const double n = rint(ph * kInvTwoPi);
+        const float r = (float)fma(-n, kTwoPi, ph);
+        float sf, cf;
+        sincosf(r, &sf, &cf);
+        s = sf;
+        c = cf;
+    }
+}
+
+template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
+    __shared__ double smem[8 * 32];
+    __shared__ double kk[3 * 1024];
+    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
+    __syncthreads();
+    double cnt = 0.0;
+    for (int k0 = 0; k0 < d.K; k0 += kSkChunk / 2) {
+        double acc[kSkChunk];
+#pragma unroll
+        for (int t = 0; t < kSkChunk; ++t) acc[t] = 0.0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+            if (d.mask && !(d.mask[i] & d.groupbit)) continue;
+            if (k0 == 0) cnt += 1.0;
+            const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
+#pragma unroll
+            for (int q = 0; q < kSkChunk / 2; ++q) {
+                const int kq = k0 + q;
+                if (kq < d.K) {
+                    const double ph = kk[3 * kq] * x + kk[3 * kq + 1] * y + kk[3 * kq + 2] * z;
+                    double s, c;
+                    phase_sincos<FP64>(ph, s, c);
+                    acc[2 * q] += c;
+                    acc[2 * q + 1] += s;
+                }
+            }
+        }
+        block_sum<kSkChunk>(acc, smem);
+        if (threadIdx.x == 0)
+            for (int q = 0; q < kSkChunk / 2; ++q)
+                if (k0 + q < d.K) {
+                    d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * (k0 + q)] = acc[2 * q];
+                    d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * (k0 + q) + 1] = acc[2 * q + 1];
+                }
+        __syncthreads();
+    }
+    double c1[1] = {cnt};
+    block_sum<1>(c1, smem);
+    if (threadIdx.x == 0) d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * d.K] = c1[0];
+}
+
+// One block per output value (2K rho components + the group count).
+__global__ void __launch_bounds__(256) k_sk_reduce(SkDev d) {
+    __shared__ double smem[32];
+    const int v = blockIdx.x;
+    double acc[1] = {0.0};
+    for (int b = threadIdx.x; b < d.nblocks; b += blockDim.x) acc[0] += d.partials[(size_t)b * (2 * d.K + 2) + v];
+    block_sum<1>(acc, smem);
+    if (threadIdx.x == 0) {
+        if (v < 2 * d.K) d.rho[v] = acc[0];
+        else *d.ngroup = acc[0];
+    }
+}
+
+template <bool FP64>
+__global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restrict__ f_src, double *__restrict__ f_dst,
+                                                  SysDev s, CellGrid g, double *vpart) {
+    __shared__ double smem[6 * 32];
+    __shared__ double kk[3 * 1024];
+    __shared__ double rr[2 * 1024];
+    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
+    for (int t = threadIdx.x; t < 2 * d.K; t += blockDim.x) rr[t] = d.rho[t];
+    __syncthreads();
+    const double a = d.coef[0];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double vir[6] = {0, 0, 0, 0, 0, 0};
+    if (i < d.n) {
+        double gx = 0, gy = 0, gz = 0;
+        if (!d.mask || (d.mask[i] & d.groupbit)) {
+            const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
+            for (int q = 0; q < d.K; ++q) {
+                const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
+                double sn, cs;
+                phase_sincos<FP64>(ph, sn, cs);
+                const double w = -rr[2 * q] * sn + rr[2 * q + 1] * cs;
+                gx += w * kk[3 * q];
+                gy += w * kk[3 * q + 1];
+                gz += w * kk[3 * q + 2];
+            }
+        }
+        const double fx = -a * gx, fy = -a * gy, fz = -a * gz;
+        f_dst[3 * i] = f_src[3 * i] + fx;
+        f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
+        f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        if (vpart) {
+            double ux = d.x[3 * i], uy = d.x[3 * i + 1], uz = d.x[3 * i + 2];
+            if (s.image) {
+                int ix, iy, iz;
+                unpack_image(s.image[i], ix, iy, iz);
+                ux += ix * g.L[0];
+                uy += iy * g.L[1];
+                uz += iz * g.L[2];
+            }
+            vir[0] = fx * ux; vir[1] = fy * uy; vir[2] = fz * uz;
+            vir[3] = fx * uy; vir[4] = fx * uz; vir[5] = fy * uz;
+        }
+    }
+    if (vpart) {
+        block_sum<6>(vir, smem);
+        if (threadIdx.x == 0)
+            for (int t = 0; t < 6; ++t) vpart[blockIdx.x * 8 + t] = vir[t];
+    }
+}
+
+}  // namespace
+
+template <typename T> void launch_debye_values(const DebyeDev<T> &d, cudaStream_t st) {
+    if (d.n == 0) return;
+    k_debye_values<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d);
+}
+template <typename T>
+void launch_debye_forces(const DebyeDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                         double *vpart, DevStatus *status, cudaStream_t st) {
+    if (d.n == 0) return;
+    k_debye_force<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+}
+template void launch_debye_values<float>(const DebyeDev<float> &, cudaStream_t);
+template void launch_debye_values<double>(const DebyeDev<double> &, cudaStream_t);
+template void launch_debye_forces<float>(const DebyeDev<float> &, const double *, double *, const SysDev &,
+                                         const CellGrid &, double *, DevStatus *, cudaStream_t);
+template void launch_debye_forces<double>(const DebyeDev<double> &, const double *, double *, const SysDev &,
+                                          const CellGrid &, double *, DevStatus *, cudaStream_t);
+
+int sk_blocks(int n) {
+    int b = (n + 255) / 256;
+    return b < kSkBlocks ? (b < 1 ? 1 : b) : kSkBlocks;
+}
+
+void launch_sk_values(const SkDev &d, cudaStream_t st) {
+    if (d.fp64) k_sk_partial<true><<<d.nblocks, 256, 0, st>>>(d);
+    else k_sk_partial<false><<<d.nblocks, 256, 0, st>>>(d);
+    k_sk_reduce<<<2 * d.K + 1, 256, 0, st>>>(d);
+}
+
+void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                      double *vpart, cudaStream_t st) {
+    if (d.n == 0) return;
+    const int nb = (d.n + 255) / 256;
+    if (d.fp64) k_sk_force<true><<<nb, 256, 0, st>>>(d, f_src, f_dst, s, g, vpart);
+    else k_sk_force<false><<<nb, 256, 0, st>>>(d, f_src, f_dst, s, g, vpart);
+}
+
+}  // namespace mtd

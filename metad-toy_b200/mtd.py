@@ -1,0 +1,230 @@
+"""Python binding of libmetad_b200.so (the C ABI declared in include/metad_b200.h).
+
+This mirrors the reference plugin's interface for one `fix metad` instance:
+the constructor takes the fix arguments (the tokens after ``fix ID group metad``),
+``post_force`` is ``FixMetadynamics::post_force``, ``compute_scalar`` /
+``compute_vector`` are the thermo outputs and ``extract`` is
+``Fix::extract("colvar_peratom:<CAL>.<prop>")``.  Errors raise ``MetadError``
+with the library's message, the way the reference stops on ``error->all``.
+
+There is no CPU fallback: if the shared library is missing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmetad_b200.so")
+HEADER = os.path.join(HERE, "..", "include", "metad_b200.h")
+
+MTD_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "PARSE", 3: "CUDA", 4: "OOM", 5: "NEIGH_OVERFLOW",
+                6: "TIMEOUT", 7: "NAN", 8: "IO", 9: "UNSUPPORTED"}
+PREC = {"mixed": 0, "fp64": 1}
+
+# Every entry point declared in include/metad_b200.h.
+EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args", "mtd_eval_expression", "mtd_set_box", "mtd_init", "mtd_post_force",
+           "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
+           "mtd_extract_peratom", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
+           "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version"]
+
+
+class MetadError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("boltz", C.c_double), ("n_groups", C.c_int),
+                ("group_names", C.POINTER(C.c_char_p)), ("group_bits", C.POINTER(C.c_int)),
+                ("hills_path", C.c_char_p), ("work_dir", C.c_char_p)]
+
+
+_lib = None
+
+
+def build(jobs=8):
+    """Compile libmetad_b200.so for sm_100a with the package Makefile."""
+    subprocess.check_call(["make", "-s", "-j%d" % jobs, "-C", HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libmetad_b200.so is not built (run `make -C metad-toy_b200` or "
+                              "__graft_entry__.build()); there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.mtd_options_default.argtypes = [C.POINTER(Options)]
+        L.mtd_create.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.POINTER(vp)]
+        L.mtd_destroy.argtypes = [vp]
+        L.mtd_set_box.argtypes = [vp, dp, dp, ip]
+        L.mtd_init.argtypes = [vp]
+        L.mtd_post_force.argtypes = [vp, C.c_int64, C.c_int, vp, vp, vp, vp, vp]
+        L.mtd_post_force_device.argtypes = [vp, C.c_int64, C.c_int, vp, vp, vp, vp, vp]
+        L.mtd_sync.argtypes = [vp]
+        L.mtd_compute_scalar.argtypes = [vp]
+        L.mtd_compute_scalar.restype = C.c_double
+        L.mtd_compute_vector.argtypes = [vp, C.c_int]
+        L.mtd_compute_vector.restype = C.c_double
+        L.mtd_cv_dim.argtypes = [vp]
+        L.mtd_extract_peratom.argtypes = [vp, C.c_char_p, dp, C.c_int]
+        L.mtd_hills_replay.argtypes = [vp, C.c_char_p]
+        L.mtd_get_grid.argtypes = [vp, dp, C.c_int64]
+        L.mtd_last_launch_count.argtypes = [vp]
+        L.mtd_max_neighbors.argtypes = [vp, C.c_char_p]
+        L.mtd_last_error.argtypes = [vp]
+        L.mtd_last_error.restype = C.c_char_p
+        L.mtd_abi_version.restype = C.c_int
+        L.mtd_parse_args.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.c_char_p, C.c_int]
+        L.mtd_eval_expression.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, dp, dp]
+        _lib = L
+    return _lib
+
+
+def _options(precision="mixed", device=0, boltz=8.617343e-5, groups=None, hills_path="", work_dir=None):
+    groups = groups or {"all": 1}
+    names = (C.c_char_p * len(groups))(*[g.encode() for g in groups])
+    bits = (C.c_int * len(groups))(*[int(b) for b in groups.values()])
+    opt = Options()
+    lib().mtd_options_default(C.byref(opt))
+    opt.precision = PREC[precision]
+    opt.device = int(device)
+    opt.boltz = float(boltz)
+    opt.n_groups = len(groups)
+    opt.group_names = C.cast(names, C.POINTER(C.c_char_p))
+    opt.group_bits = C.cast(bits, C.POINTER(C.c_int))
+    opt.hills_path = hills_path.encode() if hills_path is not None else None
+    opt.work_dir = work_dir.encode() if work_dir else None
+    return opt, (names, bits)
+
+
+def parse_args(args, groups=None):
+    """Host-only grammar check: returns "" when `args` would build a context, else the message."""
+    opt, keep = _options(groups=groups)
+    toks = [str(a).encode() for a in args]
+    argv = (C.c_char_p * max(1, len(toks)))(*toks)
+    buf = C.create_string_buffer(1024)
+    lib().mtd_parse_args(len(toks), argv, C.byref(opt), buf, 1024)
+    return buf.value.decode()
+
+
+def eval_expression(expr, values):
+    """Host evaluation of a DIM expression: (value, {symbol: derivative})."""
+    names = list(values)
+    n = len(names)
+    carr = (C.c_char_p * max(1, n))(*[k.encode() for k in names])
+    vals = np.ascontiguousarray([values[k] for k in names], dtype=np.float64)
+    out = np.zeros(1)
+    grad = np.zeros(max(1, n))
+    st = lib().mtd_eval_expression(expr.encode(), n, carr, vals.ctypes.data_as(C.POINTER(C.c_double)),
+                                   out.ctypes.data_as(C.POINTER(C.c_double)),
+                                   grad.ctypes.data_as(C.POINTER(C.c_double)))
+    if st != MTD_OK:
+        raise MetadError(st, "cannot evaluate expression %r" % expr)
+    return out[0], dict(zip(names, grad[:n]))
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Metad:
+    """One `fix metad` instance on one GPU."""
+
+    def __init__(self, args, precision="mixed", device=0, boltz=8.617343e-5, groups=None,
+                 hills_path="", work_dir=None):
+        L = lib()
+        opt, self._keep = _options(precision, device, boltz, groups, hills_path, work_dir)
+        toks = [str(a).encode() for a in args]
+        argv = (C.c_char_p * max(1, len(toks)))(*toks)
+        h = C.c_void_p()
+        st = L.mtd_create(len(toks), argv, C.byref(opt), C.byref(h))
+        self._h = h
+        if st != MTD_OK:
+            msg = L.mtd_last_error(h).decode() if h else "mtd_create failed"
+            if h:
+                L.mtd_destroy(h)
+            self._h = None
+            raise MetadError(st, msg)
+        self.cv_dim = L.mtd_cv_dim(h)
+
+    def _check(self, st):
+        if st != MTD_OK:
+            raise MetadError(st, lib().mtd_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            lib().mtd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_box(self, lo, hi, periodic=(1, 1, 1)):
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        hi = np.ascontiguousarray(hi, dtype=np.float64)
+        pe = np.ascontiguousarray(periodic, dtype=np.int32)
+        self._check(lib().mtd_set_box(self._h, lo.ctypes.data_as(C.POINTER(C.c_double)),
+                                      hi.ctypes.data_as(C.POINTER(C.c_double)),
+                                      pe.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def init(self):
+        self._check(lib().mtd_init(self._h))
+
+    def post_force(self, step, x, f, mask=None, image=None, virial=False):
+        """f (n x 3, float64, C order) is updated in place: f -= bias force."""
+        assert x.dtype == np.float64 and x.flags.c_contiguous and f.dtype == np.float64 and f.flags.c_contiguous
+        n = x.shape[0]
+        v = np.zeros(6) if virial else None
+        m = np.ascontiguousarray(mask, dtype=np.int32) if mask is not None else None
+        im = np.ascontiguousarray(image, dtype=np.int32) if image is not None else None
+        self._check(lib().mtd_post_force(self._h, int(step), n, _ptr(x), _ptr(m), _ptr(im), _ptr(f), _ptr(v)))
+        return v
+
+    def post_force_device(self, step, n, x_ptr, f_in_ptr, f_out_ptr, mask_ptr=0, image_ptr=0):
+        """Device pointers (ints); asynchronous on the context stream."""
+        self._check(lib().mtd_post_force_device(self._h, int(step), int(n), C.c_void_p(x_ptr),
+                                                C.c_void_p(mask_ptr or None), C.c_void_p(image_ptr or None),
+                                                C.c_void_p(f_in_ptr), C.c_void_p(f_out_ptr)))
+
+    def sync(self):
+        self._check(lib().mtd_sync(self._h))
+
+    def compute_scalar(self):
+        return lib().mtd_compute_scalar(self._h)
+
+    def compute_vector(self, k):
+        return lib().mtd_compute_vector(self._h, int(k))
+
+    @property
+    def cv(self):
+        return np.array([self.compute_vector(k) for k in range(self.cv_dim)])
+
+    def extract(self, key, n):
+        out = np.zeros(n)
+        self._check(lib().mtd_extract_peratom(self._h, key.encode(), out.ctypes.data_as(C.POINTER(C.c_double)), n))
+        return out
+
+    def hills_replay(self, path):
+        self._check(lib().mtd_hills_replay(self._h, path.encode()))
+
+    def grid(self, size):
+        out = np.zeros(size)
+        self._check(lib().mtd_get_grid(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), size))
+        return out
+
+    def launch_count(self):
+        return lib().mtd_last_launch_count(self._h)
+
+    def max_neighbors(self, cal):
+        return lib().mtd_max_neighbors(self._h, cal.encode())

@@ -1,0 +1,84 @@
+"""GPU parity against the FP64 oracle, through the C ABI.
+
+Tolerances: FP64 mode 1e-9 relative (the reference bar is 1e-6); mixed mode
+(FP32 per atom, FP64 sums and grid) 2e-5 relative on CV values and bias, 2e-3
+relative on the largest force component.  Neighbour counts are compared
+exactly.
+"""
+import numpy as np
+import pytest
+
+import helpers as H
+import oracle as O
+import systems
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": (1e-9, 1e-9), "mixed": (2e-5, 2e-3)}
+
+
+def _q_system(seed=11, step=0):
+    x, L = systems.config1()
+    return systems.jitter(x, 0.15, seed, step), L
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_steinh_q_one_step(precision):
+    x, L = _q_system()
+    args = H.fix_args_q()
+    m, out = H.run_gpu(args, x, L, [(0, x)], precision=precision)
+    cv, bias, f, _ = out[0]
+    o = O.steinh_q(6, x, L, 3.9, 18)
+    g = O.Grid([[0.0, 1.0]], [1000], 0.01, 0.005, 10.0, 300.0, 8.617343e-5, False)
+    g.add_hill([o["cv"]])
+    V, dV = g.value([o["cv"]])
+    fo = -dV[0] * o["grad"]
+    tcv, tf = TOL[precision]
+    assert H.rel(cv[0], o["cv"]) < tcv
+    assert H.rel(bias, V) < tcv
+    assert H.rel(f, fo) < tf
+    q = m.extract("Q6.stein_q", x.shape[0])
+    assert H.rel(q, o["Q"]) < tcv * 10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_local_ql_q4_q6_step(precision):
+    x, L = systems.small_slab(nxy=6, nz_fcc=3, nz_bcc=4, n_liq=300)
+    x = systems.jitter(x, 0.05, 3)
+    args = H.fix_args_local()
+    m, out = H.run_gpu(args, x, L, [(0, x), (10, x)], precision=precision)
+    o4 = H.oracle_local(x, L, 4)
+    o6 = H.oracle_local(x, L, 6)
+    g = O.Grid([[0, 1], [0, 1]], [200, 200], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    s = [o4["cv"], o6["cv"]]
+    tcv, tf = TOL[precision]
+    for k, (step, _) in enumerate([(0, x), (10, x)]):
+        g.add_hill(s)
+        V, dV = g.value(s)
+        fo = -(dV[0] * o4["grad"] + dV[1] * o6["grad"])
+        cv, bias, f, _ = out[k]
+        assert H.rel(cv, s) < tcv
+        assert H.rel(bias, V) < tcv
+        assert H.rel(f, fo) < tf
+    assert m.max_neighbors("Q4") == o4["nnb"].max()
+
+
+@pytest.mark.parametrize("mode", ["MEAN_SOLID", "NSOLID", "FRAC"])
+def test_local_ql_smooth_switches(mode):
+    x, L = systems.small_slab(nxy=6, nz_fcc=3, nz_bcc=4, n_liq=300)
+    x = systems.jitter(x, 0.05, 5)
+    args = H.fix_args_local(sw="FERMI", alpha=-8.0, mode=mode, cvsw=(0.35, 20.0), nbins=100)
+    m, out = H.run_gpu(args, x, L, [(0, x)], precision="fp64")
+    swr = O.make_sw("FERMI", r0=3.9, alpha=-8.0)
+    rl = O.sw_invert_for_eps(swr, 1e-6)
+    swc = O.make_sw("FERMI", r0=0.35, alpha=20.0)
+    o4 = O.steinh_l(4, x, L, rl, swr, 1e-6, swc, mode)
+    o6 = O.steinh_l(6, x, L, rl, swr, 1e-6, swc, mode)
+    g = O.Grid([[0, 1], [0, 1]], [100, 100], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    s = [o4["cv"], o6["cv"]]
+    g.add_hill(s)
+    V, dV = g.value(s)
+    fo = -(dV[0] * o4["grad"] + dV[1] * o6["grad"])
+    cv, bias, f, _ = out[0]
+    assert H.rel(cv, s) < 1e-9
+    assert H.rel(f, fo) < 1e-8
