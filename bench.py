@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the metadynamics hot path: CV + bias + force atom-steps/s.
+
+Workload (the config the headline metric is quoted on): 256,000 atoms in
+z-stacked FCC / BCC / hard-core-liquid slabs, STEINH L Q4 + Q6 (STEP
+switching at 3.9 A; the cap of 18 is parsed and reported as non-binding),
+MEAN_SOLID of each as v1, v2, a 200 x 200 well-tempered grid on [0,1]^2
+(TEMP 300, biasf 9 -> delta T = 2400 K), sigma 0.01, h 0.005 eV, PACE 10,
+mixed precision (FP32 per atom, FP64 sums and grid).  Positions are seeded
+synthetic data: four jittered copies (N(0, 0.05 A)) of the slab geometry,
+cycled step by step.
+
+A step = one FixMetadynamics::post_force: cell list, neighbour lists, Q4/Q6
+values, reductions, bias grid (deposit every PACE), dV/ds, analytic forces.
+`value` times the device-resident call (inputs in HBM); `e2e` times the C-ABI
+call on pinned host x and f, H2D and D2H copies included.  L2 is flushed
+(a 256 MB write) before every timed step, outside the timed interval.
+
+--impl reference times the reference algorithm's CPU restatement (the FP64
+oracle, OpenMP over all host cores) on the same workload; the reference
+plugin itself needs LAMMPS, which is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "metad-toy_b200")]
+
+METRIC = "CV+bias+force atom-steps/s at 256k atoms; NN vs exact hill bias, same error"
+UNIT = "atom-steps/s"
+WORKLOAD = "256k-atom FCC/BCC/liquid slabs, STEINH L Q4+Q6 MEAN_SOLID with forces, 2D 200x200 WT grid, PACE 10"
+
+
+def fix_args():
+    return ["GAUSSIAN", 0.01, 0.005, 9.0, "PACE", 10, "TEMP", 300.0,
+            "CAL", "NAME", "ST", "SW_FUNC", "STEP", "r_0", 3.9,
+            "CAL", "NAME", "Q4", "STEINH", "L", 4, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18, "SW_FUNC_r", "ST",
+            "CAL", "NAME", "Q6", "STEINH", "L", 6, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18, "SW_FUNC_r", "ST",
+            "SYMBOL", "v1", "Q4.MEAN_SOLID", "SYMBOL", "v2", "Q6.MEAN_SOLID",
+            "CV_dim", 2, "DIM", 1, 0, 1, 200, "v1", "DIM", 2, 0, 1, 200, "v2", "WT", 1]
+
+
+def load_system(seed=2024, copies=4):
+    import systems
+    cache = os.path.join(tempfile.gettempdir(), "mtd_config2_%d.npz" % seed)
+    if os.path.exists(cache):
+        z = np.load(cache)
+        x, L = z["x"], z["L"]
+    else:
+        x, L = systems.config2(seed=seed)
+        np.savez(cache, x=x, L=L)
+    xs = [np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.05, seed + 1, c), L)) for c in range(copies)]
+    return xs, L
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(tempfile.gettempdir(), "mtd_clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            p = [t.strip() for t in line.split(",")]
+            if len(p) >= 7:
+                rows.append(p)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = [names[k] for k in range(4) if any(r[3 + k].lower().startswith("active") for r in rows)]
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def kernel_bytes(name, n, nbar):
+    """Algorithmic (compulsory) HBM bytes per launch of each kernel of the step:
+    every per-atom array it must read or write once, pair records 16 B each."""
+    per_atom = {
+        "neighbors": 48 + 16 * nbar,
+        "local_q": 104 + 16 * nbar,
+        "local_lq": 228 + 16 * nbar,
+        "local_lambda": 216 + 16 * nbar,
+        "local_force": 152 + 16 * nbar,
+        "cell_bin": 32, "cell_scatter": 12, "cell_sort": 80,
+    }
+    return per_atom.get(name, 0.0) * n
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        p = json.load(open(path))
+        return p.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_dram_per_launch.json")
+    if not os.path.exists(path):
+        return None
+    try:
+        d = json.load(open(path))
+        return d.get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_baseline(xs, L, budget_s=15.0, threads=None):
+    """The FP64 oracle (C, OpenMP) running the same step on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if threads:
+        O.set_threads(threads)
+    sw = O.make_sw("STEP", r0=3.9)
+    g = O.Grid([[0, 1], [0, 1]], [200, 200], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    n = xs[0].shape[0]
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        x = xs[steps % len(xs)]
+        o4 = O.steinh_l(4, x, L, 3.9, sw)
+        o6 = O.steinh_l(6, x, L, 3.9, sw)
+        s = [o4["cv"], o6["cv"]]
+        if (steps * 1) % 10 == 0:
+            g.add_hill(s)
+        V, dV = g.value(s)
+        _ = -(dV[0] * o4["grad"] + dV[1] * o6["grad"])
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 50:
+            break
+    return {"value": n * steps / el, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+            "sample": "%d full steps of the 256,000-atom workload (FP64 oracle, both orders with forces, grid)" % steps}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    xs, L = load_system()
+    cores = os.cpu_count() or 1
+    base = cpu_baseline(xs, L, budget_s=max(10.0, 2.0 * args.steps), threads=cores)
+    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded slab geometry)",
+            "config": {"workload": WORKLOAD, "atoms": int(xs[0].shape[0])},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import mtd
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    xs, L = load_system()
+    n = xs[0].shape[0]
+    m = mtd.Metad(fix_args(), precision=args.precision, device=local)
+    m.set_box([0, 0, 0], L)
+    m.init()
+    stream = torch.cuda.current_stream()
+    m.set_stream(stream.cuda_stream)
+    dx = [torch.from_numpy(x).cuda() for x in xs]
+    f_in = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    f_out = torch.zeros_like(f_in)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    step = 0
+
+    def dev_step():
+        nonlocal step
+        m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f_in.data_ptr(), f_out.data_ptr())
+        step += 1
+
+    for _ in range(args.warmup):
+        dev_step()
+    m.sync()
+    torch.cuda.synchronize()
+    launches = m.launch_count()
+    nbar = None
+    try:
+        from scipy.spatial import cKDTree
+        t = cKDTree(xs[0], boxsize=L)
+        nbar = float((t.query_ball_point(xs[0], 3.9 - 1e-9, return_length=True) - 1).mean())
+    except Exception:
+        nbar = 8.0
+
+    # per-kernel durations (separate pass, CUDA events between launches)
+    m.profile(True)
+    for _ in range(max(5, args.steps // 3)):
+        flush.zero_()
+        dev_step()
+    m.sync()
+    prof = m.profile_report()
+    m.profile(False)
+
+    # timed, device-resident
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            dev_step()
+            ev[k][1].record(stream)
+        m.sync()
+        torch.cuda.synchronize()
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    clocks = clk.summary()
+
+    # e2e through the C ABI on pinned host buffers
+    hx = [torch.from_numpy(x).pin_memory() for x in xs]
+    hf = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    m.set_stream(0)
+    for k in range(2):
+        hf.zero_()
+        m.post_force(step, hx[step % len(hx)].numpy(), hf.numpy())
+        step += 1
+    e2e_s = 0.0
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        hf.zero_()
+        t0 = time.perf_counter()
+        m.post_force(step, hx[step % len(hx)].numpy(), hf.numpy())
+        e2e_s += time.perf_counter() - t0
+        step += 1
+
+    t = torch.tensor([dev_ms, e2e_s * 1e3], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms, e2e_ms = float(t[0]), float(t[1])
+    total_atoms = n * args.steps * world
+    value = total_atoms / (dev_ms / 1e3)
+    e2e_value = total_atoms / (e2e_ms / 1e3)
+
+    # roofline of the dominant kernel
+    peak, peak_kind = peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    dom_name, (calls, tot_ms) = dom
+    avg_ms = tot_ms / max(calls, 1)
+    nbytes = kernel_bytes(dom_name, n, nbar)
+    achieved = nbytes / (avg_ms / 1e3) / 1e9 if nbytes else None
+    roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+            "traffic": ncu_traffic(dom_name), "avg_launch_ms": avg_ms,
+            "algorithmic_bytes_per_launch": nbytes,
+            "kernels_ms_per_step": {k: v[1] / max(v[0], 1) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(xs, L, budget_s=15.0, threads=os.cpu_count())
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded FCC/BCC/liquid slabs, 4 jittered copies cycled)",
+            "config": {"workload": WORKLOAD, "atoms": n, "mean_neighbors": nbar,
+                       "max_neighbors": m.max_neighbors("Q4"), "cap_cutoff_Natoms": 18,
+                       "precision": args.precision, "l2": "flushed (256 MB write) before each timed step",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "cv": [float(v) for v in m.cv]},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
+                    "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps},
+            "gpu_launches": launches * args.steps,
+            "roofline": roof, "clocks": clocks, "cpu_baseline": cpu}
+    if rank == 0:
+        print(json.dumps(line))
+    m.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -138,6 +138,20 @@ mtd_status mtd_get_grid(mtd_ctx *ctx, double *out, int64_t count);
 /* Number of device kernels the last step launched (diagnostics). */
 int mtd_last_launch_count(const mtd_ctx *ctx);
 
+/* Runs the context's work on an external CUDA stream (a cudaStream_t, e.g. the
+ * host code's or LAMMPS/Kokkos's stream); NULL returns to the context's own
+ * stream.  The reference runs everything on the default stream
+ * (src/cvs/CVs_Steinhardt.cu:1110). */
+mtd_status mtd_set_stream(mtd_ctx *ctx, void *cuda_stream);
+
+/* Per-kernel timing with CUDA events recorded after every launch.  enable
+ * resets the totals; each step then synchronises on its last event and adds
+ * every kernel's duration to a per-name total.  mtd_profile_report writes
+ * lines "name calls total_ms\n" into buf and returns the bytes needed.
+ * The reference has no timers (its only timing is LAMMPS's Modify time). */
+mtd_status mtd_profile_enable(mtd_ctx *ctx, int enable);
+int mtd_profile_report(mtd_ctx *ctx, char *buf, int len);
+
 /* Largest neighbour count seen by the last step for CAL `name` (cap reporting). */
 int mtd_max_neighbors(mtd_ctx *ctx, const char *name);
 

@@ -199,6 +199,31 @@ bool parse_sk(Cursor &c, int &i, const GroupTable &groups, CalDef &d) {
     return true;
 }
 
+// A SYMBOL's function against its CAL kind: set_CV_calculate of each CV
+// (src/cvs/CVs_Steinhardt.cu:709-737, src/cvs/CVs_Steinhardt_Local.cu:600-645,
+// src/cvs/CVs_Strufactor.cu:616-624).  STEINH L binds `.sw` as its CV switch.
+std::string resolve_symbol(Config &cfg, const SymbolDef &s) {
+    CalDef &d = cfg.cals[s.cal];
+    bool ok = false;
+    if (d.kind == CAL_STEINH_Q) ok = (s.func == "AVE" || s.func == "SW_FUNC");
+    else if (d.kind == CAL_STEINH_L)
+        ok = (s.func == "MEAN_SOLID" || s.func == "AVE" || s.func == "NSOLID" || s.func == "SW_FUNC" || s.func == "FRAC");
+    else if (d.kind == CAL_STRU_FACTOR) ok = (s.func == "AVE" || s.func == "COUNT");
+    else ok = (s.func == "AVE");
+    if (!ok) return "Error: We can't find the func " + s.func + " for CAL " + s.cal + ".";
+    if (d.kind == CAL_STEINH_Q && s.func == "SW_FUNC") {
+        if (s.sub.empty() || !cfg.sws.count(s.sub))
+            return "Switching function " + s.sub + " used in SYMBOL but not defined in CAL!";
+    }
+    if (d.kind == CAL_STEINH_L && !s.sub.empty()) {
+        if (!cfg.sws.count(s.sub)) return "Switching function " + s.sub + " used in SYMBOL but not defined in CAL!";
+        d.sw_cv = cfg.sws[s.sub];
+    }
+    if (d.kind == CAL_STRU_FACTOR && s.func == "COUNT" && !d.sf_use_sw)
+        return "Error: STRU_FACTOR COUNT needs 'SW_func' on the CAL.";
+    return "";
+}
+
 }  // namespace
 
 double sw_invert_for_eps(const SwParams &p, double eps) {
@@ -330,6 +355,8 @@ std::string parse_fix_args(int narg, const char *const *arg, const GroupTable &g
             for (auto &o : cfg.symbols)
                 if (o.name == s.name) return "Error: SYMBOL '" + s.name + "' is duplicated.";
             if ((int)cfg.symbols.size() >= kMaxSymbols) return "Error: too many SYMBOL entries.";
+            std::string e = resolve_symbol(cfg, s);   // set_CV_calculate at add_symbol time (DimSet.cu:28-52)
+            if (!e.empty()) return e;
             cfg.symbols.push_back(s);
             i += 3;
         } else if (!std::strcmp(kw, "DIM")) {
@@ -372,27 +399,6 @@ std::string parse_fix_args(int narg, const char *const *arg, const GroupTable &g
             o << "Error: CV_dim is set to " << cfg.cv_dim << ", but DIM " << d + 1 << " is missing.";
             return o.str();
         }
-    // Resolve SYMBOL functions against their CAL kinds (set_CV_calculate of each CV).
-    for (auto &s : cfg.symbols) {
-        CalDef &d = cfg.cals[s.cal];
-        bool ok = false;
-        if (d.kind == CAL_STEINH_Q) ok = (s.func == "AVE" || s.func == "SW_FUNC");
-        else if (d.kind == CAL_STEINH_L)
-            ok = (s.func == "MEAN_SOLID" || s.func == "AVE" || s.func == "NSOLID" || s.func == "SW_FUNC" || s.func == "FRAC");
-        else if (d.kind == CAL_STRU_FACTOR) ok = (s.func == "AVE" || s.func == "COUNT");
-        else ok = (s.func == "AVE");
-        if (!ok) return "Error: We can't find the func " + s.func + " for CAL " + s.cal + ".";
-        if (d.kind == CAL_STEINH_Q && s.func == "SW_FUNC") {
-            if (s.sub.empty() || !cfg.sws.count(s.sub))
-                return "Switching function " + s.sub + " used in SYMBOL but not defined in CAL!";
-        }
-        if (d.kind == CAL_STEINH_L && !s.sub.empty()) {   // bind_sw (Local.cu:612-619)
-            if (!cfg.sws.count(s.sub)) return "Switching function " + s.sub + " used in SYMBOL but not defined in CAL!";
-            d.sw_cv = cfg.sws[s.sub];
-        }
-        if (d.kind == CAL_STRU_FACTOR && s.func == "COUNT" && !d.sf_use_sw)
-            return "Error: STRU_FACTOR COUNT needs 'SW_func' on the CAL.";
-    }
     if (!(cfg.sigma > 0)) return "Error: GAUSSIAN sigma must be > 0.";
     return "";
 }

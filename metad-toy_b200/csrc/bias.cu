@@ -83,13 +83,25 @@ __device__ double grid_value(const BiasPlan &P, const double *s, double *dV) {
 }
 
 // Band of a hill: [c - R, c + R] clipped to the grid, c = (int)((s - lo)/dcv)
-// (C truncation as in add_to_grid), R from the fix's sigma.
-__device__ __forceinline__ void hill_band(const BiasPlan &P, const double *s, int *lo, int *hi) {
+// (C truncation as in add_to_grid), R from the fix's sigma.  A centre outside
+// the grid by more than R bins (or not finite) gives an empty band, which is
+// what the reference's `for (g = lower; g <= upper; ...)` loops do.
+__device__ __forceinline__ bool hill_band(const BiasPlan &P, const double *s, int *lo, int *hi) {
+    bool nonempty = true;
     for (int k = 0; k < P.D; ++k) {
-        const int c = (int)((s[k] - P.lo[k]) / P.dcv[k]);
+        const double u = (s[k] - P.lo[k]) / P.dcv[k];
+        if (!(u > -(double)P.band[k] - 2.0 && u < (double)P.nbin[k] + (double)P.band[k] + 2.0)) {
+            lo[k] = 0;
+            hi[k] = -1;
+            nonempty = false;
+            continue;
+        }
+        const int c = (int)u;
         lo[k] = max(0, c - P.band[k]);
         hi[k] = min(P.nbin[k] - 1, c + P.band[k]);
+        if (lo[k] > hi[k]) nonempty = false;
     }
+    return nonempty;
 }
 
 __device__ __forceinline__ double hill_gauss(const BiasPlan &P, const double *s, const int *idx, double sigma) {
@@ -227,11 +239,13 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
     // 5. banded deposit, one thread per band bin
     if (do_dep) {
         int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
-        hill_band(P, sv, lo, hi);
-        int total = 1;
-        for (int k = 0; k < P.D; ++k) {
-            ext[k] = hi[k] - lo[k] + 1;
-            total *= ext[k];
+        int total = 0;
+        if (hill_band(P, sv, lo, hi)) {
+            total = 1;
+            for (int k = 0; k < P.D; ++k) {
+                ext[k] = hi[k] - lo[k] + 1;
+                total *= ext[k];
+            }
         }
         for (int t = threadIdx.x; t < total; t += blockDim.x) {
             int idx[3] = {0, 0, 0}, rem = t;
@@ -241,7 +255,7 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
             }
             size_t g = idx[0];
             for (int k = 1; k < P.D; ++k) g = g * P.nbin[k] + idx[k];
-            P.grid[g] += hill_w * hill_gauss(P, sv, idx, P.sigma);
+            if (g < (size_t)P.grid_size) P.grid[g] += hill_w * hill_gauss(P, sv, idx, P.sigma);
         }
         if (threadIdx.x == 0) {
             unsigned long long h = *P.nhills;
@@ -324,7 +338,7 @@ __global__ void k_hills_replay(const BiasPlan *__restrict__ Pp, const HillRec *_
         double acc = P.grid[g];
         for (int q = 0; q < nh; ++q) {
             int lo[3], hi[3];
-            hill_band(P, h[q].s, lo, hi);
+            if (!hill_band(P, h[q].s, lo, hi)) continue;
             bool in = true;
             for (int k = 0; k < P.D; ++k) in = in && idx[k] >= lo[k] && idx[k] <= hi[k];
             if (in) acc += h[q].w * hill_gauss(P, h[q].s, idx, h[q].sigma);
@@ -347,6 +361,7 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 
 void launch_bias_step(const BiasPlan *d_plan, long long step, int, cudaStream_t st) {
     k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
+    prof_mark("bias_step", st);
 }
 
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st) {
@@ -358,6 +373,7 @@ void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int n
 
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st) {
     k_virial_finalize<<<1, 256, 0, st>>>(vpart, nparts, out6);
+    prof_mark("virial", st);
 }
 
 }  // namespace mtd

@@ -131,7 +131,26 @@ struct mtd_ctx {
     bool pending = false;
     long long pending_step = 0;
     CellGrid last_grid{};
+    cudaStream_t own_st = nullptr;
+    Prof prof;
+    bool prof_created = false;
+    std::map<std::string, std::pair<long long, double>> prof_total;
 };
+
+namespace {
+thread_local Prof *g_prof = nullptr;
+}
+
+namespace mtd {
+void prof_set(Prof *p) { g_prof = p; }
+void prof_mark(const char *name, cudaStream_t st) {
+    Prof *p = g_prof;
+    if (!p || !p->on || p->n >= kProfMax) return;
+    p->name[p->n] = name;
+    cudaEventRecord(p->ev[p->n], st);
+    ++p->n;
+}
+}  // namespace mtd
 
 namespace {
 
@@ -365,6 +384,7 @@ void build_plan(mtd_ctx *c) {
         }
     }
     P.grid = c->d_grid;
+    P.grid_size = c->d_grid ? c->grid_size : 0;
     P.hills = c->d_hills;
     P.hill_cap = kHillCap;
     P.nhills = c->d_nhills;
@@ -639,9 +659,37 @@ void run_units(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, 
     }
 }
 
+// Adds the kernel intervals of the last profiled step to the per-name totals.
+void prof_collect(mtd_ctx *c) {
+    Prof &p = c->prof;
+    if (p.n >= 2) {
+        cudaEventSynchronize(p.ev[p.n - 1]);
+        for (int i = 1; i < p.n; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p.ev[i - 1], p.ev[i]);
+            auto &t = c->prof_total[p.name[i]];
+            t.first += 1;
+            t.second += ms;
+        }
+    }
+    p.n = 0;
+}
+
+struct ProfScope {
+    explicit ProfScope(mtd_ctx *c) {
+        if (c->prof.on) {
+            prof_collect(c);
+            prof_set(&c->prof);
+            prof_mark("start", c->st);
+        }
+    }
+    ~ProfScope() { prof_set(nullptr); }
+};
+
 mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, const int *mask, const int *image,
                         const double *fin, double *fout, bool virial) {
     if (!c->box_set) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_box must be called before the first step");
+    ProfScope prof_scope(c);
     mtd_status s0 = ensure_capacity(c, n);
     if (s0 != MTD_OK) return s0;
     CellGrid g = make_grid(c);
@@ -874,6 +922,7 @@ mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, 
         return MTD_ERR_CUDA;
     }
     cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    c->own_st = c->st;
     c->cv.assign(c->cfg.cv_dim, 0.0);
     mtd_status s = plan_units(c);
     if (s == MTD_OK) {
@@ -917,7 +966,9 @@ void mtd_destroy(mtd_ctx *c) {
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_vir) cudaFreeHost(c->h_vir);
     if (c->h_nhills) cudaFreeHost(c->h_nhills);
-    if (c->st) cudaStreamDestroy(c->st);
+    if (c->own_st) cudaStreamDestroy(c->own_st);
+    if (c->prof_created)
+        for (int i = 0; i < kProfMax; ++i) cudaEventDestroy(c->prof.ev[i]);
     if (c->f_hills) std::fclose(c->f_hills);
     if (c->f_rec) std::fclose(c->f_rec);
     delete c;
@@ -1129,6 +1180,42 @@ mtd_status mtd_get_grid(mtd_ctx *c, double *out, int64_t count) {
 }
 
 int mtd_last_launch_count(const mtd_ctx *c) { return c ? c->launches : 0; }
+
+mtd_status mtd_set_stream(mtd_ctx *c, void *stream) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    MTD_CU(cudaStreamSynchronize(c->st), "stream switch");
+    c->st = stream ? (cudaStream_t)stream : c->own_st;
+    return MTD_OK;
+}
+
+mtd_status mtd_profile_enable(mtd_ctx *c, int enable) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    if (enable && !c->prof_created) {
+        for (int i = 0; i < kProfMax; ++i) MTD_CU(cudaEventCreate(&c->prof.ev[i]), "profile events");
+        c->prof_created = true;
+    }
+    if (c->prof.on) prof_collect(c);
+    c->prof.on = enable != 0;
+    c->prof.n = 0;
+    c->prof_total.clear();
+    return MTD_OK;
+}
+
+int mtd_profile_report(mtd_ctx *c, char *buf, int len) {
+    if (!c) return 0;
+    if (c->prof.on) prof_collect(c);
+    std::string s;
+    char line[160];
+    for (auto &kv : c->prof_total) {
+        std::snprintf(line, sizeof(line), "%s %lld %.6f\n", kv.first.c_str(), kv.second.first, kv.second.second);
+        s += line;
+    }
+    if (buf && len > 0) {
+        std::strncpy(buf, s.c_str(), (size_t)len - 1);
+        buf[len - 1] = '\0';
+    }
+    return (int)s.size() + 1;
+}
 
 int mtd_max_neighbors(mtd_ctx *c, const char *name) {
     if (!c || !name) return -1;

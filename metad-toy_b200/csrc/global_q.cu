@@ -179,6 +179,7 @@ template <typename T> void launch_global_values(const GlobalDev<T> &d, cudaStrea
     case 4: k_global_values<4, T><<<nb, kBlock, 0, st>>>(d); break;
     case 6: k_global_values<6, T><<<nb, kBlock, 0, st>>>(d); break;
     }
+    prof_mark("global_values", st);
 }
 
 template <typename T>
@@ -191,6 +192,7 @@ void launch_global_forces(const GlobalDev<T> &d, const double *f_src, double *f_
     case 4: k_global_force<4, T><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status); break;
     case 6: k_global_force<6, T><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status); break;
     }
+    prof_mark("global_force", st);
 }
 
 template void launch_global_values<float>(const GlobalDev<float> &, cudaStream_t);

@@ -60,6 +60,19 @@ template <typename T> struct NeighDev {
     int M;
 };
 
+// ------------------------------------------------------------------ per-kernel timing
+// When a context enables profiling, every launcher records a CUDA event after
+// each kernel on the launch stream; consecutive events bracket one kernel.
+constexpr int kProfMax = 128;
+struct Prof {
+    bool on = false;
+    int n = 0;
+    cudaEvent_t ev[kProfMax];
+    const char *name[kProfMax];
+};
+void prof_set(Prof *p);                          // active profiler of this host thread (null: off)
+void prof_mark(const char *name, cudaStream_t st);
+
 // ------------------------------------------------------------------ neighbours
 void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st);
 template <typename T>
@@ -179,6 +192,7 @@ struct BiasPlan {
     int ncode[3];
     ExprInstr code[3][kMaxExprLen];
     double *grid;
+    long long grid_size;
     HillRec *hills;
     int hill_cap;
     unsigned long long *nhills;

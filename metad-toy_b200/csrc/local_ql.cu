@@ -365,7 +365,9 @@ __global__ void __launch_bounds__(kBlock) k_local_force(LocalDev<T> d, const dou
 template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cudaStream_t st) {
     const int nb = (d.n + kBlock - 1) / kBlock;
     k_local_q<LA, LB, T><<<nb, kBlock, 0, st>>>(d);
+    prof_mark("local_q", st);
     k_local_lq<LA, LB, T><<<nb, kBlock, 0, st>>>(d);
+    prof_mark("local_lq", st);
 }
 
 template <int LA, int LB, typename T>
@@ -375,10 +377,14 @@ void run_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const 
     const bool dsig = !(d.sw_r.type == SW_STEP);
     if (dsig) {
         k_local_lambda<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
+        prof_mark("local_lambda", st);
         k_local_force<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+        prof_mark("local_force", st);
     } else {
         k_local_lambda<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
+        prof_mark("local_lambda", st);
         k_local_force<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+        prof_mark("local_force", st);
     }
 }
 

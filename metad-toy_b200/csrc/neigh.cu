@@ -244,9 +244,13 @@ void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
     cudaMemsetAsync(s.count, 0, sizeof(int) * (size_t)g.ncell, st);
     const int nb = (s.n + kBlock - 1) / kBlock;
     if (s.n > 0) k_bin<<<nb, kBlock, 0, st>>>(g, s);
+    prof_mark("cell_bin", st);
     k_scan<<<1, 1024, 0, st>>>(s.count, s.start, g.ncell);
+    prof_mark("cell_scan", st);
     if (s.n > 0) k_scatter<<<nb, kBlock, 0, st>>>(s);
+    prof_mark("cell_scatter", st);
     k_cellsort<<<(g.ncell + kBlock - 1) / kBlock, kBlock, 0, st>>>(g, s);
+    prof_mark("cell_sort", st);
 }
 
 template <typename T>
@@ -256,7 +260,11 @@ void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, N
     const int nb = (s.n + kBlock - 1) / kBlock;
     if (ns.kind == NK_RANGE) k_neighbors<T, NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
     else k_neighbors<T, NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
-    if (ns.cap > 0) k_select_cap<T><<<nb, kBlock, 0, st>>>(g, s, ns, nd);
+    prof_mark("neighbors", st);
+    if (ns.cap > 0) {
+        k_select_cap<T><<<nb, kBlock, 0, st>>>(g, s, ns, nd);
+        prof_mark("select_cap", st);
+    }
 }
 
 template void launch_neighbors<float>(const CellGrid &, const SysDev &, const NeighSpec &, NeighDev<float>, DevStatus *,

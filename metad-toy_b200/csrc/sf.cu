@@ -248,12 +248,14 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
 template <typename T> void launch_debye_values(const DebyeDev<T> &d, cudaStream_t st) {
     if (d.n == 0) return;
     k_debye_values<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d);
+    prof_mark("debye_values", st);
 }
 template <typename T>
 void launch_debye_forces(const DebyeDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                          double *vpart, DevStatus *status, cudaStream_t st) {
     if (d.n == 0) return;
     k_debye_force<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+    prof_mark("debye_force", st);
 }
 template void launch_debye_values<float>(const DebyeDev<float> &, cudaStream_t);
 template void launch_debye_values<double>(const DebyeDev<double> &, cudaStream_t);
@@ -270,7 +272,9 @@ int sk_blocks(int n) {
 void launch_sk_values(const SkDev &d, cudaStream_t st) {
     if (d.fp64) k_sk_partial<true><<<d.nblocks, 256, 0, st>>>(d);
     else k_sk_partial<false><<<d.nblocks, 256, 0, st>>>(d);
+    prof_mark("sk_partial", st);
     k_sk_reduce<<<2 * d.K + 1, 256, 0, st>>>(d);
+    prof_mark("sk_reduce", st);
 }
 
 void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
@@ -279,6 +283,7 @@ void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const 
     const int nb = (d.n + 255) / 256;
     if (d.fp64) k_sk_force<true><<<nb, 256, 0, st>>>(d, f_src, f_dst, s, g, vpart);
     else k_sk_force<false><<<nb, 256, 0, st>>>(d, f_src, f_dst, s, g, vpart);
+    prof_mark("sk_force", st);
 }
 
 }  // namespace mtd

@@ -30,6 +30,7 @@ PREC = {"mixed": 0, "fp64": 1}
 EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args", "mtd_eval_expression", "mtd_set_box", "mtd_init", "mtd_post_force",
            "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
            "mtd_extract_peratom", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
+           "mtd_set_stream", "mtd_profile_enable", "mtd_profile_report",
            "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version"]
 
 
@@ -82,6 +83,9 @@ def lib():
         L.mtd_last_error.argtypes = [vp]
         L.mtd_last_error.restype = C.c_char_p
         L.mtd_abi_version.restype = C.c_int
+        L.mtd_set_stream.argtypes = [vp, vp]
+        L.mtd_profile_enable.argtypes = [vp, C.c_int]
+        L.mtd_profile_report.argtypes = [vp, C.c_char_p, C.c_int]
         L.mtd_parse_args.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.c_char_p, C.c_int]
         L.mtd_eval_expression.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, dp, dp]
         _lib = L
@@ -228,3 +232,21 @@ class Metad:
 
     def max_neighbors(self, cal):
         return lib().mtd_max_neighbors(self._h, cal.encode())
+
+    def set_stream(self, stream_ptr):
+        """Run on an external cudaStream_t (an int handle, e.g. torch's cuda_stream); 0 = own stream."""
+        self._check(lib().mtd_set_stream(self._h, C.c_void_p(stream_ptr or None)))
+
+    def profile(self, enable=True):
+        self._check(lib().mtd_profile_enable(self._h, 1 if enable else 0))
+
+    def profile_report(self):
+        """{kernel name: (calls, total ms)} accumulated since profile(True)."""
+        need = lib().mtd_profile_report(self._h, None, 0)
+        buf = C.create_string_buffer(max(need, 1))
+        lib().mtd_profile_report(self._h, buf, need)
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, calls, ms = line.split()
+            out[name] = (int(calls), float(ms))
+        return out

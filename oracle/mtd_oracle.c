@@ -772,7 +772,11 @@ void orc_grid_deposit(int D, const int *nbin, const double *bound, double *grid,
     for (int k = 0; k < D; k++) {
         dcv[k] = (bound[2 * k + 1] - bound[2 * k]) / nbin[k];
         int R = (int)ceil(4.0 * sigma_band / dcv[k]) + 1;
-        int c = (int)((s[k] - bound[2 * k]) / dcv[k]);
+        double u = (s[k] - bound[2 * k]) / dcv[k];
+        /* a centre far outside the grid (or not finite) leaves the band empty, as the
+         * reference's lower > upper loops do, without the int overflow of a huge cast */
+        if (!(u > -(double)R - 2.0 && u < (double)nbin[k] + R + 2.0)) return;
+        int c = (int)u;
         lo[k] = c - R < 0 ? 0 : c - R;
         hi[k] = c + R > nbin[k] - 1 ? nbin[k] - 1 : c + R;
     }

@@ -76,6 +76,7 @@ def lib():
         L.orc_sw_df.argtypes = [C.POINTER(Sw), C.c_double]
         L.orc_sw_invert_for_eps.restype = C.c_double
         L.orc_sw_invert_for_eps.argtypes = [C.POINTER(Sw), C.c_double]
+        L.orc_minimg.argtypes = [C.POINTER(Box), dp, dp, dp]
         L.orc_ylm.argtypes = [C.c_int, dp, dp, dp]
         L.orc_ylm_grad.argtypes = [C.c_int, dp, dp, dp, dp, dp]
         L.orc_steinh_q.argtypes = [C.c_int, C.c_int, dp, C.POINTER(Box), ip, C.c_double, C.c_int,
@@ -386,6 +387,8 @@ def eval_expr(expr, values):
                 raise ValueError("unknown function " + name)
             if name == "pi":
                 return const(math.pi)
+            if name == "e" and name not in idx:
+                return const(math.e)
             d = [0.0] * nd
             d[idx[name]] = 1.0
             return _Dual(values[name], d)
@@ -393,29 +396,32 @@ def eval_expr(expr, values):
             v = expr_()
             assert take() == ("op", ")")
             return v
-        if t == ("op", "-"):
-            v = unary()
-            return _Dual(-v.v, [-x for x in v.d])
-        if t == ("op", "+"):
-            return unary()
         raise ValueError("bad token %r" % (t,))
 
     def unary():
-        return primary()
+        # unary minus binds looser than '^':  -a^b = -(a^b),  a^-b = a^(-b)
+        if peek() == ("op", "-"):
+            take()
+            v = unary()
+            return _Dual(-v.v, [-x for x in v.d])
+        if peek() == ("op", "+"):
+            take()
+            return unary()
+        return power()
 
     def power():
-        b = unary()
+        b = primary()
         if peek() == ("op", "^"):
             take()
-            e = power()
+            e = unary()
             return pw(b, e)
         return b
 
     def term():
-        v = power()
+        v = unary()
         while peek() in (("op", "*"), ("op", "/")):
             op = take()[1]
-            r = power()
+            r = unary()
             v = mul(v, r) if op == "*" else div(v, r)
         return v
 

@@ -13,7 +13,7 @@ def fix_args_q(l=6, rc=3.9, cap=18, sigma=0.01, h=0.005, biasf=10.0, pace=10, wt
 
 
 def fix_args_local(rc=3.9, sw="STEP", sigma=0.01, h=0.005, biasf=9.0, temp=300.0, pace=10, wt=1, nbins=200,
-                   alpha=-8.0, mode="MEAN_SOLID", cvsw=None):
+                   alpha=-8.0, mode="MEAN_SOLID", cvsw=None, lo=0.0, hi=1.0):
     args = ["GAUSSIAN", sigma, h, biasf, "PACE", pace, "TEMP", temp]
     if sw == "STEP":
         args += ["CAL", "NAME", "SWR", "SW_FUNC", "STEP", "r_0", rc]
@@ -26,7 +26,7 @@ def fix_args_local(rc=3.9, sw="STEP", sigma=0.01, h=0.005, biasf=9.0, temp=300.0
                  "SW_FUNC_r", "SWR"]
     suffix = ".SWC" if cvsw is not None else ""
     args += ["SYMBOL", "v1", "Q4.%s%s" % (mode, suffix), "SYMBOL", "v2", "Q6.%s%s" % (mode, suffix),
-             "CV_dim", 2, "DIM", 1, 0, 1, nbins, "v1", "DIM", 2, 0, 1, nbins, "v2", "WT", wt]
+             "CV_dim", 2, "DIM", 1, lo, hi, nbins, "v1", "DIM", 2, lo, hi, nbins, "v2", "WT", wt]
     return args
 
 

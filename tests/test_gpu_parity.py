@@ -67,14 +67,16 @@ def test_local_ql_q4_q6_step(precision):
 def test_local_ql_smooth_switches(mode):
     x, L = systems.small_slab(nxy=6, nz_fcc=3, nz_bcc=4, n_liq=300)
     x = systems.jitter(x, 0.05, 5)
-    args = H.fix_args_local(sw="FERMI", alpha=-8.0, mode=mode, cvsw=(0.35, 20.0), nbins=100)
+    # NSOLID counts atoms: its grid spans [0, N] with a hill width of a few atoms
+    hi, sigma = (800.0, 8.0) if mode == "NSOLID" else (1.0, 0.01)
+    args = H.fix_args_local(sw="FERMI", alpha=-8.0, mode=mode, cvsw=(0.35, 20.0), nbins=100, hi=hi, sigma=sigma)
     m, out = H.run_gpu(args, x, L, [(0, x)], precision="fp64")
     swr = O.make_sw("FERMI", r0=3.9, alpha=-8.0)
     rl = O.sw_invert_for_eps(swr, 1e-6)
     swc = O.make_sw("FERMI", r0=0.35, alpha=20.0)
     o4 = O.steinh_l(4, x, L, rl, swr, 1e-6, swc, mode)
     o6 = O.steinh_l(6, x, L, rl, swr, 1e-6, swc, mode)
-    g = O.Grid([[0, 1], [0, 1]], [100, 100], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    g = O.Grid([[0, hi], [0, hi]], [100, 100], sigma, 0.005, 9.0, 300.0, 8.617343e-5, True)
     s = [o4["cv"], o6["cv"]]
     g.add_hill(s)
     V, dV = g.value(s)
