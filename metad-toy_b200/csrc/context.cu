@@ -331,7 +331,8 @@ mtd_status ensure_cells(mtd_ctx *c, int ncell) {
         dfree(c->start);
         const int cap = ncell + 1 + ncell / 4;
         MTD_CU(dalloc(&c->count, sizeof(int) * (size_t)cap), "cell counts");
-        MTD_CU(dalloc(&c->start, sizeof(int) * (size_t)(cap + 1)), "cell starts");
+        // ncell + 1 starts followed by the scan's per-1024-cell block totals
+        MTD_CU(dalloc(&c->start, sizeof(int) * (size_t)(cap + 1 + cap / 1024 + 2)), "cell starts");
         c->cap_cell = cap;
     }
     return MTD_OK;

@@ -46,41 +46,63 @@ __global__ void k_bin(CellGrid g, SysDev s) {
     s.slot[i] = atomicAdd(&s.count[cell], 1);
 }
 
-// Exclusive scan of the cell histogram in one block (ncell up to a few million).
-__global__ void k_scan(const int *__restrict__ count, int *__restrict__ start, int ncell) {
+// Exclusive block scan of one value per thread (blockDim.x == kScanBlock).
+constexpr int kScanBlock = 1024;
+__device__ __forceinline__ int block_excl_scan(int v, int &total) {
     __shared__ int warp_tot[32];
-    __shared__ int carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) carry = 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
     __syncthreads();
-    for (int base = 0; base < ncell; base += blockDim.x) {
-        int i = base + tid;
-        int v = (i < ncell) ? count[i] : 0;
-        int x = v;
+    if (warp == 0) {
+        int t = warp_tot[lane];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
         }
-        if (lane == 31) warp_tot[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            int t = (lane < (blockDim.x >> 5)) ? warp_tot[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, t, o);
-                if (lane >= o) t += y;
-            }
-            warp_tot[lane] = t;
-        }
-        __syncthreads();
-        int excl = carry + (warp > 0 ? warp_tot[warp - 1] : 0) + x - v;
-        if (i < ncell) start[i] = excl;
-        __syncthreads();
-        if (tid == blockDim.x - 1) carry = excl + v;
-        __syncthreads();
+        warp_tot[lane] = t;
     }
-    if (tid == 0) start[ncell] = carry;
+    __syncthreads();
+    total = warp_tot[31];
+    const int excl = (warp > 0 ? warp_tot[warp - 1] : 0) + x - v;
+    __syncthreads();
+    return excl;
+}
+
+// Three-pass exclusive scan of the cell histogram: per-block scan, scan of the
+// block totals, add-back.  The totals live in start[ncell + 1 ...].
+__global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int *__restrict__ count, int *__restrict__ start,
+                                                            int *__restrict__ bsum, int ncell) {
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    int total;
+    const int e = block_excl_scan(i < ncell ? count[i] : 0, total);
+    if (i < ncell) start[i] = e;
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_top(int *__restrict__ bsum, int nb, int *__restrict__ start,
+                                                         int ncell) {
+    int carry = 0;
+    for (int base = 0; base < nb; base += kScanBlock) {
+        const int i = base + threadIdx.x;
+        int total;
+        const int e = block_excl_scan(i < nb ? bsum[i] : 0, total);
+        if (i < nb) bsum[i] = carry + e;
+        carry += total;
+    }
+    if (threadIdx.x == 0) start[ncell] = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_add(int *__restrict__ start, const int *__restrict__ bsum,
+                                                         int ncell) {
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    if (i < ncell) start[i] += bsum[blockIdx.x];
 }
 
 __global__ void k_scatter(SysDev s) {
@@ -245,7 +267,13 @@ void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
     const int nb = (s.n + kBlock - 1) / kBlock;
     if (s.n > 0) k_bin<<<nb, kBlock, 0, st>>>(g, s);
     prof_mark("cell_bin", st);
-    k_scan<<<1, 1024, 0, st>>>(s.count, s.start, g.ncell);
+    {
+        const int sb = (g.ncell + kScanBlock - 1) / kScanBlock;
+        int *bsum = s.start + g.ncell + 1;   // scratch after the ncell + 1 starts
+        k_scan_blocks<<<sb, kScanBlock, 0, st>>>(s.count, s.start, bsum, g.ncell);
+        k_scan_top<<<1, kScanBlock, 0, st>>>(bsum, sb, s.start, g.ncell);
+        k_scan_add<<<sb, kScanBlock, 0, st>>>(s.start, bsum, g.ncell);
+    }
     prof_mark("cell_scan", st);
     if (s.n > 0) k_scatter<<<nb, kBlock, 0, st>>>(s);
     prof_mark("cell_scatter", st);
