@@ -35,7 +35,7 @@ struct Env {
     double eps = 0;
     int M = 0;
     int cap_n = 0;
-    void *pairs = nullptr;
+    int *list = nullptr;
     int *count = nullptr;
     double *key_r2 = nullptr;
     int *key_id = nullptr;
@@ -95,7 +95,7 @@ struct mtd_ctx {
     int n = 0, npad = 0, cap_n = 0, n_plan = -1;
     double *d_x = nullptr, *d_fin = nullptr, *d_fout = nullptr;
     int *d_mask = nullptr, *d_image = nullptr;
-    int *cellof = nullptr, *slot = nullptr, *perm = nullptr, *scell = nullptr, *smask = nullptr;
+    int *cellof = nullptr, *slot = nullptr, *perm = nullptr, *smask = nullptr;
     double *xs = nullptr;
     float4 *pf = nullptr;
     int *count = nullptr, *start = nullptr;
@@ -174,7 +174,6 @@ mtd_status cuda_check(mtd_ctx *c, cudaError_t e, const char *what) {
     } while (0)
 
 size_t real_size(const mtd_ctx *c) { return c->fp64 ? sizeof(double) : sizeof(float); }
-size_t pair_size(const mtd_ctx *c) { return c->fp64 ? sizeof(Pair<double>) : sizeof(Pair<float>); }
 
 int record_stride(const Unit &u) {
     if (u.kind == CAL_STEINH_L) return pad4(2 * (u.LA + 1) + (u.LB ? 2 * (u.LB + 1) : 0));
@@ -201,8 +200,11 @@ CellGrid make_grid(const mtd_ctx *c) {
         g.nc[d] = nc;
         g.periodic[d] = c->periodic[d];
         g.L[d] = L;
+        g.invL[d] = 1.0 / L;
         g.lo[d] = c->lo[d];
+        g.h[d] = L / nc;
         g.inv_h[d] = nc / L;
+        g.hf[d] = (float)(L / nc);
         g.Lf[d] = (float)L;
         g.invLf[d] = 1.0f / (float)L;
         ncell *= nc;
@@ -211,11 +213,28 @@ CellGrid make_grid(const mtd_ctx *c) {
     return g;
 }
 
-float prefilter(const mtd_ctx *c, double rc) {
-    double Lmax = 0.0;
-    for (int d = 0; d < 3; ++d) Lmax = std::fmax(Lmax, c->hi[d] - c->lo[d]);
-    const double r = rc + 1e-6 * Lmax + 1e-6;
-    return (float)(r * r);
+// Neighbour criterion of an environment; the FP32 band [lo2, hi2] around the
+// bound (2e-5 relative + 1e-4 A^2) is wide against the ~1e-6 A error of the
+// cell-relative FP32 displacements, so outside it FP32 decides exactly.
+NeighSpec neigh_spec(const Env &e) {
+    NeighSpec ns{};
+    ns.rc2 = e.rc * e.rc;
+    ns.eps = e.eps;
+    ns.sw = e.sw;
+    ns.cap = e.kind == ENV_Q ? e.cap : 0;
+    double eff = ns.rc2;
+    if (e.kind == ENV_L && e.sw.type == SW_STEP) {
+        ns.kind = NK_STEP;
+        ns.r0 = e.sw.r0;
+        eff = std::fmin(eff, e.sw.r0 * e.sw.r0);
+    } else if (e.kind == ENV_L) {
+        ns.kind = NK_SWITCH;
+    } else {
+        ns.kind = NK_RANGE;
+    }
+    ns.lo2 = (float)(eff * (1.0 - 2e-5) - 1e-4);
+    ns.hi2 = (float)(ns.kind == NK_SWITCH ? ns.rc2 * (1.0 + 2e-5) + 1e-4 : eff * (1.0 + 2e-5) + 1e-4);
+    return ns;
 }
 
 int estimate_M(const mtd_ctx *c, double rc, int n) {
@@ -229,12 +248,12 @@ int estimate_M(const mtd_ctx *c, double rc, int n) {
 }
 
 mtd_status alloc_env(mtd_ctx *c, Env &e, int npad) {
-    dfree(e.pairs);
+    dfree(e.list);
     dfree(e.count);
     dfree(e.key_r2);
     dfree(e.key_id);
     dfree(e.nkept);
-    MTD_CU(dalloc(&e.pairs, pair_size(c) * (size_t)e.M * npad), "neighbour list");
+    MTD_CU(dalloc(&e.list, sizeof(int) * (size_t)e.M * npad), "neighbour list");
     MTD_CU(dalloc(&e.count, sizeof(int) * (size_t)npad), "neighbour counts");
     if (e.kind == ENV_Q) {
         MTD_CU(dalloc(&e.key_r2, sizeof(double) * (size_t)npad), "cap keys");
@@ -293,7 +312,7 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
     if (npad > c->cap_n) {
         const int cap = npad + npad / 4;
         dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
-        dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->scell); dfree(c->smask);
+        dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask);
         dfree(c->xs); dfree(c->pf); dfree(c->d_vpart);
         MTD_CU(dalloc(&c->d_x, sizeof(double) * 3 * (size_t)cap), "x");
         MTD_CU(dalloc(&c->d_fin, sizeof(double) * 3 * (size_t)cap), "f");
@@ -303,7 +322,6 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
         MTD_CU(dalloc(&c->cellof, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->slot, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->perm, sizeof(int) * (size_t)cap), "perm");
-        MTD_CU(dalloc(&c->scell, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->smask, sizeof(int) * (size_t)cap), "mask");
         MTD_CU(dalloc(&c->xs, sizeof(double) * 3 * (size_t)cap), "x sorted");
         MTD_CU(dalloc(&c->pf, sizeof(float4) * (size_t)cap), "x float");
@@ -537,9 +555,9 @@ mtd_status plan_units(mtd_ctx *c) {
     return MTD_OK;
 }
 
-template <typename T> NeighDev<T> env_dev(const Env &e) {
-    NeighDev<T> nd;
-    nd.pairs = (Pair<T> *)e.pairs;
+NeighDev env_dev(const Env &e) {
+    NeighDev nd;
+    nd.list = e.list;
     nd.count = e.count;
     nd.key_r2 = e.key_r2;
     nd.key_id = e.key_id;
@@ -560,11 +578,47 @@ SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
     s.count = c->count;
     s.start = c->start;
     s.perm = c->perm;
-    s.scell = c->scell;
     s.smask = c->smask;
     s.xs = c->xs;
     s.pf = c->pf;
     return s;
+}
+
+template <typename T> LocalDev<T> local_dev(mtd_ctx *c, Unit &u, const CellGrid &g) {
+    LocalDev<T> d{};
+    d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.LA = u.LA; d.LB = u.LB;
+    d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
+    d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
+    d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
+    d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
+    return d;
+}
+
+template <typename T> GlobalDev<T> global_dev(mtd_ctx *c, Unit &u, const CellGrid &g) {
+    GlobalDev<T> d{};
+    d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.L = u.LA; d.groupbit = u.groupbit;
+    d.nsw = (int)u.qsw.size();
+    for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
+    d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.exact = geo_d(g, c->xs);
+    d.nb = env_dev(c->envs[u.env]);
+    d.q = (T *)u.q; d.Q = (T *)u.Q; d.partials = u.partials; d.coef = u.coef;
+    return d;
+}
+
+template <typename T> DebyeDev<T> debye_dev(mtd_ctx *c, Unit &u, const CellGrid &g) {
+    DebyeDev<T> d{};
+    d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
+    d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
+    d.S = (T *)u.S; d.partials = u.partials; d.coef = u.coef;
+    return d;
+}
+
+SkDev sk_dev(mtd_ctx *c, Unit &u, const double *x, const int *mask) {
+    SkDev d{};
+    d.n = c->n; d.K = u.K; d.groupbit = u.groupbit; d.x = x; d.mask = mask; d.k = u.kvec;
+    d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
+    d.fp64 = c->fp64;
+    return d;
 }
 
 template <typename T>
@@ -574,80 +628,40 @@ void run_units(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, 
     // CV values
     for (Unit &u : c->units) {
         if (u.kind == CAL_STEINH_L) {
-            LocalDev<T> d{};
-            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.LA = u.LA; d.LB = u.LB;
-            d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
-            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]);
-            d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
-            d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
-            launch_local_values<T>(d, st);
+            launch_local_values<T>(local_dev<T>(c, u, g), st);
             c->launches += 2;
         } else if (u.kind == CAL_STEINH_Q) {
-            GlobalDev<T> d{};
-            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.L = u.LA; d.groupbit = u.groupbit;
-            d.nsw = (int)u.qsw.size();
-            for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
-            d.smask = c->smask; d.perm = c->perm; d.xs = c->xs; d.grid = g; d.nb = env_dev<T>(c->envs[u.env]);
-            d.q = (T *)u.q; d.Q = (T *)u.Q; d.partials = u.partials; d.coef = u.coef;
-            launch_global_values<T>(d, st);
+            launch_global_values<T>(global_dev<T>(c, u, g), st);
             c->launches += 1;
         } else if (u.kind == CAL_STRU_FACTOR) {
-            DebyeDev<T> d{};
-            d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
-            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]); d.S = (T *)u.S;
-            d.partials = u.partials; d.coef = u.coef;
-            launch_debye_values<T>(d, st);
+            launch_debye_values<T>(debye_dev<T>(c, u, g), st);
             c->launches += 1;
         } else {
-            SkDev d{};
-            d.n = c->n; d.K = u.K; d.groupbit = u.groupbit; d.x = x; d.mask = mask; d.k = u.kvec;
-            d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
-            d.fp64 = c->fp64;
-            launch_sk_values(d, st);
+            launch_sk_values(sk_dev(c, u, x, mask), st);
             c->launches += 2;
         }
     }
     launch_bias_step(c->d_plan, step, 0, st);
     c->launches += 1;
-    // forces
+    // forces: the first unit reads f_in, the later ones accumulate into f_out
     bool first = true;
     int voff = 0;
     for (Unit &u : c->units) {
         if (!u.used) continue;
         const double *src = first ? fin : fout;
         double *vp = virial ? c->d_vpart + (size_t)voff * 8 : nullptr;
-        int nb = (c->n + kBlock - 1) / kBlock;
+        const int nb = (c->n + kBlock - 1) / kBlock;
         if (u.kind == CAL_STEINH_L) {
-            LocalDev<T> d{};
-            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.LA = u.LA; d.LB = u.LB;
-            d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
-            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]);
-            d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
-            d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
-            launch_local_forces<T>(d, src, fout, s, g, vp, c->d_status, st);
+            launch_local_forces<T>(local_dev<T>(c, u, g), src, fout, s, g, vp, c->d_status, st);
             c->launches += 2;
         } else if (u.kind == CAL_STEINH_Q) {
-            GlobalDev<T> d{};
-            d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.L = u.LA; d.groupbit = u.groupbit;
-            d.nsw = (int)u.qsw.size();
-            for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
-            d.smask = c->smask; d.perm = c->perm; d.xs = c->xs; d.grid = g; d.nb = env_dev<T>(c->envs[u.env]);
-            d.q = (T *)u.q; d.Q = (T *)u.Q; d.partials = u.partials; d.coef = u.coef;
-            launch_global_forces<T>(d, src, fout, s, g, vp, c->d_status, st);
+            launch_global_forces<T>(global_dev<T>(c, u, g), src, fout, s, g, vp, c->d_status, st);
             c->launches += 1;
         } else if (u.kind == CAL_STRU_FACTOR) {
-            DebyeDev<T> d{};
-            d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
-            d.smask = c->smask; d.perm = c->perm; d.nb = env_dev<T>(c->envs[u.env]); d.S = (T *)u.S;
-            d.partials = u.partials; d.coef = u.coef;
-            launch_debye_forces<T>(d, src, fout, s, g, vp, c->d_status, st);
+            launch_debye_forces<T>(debye_dev<T>(c, u, g), src, fout, s, g, vp, c->d_status, st);
             c->launches += 1;
         } else {
-            SkDev d{};
-            d.n = c->n; d.K = u.K; d.groupbit = u.groupbit; d.x = x; d.mask = mask; d.k = u.kvec;
-            d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
-            d.fp64 = c->fp64;
-            launch_sk_forces(d, src, fout, s, g, vp, st);
+            launch_sk_forces(sk_dev(c, u, x, mask), src, fout, s, g, vp, st);
             c->launches += 1;
         }
         voff += nb;
@@ -709,17 +723,10 @@ mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, cons
         s.count = c->count;
         s.start = c->start;
         launch_build_cells(g, s, c->st);
-        c->launches += 4;
+        c->launches += 6;
         for (Env &e : c->envs) {
-            NeighSpec ns{};
-            ns.kind = e.kind == ENV_L ? NK_SWITCH : NK_RANGE;
-            ns.rc2 = e.rc * e.rc;
-            ns.rcf2 = prefilter(c, e.rc);
-            ns.eps = e.eps;
-            ns.sw = e.sw;
-            ns.cap = e.kind == ENV_Q ? e.cap : 0;
-            if (c->fp64) launch_neighbors<double>(g, s, ns, env_dev<double>(e), c->d_status, c->st);
-            else launch_neighbors<float>(g, s, ns, env_dev<float>(e), c->d_status, c->st);
+            const NeighSpec ns = neigh_spec(e);
+            launch_neighbors(g, s, ns, env_dev(e), c->d_status, c->st);
             c->launches += ns.cap > 0 ? 2 : 1;
         }
     }
@@ -951,7 +958,7 @@ void mtd_destroy(mtd_ctx *c) {
     if (!c) return;
     if (c->st) cudaStreamSynchronize(c->st);
     for (Env &e : c->envs) {
-        dfree(e.pairs); dfree(e.count); dfree(e.key_r2); dfree(e.key_id); dfree(e.nkept);
+        dfree(e.list); dfree(e.count); dfree(e.key_r2); dfree(e.key_id); dfree(e.nkept);
     }
     for (Unit &u : c->units) {
         void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S};
@@ -959,7 +966,7 @@ void mtd_destroy(mtd_ctx *c) {
         dfree(u.partials); dfree(u.coef); dfree(u.kvec); dfree(u.rho); dfree(u.skn);
     }
     dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
-    dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->scell); dfree(c->smask);
+    dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask);
     dfree(c->xs); dfree(c->pf); dfree(c->count); dfree(c->start); dfree(c->d_vpart);
     dfree(c->d_plan); dfree(c->d_grid); dfree(c->d_hills); dfree(c->d_nhills); dfree(c->d_out);
     dfree(c->d_status); dfree(c->d_vir);

@@ -35,24 +35,25 @@ template <int L, typename T> __global__ void __launch_bounds__(kBlock) k_global_
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double part[4] = {0, 0, 0, 0};
     if (k < d.n) {
+        const auto a = d.geo.load(k);
         const int c = min(d.nb.count[k], d.nb.M);
         T acc[Z::SQ];
 #pragma unroll
         for (int t = 0; t < Z::SQ; ++t) acc[t] = T(0);
         int kept = 0;
         for (int t = 0; t < c; ++t) {
-            const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
-            if (!((pr.j >> kFlagBit) & 1)) continue;
-            const T r2 = pr.x * pr.x + pr.y * pr.y + pr.z * pr.z;
-            const T rinv = t_rsqrt<T>(r2);
-            ylm_accum<L, T>(pr.x * rinv, pr.y * rinv, pr.z * rinv, T(1), acc);
+            const int e = d.nb.list[(size_t)t * d.npad + k];
+            if (!((e >> kFlagBit) & 1)) continue;
+            T dx, dy, dz;
+            d.geo.disp(a, d.geo.load(e & ((1 << kFlagBit) - 1)), dx, dy, dz);
+            const T rinv = t_rsqrt<T>(dx * dx + dy * dy + dz * dz);
+            ylm_accum<L, T>(dx * rinv, dy * rinv, dz * rinv, T(1), acc);
             ++kept;
         }
         const T inv = kept > 0 ? T(1) / T(kept) : T(0);
-        T q2 = T(0);
 #pragma unroll
         for (int t = 0; t < Z::SQ; ++t) acc[t] *= inv;
-        q2 = acc[0] * acc[0];
+        T q2 = acc[0] * acc[0];
 #pragma unroll
         for (int m = 1; m <= L; ++m) q2 += T(2) * (acc[2 * m] * acc[2 * m] + acc[2 * m + 1] * acc[2 * m + 1]);
         const T Q = kept > 0 ? t_sqrt<T>(q2 * T(4.0 * kPi / (2 * L + 1))) : T(0);
@@ -83,20 +84,6 @@ __device__ __forceinline__ T lambda_scale(const GlobalDev<T> &d, int k, const do
     return (T)(dcv * (4.0 * kPi / (2 * L + 1)) / (Q * n));
 }
 
-__device__ __forceinline__ double exact_r2(const CellGrid &g, const double *xi, const double *xj) {
-    double d[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        double t = __dsub_rn(xj[c], xi[c]);
-        if (g.periodic[c]) {
-            double k = rint(__ddiv_rn(t, g.L[c]));
-            t = __dsub_rn(t, __dmul_rn(g.L[c], k));
-        }
-        d[c] = t;
-    }
-    return __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2]));
-}
-
 template <int L, typename T>
 __global__ void __launch_bounds__(kBlock) k_global_force(GlobalDev<T> d, const double *__restrict__ f_src,
                                                          double *__restrict__ f_dst, SysDev s, CellGrid g,
@@ -112,19 +99,21 @@ __global__ void __launch_bounds__(kBlock) k_global_force(GlobalDev<T> d, const d
 #pragma unroll
         for (int t = 0; t < Z::SQ; ++t) la[t] = ak * d.q[(size_t)k * Z::SQ + t] * (t >= 2 ? T(2) : T(1));
         const int myid = d.perm[k];
-        const double xk[3] = {d.xs[3 * k], d.xs[3 * k + 1], d.xs[3 * k + 2]};
+        const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
+        const auto a = d.geo.load(k);
         constexpr T sgn = (L & 1) ? T(-1) : T(1);
         T gx = T(0), gy = T(0), gz = T(0);
         const int cnt = min(d.nb.count[k], d.nb.M);
         for (int t = 0; t < cnt; ++t) {
-            const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
-            const bool kept = (pr.j >> kFlagBit) & 1;
-            const int j = pr.j & ((1 << kFlagBit) - 1);
+            const int e = d.nb.list[(size_t)t * d.npad + k];
+            const bool kept = (e >> kFlagBit) & 1;
+            const int j = e & ((1 << kFlagBit) - 1);
             bool rev = true;
             const double kr2 = d.nb.key_r2[j];
             if (kr2 != CUDART_INF) {
-                const double xj[3] = {d.xs[3 * j], d.xs[3 * j + 1], d.xs[3 * j + 2]};
-                const double r2 = exact_r2(d.grid, xj, xk);
+                const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
+                double dd[3];
+                const double r2 = exact_disp(d.exact, xj, xk, dd);
                 rev = (r2 < kr2) || (r2 == kr2 && myid <= d.nb.key_id[j]);
             }
             const T aj = rev ? lambda_scale<L, T>(d, j, c) : T(0);
@@ -135,10 +124,11 @@ __global__ void __launch_bounds__(kBlock) k_global_force(GlobalDev<T> d, const d
                 const T w = q >= 2 ? T(2) : T(1);
                 Lm[q] = (kept ? la[q] : T(0)) + sgn * aj * w * d.q[(size_t)j * Z::SQ + q];
             }
-            const T r2 = pr.x * pr.x + pr.y * pr.y + pr.z * pr.z;
-            const T rinv = t_rsqrt<T>(r2);
+            T dx, dy, dz;
+            d.geo.disp(a, d.geo.load(j), dx, dy, dz);
+            const T rinv = t_rsqrt<T>(dx * dx + dy * dy + dz * dz);
             T ax, ay, az;
-            ylm_dot_grad<L, T>(pr.x * rinv, pr.y * rinv, pr.z * rinv, rinv, Lm, ax, ay, az);
+            ylm_dot_grad<L, T>(dx * rinv, dy * rinv, dz * rinv, rinv, Lm, ax, ay, az);
             gx -= ax;
             gy -= ay;
             gz -= az;

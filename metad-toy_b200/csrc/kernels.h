@@ -2,11 +2,14 @@
 //
 // Layout in HBM (n atoms, npad = n rounded up to the block size):
 //   caller order : x_in, f_in, f_out (FP64 AoS n*3), mask, image (int n)
-//   sorted order : atoms counting-sorted by cell; perm[k] = caller index of
-//                  sorted atom k; xs (FP64 AoS raw coordinates), pf (FP32
-//                  wrapped position, float4), smask, scell
-//   pair lists   : ELL, slot-major Pair<T>[M][npad] so a warp reads 32
-//                  consecutive records per slot; count[npad]
+//   sorted order : atoms counting-sorted by cell (z fastest); perm[k] = caller
+//                  index of sorted atom k; xs (FP64 AoS raw coordinates for
+//                  exact decisions), pf (float4: FP32 offset from the cell's
+//                  lower corner + packed cell coordinates), smask
+//   neighbours   : ELL index lists, slot-major int[M][npad] (a warp reads 32
+//                  consecutive entries per slot); count[npad]; displacements
+//                  are recomputed from pf in every pass (4 B per pair instead
+//                  of a 16 B record keeps the step's working set near L2 size)
 //   per-atom CV  : AoS records of SQ reals (q_lm, LQ_lm, lambda ...) so one
 //                  neighbour gather touches one or two 128-byte lines
 #pragma once
@@ -15,6 +18,7 @@
 
 #include "common.cuh"
 #include "expr.h"
+#include "geo.cuh"
 
 namespace mtd {
 
@@ -22,37 +26,76 @@ struct CellGrid {
     int nc[3];
     int ncell;
     int periodic[3];
-    double L[3], lo[3], inv_h[3];
-    float Lf[3], invLf[3];
+    double L[3], invL[3], lo[3], h[3], inv_h[3];
+    float hf[3], Lf[3], invLf[3];
 };
+
+__host__ __device__ inline GeoF geo_f(const CellGrid &g, const float4 *pf) {
+    GeoF r;
+    r.pf = pf;
+    for (int c = 0; c < 3; ++c) {
+        r.hf[c] = g.hf[c];
+        r.Lf[c] = g.Lf[c];
+        r.invLf[c] = g.invLf[c];
+        r.nc[c] = g.nc[c];
+        r.periodic[c] = g.periodic[c];
+    }
+    return r;
+}
+__host__ __device__ inline GeoD geo_d(const CellGrid &g, const double *xs) {
+    GeoD r;
+    r.xs = xs;
+    for (int c = 0; c < 3; ++c) {
+        r.L[c] = g.L[c];
+        r.invL[c] = g.invL[c];
+        r.periodic[c] = g.periodic[c];
+    }
+    return r;
+}
+template <typename T> Geo<T> make_geo(const CellGrid &g, const float4 *pf, const double *xs);
+template <> inline Geo<float> make_geo<float>(const CellGrid &g, const float4 *pf, const double *) {
+    Geo<float> r;
+    r.g = geo_f(g, pf);
+    return r;
+}
+template <> inline Geo<double> make_geo<double>(const CellGrid &g, const float4 *, const double *xs) {
+    Geo<double> r;
+    r.g = geo_d(g, xs);
+    return r;
+}
 
 struct SysDev {
     int n, npad;
     const double *x;      // caller order, AoS n*3
     const int *mask;      // caller order, may be null (all groups)
     const int *image;     // caller order, may be null
-    int *cellof, *slot, *count, *start, *perm, *scell, *smask;
+    int *cellof, *slot, *count, *start, *perm, *smask;
     double *xs;           // sorted raw coordinates AoS npad*3
-    float4 *pf;           // sorted wrapped coordinates
+    float4 *pf;           // sorted cell-relative coordinates + packed cell
 };
 
 // Neighbour criteria (the reference's per-CV filters).
 enum NeighKind {
-    NK_RANGE = 0,   // 1e-12 <= r2 <= rc2           (STEINH Q :1358, STRU_FACTOR :1048)
-    NK_SWITCH = 1   // r2 <= rc2 and sw(r) >= eps    (STEINH L, Local.cu:1257-1262)
+    NK_RANGE = 0,    // 1e-12 <= r2 <= rc2           (STEINH Q :1358, STRU_FACTOR :1048)
+    NK_STEP = 1,     // r2 <= rc2 and r < r0         (STEINH L with a STEP switch)
+    NK_SWITCH = 2    // r2 <= rc2 and sw(r) >= eps   (STEINH L, Local.cu:1257-1262)
 };
 
+// The FP32 distance decides a candidate when it is outside [lo2, hi2]; inside
+// the band (|r^2 - bound| ~ 1e-5 relative) the FP64 test on raw coordinates
+// decides, so the neighbour sets equal the FP64 criterion exactly.
 struct NeighSpec {
     int kind;
-    double rc2;         // exact FP64 bound
-    float rcf2;         // FP32 prefilter bound (rc + guard)^2
+    double rc2;         // exact FP64 list bound
+    double r0;          // STEP threshold (r < r0)
     double eps;
     SwParams sw;
+    float lo2, hi2;     // FP32 accept-below / reject-above
     int cap;            // STEINH Q cutoff_Natoms, 0 = none
 };
 
-template <typename T> struct NeighDev {
-    Pair<T> *pairs;     // [M][npad]
+struct NeighDev {
+    int *list;          // [M][npad] sorted neighbour indices (bit kFlagBit: kept by the centre's cap)
     int *count;         // [npad] neighbours found (may exceed M: overflow)
     double *key_r2;     // STEINH Q: r2 of the last kept neighbour (inf when cap not binding)
     int *key_id;        // STEINH Q: caller index of the last kept neighbour
@@ -75,8 +118,7 @@ void prof_mark(const char *name, cudaStream_t st);
 
 // ------------------------------------------------------------------ neighbours
 void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st);
-template <typename T>
-void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev<T> nd, DevStatus *status,
+void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, DevStatus *status,
                       cudaStream_t st);
 
 // ------------------------------------------------------------------ STEINH L
@@ -87,7 +129,8 @@ template <typename T> struct LocalDev {
     SwParams sw_r, sw_cvA, sw_cvB;
     const int *smask;
     const int *perm;
-    NeighDev<T> nb;
+    Geo<T> geo;
+    NeighDev nb;
     T *q, *nf, *lq, *lqs, *e12, *lam, *g, *tu;
     double *partials;           // [nblocks][8]: S1A S0A S1B S0B N
     const double *coef;         // c1A c2A c1B c2B (written by the bias kernel)
@@ -103,9 +146,9 @@ template <typename T> struct GlobalDev {
     int groupbit, nsw;
     SwParams sw[2];             // SW_FUNC symbols of this CAL
     const int *smask, *perm;
-    const double *xs;
-    CellGrid grid;
-    NeighDev<T> nb;
+    Geo<T> geo;
+    GeoD exact;                 // FP64 raw coordinates for the cap-membership test
+    NeighDev nb;
     T *q, *Q;
     double *partials;           // [nblocks][8]: sumQ, sum f1(Q), sum f2(Q), N
     const double *coef;         // c_ave, c_sw1, c_sw2
@@ -122,7 +165,8 @@ template <typename T> struct DebyeDev {
     double rc2, qf;
     SwParams sw;
     const int *smask, *perm;
-    NeighDev<T> nb;
+    Geo<T> geo;
+    NeighDev nb;
     T *S;
     double *partials;           // [nblocks][4]: sumS, sum f(S), N
     const double *coef;         // c_ave, c_count
@@ -196,13 +240,12 @@ struct BiasPlan {
     HillRec *hills;
     int hill_cap;
     unsigned long long *nhills;
-    double *out;           // [0..D) s, D: V, D+1: deposited flag, D+2.. D+2+nsym: symbol values
+    double *out;           // [0..D) s, D: V, D+1: deposited flag, kOutSymOffset..: symbol values
 };
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
 
 void launch_bias_step(const BiasPlan *d_plan, long long step, int nunit_threads, cudaStream_t st);
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st);
-void launch_scan_status(const double *f, int n, DevStatus *status, cudaStream_t st);
 
 }  // namespace mtd

@@ -17,7 +17,9 @@
 //   dCV/dx_a = - sum_j [ sigma grad_d Re(Lam . Y(d_aj))
 //                        + sigma' dhat (c_aj + c_ja + Re(Lam . Y) - t_a - t_j) ]
 // where c_aj = Re G_a.(q_j - LQ_a), t_a = Re lam_a.q_a / NF_a.  Two orders
-// (Q4 and Q6 of one neighbour environment) are fused in one pass.
+// (Q4 and Q6 of one neighbour environment) are fused in one pass.  With a STEP
+// switch sigma = 1 and sigma' = 0 on every listed pair, so the LQ and lambda
+// passes need neighbour indices only.
 #include "kernels.h"
 #include "ylm.cuh"
 
@@ -70,39 +72,54 @@ template <int L, typename T> __device__ __forceinline__ T qnorm2(const T *v) {
     return s;
 }
 
-template <typename T>
-__device__ __forceinline__ void pair_geom(const Pair<T> &pr, const SwParams &sw, bool step, T &ux, T &uy, T &uz, T &rinv,
-                                          T &sg, T &dsg) {
-    const T r2 = pr.x * pr.x + pr.y * pr.y + pr.z * pr.z;
+// Unit bond vector, 1/r, sigma and sigma' of a listed pair.
+template <typename T, bool STEP>
+__device__ __forceinline__ void pair_geom(const LocalDev<T> &d, const typename Geo<T>::Pos &a, int j, T &ux, T &uy,
+                                          T &uz, T &rinv, T &sg, T &dsg) {
+    T dx, dy, dz;
+    d.geo.disp(a, d.geo.load(j), dx, dy, dz);
+    const T r2 = dx * dx + dy * dy + dz * dz;
     rinv = t_rsqrt<T>(r2);
-    const T r = r2 * rinv;
-    ux = pr.x * rinv;
-    uy = pr.y * rinv;
-    uz = pr.z * rinv;
-    if (step) {   // listed pairs of a STEP switch have sigma = 1 by construction
+    ux = dx * rinv;
+    uy = dy * rinv;
+    uz = dz * rinv;
+    if (STEP) {   // listed pairs of a STEP switch have sigma = 1 by construction
         sg = T(1);
         dsg = T(0);
     } else {
-        sg = sw_f<T>(sw, r);
-        dsg = sw_df<T>(sw, r);
+        const T r = r2 * rinv;
+        sg = sw_f<T>(d.sw_r, r);
+        dsg = sw_df<T>(d.sw_r, r);
     }
 }
 
+template <typename T, bool STEP>
+__device__ __forceinline__ T pair_sigma(const LocalDev<T> &d, const typename Geo<T>::Pos &a, int j) {
+    if (STEP) return T(1);
+    T dx, dy, dz;
+    d.geo.disp(a, d.geo.load(j), dx, dy, dz);
+    return sw_f<T>(d.sw_r, t_sqrt<T>(dx * dx + dy * dy + dz * dz));
+}
+
+__device__ __forceinline__ int nb_index(const NeighDev &nb, int npad, int t, int k) {
+    return __ldg(nb.list + (size_t)t * npad + k) & ((1 << kFlagBit) - 1);
+}
+
 // Pass 1: q_lm and NF for every atom.
-template <int LA, int LB, typename T> __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
+template <int LA, int LB, typename T, bool STEP>
+__global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
     using S = LSet<LA, LB>;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
-    const bool step = d.sw_r.type == SW_STEP;
+    const auto a = d.geo.load(k);
     const int c = min(d.nb.count[k], d.nb.M);
     T acc[S::SQ];
 #pragma unroll
     for (int t = 0; t < S::SQ; ++t) acc[t] = T(0);
     T nf = T(0);
     for (int t = 0; t < c; ++t) {
-        const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
         T ux, uy, uz, rinv, sg, dsg;
-        pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
+        pair_geom<T, STEP>(d, a, nb_index(d.nb, d.npad, t, k), ux, uy, uz, rinv, sg, dsg);
         nf += sg;
         ylm_accum<LA, T>(ux, uy, uz, sg, acc);
         if constexpr (LB > 0) ylm_accum<LB, T>(ux, uy, uz, sg, acc + S::SA);
@@ -116,12 +133,12 @@ template <int LA, int LB, typename T> __global__ void __launch_bounds__(kBlock) 
 }
 
 // Pass 2: LQ_lm, LQ, the e1/e2 weights of the adjoint and block partial sums.
-template <int LA, int LB, typename T> __global__ void __launch_bounds__(kBlock) k_local_lq(LocalDev<T> d) {
+template <int LA, int LB, typename T, bool STEP>
+__global__ void __launch_bounds__(kBlock) k_local_lq(LocalDev<T> d) {
     using S = LSet<LA, LB>;
     __shared__ double smem[5 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = k < d.n;
-    const bool step = d.sw_r.type == SW_STEP;
     double part[5] = {0, 0, 0, 0, 0};
     if (valid) {
         const bool ing = (d.smask[k] & d.groupbit) != 0;
@@ -130,13 +147,13 @@ template <int LA, int LB, typename T> __global__ void __launch_bounds__(kBlock) 
         T lqA = T(0), lqB = T(0);
         if (ing && nfk > T(0)) {
             load_rec(d.q + (size_t)k * S::SQ, A);
+            const auto a = d.geo.load(k);
             const int c = min(d.nb.count[k], d.nb.M);
             for (int t = 0; t < c; ++t) {
-                const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
-                T ux, uy, uz, rinv, sg, dsg;
-                pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
+                const int j = nb_index(d.nb, d.npad, t, k);
+                const T sg = pair_sigma<T, STEP>(d, a, j);
                 T qj[S::SQ];
-                load_rec(d.q + (size_t)pr.j * S::SQ, qj);
+                load_rec(d.q + (size_t)j * S::SQ, qj);
 #pragma unroll
                 for (int s = 0; s < S::SQ; ++s) A[s] += sg * qj[s];
             }
@@ -201,9 +218,10 @@ __device__ __forceinline__ void add_g(T *acc, const T *lq, T w, T s) {
 }
 
 // Pass 3 (after the bias kernel): lam_k / NF_k, and for smooth switches G_k, t_k, u_k.
-template <int LA, int LB, typename T, bool DSIG>
+template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
     using S = LSet<LA, LB>;
+    constexpr bool DSIG = !STEP;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
     const T c1A = (T)d.coef[0], c2A = (T)d.coef[1], c1B = (T)d.coef[2], c2B = (T)d.coef[3];
@@ -220,14 +238,10 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
         }
         return;
     }
-    const bool step = d.sw_r.type == SW_STEP;
     T lqk[S::SQ];
     load_rec(d.lq + (size_t)k * S::SQ, lqk);
-    const float4 dummy = make_float4(0, 0, 0, 0);
-    (void)dummy;
-    T ek[4] = {d.e12[4 * k], d.e12[4 * k + 1], d.e12[4 * k + 2], d.e12[4 * k + 3]};
-    const T wA = c1A * ek[0] + c2A * ek[1];
-    const T wB = c1B * ek[2] + c2B * ek[3];
+    const T wA = c1A * d.e12[4 * k] + c2A * d.e12[4 * k + 1];
+    const T wB = c1B * d.e12[4 * k + 2] + c2B * d.e12[4 * k + 3];
     add_g<LA, T>(lam, lqk, wA, T(1));
     if constexpr (LB > 0) add_g<LB, T>(lam + S::SA, lqk + S::SA, wB, T(1));
     T Gk[S::SQ];
@@ -235,16 +249,16 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
 #pragma unroll
         for (int s = 0; s < S::SQ; ++s) Gk[s] = lam[s];
     }
+    const auto a = d.geo.load(k);
     const int c = min(d.nb.count[k], d.nb.M);
     for (int t = 0; t < c; ++t) {
-        const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
-        T ux, uy, uz, rinv, sg, dsg;
-        pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
-        const int j = pr.j;
-        const T ej0 = d.e12[4 * j], ej1 = d.e12[4 * j + 1], ej2 = d.e12[4 * j + 2], ej3 = d.e12[4 * j + 3];
-        const T wjA = c1A * ej0 + c2A * ej1;
-        const T wjB = c1B * ej2 + c2B * ej3;
+        const int j = nb_index(d.nb, d.npad, t, k);
+        T ej[4];
+        load_rec(d.e12 + 4 * (size_t)j, ej);
+        const T wjA = c1A * ej[0] + c2A * ej[1];
+        const T wjB = c1B * ej[2] + c2B * ej[3];
         if (wjA == T(0) && wjB == T(0)) continue;
+        const T sg = pair_sigma<T, STEP>(d, a, j);
         T lqj[S::SQ];
         load_rec(d.lq + (size_t)j * S::SQ, lqj);
         add_g<LA, T>(lam, lqj, wjA, sg);
@@ -271,17 +285,17 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
 }
 
 // Pass 4: gather forces, f_dst = f_src - dV/dx, plus the virial block partials.
-template <int LA, int LB, typename T, bool DSIG>
+template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
                                                         double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                         double *vpart, DevStatus *status) {
     using S = LSet<LA, LB>;
+    constexpr bool DSIG = !STEP;
     __shared__ double smem[6 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = k < d.n;
     double vir[6] = {0, 0, 0, 0, 0, 0};
     if (valid) {
-        const bool step = d.sw_r.type == SW_STEP;
         T la[S::SQ];
         load_rec(d.lam + (size_t)k * S::SQ, la);
         T qa[S::SQ], ga[S::SQ];
@@ -292,15 +306,15 @@ __global__ void __launch_bounds__(kBlock) k_local_force(LocalDev<T> d, const dou
 #pragma unroll
             for (int t = 0; t < 4; ++t) tua[t] = d.tu[4 * k + t];
         }
+        const auto a = d.geo.load(k);
         T gx = T(0), gy = T(0), gz = T(0);
         const int c = min(d.nb.count[k], d.nb.M);
         constexpr T sgnA = (LA & 1) ? T(-1) : T(1);
         constexpr T sgnB = (LB & 1) ? T(-1) : T(1);
         for (int t = 0; t < c; ++t) {
-            const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+            const int j = nb_index(d.nb, d.npad, t, k);
             T ux, uy, uz, rinv, sg, dsg;
-            pair_geom(pr, d.sw_r, step, ux, uy, uz, rinv, sg, dsg);
-            const int j = pr.j;
+            pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
             T lj[S::SQ];
             load_rec(d.lam + (size_t)j * S::SQ, lj);
             T Lm[S::SQ];
@@ -364,18 +378,24 @@ __global__ void __launch_bounds__(kBlock) k_local_force(LocalDev<T> d, const dou
 
 template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cudaStream_t st) {
     const int nb = (d.n + kBlock - 1) / kBlock;
-    k_local_q<LA, LB, T><<<nb, kBlock, 0, st>>>(d);
-    prof_mark("local_q", st);
-    k_local_lq<LA, LB, T><<<nb, kBlock, 0, st>>>(d);
-    prof_mark("local_lq", st);
+    if (d.sw_r.type == SW_STEP) {
+        k_local_q<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
+        prof_mark("local_q", st);
+        k_local_lq<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
+        prof_mark("local_lq", st);
+    } else {
+        k_local_q<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
+        prof_mark("local_q", st);
+        k_local_lq<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
+        prof_mark("local_lq", st);
+    }
 }
 
 template <int LA, int LB, typename T>
 void run_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                 double *vpart, DevStatus *status, cudaStream_t st) {
     const int nb = (d.n + kBlock - 1) / kBlock;
-    const bool dsig = !(d.sw_r.type == SW_STEP);
-    if (dsig) {
+    if (d.sw_r.type == SW_STEP) {
         k_local_lambda<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
         prof_mark("local_lambda", st);
         k_local_force<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);

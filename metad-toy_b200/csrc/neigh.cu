@@ -5,13 +5,13 @@
 // get_environment_Steinhardt_LocalQ (src/cvs/CVs_Steinhardt_Local.cu:1210-1285)
 // and get_environment_Strufactor (src/cvs/CVs_Strufactor.cu:1014-1080).
 //
-// Pipeline per step: bin atoms to cells (counting sort: histogram, one-block
-// scan, scatter, per-cell sort by caller index for a deterministic order), then
-// one thread per sorted atom scans the 27 neighbour cells.  A candidate passes
-// an FP32 prefilter on wrapped float positions with a guard band, then the
-// neighbour decision is taken in FP64 on the caller's raw coordinates with
-// the same operation order as the FP64 oracle (minimum image, no FMA), so the
-// neighbour sets are exact.
+// Per step: bin atoms to cells (counting sort: histogram, three-pass scan,
+// scatter, per-cell sort by caller index so the order is deterministic), then
+// one thread per sorted atom walks its 9 neighbour-cell columns (z-adjacent
+// cells are contiguous in the sorted order).  A candidate is decided by its
+// FP32 cell-relative distance unless it lies within ~1e-5 of the bound, where
+// the FP64 test on the caller's raw coordinates (the FP64 oracle's operation
+// order) decides -- the neighbour sets are exact.
 #include "kernels.h"
 
 #include <math_constants.h>
@@ -20,14 +20,13 @@ namespace mtd {
 
 namespace {
 
-__device__ __forceinline__ int wrap_cell(double v, const CellGrid &g, int c, float &wf) {
-    double w = v - g.lo[c];
+__device__ __forceinline__ int cell_coord(double v, const CellGrid &g, int c, double &w) {
+    w = v - g.lo[c];
     if (g.periodic[c]) {
-        w = w - g.L[c] * floor(w / g.L[c]);
+        w = w - g.L[c] * floor(w * g.invL[c]);
         if (w >= g.L[c]) w -= g.L[c];
         if (w < 0.0) w = 0.0;
     }
-    wf = (float)w;
     int k = (int)(w * g.inv_h[c]);
     if (k < 0) k = 0;
     if (k >= g.nc[c]) k = g.nc[c] - 1;
@@ -37,11 +36,11 @@ __device__ __forceinline__ int wrap_cell(double v, const CellGrid &g, int c, flo
 __global__ void k_bin(CellGrid g, SysDev s) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
-    float wf;
-    int cx = wrap_cell(s.x[3 * i + 0], g, 0, wf);
-    int cy = wrap_cell(s.x[3 * i + 1], g, 1, wf);
-    int cz = wrap_cell(s.x[3 * i + 2], g, 2, wf);
-    int cell = (cx * g.nc[1] + cy) * g.nc[2] + cz;
+    double w;
+    const int cx = cell_coord(s.x[3 * i + 0], g, 0, w);
+    const int cy = cell_coord(s.x[3 * i + 1], g, 1, w);
+    const int cz = cell_coord(s.x[3 * i + 2], g, 2, w);
+    const int cell = (cx * g.nc[1] + cy) * g.nc[2] + cz;
     s.cellof[i] = cell;
     s.slot[i] = atomicAdd(&s.count[cell], 1);
 }
@@ -126,96 +125,103 @@ __global__ void k_cellsort(CellGrid g, SysDev s) {
         }
         s.perm[t + 1] = v;
     }
+    const int cz = c % g.nc[2], cy = (c / g.nc[2]) % g.nc[1], cx = c / (g.nc[2] * g.nc[1]);
     for (int k = b; k < e; ++k) {
         int i = s.perm[k];
-        double x0 = s.x[3 * i], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
+        const double x0 = s.x[3 * i], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
         s.xs[3 * k] = x0;
         s.xs[3 * k + 1] = x1;
         s.xs[3 * k + 2] = x2;
+        double w0, w1, w2;
+        cell_coord(x0, g, 0, w0);
+        cell_coord(x1, g, 1, w1);
+        cell_coord(x2, g, 2, w2);
         float4 p;
-        wrap_cell(x0, g, 0, p.x);
-        wrap_cell(x1, g, 1, p.y);
-        wrap_cell(x2, g, 2, p.z);
-        p.w = 0.f;
+        p.x = (float)(w0 - cx * g.h[0]);
+        p.y = (float)(w1 - cy * g.h[1]);
+        p.z = (float)(w2 - cz * g.h[2]);
+        p.w = __int_as_float(pack_cell(cx, cy, cz));
         s.pf[k] = p;
-        s.scell[k] = c;
         s.smask[k] = s.mask ? s.mask[i] : -1;
     }
 }
 
-// Minimum-image displacement and r^2 in FP64 with the oracle's operation order.
-__device__ __forceinline__ double exact_disp(const CellGrid &g, const double *xi, const double *xj, double *d) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        double t = __dsub_rn(xj[c], xi[c]);
-        if (g.periodic[c]) {
-            double k = rint(__ddiv_rn(t, g.L[c]));
-            t = __dsub_rn(t, __dmul_rn(g.L[c], k));
-        }
-        d[c] = t;
-    }
-    return __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2]));
+// FP64 decision on raw coordinates (the oracle's criterion, operation by operation).
+template <int KIND>
+__device__ __noinline__ bool exact_decide(const GeoD &gd, const NeighSpec &ns, const double *xk, const double *xj) {
+    double d[3];
+    const double r2 = exact_disp(gd, xk, xj, d);
+    if (KIND == NK_RANGE) return (r2 <= ns.rc2) && (r2 >= 1e-12);
+    if (KIND == NK_STEP) return (r2 <= ns.rc2) && (__dsqrt_rn(r2) < ns.r0);
+    return (r2 <= ns.rc2) && (sw_f<double>(ns.sw, __dsqrt_rn(r2)) >= ns.eps);
 }
 
-__device__ __forceinline__ int stencil(const CellGrid &g, int c, int ci, int *out) {
-    const int nc = g.nc[c];
-    if (nc == 1) { out[0] = 0; return 1; }
-    if (g.periodic[c]) {
-        if (nc == 2) { out[0] = 0; out[1] = 1; return 2; }
-        out[0] = ci == 0 ? nc - 1 : ci - 1;
-        out[1] = ci;
-        out[2] = ci == nc - 1 ? 0 : ci + 1;
-        return 3;
-    }
-    int k = 0;
-    if (ci > 0) out[k++] = ci - 1;
-    out[k++] = ci;
-    if (ci < nc - 1) out[k++] = ci + 1;
-    return k;
-}
-
-template <typename T, int KIND>
-__global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, NeighSpec ns, NeighDev<T> nd, DevStatus *status) {
+template <int KIND>
+__global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
+                                                      DevStatus *status) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
-    const float4 p = s.pf[k];
-    const int c = s.scell[k];
-    const int cz = c % g.nc[2], cy = (c / g.nc[2]) % g.nc[1], cx = c / (g.nc[2] * g.nc[1]);
-    int sx[3], sy[3], sz[3];
-    const int nx = stencil(g, 0, cx, sx), ny = stencil(g, 1, cy, sy), nz = stencil(g, 2, cz, sz);
-    const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
+    const GeoF gf = geo_f(g, s.pf);
+    const GeoD gd = geo_d(g, s.xs);
+    const float4 a = s.pf[k];
+    const int w = __float_as_int(a.w);
+    const int cx = w & 1023, cy = (w >> 10) & 1023, cz = w >> 20;
+    const int nz = g.nc[2];
     int cnt = 0;
-    for (int a = 0; a < nx; ++a)
-        for (int b = 0; b < ny; ++b)
-            for (int e = 0; e < nz; ++e) {
-                const int cc = (sx[a] * g.nc[1] + sy[b]) * g.nc[2] + sz[e];
-                const int jb = s.start[cc], je = s.start[cc + 1];
+    for (int ox = -1; ox <= 1; ++ox) {
+        int x = cx + ox;
+        if (g.periodic[0]) {
+            if (g.nc[0] < 3 && ox != 0 && (g.nc[0] == 1 || ox == -1)) continue;
+            x = (x + g.nc[0]) % g.nc[0];
+        } else if (x < 0 || x >= g.nc[0]) continue;
+        for (int oy = -1; oy <= 1; ++oy) {
+            int y = cy + oy;
+            if (g.periodic[1]) {
+                if (g.nc[1] < 3 && oy != 0 && (g.nc[1] == 1 || oy == -1)) continue;
+                y = (y + g.nc[1]) % g.nc[1];
+            } else if (y < 0 || y >= g.nc[1]) continue;
+            const int col = (x * g.nc[1] + y) * nz;
+            // z cells of the column: one contiguous range unless the stencil wraps
+            int zr[3][2], nr = 0;
+            if (nz >= 3 && cz >= 1 && cz <= nz - 2) {
+                zr[0][0] = cz - 1;
+                zr[0][1] = cz + 1;
+                nr = 1;
+            } else if (nz >= 3 && g.periodic[2]) {
+                if (cz == 0) {
+                    zr[0][0] = 0; zr[0][1] = 1; zr[1][0] = nz - 1; zr[1][1] = nz - 1; nr = 2;
+                } else {
+                    zr[0][0] = nz - 2; zr[0][1] = nz - 1; zr[1][0] = 0; zr[1][1] = 0; nr = 2;
+                }
+            } else {
+                zr[0][0] = max(cz - 1, 0);
+                zr[0][1] = min(cz + 1, nz - 1);
+                nr = 1;
+            }
+            for (int r = 0; r < nr; ++r) {
+                const int jb = s.start[col + zr[r][0]], je = s.start[col + zr[r][1] + 1];
                 for (int j = jb; j < je; ++j) {
                     if (j == k) continue;
-                    const float4 q = s.pf[j];
-                    float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-                    if (g.periodic[0]) dx -= g.Lf[0] * rintf(dx * g.invLf[0]);
-                    if (g.periodic[1]) dy -= g.Lf[1] * rintf(dy * g.invLf[1]);
-                    if (g.periodic[2]) dz -= g.Lf[2] * rintf(dz * g.invLf[2]);
-                    if (dx * dx + dy * dy + dz * dz > ns.rcf2) continue;
-                    const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
-                    double d[3];
-                    const double r2 = exact_disp(g, xk, xj, d);
-                    bool ok;
-                    if (KIND == NK_RANGE) ok = (r2 <= ns.rc2) && (r2 >= 1e-12);
-                    else ok = (r2 <= ns.rc2) && (sw_f<double>(ns.sw, __dsqrt_rn(r2)) >= ns.eps);
-                    if (!ok) continue;
-                    if (cnt < nd.M) {
-                        Pair<T> pr;
-                        pr.x = (T)d[0];
-                        pr.y = (T)d[1];
-                        pr.z = (T)d[2];
-                        pr.j = j;
-                        nd.pairs[(size_t)cnt * s.npad + k] = pr;
+                    const float4 b = s.pf[j];
+                    float dx, dy, dz;
+                    disp_f(gf, a, b, dx, dy, dz);
+                    const float r2f = dx * dx + dy * dy + dz * dz;
+                    if (r2f > ns.hi2) continue;
+                    bool in;
+                    if (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f) {
+                        in = true;
+                    } else {
+                        const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
+                        const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
+                        in = exact_decide<KIND>(gd, ns, xk, xj);
                     }
+                    if (!in) continue;
+                    if (cnt < nd.M) nd.list[(size_t)cnt * s.npad + k] = j;
                     ++cnt;
                 }
             }
+        }
+    }
     nd.count[k] = cnt;
     if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
 }
@@ -224,20 +230,19 @@ constexpr int kMaxCapList = 64;
 
 // STEINH Q cap: keep the `cap` nearest by (r2, caller index), the order of the
 // reference's strict-'>' insertion with ties resolved canonically.
-template <typename T>
-__global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, NeighSpec ns, NeighDev<T> nd) {
+__global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
+    const GeoD gd = geo_d(g, s.xs);
     const int c = min(nd.count[k], min(nd.M, kMaxCapList));
     double r2[kMaxCapList];
     int id[kMaxCapList];
     const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
     for (int t = 0; t < c; ++t) {
-        Pair<T> pr = nd.pairs[(size_t)t * s.npad + k];
-        const int j = pr.j;
+        const int j = nd.list[(size_t)t * s.npad + k];
         const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
         double d[3];
-        r2[t] = exact_disp(g, xk, xj, d);
+        r2[t] = exact_disp(gd, xk, xj, d);
         id[t] = s.perm[j];
     }
     double kr2 = CUDART_INF;
@@ -246,10 +251,7 @@ __global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, Nei
         int rank = 0;
         for (int u = 0; u < c; ++u)
             if (r2[u] < r2[t] || (r2[u] == r2[t] && id[u] < id[t])) ++rank;
-        if (rank < ns.cap) {
-            Pair<T> *pp = &nd.pairs[(size_t)t * s.npad + k];
-            pp->j |= (1 << kFlagBit);
-        }
+        if (rank < ns.cap) nd.list[(size_t)t * s.npad + k] |= (1 << kFlagBit);
         if (c > ns.cap && rank == ns.cap - 1) {
             kr2 = r2[t];
             kid = id[t];
@@ -281,23 +283,18 @@ void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
     prof_mark("cell_sort", st);
 }
 
-template <typename T>
-void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev<T> nd, DevStatus *status,
+void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, DevStatus *status,
                       cudaStream_t st) {
     if (s.n == 0) return;
     const int nb = (s.n + kBlock - 1) / kBlock;
-    if (ns.kind == NK_RANGE) k_neighbors<T, NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
-    else k_neighbors<T, NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    if (ns.kind == NK_RANGE) k_neighbors<NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    else if (ns.kind == NK_STEP) k_neighbors<NK_STEP><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    else k_neighbors<NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
     prof_mark("neighbors", st);
     if (ns.cap > 0) {
-        k_select_cap<T><<<nb, kBlock, 0, st>>>(g, s, ns, nd);
+        k_select_cap<<<nb, kBlock, 0, st>>>(g, s, ns, nd);
         prof_mark("select_cap", st);
     }
 }
-
-template void launch_neighbors<float>(const CellGrid &, const SysDev &, const NeighSpec &, NeighDev<float>, DevStatus *,
-                                      cudaStream_t);
-template void launch_neighbors<double>(const CellGrid &, const SysDev &, const NeighSpec &, NeighDev<double>,
-                                       DevStatus *, cudaStream_t);
 
 }  // namespace mtd

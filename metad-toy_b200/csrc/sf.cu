@@ -44,10 +44,12 @@ template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(D
         if (d.smask[k] & d.groupbit) {
             const int c = min(d.nb.count[k], d.nb.M);
             const T rc2 = (T)d.rc2, qf = (T)d.qf;
+            const auto a = d.geo.load(k);
             for (int t = 0; t < c; ++t) {
-                const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
+                T dx, dy, dz;
+                d.geo.disp(a, d.geo.load(d.nb.list[(size_t)t * d.npad + k]), dx, dy, dz);
                 T gv, dg;
-                debye_g<T>(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z, rc2, qf, gv, dg);
+                debye_g<T>(dx * dx + dy * dy + dz * dz, rc2, qf, gv, dg);
                 S += gv;
             }
             S += T(1);
@@ -83,17 +85,20 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
         const T rc2 = (T)d.rc2, qf = (T)d.qf;
         T gx = T(0), gy = T(0), gz = T(0);
         const int c = min(d.nb.count[k], d.nb.M);
+        const auto a = d.geo.load(k);
         for (int t = 0; t < c; ++t) {
-            const Pair<T> pr = d.nb.pairs[(size_t)t * d.npad + k];
-            const T w = ak + debye_a<T>(d, pr.j, c0, c1);
+            const int j = d.nb.list[(size_t)t * d.npad + k];
+            const T w = ak + debye_a<T>(d, j, c0, c1);
             if (w == T(0)) continue;
-            const T r2 = pr.x * pr.x + pr.y * pr.y + pr.z * pr.z;
+            T dx, dy, dz;
+            d.geo.disp(a, d.geo.load(j), dx, dy, dz);
+            const T r2 = dx * dx + dy * dy + dz * dz;
             T gv, dg;
             debye_g<T>(r2, rc2, qf, gv, dg);
             const T f = w * dg * t_rsqrt<T>(r2);
-            gx -= f * pr.x;
-            gy -= f * pr.y;
-            gz -= f * pr.z;
+            gx -= f * dx;
+            gy -= f * dy;
+            gz -= f * dz;
         }
         const int i = d.perm[k];
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;

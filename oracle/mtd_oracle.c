@@ -201,7 +201,8 @@ void orc_minimg(const orc_box *b, const double *xi, const double *xj, double *d)
     for (int c = 0; c < 3; c++) {
         double t = xj[c] - xi[c];
         if (b->periodic[c]) {
-            double k = rint(t / b->L[c]);
+            double inv = 1.0 / b->L[c];
+            double k = rint(t * inv);
             double s = b->L[c] * k;
             t = t - s;
         }
