@@ -30,42 +30,50 @@ __device__ __forceinline__ void center_frac_clamp(double cv, double lo, double h
     if (i > nb - 3) { i = nb - 3; f = 1.0; }
 }
 
-// Catmull-Rom value and gradient on the bin-centred grid (dimension 0 slowest).
-__device__ double grid_value(const BiasPlan &P, const double *s, double *dV) {
-    int ix[3];
-    double fx[3];
+// Catmull-Rom stencil of s: base indices ix (clamped) and fractions fx.
+__device__ __forceinline__ void stencil_locate(const BiasPlan &P, const double *s, int *ix, double *fx) {
     for (int k = 0; k < P.D; ++k) center_frac_clamp(s[k], P.lo[k], P.dcv[k], P.nbin[k], ix[k], fx[k]);
-    const double *G = P.grid;
+}
+
+// The 4^D grid values around the stencil, loaded by all threads at once into
+// S[((u * 4) + t) * 4 + q] = grid[ix0 - 1 + q][ix1 - 1 + t][ix2 - 1 + u].
+__device__ __forceinline__ void stencil_load(const BiasPlan &P, const int *ix, double *S) {
+    const int nst = P.D == 1 ? 4 : (P.D == 2 ? 16 : 64);
+    for (int e = threadIdx.x; e < nst; e += blockDim.x) {
+        const int q = e & 3, t = (e >> 2) & 3, u = e >> 4;
+        size_t g = (size_t)(ix[0] - 1 + q);
+        if (P.D >= 2) g = g * P.nbin[1] + (ix[1] - 1 + t);
+        if (P.D >= 3) g = g * P.nbin[2] + (ix[2] - 1 + u);
+        S[e] = P.grid[g];
+    }
+}
+
+// Catmull-Rom value and gradient on the bin-centred grid (dimension 0 slowest)
+// from a loaded stencil.
+__device__ double grid_value(const BiasPlan &P, const double *S, const double *fx, double *dV) {
     double V;
     if (P.D == 1) {
-        const double *p = G + ix[0] - 1;
+        const double *p = S;
         V = cr_value(p[0], p[1], p[2], p[3], fx[0]);
         dV[0] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]) / P.dcv[0];
         if (isnan(dV[0])) dV[0] = 0.0;
     } else if (P.D == 2) {
         double col[4], dcol[4];
-        const int n1 = P.nbin[1];
         for (int t = 0; t < 4; ++t) {
-            const int jj = ix[1] - 1 + t;
-            double p0 = G[(ix[0] - 1) * n1 + jj], p1 = G[ix[0] * n1 + jj];
-            double p2 = G[(ix[0] + 1) * n1 + jj], p3 = G[(ix[0] + 2) * n1 + jj];
-            col[t] = cr_value(p0, p1, p2, p3, fx[0]);
-            dcol[t] = cr_deriv(p0, p1, p2, p3, fx[0]);
+            const double *p = S + 4 * t;
+            col[t] = cr_value(p[0], p[1], p[2], p[3], fx[0]);
+            dcol[t] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]);
         }
         V = cr_value(col[0], col[1], col[2], col[3], fx[1]);
         dV[0] = cr_value(dcol[0], dcol[1], dcol[2], dcol[3], fx[1]) / P.dcv[0];
         dV[1] = cr_deriv(col[0], col[1], col[2], col[3], fx[1]) / P.dcv[1];
         if (isnan(dV[0]) || isnan(dV[1])) { dV[0] = 0.0; dV[1] = 0.0; }
     } else {
-        const int n1 = P.nbin[1], n2 = P.nbin[2];
         double a[4], da[4], b0[4];
         for (int u = 0; u < 4; ++u) {
-            const int kk = ix[2] - 1 + u;
             double c[4], dc[4];
             for (int t = 0; t < 4; ++t) {
-                const int jj = ix[1] - 1 + t;
-                double p[4];
-                for (int q = 0; q < 4; ++q) p[q] = G[((ix[0] - 1 + q) * n1 + jj) * n2 + kk];
+                const double *p = S + (u * 4 + t) * 4;
                 c[t] = cr_value(p[0], p[1], p[2], p[3], fx[0]);
                 dc[t] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]);
             }
@@ -178,12 +186,22 @@ __device__ double eval_code(const ExprInstr *code, int n, const double *sym, int
 }
 
 __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
-    const BiasPlan &P = *Pp;
+    // the plan is read many times by thread 0: stage it in shared memory with one parallel load
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    {
+        static_assert(sizeof(BiasPlan) % 8 == 0, "plan size");
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(Pp);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(plan_raw);
+        for (int e = threadIdx.x; e < (int)(sizeof(BiasPlan) / 8); e += blockDim.x) dst[e] = src[e];
+        __syncthreads();
+    }
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
     __shared__ double smem[8 * 32];
     __shared__ double usum[kMaxUnits][8];
     __shared__ double sv[kMaxDim];
     __shared__ double hill_w;
     __shared__ int do_dep;
+    __shared__ double sten[64];
     // 1. deterministic reductions of every unit's block partials
     for (int u = 0; u < P.nunit; ++u) {
         const UnitPlan &U = P.unit[u];
@@ -227,15 +245,23 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
         }
         // 3. DIM expressions with exact chain factors
         for (int dd = 0; dd < P.D; ++dd) sv[dd] = eval_code(P.code[dd], P.ncode[dd], sym, P.nsym, jac[dd]);
-        // 4. well-tempered height from V(s) before the deposit
         do_dep = (P.pace != 0) && (step % P.pace == 0);
-        if (do_dep) {
-            double dV[kMaxDim];
-            double Vb = P.wt ? grid_value(P, sv, dV) : 0.0;
-            hill_w = P.h0 * exp(-(Vb) / (P.temp * P.kb * (P.biasf - 1.0)));
-        }
     }
     __syncthreads();
+    int ix[3] = {1, 1, 1};
+    double fx[3] = {0, 0, 0};
+    stencil_locate(P, sv, ix, fx);
+    // 4. well-tempered height from V(s) before the deposit
+    if (do_dep) {
+        if (P.wt) stencil_load(P, ix, sten);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double dV[kMaxDim];
+            const double Vb = P.wt ? grid_value(P, sten, fx, dV) : 0.0;
+            hill_w = P.h0 * exp(-(Vb) / (P.temp * P.kb * (P.biasf - 1.0)));
+        }
+        __syncthreads();
+    }
     // 5. banded deposit, one thread per band bin
     if (do_dep) {
         int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
@@ -269,10 +295,12 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
         }
     }
     __syncthreads();
+    stencil_load(P, ix, sten);
+    __syncthreads();
     if (threadIdx.x == 0) {
         // 6. V and dV/ds at s after the deposit, chain rule to every symbol
         double dV[kMaxDim] = {0, 0, 0, 0};
-        const double V = grid_value(P, sv, dV);
+        const double V = grid_value(P, sten, fx, dV);
         double alpha[kMaxSymbols];
         for (int q = 0; q < P.nsym; ++q) {
             double a = 0.0;
