@@ -226,6 +226,71 @@ __global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, Neig
     if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
 }
 
+// Fast path, valid when every periodic dimension has at least three cells:
+// the 27 stencil cells are then distinct and the displacement to an atom of
+// the cell at offset o is exactly o h + (off_j - off_k), so each cell's shift
+// o h - off_k is formed once and a candidate costs one load and three adds.
+template <int KIND>
+__global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
+                                                           DevStatus *status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= s.n) return;
+    const GeoD gd = geo_d(g, s.xs);
+    const float4 a = s.pf[k];
+    const int w = __float_as_int(a.w);
+    const int cx = w & 1023, cy = (w >> 10) & 1023, cz = w >> 20;
+    const int nx = g.nc[0], ny = g.nc[1], nz = g.nc[2];
+    int cnt = 0;
+#pragma unroll 1
+    for (int ox = -1; ox <= 1; ++ox) {
+        int x = cx + ox;
+        if (x < 0 || x >= nx) {
+            if (!g.periodic[0]) continue;
+            x += x < 0 ? nx : -nx;
+        }
+        const float sx = (float)ox * g.hf[0] - a.x;
+#pragma unroll 1
+        for (int oy = -1; oy <= 1; ++oy) {
+            int y = cy + oy;
+            if (y < 0 || y >= ny) {
+                if (!g.periodic[1]) continue;
+                y += y < 0 ? ny : -ny;
+            }
+            const float sy = (float)oy * g.hf[1] - a.y;
+            const int col = (x * ny + y) * nz;
+#pragma unroll
+            for (int oz = -1; oz <= 1; ++oz) {
+                int z = cz + oz;
+                if (z < 0 || z >= nz) {
+                    if (!g.periodic[2]) continue;
+                    z += z < 0 ? nz : -nz;
+                }
+                const float sz = (float)oz * g.hf[2] - a.z;
+                const int jb = __ldg(s.start + col + z), je = __ldg(s.start + col + z + 1);
+                for (int j = jb; j < je; ++j) {
+                    const float4 b = __ldg(s.pf + j);
+                    const float dx = b.x + sx, dy = b.y + sy, dz = b.z + sz;
+                    const float r2f = dx * dx + dy * dy + dz * dz;
+                    if (r2f > ns.hi2 || j == k) continue;
+                    bool in;
+                    if (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f) {
+                        in = true;
+                    } else {
+                        const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
+                        const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
+                        in = exact_decide<KIND>(gd, ns, xk, xj);
+                    }
+                    if (!in) continue;
+                    if (cnt < nd.M) nd.list[(size_t)cnt * s.npad + k] = j;
+                    ++cnt;
+                }
+            }
+        }
+    }
+    nd.count[k] = cnt;
+    if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
+}
+
 constexpr int kMaxCapList = 64;
 
 // STEINH Q cap: keep the `cap` nearest by (r2, caller index), the order of the
@@ -287,7 +352,14 @@ void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, N
                       cudaStream_t st) {
     if (s.n == 0) return;
     const int nb = (s.n + kBlock - 1) / kBlock;
-    if (ns.kind == NK_RANGE) k_neighbors<NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    bool fast = true;
+    for (int c = 0; c < 3; ++c)
+        if (g.periodic[c] && g.nc[c] < 3) fast = false;
+    if (fast) {
+        if (ns.kind == NK_RANGE) k_neighbors_fast<NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+        else if (ns.kind == NK_STEP) k_neighbors_fast<NK_STEP><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+        else k_neighbors_fast<NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    } else if (ns.kind == NK_RANGE) k_neighbors<NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
     else if (ns.kind == NK_STEP) k_neighbors<NK_STEP><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
     else k_neighbors<NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
     prof_mark("neighbors", st);
