@@ -112,17 +112,27 @@ class ClockSampler:
 
 
 def kernel_bytes(name, n, nbar):
-    """Algorithmic (compulsory) HBM bytes per launch of each kernel of the step:
-    every per-atom array it must read or write once, pair records 16 B each."""
+    """Algorithmic (compulsory) HBM bytes per launch of each kernel of the step
+    for STEINH L Q4+Q6 in mixed precision (records of 24 FP32 = 96 B): every
+    per-atom array the kernel must read or write once, 4-byte neighbour indices."""
     per_atom = {
-        "neighbors": 48 + 16 * nbar,
-        "local_q": 104 + 16 * nbar,
-        "local_lq": 228 + 16 * nbar,
-        "local_lambda": 216 + 16 * nbar,
-        "local_force": 152 + 16 * nbar,
-        "cell_bin": 32, "cell_scatter": 12, "cell_sort": 80,
+        "cell_bin": 32,                       # x 24 -> cell 4, slot 4
+        "cell_scatter": 12,                   # cell, slot -> perm
+        "cell_sort": 80,                      # perm, x, mask -> xs 24, pf 16, smask, perm
+        "neighbors": 24 + 4 * nbar,           # pf 16, cell starts ~4, count 4, indices
+        "local_q": 120 + 4 * nbar,            # pf 16, count, indices -> q 96, NF 4
+        "local_lq": 228 + 4 * nbar,           # q 96, NF, mask, count, indices -> LQ 96, |LQ| 8, e1/e2 16
+        "local_lambda": 216 + 4 * nbar,       # e1/e2 16, LQ 96, NF, count, indices -> lambda 96
+        "local_force": 168 + 4 * nbar,        # lambda 96, pf 16, count, indices, perm, f_in 24 -> f_out 24
     }
     return per_atom.get(name, 0.0) * n
+
+
+def pipeline_bytes(nbar):
+    """Compulsory DRAM bytes per atom-step of the whole dependency-minimal
+    pipeline (x repack, four passes over positions and lists, q/LQ/adjoint
+    records written and read, force read-modify-write): 1070 + 16 nbar."""
+    return 1070.0 + 16.0 * nbar
 
 
 def peaks():
@@ -311,7 +321,10 @@ def main():
             "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
             "traffic": ncu_traffic(dom_name), "avg_launch_ms": avg_ms,
             "algorithmic_bytes_per_launch": nbytes,
-            "kernels_ms_per_step": {k: v[1] / max(v[0], 1) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+            "kernels_ms_per_step": {k: v[1] / max(v[0], 1) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "pipeline": {"bytes_per_atom_step": pipeline_bytes(nbar),
+                         "achieved": pipeline_bytes(nbar) * n / (dev_ms / args.steps / 1e3) / 1e9,
+                         "frac": pipeline_bytes(nbar) * n / (dev_ms / args.steps / 1e3) / 1e9 / peak}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
