@@ -158,6 +158,32 @@ int mtd_max_neighbors(mtd_ctx *ctx, const char *name);
 const char *mtd_last_error(const mtd_ctx *ctx);
 int mtd_abi_version(void);
 
+/* k-vector structure factor of a group, computed with NO device allocation.
+ * No counterpart in the reference (its structure factor lives in
+ * Stru_factor, src/cvs/CVs_Strufactor.cu, and allocates per call); this is an
+ * allocation-free variant of the STRU_FACTOR_K unit of a context:
+ *   rho(k) = sum_{i in group} exp(i k.x_i),   S = sum_k |rho(k)|^2 / (N K).
+ * For callers that cannot allocate device memory at the point of the call:
+ * an MD engine that computes this CV between its own kernels on several
+ * streams (cudaMalloc / cudaFree synchronise the device and would serialise
+ * them) or that runs with all device memory reserved up front by its own pool.
+ *   n, d_x      atoms, device FP64 AoS n*3 (caller order)
+ *   d_mask      device group bitmask per atom, NULL = every atom; groupbit as in mtd_options
+ *   nk, d_k     1 <= nk <= 1024 k-vectors, device FP64 AoS nk*3
+ *   precision   MTD_PREC_FP64, or MTD_PREC_MIXED: FP32 sincos of the reduced FP64 phase
+ *   d_rho       device 2*nk doubles (Re, Im per k) or NULL
+ *   d_s         device 1 double: S
+ *   stream      cudaStream_t or NULL; the call only enqueues work
+ *   err/errlen  optional message buffer
+ * Block partials go to a fixed 1 MiB file-scope device array; no part of it
+ * has to start at zero (each call writes every entry it reads).  The first
+ * call on a device (that device current) resolves the array's address with
+ * cudaGetSymbolAddress: make it before any stream capture.  Calls in flight at
+ * the same time on one device share the array and race: order them on one
+ * stream.  nk outside [1, 1024] returns MTD_ERR_INVALID_ARG. */
+mtd_status mtd_sk_noalloc(int n, const double *d_x, const int *d_mask, int groupbit, int nk, const double *d_k,
+                          int precision, double *d_rho, double *d_s, void *stream, char *err, int errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,7 +31,7 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
            "mtd_extract_peratom", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
            "mtd_set_stream", "mtd_profile_enable", "mtd_profile_report",
-           "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version"]
+           "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc"]
 
 
 class MetadError(RuntimeError):
@@ -88,6 +88,8 @@ def lib():
         L.mtd_profile_report.argtypes = [vp, C.c_char_p, C.c_int]
         L.mtd_parse_args.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.c_char_p, C.c_int]
         L.mtd_eval_expression.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, dp, dp]
+        L.mtd_sk_noalloc.argtypes = [C.c_int, vp, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, C.c_char_p,
+                                     C.c_int]
         _lib = L
     return _lib
 
@@ -117,6 +119,17 @@ def parse_args(args, groups=None):
     buf = C.create_string_buffer(1024)
     lib().mtd_parse_args(len(toks), argv, C.byref(opt), buf, 1024)
     return buf.value.decode()
+
+
+def sk_noalloc(n, x_ptr, k_ptr, nk, s_ptr, rho_ptr=0, mask_ptr=0, groupbit=1, precision="mixed", stream=0):
+    """Allocation-free k-vector S(k) on device buffers (integer device pointers);
+    enqueues on `stream` (a cudaStream_t handle, 0 = default) and returns."""
+    buf = C.create_string_buffer(256)
+    st = lib().mtd_sk_noalloc(int(n), C.c_void_p(x_ptr or None), C.c_void_p(mask_ptr or None), int(groupbit),
+                              int(nk), C.c_void_p(k_ptr or None), PREC[precision], C.c_void_p(rho_ptr or None),
+                              C.c_void_p(s_ptr or None), C.c_void_p(stream or None), buf, 256)
+    if st != 0:
+        raise MetadError(st, buf.value.decode())
 
 
 def eval_expression(expr, values):
