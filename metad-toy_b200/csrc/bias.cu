@@ -185,17 +185,10 @@ __device__ double eval_code(const ExprInstr *code, int n, const double *sym, int
     return st[0].v;
 }
 
-__global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
-    // the plan is read many times by thread 0: stage it in shared memory with one parallel load
-    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
-    {
-        static_assert(sizeof(BiasPlan) % 8 == 0, "plan size");
-        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(Pp);
-        unsigned long long *dst = reinterpret_cast<unsigned long long *>(plan_raw);
-        for (int e = threadIdx.x; e < (int)(sizeof(BiasPlan) / 8); e += blockDim.x) dst[e] = src[e];
-        __syncthreads();
-    }
-    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+// The plan is a __grid_constant__ kernel parameter (about 4.5 KB, within the
+// 32 KB parameter limit): thread 0's many reads of it are constant-bank reads
+// and no copy into shared memory is needed.
+__global__ void __launch_bounds__(256) k_bias_step(const __grid_constant__ BiasPlan P, long long step) {
     __shared__ double smem[8 * 32];
     __shared__ double usum[kMaxUnits][8];
     __shared__ double sv[kMaxDim];
@@ -251,19 +244,19 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
     int ix[3] = {1, 1, 1};
     double fx[3] = {0, 0, 0};
     stencil_locate(P, sv, ix, fx);
+    stencil_load(P, ix, sten);   // grid around s before this step's deposit
+    __syncthreads();
     // 4. well-tempered height from V(s) before the deposit
     if (do_dep) {
-        if (P.wt) stencil_load(P, ix, sten);
-        __syncthreads();
         if (threadIdx.x == 0) {
             double dV[kMaxDim];
             const double Vb = P.wt ? grid_value(P, sten, fx, dV) : 0.0;
             hill_w = P.h0 * exp(-(Vb) / (P.temp * P.kb * (P.biasf - 1.0)));
         }
         __syncthreads();
-    }
-    // 5. banded deposit, one thread per band bin
-    if (do_dep) {
+        // 5. banded deposit, one thread per band bin; the stencil takes the same
+        //    increment as the grid (same operands, same rounding), so V and
+        //    dV/ds after the deposit need no second grid read
         int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
         int total = 0;
         if (hill_band(P, sv, lo, hi)) {
@@ -283,6 +276,14 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
             for (int k = 1; k < P.D; ++k) g = g * P.nbin[k] + idx[k];
             if (g < (size_t)P.grid_size) P.grid[g] += hill_w * hill_gauss(P, sv, idx, P.sigma);
         }
+        const int nst = P.D == 1 ? 4 : (P.D == 2 ? 16 : 64);
+        if (total > 0 && threadIdx.x < nst) {
+            const int e = threadIdx.x;
+            const int idx[3] = {ix[0] - 1 + (e & 3), ix[1] - 1 + ((e >> 2) & 3), ix[2] - 1 + (e >> 4)};
+            bool in = true;
+            for (int k = 0; k < P.D; ++k) in = in && idx[k] >= lo[k] && idx[k] <= hi[k];
+            if (in) sten[e] += hill_w * hill_gauss(P, sv, idx, P.sigma);
+        }
         if (threadIdx.x == 0) {
             unsigned long long h = *P.nhills;
             HillRec r;
@@ -293,10 +294,8 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
             P.hills[h % (unsigned long long)P.hill_cap] = r;
             *P.nhills = h + 1;
         }
+        __syncthreads();
     }
-    __syncthreads();
-    stencil_load(P, ix, sten);
-    __syncthreads();
     if (threadIdx.x == 0) {
         // 6. V and dV/ds at s after the deposit, chain rule to every symbol
         double dV[kMaxDim] = {0, 0, 0, 0};
@@ -387,8 +386,8 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 
 }  // namespace
 
-void launch_bias_step(const BiasPlan *d_plan, long long step, int, cudaStream_t st) {
-    k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
+void launch_bias_step(const BiasPlan &plan, long long step, cudaStream_t st) {
+    k_bias_step<<<1, 256, 0, st>>>(plan, step);
     prof_mark("bias_step", st);
 }
 

@@ -175,8 +175,8 @@ mtd_status cuda_check(mtd_ctx *c, cudaError_t e, const char *what) {
 
 size_t real_size(const mtd_ctx *c) { return c->fp64 ? sizeof(double) : sizeof(float); }
 
-int record_stride(const Unit &u) {
-    if (u.kind == CAL_STEINH_L) return pad4(2 * (u.LA + 1) + (u.LB ? 2 * (u.LB + 1) : 0));
+int record_stride(const mtd_ctx *c, const Unit &u) {
+    if (u.kind == CAL_STEINH_L) return local_record_stride(u.LA, u.LB, c->fp64 ? 1 : 0);
     if (u.kind == CAL_STEINH_Q) return pad4(2 * (u.LA + 1));
     return 0;
 }
@@ -266,7 +266,7 @@ mtd_status alloc_env(mtd_ctx *c, Env &e, int npad) {
 
 mtd_status alloc_unit(mtd_ctx *c, Unit &u, int npad) {
     const size_t R = real_size(c);
-    const int SQ = record_stride(u);
+    const int SQ = record_stride(c, u);
     const int nb = (npad + kBlock - 1) / kBlock;
     void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S};
     for (void **a : arrs) dfree(*a);
@@ -586,7 +586,7 @@ SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
 
 template <typename T> LocalDev<T> local_dev(mtd_ctx *c, Unit &u, const CellGrid &g) {
     LocalDev<T> d{};
-    d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.LA = u.LA; d.LB = u.LB;
+    d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(c, u); d.LA = u.LA; d.LB = u.LB;
     d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
     d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
@@ -596,7 +596,7 @@ template <typename T> LocalDev<T> local_dev(mtd_ctx *c, Unit &u, const CellGrid 
 
 template <typename T> GlobalDev<T> global_dev(mtd_ctx *c, Unit &u, const CellGrid &g) {
     GlobalDev<T> d{};
-    d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(u); d.L = u.LA; d.groupbit = u.groupbit;
+    d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(c, u); d.L = u.LA; d.groupbit = u.groupbit;
     d.nsw = (int)u.qsw.size();
     for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.exact = geo_d(g, c->xs);
@@ -641,7 +641,7 @@ void run_units(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, 
             c->launches += 2;
         }
     }
-    launch_bias_step(c->d_plan, step, 0, st);
+    launch_bias_step(c->plan, step, st);
     c->launches += 1;
     // forces: the first unit reads f_in, the later ones accumulate into f_out
     bool first = true;

@@ -136,6 +136,8 @@ template <typename T> struct LocalDev {
     const double *coef;         // c1A c2A c1B c2B (written by the bias kernel)
 };
 template <typename T> void launch_local_values(const LocalDev<T> &d, cudaStream_t st);
+// Reals per STEINH L record (both orders): a multiple of 32 bytes.
+int local_record_stride(int LA, int LB, int fp64);
 template <typename T>
 void launch_local_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                          double *vpart, DevStatus *status, cudaStream_t st);
@@ -244,7 +246,7 @@ struct BiasPlan {
 };
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
 
-void launch_bias_step(const BiasPlan *d_plan, long long step, int nunit_threads, cudaStream_t st);
+void launch_bias_step(const BiasPlan &plan, long long step, cudaStream_t st);
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st);
 

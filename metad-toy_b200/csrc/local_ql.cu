@@ -27,11 +27,35 @@ namespace mtd {
 
 namespace {
 
-template <int LA, int LB> struct LSet {
+// Record layout: orders A then B, (Re, Im) per m; the stride is a multiple of
+// 32 bytes so a record is read with 256-bit loads (8 floats or 4 doubles).
+template <int LA, int LB, typename T> struct LSet {
     static constexpr int SA = 2 * (LA + 1);
     static constexpr int SB = LB ? 2 * (LB + 1) : 0;
-    static constexpr int SQ = pad4(SA + SB);
+    static constexpr int V32 = 32 / (int)sizeof(T);
+    static constexpr int SQ = (SA + SB + V32 - 1) / V32 * V32;
 };
+
+// Reads a whole record with 32-byte vector loads (one L1 wavefront per 32
+// bytes instead of per 16).  p must be 32-byte aligned: record strides are
+// multiples of 32 bytes and the arrays come from cudaMalloc.
+template <int N> __device__ __forceinline__ void load_rec32(const float *__restrict__ p, float (&v)[N]) {
+    static_assert(N % 8 == 0, "record stride must be a multiple of 32 bytes");
+#pragma unroll
+    for (int i = 0; i < N / 8; ++i)
+        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=f"(v[8 * i]), "=f"(v[8 * i + 1]), "=f"(v[8 * i + 2]), "=f"(v[8 * i + 3]),
+                       "=f"(v[8 * i + 4]), "=f"(v[8 * i + 5]), "=f"(v[8 * i + 6]), "=f"(v[8 * i + 7])
+                     : "l"(p + 8 * i));
+}
+template <int N> __device__ __forceinline__ void load_rec32(const double *__restrict__ p, double (&v)[N]) {
+    static_assert(N % 4 == 0, "record stride must be a multiple of 32 bytes");
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i)
+        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+                     : "=d"(v[4 * i]), "=d"(v[4 * i + 1]), "=d"(v[4 * i + 2]), "=d"(v[4 * i + 3])
+                     : "l"(p + 4 * i));
+}
 
 template <typename T, int N> __device__ __forceinline__ void load_rec(const T *__restrict__ p, T (&v)[N]) {
     static_assert(N % 4 == 0, "record stride");
@@ -108,7 +132,7 @@ __device__ __forceinline__ int nb_index(const NeighDev &nb, int npad, int t, int
 // Pass 1: q_lm and NF for every atom.
 template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
-    using S = LSet<LA, LB>;
+    using S = LSet<LA, LB, T>;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
     const auto a = d.geo.load(k);
@@ -135,7 +159,7 @@ __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
 // Pass 2: LQ_lm, LQ, the e1/e2 weights of the adjoint and block partial sums.
 template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_lq(LocalDev<T> d) {
-    using S = LSet<LA, LB>;
+    using S = LSet<LA, LB, T>;
     __shared__ double smem[5 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = k < d.n;
@@ -146,14 +170,14 @@ __global__ void __launch_bounds__(kBlock) k_local_lq(LocalDev<T> d) {
         T A[S::SQ];
         T lqA = T(0), lqB = T(0);
         if (ing && nfk > T(0)) {
-            load_rec(d.q + (size_t)k * S::SQ, A);
+            load_rec32(d.q + (size_t)k * S::SQ, A);
             const auto a = d.geo.load(k);
             const int c = min(d.nb.count[k], d.nb.M);
             for (int t = 0; t < c; ++t) {
                 const int j = nb_index(d.nb, d.npad, t, k);
                 const T sg = pair_sigma<T, STEP>(d, a, j);
                 T qj[S::SQ];
-                load_rec(d.q + (size_t)j * S::SQ, qj);
+                load_rec32(d.q + (size_t)j * S::SQ, qj);
 #pragma unroll
                 for (int s = 0; s < S::SQ; ++s) A[s] += sg * qj[s];
             }
@@ -220,7 +244,7 @@ __device__ __forceinline__ void add_g(T *acc, const T *lq, T w, T s) {
 // Pass 3 (after the bias kernel): lam_k / NF_k, and for smooth switches G_k, t_k, u_k.
 template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
-    using S = LSet<LA, LB>;
+    using S = LSet<LA, LB, T>;
     constexpr bool DSIG = !STEP;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
@@ -239,7 +263,7 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
         return;
     }
     T lqk[S::SQ];
-    load_rec(d.lq + (size_t)k * S::SQ, lqk);
+    load_rec32(d.lq + (size_t)k * S::SQ, lqk);
     const T wA = c1A * d.e12[4 * k] + c2A * d.e12[4 * k + 1];
     const T wB = c1B * d.e12[4 * k + 2] + c2B * d.e12[4 * k + 3];
     add_g<LA, T>(lam, lqk, wA, T(1));
@@ -260,14 +284,14 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
         if (wjA == T(0) && wjB == T(0)) continue;
         const T sg = pair_sigma<T, STEP>(d, a, j);
         T lqj[S::SQ];
-        load_rec(d.lq + (size_t)j * S::SQ, lqj);
+        load_rec32(d.lq + (size_t)j * S::SQ, lqj);
         add_g<LA, T>(lam, lqj, wjA, sg);
         if constexpr (LB > 0) add_g<LB, T>(lam + S::SA, lqj + S::SA, wjB, sg);
     }
     const T inv = T(1) / nfk;
     if constexpr (DSIG) {
         T qk[S::SQ];
-        load_rec(d.q + (size_t)k * S::SQ, qk);
+        load_rec32(d.q + (size_t)k * S::SQ, qk);
         T tA = T(0), tB = T(0), uA = T(0), uB = T(0);
 #pragma unroll
         for (int s = 0; s < S::SA; ++s) { tA += lam[s] * qk[s]; uA += Gk[s] * lqk[s]; }
@@ -289,7 +313,7 @@ template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
                                                         double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                         double *vpart, DevStatus *status) {
-    using S = LSet<LA, LB>;
+    using S = LSet<LA, LB, T>;
     constexpr bool DSIG = !STEP;
     __shared__ double smem[6 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -424,6 +448,12 @@ void run_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const 
         default: break;                                                                      \
         }                                                                                    \
     } while (0)
+
+int local_record_stride(int LA, int LB, int fp64) {
+    const int n = 2 * (LA + 1) + (LB ? 2 * (LB + 1) : 0);
+    const int v = fp64 ? 4 : 8;
+    return (n + v - 1) / v * v;
+}
 
 template <typename T> void launch_local_values(const LocalDev<T> &d, cudaStream_t st) {
     if (d.n == 0) return;
