@@ -49,45 +49,51 @@ __device__ __forceinline__ void stencil_load(const BiasPlan &P, const int *ix, d
 }
 
 // Catmull-Rom value and gradient on the bin-centred grid (dimension 0 slowest)
-// from a loaded stencil.
-__device__ double grid_value(const BiasPlan &P, const double *S, const double *fx, double *dV) {
-    double V;
-    if (P.D == 1) {
-        const double *p = S;
-        V = cr_value(p[0], p[1], p[2], p[3], fx[0]);
-        dV[0] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]) / P.dcv[0];
-        if (isnan(dV[0])) dV[0] = 0.0;
-    } else if (P.D == 2) {
-        double col[4], dcol[4];
-        for (int t = 0; t < 4; ++t) {
-            const double *p = S + 4 * t;
-            col[t] = cr_value(p[0], p[1], p[2], p[3], fx[0]);
-            dcol[t] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]);
-        }
-        V = cr_value(col[0], col[1], col[2], col[3], fx[1]);
-        dV[0] = cr_value(dcol[0], dcol[1], dcol[2], dcol[3], fx[1]) / P.dcv[0];
-        dV[1] = cr_deriv(col[0], col[1], col[2], col[3], fx[1]) / P.dcv[1];
-        if (isnan(dV[0]) || isnan(dV[1])) { dV[0] = 0.0; dV[1] = 0.0; }
-    } else {
-        double a[4], da[4], b0[4];
-        for (int u = 0; u < 4; ++u) {
-            double c[4], dc[4];
-            for (int t = 0; t < 4; ++t) {
-                const double *p = S + (u * 4 + t) * 4;
-                c[t] = cr_value(p[0], p[1], p[2], p[3], fx[0]);
-                dc[t] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]);
-            }
-            a[u] = cr_value(c[0], c[1], c[2], c[3], fx[1]);
-            da[u] = cr_deriv(c[0], c[1], c[2], c[3], fx[1]);
-            b0[u] = cr_value(dc[0], dc[1], dc[2], dc[3], fx[1]);
-        }
-        V = cr_value(a[0], a[1], a[2], a[3], fx[2]);
-        dV[0] = cr_value(b0[0], b0[1], b0[2], b0[3], fx[2]) / P.dcv[0];
-        dV[1] = cr_value(da[0], da[1], da[2], da[3], fx[2]) / P.dcv[1];
-        dV[2] = cr_deriv(a[0], a[1], a[2], a[3], fx[2]) / P.dcv[2];
-        if (isnan(dV[0]) || isnan(dV[1]) || isnan(dV[2])) dV[0] = dV[1] = dV[2] = 0.0;
+// from a loaded stencil, with the stencil rows spread over threads (all
+// threads of the block call it): rows along dimension 0 first, then the
+// combination along dimensions 1 and 2 (tensor product, dimension 0 inner).
+// Ends synchronised.
+__device__ void grid_value_block(const BiasPlan &P, const double *S, const double *fx, double (*row)[16],
+                                 double *V, double *dV) {
+    const int nrow = P.D == 1 ? 1 : (P.D == 2 ? 4 : 16);
+    if (threadIdx.x < nrow) {
+        const double *p = S + 4 * threadIdx.x;
+        row[0][threadIdx.x] = cr_value(p[0], p[1], p[2], p[3], fx[0]);
+        row[1][threadIdx.x] = cr_deriv(p[0], p[1], p[2], p[3], fx[0]);
     }
-    return V;
+    __syncthreads();
+    if (P.D == 3 && threadIdx.x < 4) {
+        const int u = threadIdx.x;
+        const double *c = row[0] + 4 * u, *dc = row[1] + 4 * u;
+        const double a = cr_value(c[0], c[1], c[2], c[3], fx[1]);
+        const double da = cr_deriv(c[0], c[1], c[2], c[3], fx[1]);
+        const double b0 = cr_value(dc[0], dc[1], dc[2], dc[3], fx[1]);
+        row[2][u] = a;
+        row[2][4 + u] = da;
+        row[2][8 + u] = b0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (P.D == 1) {
+            *V = row[0][0];
+            dV[0] = row[1][0] / P.dcv[0];
+            if (isnan(dV[0])) dV[0] = 0.0;
+        } else if (P.D == 2) {
+            const double *col = row[0], *dcol = row[1];
+            *V = cr_value(col[0], col[1], col[2], col[3], fx[1]);
+            dV[0] = cr_value(dcol[0], dcol[1], dcol[2], dcol[3], fx[1]) / P.dcv[0];
+            dV[1] = cr_deriv(col[0], col[1], col[2], col[3], fx[1]) / P.dcv[1];
+            if (isnan(dV[0]) || isnan(dV[1])) { dV[0] = 0.0; dV[1] = 0.0; }
+        } else {
+            const double *a = row[2], *da = row[2] + 4, *b0 = row[2] + 8;
+            *V = cr_value(a[0], a[1], a[2], a[3], fx[2]);
+            dV[0] = cr_value(b0[0], b0[1], b0[2], b0[3], fx[2]) / P.dcv[0];
+            dV[1] = cr_value(da[0], da[1], da[2], da[3], fx[2]) / P.dcv[1];
+            dV[2] = cr_deriv(a[0], a[1], a[2], a[3], fx[2]) / P.dcv[2];
+            if (isnan(dV[0]) || isnan(dV[1]) || isnan(dV[2])) dV[0] = dV[1] = dV[2] = 0.0;
+        }
+    }
+    __syncthreads();
 }
 
 // Band of a hill: [c - R, c + R] clipped to the grid, c = (int)((s - lo)/dcv)
@@ -185,61 +191,90 @@ __device__ double eval_code(const ExprInstr *code, int n, const double *sym, int
     return st[0].v;
 }
 
-// The plan is a __grid_constant__ kernel parameter (about 4.5 KB, within the
-// 32 KB parameter limit): thread 0's many reads of it are constant-bank reads
-// and no copy into shared memory is needed.
-__global__ void __launch_bounds__(256) k_bias_step(const __grid_constant__ BiasPlan P, long long step) {
+// The plan (a few KB in device memory) is staged in shared memory by all
+// threads at once, together with the first partial-sum loads: thread 0's
+// serial sections then read shared memory only.
+__global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    {
+        static_assert(sizeof(BiasPlan) % 16 == 0, "plan size");
+        const double2 *src = reinterpret_cast<const double2 *>(Pp);
+        double2 *dst = reinterpret_cast<double2 *>(plan_raw);
+        for (int e = threadIdx.x; e < (int)(sizeof(BiasPlan) / 16); e += blockDim.x) dst[e] = src[e];
+        __syncthreads();
+    }
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
     __shared__ double smem[8 * 32];
     __shared__ double usum[kMaxUnits][8];
     __shared__ double sv[kMaxDim];
     __shared__ double hill_w;
     __shared__ int do_dep;
     __shared__ double sten[64];
-    // 1. deterministic reductions of every unit's block partials
+    // 1. deterministic reductions of every unit's block partials: rows of 8
+    //    doubles read as two 32-byte vectors, four rows in flight per thread
     for (int u = 0; u < P.nunit; ++u) {
         const UnitPlan &U = P.unit[u];
         double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (U.partials) {
+        if (U.partials && U.pstride != 8) {
             for (int b = threadIdx.x; b < U.nparts; b += blockDim.x)
                 for (int t = 0; t < U.nvals && t < 8; ++t) v[t] += U.partials[(size_t)b * U.pstride + t];
+        } else if (U.partials) {
+            const double4 *rows = reinterpret_cast<const double4 *>(U.partials);
+            const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+            for (int b0 = 0; b0 < U.nparts; b0 += 4 * blockDim.x) {
+                double4 r[8];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int b = b0 + threadIdx.x + q * blockDim.x;
+                    r[2 * q] = b < U.nparts ? rows[2 * (size_t)b] : zero;
+                    r[2 * q + 1] = b < U.nparts ? rows[2 * (size_t)b + 1] : zero;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    v[0] += r[2 * q].x; v[1] += r[2 * q].y; v[2] += r[2 * q].z; v[3] += r[2 * q].w;
+                    v[4] += r[2 * q + 1].x; v[5] += r[2 * q + 1].y; v[6] += r[2 * q + 1].z; v[7] += r[2 * q + 1].w;
+                }
+            }
         }
         block_sum<8>(v, smem);
         if (threadIdx.x == 0)
-            for (int t = 0; t < 8; ++t) usum[u][t] = v[t];
+            for (int t = 0; t < 8; ++t) usum[u][t] = t < U.nvals ? v[t] : 0.0;
         __syncthreads();
     }
-    double jac[kMaxDim][kMaxSymbols];
-    if (threadIdx.x == 0) {
-        // 2. symbol values
-        double sym[kMaxSymbols];
-        for (int q = 0; q < P.nsym; ++q) {
-            const SymPlan &S = P.sym[q];
-            const double *us = usum[S.unit];
-            double v = 0.0;
-            switch (S.kind) {
-            case SYM_Q_AVE: v = us[3] > 0 ? us[0] / us[3] : 0.0; break;
-            case SYM_Q_SW: v = us[1 + S.slot]; break;
-            case SYM_L_MEAN: v = us[2 * S.slot + 1] != 0.0 ? us[2 * S.slot] / us[2 * S.slot + 1] : 0.0; break;
-            case SYM_L_NSOLID: v = us[2 * S.slot + 1]; break;
-            case SYM_L_FRAC: v = us[4] > 0 ? us[2 * S.slot + 1] / us[4] : 0.0; break;
-            case SYM_SF_AVE: v = us[2] > 0 ? us[0] / us[2] : 0.0; break;
-            case SYM_SF_COUNT: v = us[1]; break;
-            case SYM_SK_AVE: {
-                const UnitPlan &U = P.unit[S.unit];
-                const double N = *U.sk_n;
-                double acc = 0.0;
-                for (int k = 0; k < U.K; ++k) acc += U.rho[2 * k] * U.rho[2 * k] + U.rho[2 * k + 1] * U.rho[2 * k + 1];
-                v = (N > 0 && U.K > 0) ? acc / N / U.K : 0.0;
-                break;
-            }
-            }
-            sym[q] = v;
-            P.out[kOutSymOffset + q] = v;
+    __shared__ double s_sym[kMaxSymbols], s_jac[kMaxDim][kMaxSymbols], s_alpha[kMaxSymbols];
+    __shared__ double s_dV[kMaxDim], s_V;
+    __shared__ double s_row[3][16];
+    // 2. symbol values, one thread per symbol
+    if (threadIdx.x < P.nsym) {
+        const int q = threadIdx.x;
+        const SymPlan &S = P.sym[q];
+        const double *us = usum[S.unit];
+        double v = 0.0;
+        switch (S.kind) {
+        case SYM_Q_AVE: v = us[3] > 0 ? us[0] / us[3] : 0.0; break;
+        case SYM_Q_SW: v = us[1 + S.slot]; break;
+        case SYM_L_MEAN: v = us[2 * S.slot + 1] != 0.0 ? us[2 * S.slot] / us[2 * S.slot + 1] : 0.0; break;
+        case SYM_L_NSOLID: v = us[2 * S.slot + 1]; break;
+        case SYM_L_FRAC: v = us[4] > 0 ? us[2 * S.slot + 1] / us[4] : 0.0; break;
+        case SYM_SF_AVE: v = us[2] > 0 ? us[0] / us[2] : 0.0; break;
+        case SYM_SF_COUNT: v = us[1]; break;
+        case SYM_SK_AVE: {
+            const UnitPlan &U = P.unit[S.unit];
+            const double N = *U.sk_n;
+            double acc = 0.0;
+            for (int k = 0; k < U.K; ++k) acc += U.rho[2 * k] * U.rho[2 * k] + U.rho[2 * k + 1] * U.rho[2 * k + 1];
+            v = (N > 0 && U.K > 0) ? acc / N / U.K : 0.0;
+            break;
         }
-        // 3. DIM expressions with exact chain factors
-        for (int dd = 0; dd < P.D; ++dd) sv[dd] = eval_code(P.code[dd], P.ncode[dd], sym, P.nsym, jac[dd]);
-        do_dep = (P.pace != 0) && (step % P.pace == 0);
+        }
+        s_sym[q] = v;
+        P.out[kOutSymOffset + q] = v;
     }
+    __syncthreads();
+    // 3. DIM expressions with exact chain factors, one thread per dimension
+    if (threadIdx.x < P.D) sv[threadIdx.x] = eval_code(P.code[threadIdx.x], P.ncode[threadIdx.x], s_sym, P.nsym,
+                                                        s_jac[threadIdx.x]);
+    if (threadIdx.x == 0) do_dep = (P.pace != 0) && (step % P.pace == 0);
     __syncthreads();
     int ix[3] = {1, 1, 1};
     double fx[3] = {0, 0, 0};
@@ -248,11 +283,8 @@ __global__ void __launch_bounds__(256) k_bias_step(const __grid_constant__ BiasP
     __syncthreads();
     // 4. well-tempered height from V(s) before the deposit
     if (do_dep) {
-        if (threadIdx.x == 0) {
-            double dV[kMaxDim];
-            const double Vb = P.wt ? grid_value(P, sten, fx, dV) : 0.0;
-            hill_w = P.h0 * exp(-(Vb) / (P.temp * P.kb * (P.biasf - 1.0)));
-        }
+        if (P.wt) grid_value_block(P, sten, fx, s_row, &s_V, s_dV);
+        if (threadIdx.x == 0) hill_w = P.h0 * exp(-(P.wt ? s_V : 0.0) / (P.temp * P.kb * (P.biasf - 1.0)));
         __syncthreads();
         // 5. banded deposit, one thread per band bin; the stencil takes the same
         //    increment as the grid (same operands, same rounding), so V and
@@ -296,56 +328,59 @@ __global__ void __launch_bounds__(256) k_bias_step(const __grid_constant__ BiasP
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        // 6. V and dV/ds at s after the deposit, chain rule to every symbol
-        double dV[kMaxDim] = {0, 0, 0, 0};
-        const double V = grid_value(P, sten, fx, dV);
-        double alpha[kMaxSymbols];
-        for (int q = 0; q < P.nsym; ++q) {
-            double a = 0.0;
-            for (int dd = 0; dd < P.D; ++dd) a += dV[dd] * jac[dd][q];
-            alpha[q] = a;
-        }
+    // 6. V and dV/ds at s after the deposit, chain rule to every symbol
+    grid_value_block(P, sten, fx, s_row, &s_V, s_dV);
+    if (threadIdx.x < P.nsym) {
+        const int q = threadIdx.x;
+        double a = 0.0;
+        for (int dd = 0; dd < P.D; ++dd) a += s_dV[dd] * s_jac[dd][q];
+        s_alpha[q] = a;
+    }
+    if (threadIdx.x == 32) {
         for (int dd = 0; dd < P.D; ++dd) P.out[dd] = sv[dd];
-        P.out[P.D] = V;
+        P.out[P.D] = s_V;
         P.out[P.D + 1] = do_dep ? 1.0 : 0.0;
-        // 7. per-unit force coefficients
-        for (int u = 0; u < P.nunit; ++u) {
-            const UnitPlan &U = P.unit[u];
-            const double *us = usum[u];
+    }
+    __syncthreads();
+    // 7. per-unit force coefficients: one thread per (unit, l slot)
+    if (threadIdx.x < 2 * P.nunit) {
+        const int u = threadIdx.x >> 1, slot = threadIdx.x & 1;
+        const UnitPlan &U = P.unit[u];
+        const double *us = usum[u];
+        if (U.kind == 1) {   // STEINH L: c1 = aM/W, c2 = -aM cv/W + aN + aF/max(N,1) per order
+            double aM = 0, aN = 0, aF = 0;
+            for (int q = 0; q < P.nsym; ++q) {
+                if (P.sym[q].unit != u || P.sym[q].slot != slot) continue;
+                if (P.sym[q].kind == SYM_L_MEAN) aM += s_alpha[q];
+                if (P.sym[q].kind == SYM_L_NSOLID) aN += s_alpha[q];
+                if (P.sym[q].kind == SYM_L_FRAC) aF += s_alpha[q];
+            }
+            const double S1 = us[2 * slot], S0 = us[2 * slot + 1], N = us[4];
+            const double W = fmax(S0, 1e-300);
+            const double cv = S0 != 0.0 ? S1 / S0 : 0.0;
+            U.coef[2 * slot] = aM / W;
+            U.coef[2 * slot + 1] = -aM * cv / W + aN + aF / fmax(N, 1.0);
+            if (slot == 0)
+                for (int t = 4; t < 8; ++t) U.coef[t] = 0.0;
+        } else if (slot == 0) {
             double c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            if (U.kind == 1) {   // STEINH L: c1 = aM/W, c2 = -aM cv/W + aN + aF/max(N,1) per order
-                for (int slot = 0; slot < 2; ++slot) {
-                    double aM = 0, aN = 0, aF = 0;
-                    for (int q = 0; q < P.nsym; ++q) {
-                        if (P.sym[q].unit != u || P.sym[q].slot != slot) continue;
-                        if (P.sym[q].kind == SYM_L_MEAN) aM += alpha[q];
-                        if (P.sym[q].kind == SYM_L_NSOLID) aN += alpha[q];
-                        if (P.sym[q].kind == SYM_L_FRAC) aF += alpha[q];
-                    }
-                    const double S1 = us[2 * slot], S0 = us[2 * slot + 1], N = us[4];
-                    const double W = fmax(S0, 1e-300);
-                    const double cv = S0 != 0.0 ? S1 / S0 : 0.0;
-                    c[2 * slot] = aM / W;
-                    c[2 * slot + 1] = -aM * cv / W + aN + aF / fmax(N, 1.0);
-                }
-            } else if (U.kind == 0) {   // STEINH Q: c_ave = a/N, c_sw = a
+            if (U.kind == 0) {   // STEINH Q: c_ave = a/N, c_sw = a
                 for (int q = 0; q < P.nsym; ++q) {
                     if (P.sym[q].unit != u) continue;
-                    if (P.sym[q].kind == SYM_Q_AVE) c[0] += us[3] > 0 ? alpha[q] / us[3] : 0.0;
-                    if (P.sym[q].kind == SYM_Q_SW) c[1 + P.sym[q].slot] += alpha[q];
+                    if (P.sym[q].kind == SYM_Q_AVE) c[0] += us[3] > 0 ? s_alpha[q] / us[3] : 0.0;
+                    if (P.sym[q].kind == SYM_Q_SW) c[1 + P.sym[q].slot] += s_alpha[q];
                 }
             } else if (U.kind == 2) {   // STRU_FACTOR: c_ave = a/N, c_count = a
                 for (int q = 0; q < P.nsym; ++q) {
                     if (P.sym[q].unit != u) continue;
-                    if (P.sym[q].kind == SYM_SF_AVE) c[0] += us[2] > 0 ? alpha[q] / us[2] : 0.0;
-                    if (P.sym[q].kind == SYM_SF_COUNT) c[1] += alpha[q];
+                    if (P.sym[q].kind == SYM_SF_AVE) c[0] += us[2] > 0 ? s_alpha[q] / us[2] : 0.0;
+                    if (P.sym[q].kind == SYM_SF_COUNT) c[1] += s_alpha[q];
                 }
             } else {   // S(k): 2 a / (N K)
                 const double N = U.sk_n ? *U.sk_n : 0.0;
                 for (int q = 0; q < P.nsym; ++q)
                     if (P.sym[q].unit == u && P.sym[q].kind == SYM_SK_AVE && N > 0 && U.K > 0)
-                        c[0] += 2.0 * alpha[q] / (N * U.K);
+                        c[0] += 2.0 * s_alpha[q] / (N * U.K);
             }
             for (int t = 0; t < 8; ++t) U.coef[t] = c[t];
         }
@@ -386,8 +421,8 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 
 }  // namespace
 
-void launch_bias_step(const BiasPlan &plan, long long step, cudaStream_t st) {
-    k_bias_step<<<1, 256, 0, st>>>(plan, step);
+void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st) {
+    k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
     prof_mark("bias_step", st);
 }
 

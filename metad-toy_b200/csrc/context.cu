@@ -641,7 +641,7 @@ void run_units(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, 
             c->launches += 2;
         }
     }
-    launch_bias_step(c->plan, step, st);
+    launch_bias_step(c->d_plan, step, st);
     c->launches += 1;
     // forces: the first unit reads f_in, the later ones accumulate into f_out
     bool first = true;

@@ -246,7 +246,7 @@ struct BiasPlan {
 };
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
 
-void launch_bias_step(const BiasPlan &plan, long long step, cudaStream_t st);
+void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st);
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st);
 
