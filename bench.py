@@ -198,6 +198,109 @@ def run_reference(args, rank):
     return 0
 
 
+def secondary_workload(name):
+    """The parity configs timed on request (`--workload sk|q`); the default
+    workload above is the one the headline metric is quoted on."""
+    import systems
+    if name == "sk":
+        x, L = systems.config3()
+        args = ["GAUSSIAN", 0.05, 0.005, 10.0, "PACE", 10,
+                "CAL", "NAME", "SK", "STRU_FACTOR_K", "all", "nk", 96, "kmag", systems.KMAG_111, "seed", 3,
+                "SYMBOL", "v1", "SK.AVE", "CV_dim", 1, "DIM", 1, 0.0, 10.0, 2000, "v1", "WT", 0]
+        desc = ("1,048,576-atom jittered FCC (a 5.26 A, sigma 0.2 A), k-vector S(k) over 96 directions on "
+                "|k| = 2 pi sqrt(3)/a with forces, 1D 2000-bin grid, PACE 10")
+        seeds = [(11, 0.2), (12, 0.2)]
+    else:
+        x, L = systems.config1()
+        x = systems.jitter(x, 0.15, 2024)
+        args = ["GAUSSIAN", 0.01, 0.005, 10.0, "PACE", 10,
+                "CAL", "NAME", "Q6", "STEINH", "Q", 6, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18,
+                "SYMBOL", "v1", "Q6.AVE", "CV_dim", 1, "DIM", 1, 0.0, 1.0, 1000, "v1", "WT", 0]
+        desc = "4,000-atom FCC (a 5.26 A, jitter 0.15 A), STEINH Q 6 cutoff 3.9 cap 18 with forces, 1D 1000-bin grid"
+        seeds = [(21, 0.15), (22, 0.15)]
+    base = systems.fcc(64, 5.26) if name == "sk" else systems.config1()[0]
+    xs = [x] + [np.ascontiguousarray(systems.wrap(systems.jitter(base, sg, sd), L)) for sd, sg in seeds]
+    xs = [np.ascontiguousarray(systems.wrap(v, L)) for v in xs]
+    return args, xs, L, desc
+
+
+def run_secondary(args, local):
+    import torch
+    import mtd
+    torch.cuda.set_device(local)
+    fa, xs, L, desc = secondary_workload(args.workload)
+    n = xs[0].shape[0]
+    prec = "fp64" if args.workload == "q" else args.precision
+    m = mtd.Metad(fa, precision=prec, device=local)
+    m.set_box([0, 0, 0], L)
+    m.init()
+    stream = torch.cuda.current_stream()
+    m.set_stream(stream.cuda_stream)
+    dx = [torch.from_numpy(x).cuda() for x in xs]
+    f = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    step = 0
+    for _ in range(args.warmup):
+        m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
+        step += 1
+    m.sync()
+    m.profile(True)
+    for _ in range(max(5, args.steps // 3)):
+        flush.zero_()
+        m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
+        step += 1
+    m.sync()
+    prof = m.profile_report()
+    m.profile(False)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    hx = [torch.from_numpy(x).pin_memory() for x in xs]
+    hf = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    with ClockSampler(local) as clk:
+        t_end = time.perf_counter() + 0.6
+        while time.perf_counter() < t_end:
+            m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
+            step += 1
+            m.sync()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
+            ev[k][1].record(stream)
+            step += 1
+        m.sync()
+        torch.cuda.synchronize()
+        dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+        m.set_stream(0)
+        e2e_s = 0.0
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            hf.zero_()
+            t0 = time.perf_counter()
+            m.post_force(step, hx[step % len(hx)].numpy(), hf.numpy())
+            e2e_s += time.perf_counter() - t0
+            step += 1
+    launches = m.launch_count()
+    kernels = {k: v[1] / max(v[0], 1) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+    line = {"metric": "CV+bias+force atom-steps/s", "workload": args.workload,
+            "value": n * args.steps / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "dtype": "f32" if prec == "mixed" else "f64", "data": "synthetic (seeded)",
+            "config": {"workload": desc, "atoms": n, "precision": prec,
+                       "l2": "flushed (256 MB write) before each timed step", "cv": [float(v) for v in m.cv]},
+            "e2e": {"value": n * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
+                    "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_s * 1e3 / args.steps},
+            "gpu_launches": launches * args.steps, "kernels_ms_per_step": kernels, "clocks": clk.summary()}
+    if args.workload == "sk":
+        pairs = n * 96
+        ms = {k: v for k, v in kernels.items()}
+        line["sk_pairs_per_s"] = {k: pairs / (v / 1e3) for k, v in ms.items() if k.startswith("sk_") and v > 0}
+    print(json.dumps(line))
+    m.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,6 +309,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="local", choices=["local", "sk", "q"],
+                    help="local: the headline 256k-atom STEINH L workload; sk: 1M-atom k-vector S(k); "
+                         "q: 4,000-atom STEINH Q (FP64)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -213,6 +319,8 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank)
     args.warmup = max(args.warmup, 3)
+    if args.workload != "local":
+        return run_secondary(args, local)
 
     import torch
     import mtd

@@ -163,4 +163,28 @@ __device__ __forceinline__ void unpack_image(int img, int &ix, int &iy, int &iz)
     iy = ((img >> 10) & 1023) - 512;
     iz = (img >> 20) - 512;
 }
+// sin and cos of an FP64 phase for the mixed-precision k-vector sums: the
+// phase is reduced in FP64 by the nearest multiple of pi/2 (quadrant q), the
+// remainder |r| <= pi/4 goes to FP32, and sin r, cos r come from their Taylor
+// series to degree 9 and 10 (remainders below 2e-9 and 2e-10 on |r| <= pi/4,
+// under the FP32 rounding of the result), rotated back by the quadrant.
+__device__ __forceinline__ void phase_sincos_f32(double ph, float &s, float &c) {
+    const double n = rint(ph * 0.63661977236758134308);                 // 2 / pi
+    const float r = (float)fma(-n, 1.5707963267948966192, ph);          // pi / 2
+    const int q = (int)(long long)n & 3;
+    const float r2 = r * r;
+    float sp = fmaf(r2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+    sp = fmaf(sp, r2, 1.0f / 120.0f);
+    sp = fmaf(sp, r2, -1.0f / 6.0f);
+    const float s0 = fmaf(sp * r2, r, r);
+    float cp = fmaf(r2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
+    cp = fmaf(cp, r2, -1.0f / 720.0f);
+    cp = fmaf(cp, r2, 1.0f / 24.0f);
+    cp = fmaf(cp, r2, -0.5f);
+    const float c0 = fmaf(cp, r2, 1.0f);
+    const float ss = (q & 1) ? c0 : s0, cc = (q & 1) ? s0 : c0;
+    s = (q & 2) ? -ss : ss;
+    c = ((q + 1) & 2) ? -cc : cc;
+}
+
 }  // namespace mtd

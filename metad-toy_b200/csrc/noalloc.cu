@@ -28,21 +28,17 @@ constexpr int kNaScratchDoubles = 1 << 17;           // 1 MiB of block partials
 constexpr int kNaMaxBlocks = 148 * 4;                // partial-sum grid when the scratch allows
 constexpr int kNaMaxDevices = 64;
 constexpr int kNaChunk = 8;                          // reals per register tile (4 k-vectors)
-constexpr double kNaTwoPi = 6.283185307179586476925286766559;
-constexpr double kNaInvTwoPi = 0.15915494309189533576888376337251;
 
 static __device__ __align__(256) double g_na_scratch[kNaScratchDoubles];
 
-// FP64: sincos of the FP64 phase.  Mixed: FP64 phase reduced to [-pi, pi] by
-// a rounded multiple of 2 pi, then FP32 sincosf.
+// FP64: sincos of the FP64 phase.  Mixed: FP64 quadrant reduction, FP32
+// series (phase_sincos_f32, the context's S(k) arithmetic).
 template <bool FP64> __device__ __forceinline__ void na_sincos(double ph, double &s, double &c) {
     if (FP64) {
         sincos(ph, &s, &c);
     } else {
-        const double m = rint(ph * kNaInvTwoPi);
-        const float r = (float)fma(-m, kNaTwoPi, ph);
         float sf, cf;
-        sincosf(r, &sf, &cf);
+        phase_sincos_f32(ph, sf, cf);
         s = sf;
         c = cf;
     }

@@ -127,26 +127,22 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
 }
 
 // ------------------------------------------------------------------ S(k)
-constexpr int kSkChunk = 8;        // k-vectors per register tile
+constexpr int kSkChunk = 16;       // reals per register tile (8 k-vectors per pass over the atoms)
 constexpr int kSkBlocks = 148 * 8;  // grid for the partial sums (8 blocks per SM)
-constexpr double kTwoPi = 6.283185307179586476925286766559;
-constexpr double kInvTwoPi = 0.15915494309189533576888376337251;
 
 template <bool FP64> __device__ __forceinline__ void phase_sincos(double ph, double &s, double &c) {
     if (FP64) {
         sincos(ph, &s, &c);
     } else {
-        const double n = rint(ph * kInvTwoPi);
-        const float r = (float)fma(-n, kTwoPi, ph);
         float sf, cf;
-        sincosf(r, &sf, &cf);
+        phase_sincos_f32(ph, sf, cf);
         s = sf;
         c = cf;
     }
 }
 
 template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
-    __shared__ double smem[8 * 32];
+    __shared__ double smem[kSkChunk * 32];
     __shared__ double kk[3 * 1024];
     for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
     __syncthreads();

@@ -59,6 +59,25 @@ def test_kvector_structure_factor(precision):
     assert H.rel(f, -dV[0] * o["grad"]) < tf
 
 
+def test_kvector_structure_factor_full_size():
+    """1,048,576 atoms, 96 k-vectors on the first FCC Bragg shell: mixed mode
+    against the FP64 oracle (S 1e-5, forces 1e-4 of the largest component)."""
+    x, L = systems.config3()
+    kvec = systems.kvectors(96, systems.KMAG_111, 3)
+    args = ["GAUSSIAN", 0.05, 0.005, 10.0, "PACE", 10,
+            "CAL", "NAME", "SK", "STRU_FACTOR_K", "all", "nk", 96, "kmag", systems.KMAG_111, "seed", 3,
+            "SYMBOL", "v1", "SK.AVE", "CV_dim", 1, "DIM", 1, 0.0, 10.0, 2000, "v1", "WT", 0]
+    m, out = H.run_gpu(args, x, L, [(0, x)], precision="mixed")
+    o = O.sk(x, kvec)
+    g = O.Grid([[0.0, 10.0]], [2000], 0.05, 0.005, 10.0, 300.0, 8.617343e-5, False)
+    g.add_hill([o["cv"]])
+    V, dV = g.value([o["cv"]])
+    cv, bias, f, _ = out[0]
+    assert H.rel(cv[0], o["cv"]) < 1e-5
+    assert H.rel(bias, V) < 1e-5
+    assert H.rel(f, -dV[0] * o["grad"]) < 1e-4
+
+
 def test_grid_many_steps_matches_oracle():
     """C1 protocol on 30 steps: jittered FCC re-drawn every step, PACE 10, WT 1;
     the whole 1000-bin grid is compared after the run."""
