@@ -184,6 +184,63 @@ int mtd_abi_version(void);
 mtd_status mtd_sk_noalloc(int n, const double *d_x, const int *d_mask, int groupbit, int nk, const double *d_k,
                           int precision, double *d_rho, double *d_s, void *stream, char *err, int errlen);
 
+/* ---------------------------------------------------------------- learned bias
+ * V_theta(s) for CV_dim >= 3, where the grid blows up: an MLP D -> 128 -> 128
+ * -> 1 (SiLU, BF16 weights, FP32 accumulation, the 128 x 128 layer and its
+ * backward contractions on the tensor cores), trained on the device on the
+ * FP64 hill sum of the hills deposited so far.  The exact sum stays the judge
+ * of its error (mtd_nnbias_validate) and the fallback (use_nn = -1 below).
+ * No counterpart in the reference, whose only bias representations are the
+ * grids (src/grids/GH_t0_uniformGrid.cu, src/grids/GH_t1_sparseGrid.cu).
+ * Hills are isotropic Gaussians h exp(-|s - c|^2 / (2 sigma^2)).  Inputs are
+ * normalised over the box [lo, hi]; calls on one object are not thread-safe. */
+typedef struct mtd_nnbias mtd_nnbias;
+
+/* 1 <= D <= 4; He-initialised weights from seed.  *out is set even on failure. */
+mtd_status mtd_nnbias_create(int D, const double *lo, const double *hi, unsigned long long seed, mtd_nnbias **out);
+void mtd_nnbias_destroy(mtd_nnbias *nb);
+const char *mtd_nnbias_last_error(const mtd_nnbias *nb);
+
+/* Appends n hills: centres (n*D), heights (n), widths (n). */
+mtd_status mtd_nnbias_add_hills(mtd_nnbias *nb, int n, const double *centers, const double *heights,
+                                const double *sigmas);
+int mtd_nnbias_num_hills(const mtd_nnbias *nb);
+
+/* Exact FP64 hill sum V (npts) and dV/ds (npts*D, may be NULL) at host points (npts*D). */
+mtd_status mtd_nnbias_exact(mtd_nnbias *nb, int npts, const double *pts, double *V, double *dV);
+
+/* The network's V and dV/ds at host points, batched on the tensor cores. */
+mtd_status mtd_nnbias_eval(mtd_nnbias *nb, int npts, const double *pts, double *V, double *dV);
+
+/* Fit: ntrain sampled points (half near hill centres, half uniform in the box)
+ * with exact targets, iters Adam steps (lr, cosine decay over the second half)
+ * on minibatches of `batch`; final_loss = mean squared error in V units^2. */
+mtd_status mtd_nnbias_fit(mtd_nnbias *nb, int ntrain, int iters, int batch, double lr, unsigned long long seed,
+                          double *final_loss);
+
+/* max and RMS of |V_theta - V_exact| on npts sampled points; the network
+ * becomes usable (mtd_nnbias_usable) when max <= tol. */
+mtd_status mtd_nnbias_validate(mtd_nnbias *nb, int npts, unsigned long long seed, double tol, double *max_err,
+                               double *rms_err);
+int mtd_nnbias_usable(const mtd_nnbias *nb);
+
+/* Bias at one device-resident point (D doubles) into d_V (1) and d_dV (D),
+ * enqueued on `stream` (cudaStream_t, NULL = the object's stream):
+ * use_nn = 1 network, 0 exact sum, -1 network if the last validation passed
+ * else the exact sum.  One call in flight per object. */
+mtd_status mtd_nnbias_point_device(mtd_nnbias *nb, const double *d_s, double *d_V, double *d_dV, int use_nn,
+                                   void *stream);
+
+/* Checks: the FP32 master parameters (17,281 floats: W1[128][4], b1[128],
+ * W2[128][128], b2[128], w3[128], b3), the output scale, and one gradient of
+ * the mean squared error sum_i (V_theta(s_i)/vscale - t_i/vscale)^2 / npts on
+ * given points and targets, without an update. */
+mtd_status mtd_nnbias_get_params(mtd_nnbias *nb, float *out);
+mtd_status mtd_nnbias_set_params(mtd_nnbias *nb, const float *in, double vscale);
+double mtd_nnbias_vscale(const mtd_nnbias *nb);
+mtd_status mtd_nnbias_loss_grad(mtd_nnbias *nb, int npts, const double *pts, const double *targets, double vscale,
+                                float *grad, double *loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,7 +31,11 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
            "mtd_extract_peratom", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
            "mtd_set_stream", "mtd_profile_enable", "mtd_profile_report",
-           "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc"]
+           "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc",
+           "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
+           "mtd_nnbias_num_hills", "mtd_nnbias_exact", "mtd_nnbias_eval", "mtd_nnbias_fit", "mtd_nnbias_validate",
+           "mtd_nnbias_usable", "mtd_nnbias_point_device", "mtd_nnbias_get_params", "mtd_nnbias_set_params",
+           "mtd_nnbias_vscale", "mtd_nnbias_loss_grad"]
 
 
 class MetadError(RuntimeError):
@@ -88,6 +92,23 @@ def lib():
         L.mtd_profile_report.argtypes = [vp, C.c_char_p, C.c_int]
         L.mtd_parse_args.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.c_char_p, C.c_int]
         L.mtd_eval_expression.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, dp, dp]
+        L.mtd_nnbias_create.argtypes = [C.c_int, dp, dp, C.c_uint64, C.POINTER(vp)]
+        L.mtd_nnbias_destroy.argtypes = [vp]
+        L.mtd_nnbias_last_error.argtypes = [vp]
+        L.mtd_nnbias_last_error.restype = C.c_char_p
+        L.mtd_nnbias_add_hills.argtypes = [vp, C.c_int, dp, dp, dp]
+        L.mtd_nnbias_num_hills.argtypes = [vp]
+        L.mtd_nnbias_exact.argtypes = [vp, C.c_int, dp, dp, dp]
+        L.mtd_nnbias_eval.argtypes = [vp, C.c_int, dp, dp, dp]
+        L.mtd_nnbias_fit.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64, dp]
+        L.mtd_nnbias_validate.argtypes = [vp, C.c_int, C.c_uint64, C.c_double, dp, dp]
+        L.mtd_nnbias_usable.argtypes = [vp]
+        L.mtd_nnbias_point_device.argtypes = [vp, vp, vp, vp, C.c_int, vp]
+        L.mtd_nnbias_get_params.argtypes = [vp, C.POINTER(C.c_float)]
+        L.mtd_nnbias_set_params.argtypes = [vp, C.POINTER(C.c_float), C.c_double]
+        L.mtd_nnbias_vscale.argtypes = [vp]
+        L.mtd_nnbias_vscale.restype = C.c_double
+        L.mtd_nnbias_loss_grad.argtypes = [vp, C.c_int, dp, dp, C.c_double, C.POINTER(C.c_float), dp]
         L.mtd_sk_noalloc.argtypes = [C.c_int, vp, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, C.c_char_p,
                                      C.c_int]
         _lib = L
@@ -263,3 +284,108 @@ class Metad:
             name, calls, ms = line.split()
             out[name] = (int(calls), float(ms))
         return out
+
+
+NN_PARAMS = 17281
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class NNBias:
+    """Learned bias V_theta(s) (MLP D -> 128 -> 128 -> 1, BF16 weights, trained
+    on the device on the FP64 hill sum, which stays its judge and fallback)."""
+
+    def __init__(self, lo, hi, seed=1):
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        hi = np.ascontiguousarray(hi, dtype=np.float64)
+        self.D = lo.shape[0]
+        h = C.c_void_p()
+        st = lib().mtd_nnbias_create(self.D, _dp(lo), _dp(hi), int(seed), C.byref(h))
+        self._h = h
+        if st != 0:
+            msg = lib().mtd_nnbias_last_error(h).decode() if h else ""
+            lib().mtd_nnbias_destroy(h)
+            self._h = None
+            raise MetadError(st, msg)
+
+    def _check(self, st):
+        if st != 0:
+            raise MetadError(st, lib().mtd_nnbias_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            lib().mtd_nnbias_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_hills(self, centers, heights, sigmas):
+        c = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, self.D)
+        h = np.ascontiguousarray(heights, dtype=np.float64).reshape(-1)
+        s = np.ascontiguousarray(sigmas, dtype=np.float64).reshape(-1)
+        self._check(lib().mtd_nnbias_add_hills(self._h, c.shape[0], _dp(c), _dp(h), _dp(s)))
+
+    @property
+    def num_hills(self):
+        return lib().mtd_nnbias_num_hills(self._h)
+
+    def exact(self, pts):
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, self.D)
+        V = np.zeros(p.shape[0])
+        dV = np.zeros_like(p)
+        self._check(lib().mtd_nnbias_exact(self._h, p.shape[0], _dp(p), _dp(V), _dp(dV)))
+        return V, dV
+
+    def eval(self, pts):
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, self.D)
+        V = np.zeros(p.shape[0])
+        dV = np.zeros_like(p)
+        self._check(lib().mtd_nnbias_eval(self._h, p.shape[0], _dp(p), _dp(V), _dp(dV)))
+        return V, dV
+
+    def fit(self, ntrain=262144, iters=2000, batch=4096, lr=2e-3, seed=1):
+        loss = C.c_double()
+        self._check(lib().mtd_nnbias_fit(self._h, int(ntrain), int(iters), int(batch), float(lr), int(seed),
+                                         C.byref(loss)))
+        return loss.value
+
+    def validate(self, npts=65536, seed=7, tol=1e-3):
+        mx, rms = C.c_double(), C.c_double()
+        self._check(lib().mtd_nnbias_validate(self._h, int(npts), int(seed), float(tol), C.byref(mx), C.byref(rms)))
+        return mx.value, rms.value
+
+    @property
+    def usable(self):
+        return bool(lib().mtd_nnbias_usable(self._h))
+
+    def point_device(self, s_ptr, v_ptr, dv_ptr, use_nn=-1, stream=0):
+        self._check(lib().mtd_nnbias_point_device(self._h, C.c_void_p(s_ptr), C.c_void_p(v_ptr),
+                                                  C.c_void_p(dv_ptr), int(use_nn), C.c_void_p(stream or None)))
+
+    def get_params(self):
+        w = np.zeros(NN_PARAMS, dtype=np.float32)
+        self._check(lib().mtd_nnbias_get_params(self._h, w.ctypes.data_as(C.POINTER(C.c_float))))
+        return w
+
+    def set_params(self, w, vscale):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(lib().mtd_nnbias_set_params(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), float(vscale)))
+
+    @property
+    def vscale(self):
+        return lib().mtd_nnbias_vscale(self._h)
+
+    def loss_grad(self, pts, targets, vscale):
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, self.D)
+        t = np.ascontiguousarray(targets, dtype=np.float64)
+        g = np.zeros(NN_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        self._check(lib().mtd_nnbias_loss_grad(self._h, p.shape[0], _dp(p), _dp(t), float(vscale),
+                                               g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
+        return g, loss.value

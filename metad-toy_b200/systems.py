@@ -166,3 +166,23 @@ def small_slab(seed=7, nxy=5, nz_fcc=2, nz_bcc=3, n_liq=200):
     crystal = np.concatenate([fcc_x, bcc_x])
     liq = hardcore_liquid(n_liq, z1, z1 + thick, L, 3.0, seed, fixed=crystal)
     return wrap(np.concatenate([crystal, liq]), L), L
+
+
+CV4_LO = np.array([0.20, 0.35, 0.0, 0.05])
+CV4_HI = np.array([0.45, 0.60, 1.0, 0.35])
+
+
+def cv4_hills(n=20000, seed=5, sigma=0.02, height=0.005):
+    """Hill centres of a seeded 4D CV trajectory (Q4.AVE, Q6.AVE, local-Q6
+    fraction, S(k)): an Ornstein-Uhlenbeck walk reflected into CV4_LO..CV4_HI,
+    one hill per PACE, steps of 0.35 sigma per dimension."""
+    rng = np.random.default_rng(seed)
+    span = CV4_HI - CV4_LO
+    x = CV4_LO + 0.5 * span
+    c = np.zeros((n, 4))
+    for i in range(n):
+        x = x + 0.35 * sigma * rng.standard_normal(4) - 0.002 * (x - (CV4_LO + 0.5 * span))
+        x = np.where(x < CV4_LO, 2 * CV4_LO - x, x)
+        x = np.where(x > CV4_HI, 2 * CV4_HI - x, x)
+        c[i] = x
+    return c, np.full(n, height), np.full(n, sigma)
