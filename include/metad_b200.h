@@ -184,6 +184,43 @@ int mtd_abi_version(void);
 mtd_status mtd_sk_noalloc(int n, const double *d_x, const int *d_mask, int groupbit, int nk, const double *d_k,
                           int precision, double *d_rho, double *d_s, void *stream, char *err, int errlen);
 
+/* ---------------------------------------------------------------- multiple walkers
+ * nwalk replicas (uneven atom counts, own boxes) that share one bias grid.
+ * Every walker is a context built from the same `fix metad` arguments; one
+ * step computes all walkers' CVs concurrently, deposits their hills in walker
+ * order with WT heights taken from the grid as it stood at the start of the
+ * step, then evaluates every walker's V, dV/ds and forces on the updated grid.
+ * One HILLS file for the group (rows in walker order per deposit step).
+ * No counterpart in the reference (one walker per `fix metad`); the deposit
+ * rule is GH_t0_uniformGrid::add_hill (src/grids/GH_t0_uniformGrid.cu:195-208)
+ * applied to each walker's hill in turn.  METAD_RESTART is not replayed for a
+ * group. */
+typedef struct mtd_walkers mtd_walkers;
+
+mtd_status mtd_walkers_create(int nwalk, int narg, const char *const *arg, const mtd_options *opt,
+                              mtd_walkers **out);
+void mtd_walkers_destroy(mtd_walkers *W);
+const char *mtd_walkers_last_error(const mtd_walkers *W);
+int mtd_walkers_count(const mtd_walkers *W);
+mtd_status mtd_walkers_set_box(mtd_walkers *W, int k, const double lo[3], const double hi[3], const int periodic[3]);
+mtd_status mtd_walkers_init(mtd_walkers *W);
+
+/* Capture the step in a CUDA graph (one graph launch per MD step once the
+ * atom counts and array pointers repeat); 0 = plain launches. */
+mtd_status mtd_walkers_enable_graph(mtd_walkers *W, int enable);
+
+/* One MD step on device arrays: d_x[k] (n[k] x 3 FP64, caller order) and
+ * d_f[k] updated in place (f -= dV/dx).  Asynchronous; mtd_walkers_sync
+ * collects outputs and device errors (a neighbour overflow grows the lists and
+ * asks for the step to be repeated). */
+mtd_status mtd_walkers_step_device(mtd_walkers *W, int64_t step, const int *n, const double *const *d_x,
+                                   double *const *d_f);
+mtd_status mtd_walkers_sync(mtd_walkers *W);
+double mtd_walkers_cv(const mtd_walkers *W, int k, int d);
+double mtd_walkers_bias(const mtd_walkers *W, int k);
+mtd_status mtd_walkers_get_grid(mtd_walkers *W, double *out, int64_t count);
+int mtd_walkers_last_launch_count(const mtd_walkers *W);
+
 /* ---------------------------------------------------------------- learned bias
  * V_theta(s) for CV_dim >= 3, where the grid blows up: an MLP D -> 128 -> 128
  * -> 1 (SiLU, BF16 weights, FP32 accumulation, the 128 x 128 layer and its

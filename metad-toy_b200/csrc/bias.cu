@@ -191,27 +191,24 @@ __device__ double eval_code(const ExprInstr *code, int n, const double *sym, int
     return st[0].v;
 }
 
-// The plan (a few KB in device memory) is staged in shared memory by all
-// threads at once, together with the first partial-sum loads: thread 0's
-// serial sections then read shared memory only.
-__global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
-    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
-    {
-        static_assert(sizeof(BiasPlan) % 16 == 0, "plan size");
-        const double2 *src = reinterpret_cast<const double2 *>(Pp);
-        double2 *dst = reinterpret_cast<double2 *>(plan_raw);
-        for (int e = threadIdx.x; e < (int)(sizeof(BiasPlan) / 16); e += blockDim.x) dst[e] = src[e];
-        __syncthreads();
-    }
-    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
-    __shared__ double smem[8 * 32];
-    __shared__ double usum[kMaxUnits][8];
-    __shared__ double sv[kMaxDim];
-    __shared__ double hill_w;
-    __shared__ int do_dep;
-    __shared__ double sten[64];
-    // 1. deterministic reductions of every unit's block partials: rows of 8
-    //    doubles read as two 32-byte vectors, four rows in flight per thread
+// ------------------------------------------------------------------ bias phases
+// The per-step work is written as phases over one block of 256 threads so the
+// single-context kernel and the multi-walker kernels share it.
+
+// The plan (a few KB in device memory) staged in shared memory by all threads.
+__device__ __forceinline__ void stage_plan(const BiasPlan *__restrict__ Pp, unsigned char *plan_raw) {
+    static_assert(sizeof(BiasPlan) % 16 == 0, "plan size");
+    const double2 *src = reinterpret_cast<const double2 *>(Pp);
+    double2 *dst = reinterpret_cast<double2 *>(plan_raw);
+    for (int e = threadIdx.x; e < (int)(sizeof(BiasPlan) / 16); e += blockDim.x) dst[e] = src[e];
+    __syncthreads();
+}
+
+// Phases 1-3: deterministic reductions of every unit's block partials (rows
+// of 8 doubles, four rows in flight per thread), symbol values (one thread
+// each), DIM expressions with exact chain factors (one thread per dimension).
+__device__ void phase_cvs(const BiasPlan &P, double *smem, double (*usum)[8], double *s_sym,
+                          double (*s_jac)[kMaxSymbols], double *sv) {
     for (int u = 0; u < P.nunit; ++u) {
         const UnitPlan &U = P.unit[u];
         double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -241,10 +238,6 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
             for (int t = 0; t < 8; ++t) usum[u][t] = t < U.nvals ? v[t] : 0.0;
         __syncthreads();
     }
-    __shared__ double s_sym[kMaxSymbols], s_jac[kMaxDim][kMaxSymbols], s_alpha[kMaxSymbols];
-    __shared__ double s_dV[kMaxDim], s_V;
-    __shared__ double s_row[3][16];
-    // 2. symbol values, one thread per symbol
     if (threadIdx.x < P.nsym) {
         const int q = threadIdx.x;
         const SymPlan &S = P.sym[q];
@@ -271,65 +264,69 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
         P.out[kOutSymOffset + q] = v;
     }
     __syncthreads();
-    // 3. DIM expressions with exact chain factors, one thread per dimension
     if (threadIdx.x < P.D) sv[threadIdx.x] = eval_code(P.code[threadIdx.x], P.ncode[threadIdx.x], s_sym, P.nsym,
                                                         s_jac[threadIdx.x]);
-    if (threadIdx.x == 0) do_dep = (P.pace != 0) && (step % P.pace == 0);
     __syncthreads();
-    int ix[3] = {1, 1, 1};
-    double fx[3] = {0, 0, 0};
-    stencil_locate(P, sv, ix, fx);
-    stencil_load(P, ix, sten);   // grid around s before this step's deposit
-    __syncthreads();
-    // 4. well-tempered height from V(s) before the deposit
-    if (do_dep) {
-        if (P.wt) grid_value_block(P, sten, fx, s_row, &s_V, s_dV);
-        if (threadIdx.x == 0) hill_w = P.h0 * exp(-(P.wt ? s_V : 0.0) / (P.temp * P.kb * (P.biasf - 1.0)));
-        __syncthreads();
-        // 5. banded deposit, one thread per band bin; the stencil takes the same
-        //    increment as the grid (same operands, same rounding), so V and
-        //    dV/ds after the deposit need no second grid read
-        int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
-        int total = 0;
-        if (hill_band(P, sv, lo, hi)) {
-            total = 1;
-            for (int k = 0; k < P.D; ++k) {
-                ext[k] = hi[k] - lo[k] + 1;
-                total *= ext[k];
-            }
+}
+
+// Phase 4: well-tempered height from V(s) on the stencil before the deposit.
+__device__ double phase_wt_height(const BiasPlan &P, const double *sten, const double *fx, double (*row)[16],
+                                  double *s_V, double *s_dV) {
+    if (P.wt) grid_value_block(P, sten, fx, row, s_V, s_dV);
+    return P.h0 * exp(-(P.wt ? *s_V : 0.0) / (P.temp * P.kb * (P.biasf - 1.0)));
+}
+
+// Phase 5: banded deposit of one hill, one thread per band bin; the stencil
+// (when given) takes the same increment as the grid (same operands, same
+// rounding), so V and dV/ds after the deposit need no second grid read.
+__device__ void phase_deposit(const BiasPlan &P, const double *s, double w, const int *ix, double *sten) {
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
+    int total = 0;
+    if (hill_band(P, s, lo, hi)) {
+        total = 1;
+        for (int k = 0; k < P.D; ++k) {
+            ext[k] = hi[k] - lo[k] + 1;
+            total *= ext[k];
         }
-        for (int t = threadIdx.x; t < total; t += blockDim.x) {
-            int idx[3] = {0, 0, 0}, rem = t;
-            for (int k = P.D - 1; k >= 0; --k) {
-                idx[k] = lo[k] + rem % ext[k];
-                rem /= ext[k];
-            }
-            size_t g = idx[0];
-            for (int k = 1; k < P.D; ++k) g = g * P.nbin[k] + idx[k];
-            if (g < (size_t)P.grid_size) P.grid[g] += hill_w * hill_gauss(P, sv, idx, P.sigma);
-        }
-        const int nst = P.D == 1 ? 4 : (P.D == 2 ? 16 : 64);
-        if (total > 0 && threadIdx.x < nst) {
-            const int e = threadIdx.x;
-            const int idx[3] = {ix[0] - 1 + (e & 3), ix[1] - 1 + ((e >> 2) & 3), ix[2] - 1 + (e >> 4)};
-            bool in = true;
-            for (int k = 0; k < P.D; ++k) in = in && idx[k] >= lo[k] && idx[k] <= hi[k];
-            if (in) sten[e] += hill_w * hill_gauss(P, sv, idx, P.sigma);
-        }
-        if (threadIdx.x == 0) {
-            unsigned long long h = *P.nhills;
-            HillRec r;
-            r.step = step;
-            for (int k = 0; k < 3; ++k) r.s[k] = k < P.D ? sv[k] : 0.0;
-            r.w = hill_w;
-            r.sigma = P.sigma;
-            P.hills[h % (unsigned long long)P.hill_cap] = r;
-            *P.nhills = h + 1;
-        }
-        __syncthreads();
     }
-    // 6. V and dV/ds at s after the deposit, chain rule to every symbol
-    grid_value_block(P, sten, fx, s_row, &s_V, s_dV);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int idx[3] = {0, 0, 0}, rem = t;
+        for (int k = P.D - 1; k >= 0; --k) {
+            idx[k] = lo[k] + rem % ext[k];
+            rem /= ext[k];
+        }
+        size_t g = idx[0];
+        for (int k = 1; k < P.D; ++k) g = g * P.nbin[k] + idx[k];
+        if (g < (size_t)P.grid_size) P.grid[g] += w * hill_gauss(P, s, idx, P.sigma);
+    }
+    const int nst = P.D == 1 ? 4 : (P.D == 2 ? 16 : 64);
+    if (sten && total > 0 && threadIdx.x < nst) {
+        const int e = threadIdx.x;
+        const int idx[3] = {ix[0] - 1 + (e & 3), ix[1] - 1 + ((e >> 2) & 3), ix[2] - 1 + (e >> 4)};
+        bool in = true;
+        for (int k = 0; k < P.D; ++k) in = in && idx[k] >= lo[k] && idx[k] <= hi[k];
+        if (in) sten[e] += w * hill_gauss(P, s, idx, P.sigma);
+    }
+}
+
+__device__ __forceinline__ void record_hill(const BiasPlan &P, long long step, const double *s, double w) {
+    const unsigned long long h = *P.nhills;
+    HillRec r;
+    r.step = step;
+    for (int k = 0; k < 3; ++k) r.s[k] = k < P.D ? s[k] : 0.0;
+    r.w = w;
+    r.sigma = P.sigma;
+    P.hills[h % (unsigned long long)P.hill_cap] = r;
+    *P.nhills = h + 1;
+}
+
+// Phases 6-7: V and dV/ds on the (post-deposit) stencil, chain rule to every
+// symbol, outputs, and the per-unit force coefficients (one thread per unit and
+// l slot).
+__device__ void phase_coef(const BiasPlan &P, const double *sten, const double *fx, const double *sv,
+                           const double (*s_jac)[kMaxSymbols], const double (*usum)[8], int dep, double (*row)[16],
+                           double *s_V, double *s_dV, double *s_alpha) {
+    grid_value_block(P, sten, fx, row, s_V, s_dV);
     if (threadIdx.x < P.nsym) {
         const int q = threadIdx.x;
         double a = 0.0;
@@ -338,11 +335,10 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
     }
     if (threadIdx.x == 32) {
         for (int dd = 0; dd < P.D; ++dd) P.out[dd] = sv[dd];
-        P.out[P.D] = s_V;
-        P.out[P.D + 1] = do_dep ? 1.0 : 0.0;
+        P.out[P.D] = *s_V;
+        P.out[P.D + 1] = dep ? 1.0 : 0.0;
     }
     __syncthreads();
-    // 7. per-unit force coefficients: one thread per (unit, l slot)
     if (threadIdx.x < 2 * P.nunit) {
         const int u = threadIdx.x >> 1, slot = threadIdx.x & 1;
         const UnitPlan &U = P.unit[u];
@@ -387,6 +383,105 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
     }
 }
 
+struct BiasShared {
+    double smem[8 * 32];
+    double usum[kMaxUnits][8];
+    double sv[kMaxDim];
+    double sten[64];
+    double s_sym[kMaxSymbols], s_jac[kMaxDim][kMaxSymbols], s_alpha[kMaxSymbols];
+    double s_dV[kMaxDim], s_V;
+    double row[3][16];
+};
+
+// One context, one step: all phases in one block.
+__global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ BiasShared S;
+    stage_plan(Pp, plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    phase_cvs(P, S.smem, S.usum, S.s_sym, S.s_jac, S.sv);
+    const int dep = (P.pace != 0) && (step % P.pace == 0);
+    int ix[3] = {1, 1, 1};
+    double fx[3] = {0, 0, 0};
+    stencil_locate(P, S.sv, ix, fx);
+    stencil_load(P, ix, S.sten);   // grid around s before this step's deposit
+    __syncthreads();
+    if (dep) {
+        const double w = phase_wt_height(P, S.sten, fx, S.row, &S.s_V, S.s_dV);
+        phase_deposit(P, S.sv, w, ix, S.sten);
+        if (threadIdx.x == 0) record_hill(P, step, S.sv, w);
+        __syncthreads();
+    }
+    phase_coef(P, S.sten, fx, S.sv, S.s_jac, S.usum, dep, S.row, &S.s_V, S.s_dV, S.s_alpha);
+}
+
+// ------------------------------------------------------------------ multiple walkers
+// W walkers share one grid.  A: per walker (one block each) the CV values and,
+// on a deposit step, the WT height from the grid as it stands at the start of
+// the step.  B: the W hills deposited in walker order (one block; every bin
+// receives its increments in walker order).  C: per walker V, dV/ds on the
+// updated grid and the force coefficients.  The step is read from device
+// memory so the three launches can sit in a CUDA graph.
+__global__ void __launch_bounds__(256) k_walk_cvs(const BiasPlan *const *__restrict__ plans,
+                                                  const long long *__restrict__ d_step, WalkState *ws) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ BiasShared S;
+    stage_plan(plans[blockIdx.x], plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    const long long step = *d_step;
+    phase_cvs(P, S.smem, S.usum, S.s_sym, S.s_jac, S.sv);
+    const int dep = (P.pace != 0) && (step % P.pace == 0);
+    WalkState &W = ws[blockIdx.x];
+    if (dep) {
+        int ix[3] = {1, 1, 1};
+        double fx[3] = {0, 0, 0};
+        stencil_locate(P, S.sv, ix, fx);
+        stencil_load(P, ix, S.sten);
+        __syncthreads();
+        const double w = phase_wt_height(P, S.sten, fx, S.row, &S.s_V, S.s_dV);
+        if (threadIdx.x == 0) W.hill_w = w;
+    }
+    for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) W.usum[e / 8][e % 8] = S.usum[e / 8][e % 8];
+    for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
+        W.jac[e / kMaxSymbols][e % kMaxSymbols] = S.s_jac[e / kMaxSymbols][e % kMaxSymbols];
+    if (threadIdx.x < kMaxDim) W.s[threadIdx.x] = threadIdx.x < P.D ? S.sv[threadIdx.x] : 0.0;
+    if (threadIdx.x == 0) W.dep = dep;
+}
+
+__global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__restrict__ plans, int nwalk,
+                                                      const long long *__restrict__ d_step, const WalkState *ws) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    stage_plan(plans[0], plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    if (!ws[0].dep) return;   // every walker shares PACE
+    const long long step = *d_step;
+    int ix[3] = {1, 1, 1};
+    for (int w = 0; w < nwalk; ++w) {
+        phase_deposit(P, ws[w].s, ws[w].hill_w, ix, nullptr);
+        if (threadIdx.x == 0) record_hill(P, step, ws[w].s, ws[w].hill_w);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__restrict__ plans, const WalkState *ws) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ BiasShared S;
+    stage_plan(plans[blockIdx.x], plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    const WalkState &W = ws[blockIdx.x];
+    for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) S.usum[e / 8][e % 8] = W.usum[e / 8][e % 8];
+    for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
+        S.s_jac[e / kMaxSymbols][e % kMaxSymbols] = W.jac[e / kMaxSymbols][e % kMaxSymbols];
+    if (threadIdx.x < kMaxDim) S.sv[threadIdx.x] = W.s[threadIdx.x];
+    __syncthreads();
+    int ix[3] = {1, 1, 1};
+    double fx[3] = {0, 0, 0};
+    stencil_locate(P, S.sv, ix, fx);
+    stencil_load(P, ix, S.sten);
+    __syncthreads();
+    phase_coef(P, S.sten, fx, S.sv, S.s_jac, S.usum, W.dep, S.row, &S.s_V, S.s_dV, S.s_alpha);
+}
+
 // HILLS replay: every thread owns grid bins and adds the hills in file order,
 // so the FP64 sum order per bin is the file order.
 __global__ void k_hills_replay(const BiasPlan *__restrict__ Pp, const HillRec *__restrict__ h, int nh, int ncell) {
@@ -424,6 +519,14 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st) {
     k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
     prof_mark("bias_step", st);
+}
+
+void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
+                      cudaStream_t st) {
+    k_walk_cvs<<<nwalk, 256, 0, st>>>(d_plans, d_step, ws);
+    k_walk_deposit<<<1, 256, 0, st>>>(d_plans, nwalk, d_step, ws);
+    k_walk_coef<<<nwalk, 256, 0, st>>>(d_plans, ws);
+    prof_mark("walk_bias", st);
 }
 
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st) {

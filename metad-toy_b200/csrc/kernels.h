@@ -247,6 +247,17 @@ struct BiasPlan {
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st);
+
+// Per-walker state handed between the multi-walker bias kernels.
+struct WalkState {
+    double s[kMaxDim];
+    double hill_w;
+    int dep, pad;
+    double jac[kMaxDim][kMaxSymbols];
+    double usum[kMaxUnits][8];
+};
+void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
+                      cudaStream_t st);
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st);
 

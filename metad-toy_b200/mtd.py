@@ -35,7 +35,11 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
            "mtd_nnbias_num_hills", "mtd_nnbias_exact", "mtd_nnbias_eval", "mtd_nnbias_fit", "mtd_nnbias_validate",
            "mtd_nnbias_usable", "mtd_nnbias_point_device", "mtd_nnbias_get_params", "mtd_nnbias_set_params",
-           "mtd_nnbias_vscale", "mtd_nnbias_loss_grad"]
+           "mtd_nnbias_vscale", "mtd_nnbias_loss_grad",
+           "mtd_walkers_create", "mtd_walkers_destroy", "mtd_walkers_last_error", "mtd_walkers_count",
+           "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
+           "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
+           "mtd_walkers_last_launch_count"]
 
 
 class MetadError(RuntimeError):
@@ -92,6 +96,22 @@ def lib():
         L.mtd_profile_report.argtypes = [vp, C.c_char_p, C.c_int]
         L.mtd_parse_args.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.c_char_p, C.c_int]
         L.mtd_eval_expression.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, dp, dp]
+        L.mtd_walkers_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.POINTER(vp)]
+        L.mtd_walkers_destroy.argtypes = [vp]
+        L.mtd_walkers_last_error.argtypes = [vp]
+        L.mtd_walkers_last_error.restype = C.c_char_p
+        L.mtd_walkers_count.argtypes = [vp]
+        L.mtd_walkers_set_box.argtypes = [vp, C.c_int, dp, dp, ip]
+        L.mtd_walkers_init.argtypes = [vp]
+        L.mtd_walkers_enable_graph.argtypes = [vp, C.c_int]
+        L.mtd_walkers_step_device.argtypes = [vp, C.c_int64, ip, C.POINTER(vp), C.POINTER(vp)]
+        L.mtd_walkers_sync.argtypes = [vp]
+        L.mtd_walkers_cv.argtypes = [vp, C.c_int, C.c_int]
+        L.mtd_walkers_cv.restype = C.c_double
+        L.mtd_walkers_bias.argtypes = [vp, C.c_int]
+        L.mtd_walkers_bias.restype = C.c_double
+        L.mtd_walkers_get_grid.argtypes = [vp, dp, C.c_int64]
+        L.mtd_walkers_last_launch_count.argtypes = [vp]
         L.mtd_nnbias_create.argtypes = [C.c_int, dp, dp, C.c_uint64, C.POINTER(vp)]
         L.mtd_nnbias_destroy.argtypes = [vp]
         L.mtd_nnbias_last_error.argtypes = [vp]
@@ -389,3 +409,72 @@ class NNBias:
         self._check(lib().mtd_nnbias_loss_grad(self._h, p.shape[0], _dp(p), _dp(t), float(vscale),
                                                g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
         return g, loss.value
+
+
+class Walkers:
+    """nwalk walkers sharing one bias grid (mtd_walkers_*); every walker is a
+    context built from the same `fix metad` arguments."""
+
+    def __init__(self, nwalk, args, precision="mixed", device=0, groups=None, hills_path="", work_dir=None):
+        opt, self._keep = _options(precision, device, groups=groups, hills_path=hills_path, work_dir=work_dir)
+        toks = [str(a).encode() for a in args]
+        argv = (C.c_char_p * max(1, len(toks)))(*toks)
+        h = C.c_void_p()
+        st = lib().mtd_walkers_create(int(nwalk), len(toks), argv, C.byref(opt), C.byref(h))
+        self._h = h
+        self.n = int(nwalk)
+        if st != 0:
+            msg = lib().mtd_walkers_last_error(h).decode() if h else ""
+            lib().mtd_walkers_destroy(h)
+            self._h = None
+            raise MetadError(st, msg)
+
+    def _check(self, st):
+        if st != 0:
+            raise MetadError(st, lib().mtd_walkers_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            lib().mtd_walkers_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_box(self, k, lo, hi, periodic=(1, 1, 1)):
+        lo = np.ascontiguousarray(lo, dtype=np.float64)
+        hi = np.ascontiguousarray(hi, dtype=np.float64)
+        per = (C.c_int * 3)(*[int(p) for p in periodic])
+        self._check(lib().mtd_walkers_set_box(self._h, int(k), _dp(lo), _dp(hi), per))
+
+    def init(self):
+        self._check(lib().mtd_walkers_init(self._h))
+
+    def enable_graph(self, on=True):
+        self._check(lib().mtd_walkers_enable_graph(self._h, 1 if on else 0))
+
+    def step_device(self, step, ns, x_ptrs, f_ptrs):
+        n = (C.c_int * self.n)(*[int(v) for v in ns])
+        xp = (C.c_void_p * self.n)(*[int(p) for p in x_ptrs])
+        fp = (C.c_void_p * self.n)(*[int(p) for p in f_ptrs])
+        self._check(lib().mtd_walkers_step_device(self._h, int(step), n, xp, fp))
+
+    def sync(self):
+        self._check(lib().mtd_walkers_sync(self._h))
+
+    def cv(self, k, dim):
+        return np.array([lib().mtd_walkers_cv(self._h, int(k), d) for d in range(dim)])
+
+    def bias(self, k):
+        return lib().mtd_walkers_bias(self._h, int(k))
+
+    def grid(self, size):
+        out = np.zeros(size)
+        self._check(lib().mtd_walkers_get_grid(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), int(size)))
+        return out
+
+    def launch_count(self):
+        return lib().mtd_walkers_last_launch_count(self._h)

@@ -1,0 +1,89 @@
+"""Multiple walkers sharing one grid (mtd_walkers_*), through the C ABI, against
+the FP64 oracle: every walker's CVs from its own atoms, WT heights from the
+grid as it stood at the start of the step, hills deposited in walker order,
+V and dV/ds on the updated grid, forces.  FP64 mode: 1e-9 relative on CVs and
+bias, 1e-8 on forces.  The CUDA-graph path must reproduce the plain launches
+bit for bit."""
+import numpy as np
+import pytest
+
+import helpers as H
+import mtd
+import oracle as O
+import systems
+
+pytestmark = pytest.mark.gpu
+
+
+def _walker_systems():
+    out = []
+    for k, (nxy, nzf, nzb, nliq) in enumerate([(5, 2, 3, 120), (6, 3, 4, 300), (5, 3, 2, 200)]):
+        x, L = systems.small_slab(seed=20 + k, nxy=nxy, nz_fcc=nzf, nz_bcc=nzb, n_liq=nliq)
+        out.append((np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.05, 30 + k), L)), L))
+    return out
+
+
+def _run(args, syss, steps, graph, hills_path=""):
+    import torch
+
+    W = mtd.Walkers(len(syss), args, precision="fp64", hills_path=hills_path)
+    for k, (x, L) in enumerate(syss):
+        W.set_box(k, [0, 0, 0], L)
+    W.init()
+    W.enable_graph(graph)
+    dx = [torch.from_numpy(x).cuda() for x, _ in syss]
+    df = [torch.zeros_like(v) for v in dx]
+    out = []
+    for step in steps:
+        for v in df:
+            v.zero_()
+        W.step_device(step, [x.shape[0] for x, _ in syss], [v.data_ptr() for v in dx], [v.data_ptr() for v in df])
+        W.sync()
+        out.append([(W.cv(k, 2), W.bias(k), df[k].cpu().numpy()) for k in range(len(syss))])
+    grid = W.grid(200 * 200)
+    W.close()
+    return out, grid
+
+
+def test_walkers_match_oracle_synchronous_deposit():
+    syss = _walker_systems()
+    steps = [0, 1, 2, 3]
+    out, grid = _run(H.fix_args_local(pace=2), syss, steps, graph=False)
+    ref = [(H.oracle_local(x, L, 4), H.oracle_local(x, L, 6)) for x, L in syss]
+    g = O.Grid([[0, 1], [0, 1]], [200, 200], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    s = [[o4["cv"], o6["cv"]] for o4, o6 in ref]
+    for i, step in enumerate(steps):
+        if step % 2 == 0:
+            heights = [0.005 * np.exp(-g.value(sw)[0] / (300.0 * 8.617343e-5 * 8.0)) for sw in s]
+            for sw, w in zip(s, heights):
+                g.deposit(sw, w)
+        for k, (o4, o6) in enumerate(ref):
+            V, dV = g.value(s[k])
+            cv, bias, f = out[i][k]
+            assert H.rel(cv, s[k]) < 1e-9
+            assert H.rel(bias, V) < 1e-9
+            assert H.rel(f, -(dV[0] * o4["grad"] + dV[1] * o6["grad"])) < 1e-8
+    assert H.rel(grid, g.grid) < 1e-12
+
+
+def test_walkers_graph_replay_is_bitwise_identical():
+    syss = _walker_systems()
+    steps = list(range(6))
+    plain, g1 = _run(H.fix_args_local(pace=2), syss, steps, graph=False)
+    graph, g2 = _run(H.fix_args_local(pace=2), syss, steps, graph=True)
+    for a, b in zip(plain, graph):
+        for (cv1, b1, f1), (cv2, b2, f2) in zip(a, b):
+            assert np.array_equal(cv1, cv2) and b1 == b2 and np.array_equal(f1, f2)
+    assert np.array_equal(g1, g2)
+
+
+def test_walkers_hills_file_in_walker_order(tmp_path):
+    syss = _walker_systems()
+    path = str(tmp_path / "HILLS")
+    out, _ = _run(H.fix_args_local(pace=2), syss, range(4), graph=False, hills_path=path)
+    rows = [l.split() for l in open(path) if not l.startswith("#")]
+    assert len(rows) == 2 * len(syss)
+    for r, (step, k) in zip(rows, [(0, 0), (0, 1), (0, 2), (2, 0), (2, 1), (2, 2)]):
+        assert int(r[0]) == step
+        cv = out[step][k][0]
+        assert abs(float(r[1]) - cv[0]) < 1e-12 and abs(float(r[2]) - cv[1]) < 1e-12
