@@ -370,6 +370,66 @@ def run_nnbias(args, local):
     return 0
 
 
+def walker_args():
+    """The headline workload's CVs on a 256 x 256 WT grid (config of the
+    multi-walker case)."""
+    a = fix_args()
+    i = a.index("DIM")
+    return a[:i] + ["DIM", 1, 0, 1, 256, "v1", "DIM", 2, 0, 1, 256, "v2", "WT", 1]
+
+
+def run_walkers(args, local):
+    """32 walkers, atom counts drawn from U{2000..64000} (seeded), FCC / disordered
+    slabs, sharing one 2D WT grid; one MD step = every walker's CVs, the
+    synchronous deposit and every walker's forces."""
+    import torch
+    import mtd
+    import systems
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(44)
+    ns = rng.integers(2000, 64001, size=32)
+    syss = [systems.walker_system(int(n), 100 + k) for k, n in enumerate(ns)]
+    ns = [x.shape[0] for x, _ in syss]
+    res = {}
+    for graph in (False, True):
+        W = mtd.Walkers(len(syss), walker_args(), precision=args.precision)
+        for k, (x, L) in enumerate(syss):
+            W.set_box(k, [0, 0, 0], L)
+        W.init()
+        W.enable_graph(graph)
+        dx = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x, _ in syss]
+        df = [torch.zeros_like(v) for v in dx]
+        xp, fp = [v.data_ptr() for v in dx], [v.data_ptr() for v in df]
+        step = 0
+        for _ in range(max(3, args.warmup)):
+            W.step_device(step, ns, xp, fp)
+            W.sync()
+            step += 1
+        launches = W.launch_count()
+        stream = torch.cuda.current_stream()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            W.step_device(step, ns, xp, fp)
+            W.sync()
+            step += 1
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) / args.steps
+        res["graph" if graph else "plain"] = {"ms_per_step": wall * 1e3,
+                                              "atom_steps_per_s": sum(ns) / wall, "launches_per_step": launches}
+        cvs = [W.cv(k, 2).tolist() for k in range(3)]
+        W.close()
+    line = {"metric": "multi-walker CV+bias+force atom-steps/s (all walkers)", "workload": "walkers",
+            "value": res["graph"]["atom_steps_per_s"], "unit": UNIT, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "walkers": len(ns), "atoms_total": int(sum(ns)),
+            "atoms_min": int(min(ns)), "atoms_max": int(max(ns)), "precision": args.precision,
+            "timing": "host wall clock per step including the per-step synchronisation and output collection",
+            "graph": res["graph"], "plain": res["plain"], "cv_first_walkers": cvs,
+            "config": "STEINH L Q4+Q6 STEP 3.9 A, MEAN_SOLID, shared 2D 256x256 WT grid, PACE 10"}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,9 +438,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="local", choices=["local", "sk", "q", "nn"],
+    ap.add_argument("--workload", default="local", choices=["local", "sk", "q", "nn", "walkers"],
                     help="local: the headline 256k-atom STEINH L workload; sk: 1M-atom k-vector S(k); "
-                         "q: 4,000-atom STEINH Q (FP64); nn: learned 4D bias vs exact hill sum")
+                         "q: 4,000-atom STEINH Q (FP64); nn: learned 4D bias vs exact hill sum; "
+                         "walkers: 32 walkers sharing one grid")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -390,6 +451,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.workload == "nn":
         return run_nnbias(args, local)
+    if args.workload == "walkers":
+        return run_walkers(args, local)
     if args.workload != "local":
         return run_secondary(args, local)
 

@@ -186,3 +186,27 @@ def cv4_hills(n=20000, seed=5, sigma=0.02, height=0.005):
         x = np.where(x > CV4_HI, 2 * CV4_HI - x, x)
         c[i] = x
     return c, np.full(n, height), np.full(n, sigma)
+
+
+def walker_system(n, seed, a=5.26, nxy=6, rho_liq=0.021, jitter_liq=0.4, gap=1.0):
+    """n atoms: an FCC slab (nxy x nxy cells, a) holding about half of them and a
+    disordered slab at rho_liq (a simple-cubic lattice at that density with
+    N(0, jitter_liq) displacements) holding the rest, periodic box."""
+    rng = np.random.default_rng(seed)
+    Lxy = nxy * a
+    per_layer = 4 * nxy * nxy
+    nz = max(1, int(round(0.5 * n / per_layer)))
+    while nz > 1 and nz * per_layer > n - 64:
+        nz -= 1
+    crystal = lattice(nxy, nxy, nz, a, FCC_BASIS)
+    n_liq = n - crystal.shape[0]
+    z0 = nz * a + gap
+    spacing = (1.0 / rho_liq) ** (1.0 / 3.0)
+    m = max(1, int(round(Lxy / spacing)))
+    d = Lxy / m
+    nzl = int(math.ceil(n_liq / (m * m)))
+    g = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(nzl), indexing="ij"), -1).reshape(-1, 3)
+    g = g[np.lexsort((g[:, 0], g[:, 1], g[:, 2]))][:n_liq]
+    liq = (g + 0.5) * np.array([d, d, d]) + np.array([0.0, 0.0, z0]) + rng.normal(0.0, jitter_liq, (n_liq, 3))
+    L = np.array([Lxy, Lxy, z0 + nzl * d + gap])
+    return wrap(np.concatenate([crystal, liq]), L), L
