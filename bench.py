@@ -314,7 +314,7 @@ def run_nnbias(args, local):
     nb = mtd.NNBias(systems.CV4_LO, systems.CV4_HI, seed=3)
     nb.add_hills(c, h, sg)
     t0 = time.perf_counter()
-    nb.fit(ntrain=262144, iters=20000, batch=8192, lr=3e-3, seed=2)
+    nb.fit(ntrain=262144, iters=args.nn_iters, batch=8192, lr=3e-3, seed=2)
     fit_s = time.perf_counter() - t0
     mx, rms = nb.validate(npts=65536, seed=7, tol=1e-3)
     stream = torch.cuda.current_stream()
@@ -362,7 +362,7 @@ def run_nnbias(args, local):
             "batch_65536_points_s": {"exact": ex_s, "nn": nn_s},
             "hills": int(len(h)), "vmax_eV": nb.vscale, "max_abs_err_eV": mx, "rms_err_eV": rms,
             "tolerance_eV": 1e-3, "tolerance_met": bool(mx <= 1e-3), "fit_s": fit_s,
-            "fit": {"ntrain": 262144, "iters": 20000, "batch": 8192, "lr": 3e-3},
+            "fit": {"ntrain": 262144, "iters": args.nn_iters, "batch": 8192, "lr": 3e-3},
             "network": "4-128-128-1 SiLU, BF16 weights, FP32 accumulation (128x128 layer on tcgen05)",
             "params": 17281, "grid_equivalent_bytes": 8 * 200 ** 4, "steps": args.steps}
     print(json.dumps(line))
@@ -442,6 +442,7 @@ def main():
                     help="local: the headline 256k-atom STEINH L workload; sk: 1M-atom k-vector S(k); "
                          "q: 4,000-atom STEINH Q (FP64); nn: learned 4D bias vs exact hill sum; "
                          "walkers: 32 walkers sharing one grid")
+    ap.add_argument("--nn-iters", type=int, default=20000, help="Adam steps of the learned-bias fit (--workload nn)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
