@@ -133,6 +133,8 @@ struct mtd_ctx {
     CellGrid last_grid{};
     SysDev last_sys{};
     cudaStream_t own_st = nullptr;
+    cudaStream_t side_st = nullptr;      // host -> device force upload beside the CV passes
+    cudaEvent_t f_ready = nullptr;
     Prof prof;
     bool prof_created = false;
     std::map<std::string, std::pair<long long, double>> prof_total;
@@ -754,14 +756,17 @@ mtd_status enqueue_forces(mtd_ctx *c, long long step, const double *x, const int
     return MTD_OK;
 }
 
+// f_ready (may be null): an event the force kernels wait for (forces uploaded
+// on the side stream while the CV passes run).
 mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, const int *mask, const int *image,
-                        const double *fin, double *fout, bool virial) {
+                        const double *fin, double *fout, bool virial, cudaEvent_t f_ready = nullptr) {
     ProfScope prof_scope(c);
     c->launches = 0;
     mtd_status s = enqueue_values(c, n, x, mask, image);
     if (s != MTD_OK) return s;
     launch_bias_step(c->d_plan, step, c->st);
     c->launches += 1;
+    if (f_ready) MTD_CU(cudaStreamWaitEvent(c->st, f_ready, 0), "force upload");
     return enqueue_forces(c, step, x, mask, fin, fout, virial);
 }
 
@@ -952,6 +957,8 @@ mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, 
     }
     cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
     c->own_st = c->st;
+    cudaStreamCreateWithFlags(&c->side_st, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&c->f_ready, cudaEventDisableTiming);
     c->cv.assign(c->cfg.cv_dim, 0.0);
     mtd_status s = plan_units(c);
     if (s == MTD_OK) {
@@ -996,6 +1003,8 @@ void mtd_destroy(mtd_ctx *c) {
     if (c->h_vir) cudaFreeHost(c->h_vir);
     if (c->h_nhills) cudaFreeHost(c->h_nhills);
     if (c->own_st) cudaStreamDestroy(c->own_st);
+    if (c->side_st) cudaStreamDestroy(c->side_st);
+    if (c->f_ready) cudaEventDestroy(c->f_ready);
     if (c->prof_created)
         for (int i = 0; i < kProfMax; ++i) cudaEventDestroy(c->prof.ev[i]);
     if (c->f_hills) std::fclose(c->f_hills);
@@ -1075,14 +1084,19 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
     mtd_status s = ensure_capacity(c, n);
     if (s != MTD_OK) return s;
     const size_t b3 = sizeof(double) * 3 * (size_t)n;
+    // x (and mask) first on the step's stream; f (and image, read by the force
+    // kernels only) on the side stream, overlapping the CV passes
     MTD_CU(cudaMemcpyAsync(c->d_x, x, b3, cudaMemcpyHostToDevice, c->st), "x upload");
-    MTD_CU(cudaMemcpyAsync(c->d_fin, f, b3, cudaMemcpyHostToDevice, c->st), "f upload");
     if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
-    if (image && virial) MTD_CU(cudaMemcpyAsync(c->d_image, image, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "image upload");
+    MTD_CU(cudaEventRecord(c->f_ready, c->st), "force upload");   // the side copies start after the previous step
+    MTD_CU(cudaStreamWaitEvent(c->side_st, c->f_ready, 0), "force upload");
+    MTD_CU(cudaMemcpyAsync(c->d_fin, f, b3, cudaMemcpyHostToDevice, c->side_st), "f upload");
+    if (image && virial) MTD_CU(cudaMemcpyAsync(c->d_image, image, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->side_st), "image upload");
+    MTD_CU(cudaEventRecord(c->f_ready, c->side_st), "force upload");
     for (int attempt = 0; attempt < 4; ++attempt) {
         MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
         s = enqueue_step(c, step, n, c->d_x, mask ? c->d_mask : nullptr, (image && virial) ? c->d_image : nullptr,
-                         c->d_fin, c->d_fout, virial != nullptr);
+                         c->d_fin, c->d_fout, virial != nullptr, c->f_ready);
         if (s != MTD_OK) return s;
         MTD_CU(cudaStreamSynchronize(c->st), "step");
         if (c->h_status->overflow == 0) break;
