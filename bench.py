@@ -370,6 +370,22 @@ def run_nnbias(args, local):
     return 0
 
 
+def max_over_ranks(vals, dist, device):
+    """Timings (ms) reduced to their maximum over the ranks (the slowest replica
+    sets the job's time); identity without a process group."""
+    import torch
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def replica_throughput(n_atoms, steps, world, ms):
+    """Whole-job atom-steps/s: every rank runs its own replica of n_atoms for
+    `steps` steps (weak scaling, no data-path collective) within `ms`."""
+    return n_atoms * steps * world / (ms / 1e3)
+
+
 def walker_args():
     """The headline workload's CVs on a 256 x 256 WT grid (config of the
     multi-walker case)."""
@@ -545,13 +561,9 @@ def main():
             step += 1
     clocks = clk.summary()
 
-    t = torch.tensor([dev_ms, e2e_s * 1e3], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_ms, e2e_ms = float(t[0]), float(t[1])
-    total_atoms = n * args.steps * world
-    value = total_atoms / (dev_ms / 1e3)
-    e2e_value = total_atoms / (e2e_ms / 1e3)
+    dev_ms, e2e_ms = max_over_ranks([dev_ms, e2e_s * 1e3], dist, "cuda")
+    value, e2e_value = replica_throughput(n, args.steps, world, dev_ms), replica_throughput(n, args.steps, world,
+                                                                                           e2e_ms)
 
     # roofline of the dominant kernel
     peak, peak_kind = peaks()
