@@ -156,6 +156,12 @@ int mtd_profile_report(mtd_ctx *ctx, char *buf, int len);
 int mtd_max_neighbors(mtd_ctx *ctx, const char *name);
 
 const char *mtd_last_error(const mtd_ctx *ctx);
+
+/* Hill-list bias state of a context (CV_dim 4 or NN_BIAS 1): hills deposited,
+ * hills the learned bias was last fitted on, and whether that fit passed its
+ * validation (then V = network + exact sum over the hills since the fit; else
+ * the exact sum).  No counterpart in the reference. */
+mtd_status mtd_nn_state(const mtd_ctx *ctx, int *hills, int *hills_fitted, int *usable);
 int mtd_abi_version(void);
 
 /* k-vector structure factor of a group, computed with NO device allocation.

@@ -382,6 +382,23 @@ std::string parse_fix_args(int narg, const char *const *arg, const GroupTable &g
             if (!need_int(c, i + 1, v, "METAD_RESTART")) return c.err;
             cfg.restart = v != 0;
             i += 2;
+        } else if (!std::strcmp(kw, "NN_BIAS")) {   // extension: learned bias for CV_dim >= 3
+            int v = 0;
+            if (!need_int(c, i + 1, v, "NN_BIAS")) return c.err;
+            cfg.nn = v != 0;
+            i += 2;
+        } else if (!std::strcmp(kw, "NN_TOL")) {
+            if (!need_double(c, i + 1, cfg.nn_tol, "NN_TOL")) return c.err;
+            if (!(cfg.nn_tol > 0)) return "Error: NN_TOL must be > 0.";
+            i += 2;
+        } else if (!std::strcmp(kw, "NN_REFIT")) {
+            if (!need_int(c, i + 1, cfg.nn_refit, "NN_REFIT")) return c.err;
+            if (cfg.nn_refit < 1) return "Error: NN_REFIT must be >= 1.";
+            i += 2;
+        } else if (!std::strcmp(kw, "NN_ITERS")) {
+            if (!need_int(c, i + 1, cfg.nn_iters, "NN_ITERS")) return c.err;
+            if (cfg.nn_iters < 1) return "Error: NN_ITERS must be >= 1.";
+            i += 2;
         } else if (!std::strcmp(kw, "WT")) {
             int v = 0;
             if (!need_int(c, i + 1, v, "WT")) return c.err;
@@ -391,7 +408,7 @@ std::string parse_fix_args(int narg, const char *const *arg, const GroupTable &g
             return std::string("Error: Unknown keyword in fix metadynamics command: ") + kw;
         }
     }
-    if (cfg.cv_dim > 3) return "Only 1D-3D are supported for optimized grid.";
+    if (cfg.cv_dim > 4) return "Only 1D-3D are supported for optimized grid (4D with the hill-list bias).";
     if (!cfg.cv_dim_set) cfg.dims.assign(cfg.cv_dim, DimDef{});
     for (int d = 0; d < cfg.cv_dim; ++d)
         if (!cfg.dims[d].set) {

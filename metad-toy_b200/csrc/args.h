@@ -66,6 +66,12 @@ struct Config {
     int hill_type = 0;
     bool restart = false;
     bool wt = false;
+    // hill-list bias (no grid): CV_dim 4, or any CV_dim with NN_BIAS 1
+    bool nn = false;              // NN_BIAS 1: learned bias judged by, and falling back to, the exact hill sum
+    double nn_tol = 1e-3;         // NN_TOL: max |V_theta - V_exact| on validation points
+    int nn_refit = 1000;          // NN_REFIT: new hills between fits
+    int nn_iters = 2000;          // NN_ITERS: Adam steps per fit
+    bool hill_list() const { return nn || cv_dim > 3; }
     std::map<std::string, SwParams> sws;
     std::map<std::string, CalDef> cals;     // std::map: alphabetical order, as cal_registry
     std::vector<SymbolDef> symbols;

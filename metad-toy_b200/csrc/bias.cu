@@ -313,7 +313,7 @@ __device__ __forceinline__ void record_hill(const BiasPlan &P, long long step, c
     const unsigned long long h = *P.nhills;
     HillRec r;
     r.step = step;
-    for (int k = 0; k < 3; ++k) r.s[k] = k < P.D ? s[k] : 0.0;
+    for (int k = 0; k < kMaxDim; ++k) r.s[k] = k < P.D ? s[k] : 0.0;
     r.w = w;
     r.sigma = P.sigma;
     P.hills[h % (unsigned long long)P.hill_cap] = r;
@@ -323,10 +323,21 @@ __device__ __forceinline__ void record_hill(const BiasPlan &P, long long step, c
 // Phases 6-7: V and dV/ds on the (post-deposit) stencil, chain rule to every
 // symbol, outputs, and the per-unit force coefficients (one thread per unit and
 // l slot).
+__device__ void phase_coef_from_v(const BiasPlan &P, const double *sv, const double (*s_jac)[kMaxSymbols],
+                                  const double (*usum)[8], int dep, const double *s_V, const double *s_dV,
+                                  double *s_alpha);
+
 __device__ void phase_coef(const BiasPlan &P, const double *sten, const double *fx, const double *sv,
                            const double (*s_jac)[kMaxSymbols], const double (*usum)[8], int dep, double (*row)[16],
                            double *s_V, double *s_dV, double *s_alpha) {
     grid_value_block(P, sten, fx, row, s_V, s_dV);
+    phase_coef_from_v(P, sv, s_jac, usum, dep, s_V, s_dV, s_alpha);
+}
+
+// V and dV/ds already in shared memory (all threads call it).
+__device__ void phase_coef_from_v(const BiasPlan &P, const double *sv, const double (*s_jac)[kMaxSymbols],
+                                  const double (*usum)[8], int dep, const double *s_V, const double *s_dV,
+                                  double *s_alpha) {
     if (threadIdx.x < P.nsym) {
         const int q = threadIdx.x;
         double a = 0.0;
@@ -413,6 +424,52 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
         __syncthreads();
     }
     phase_coef(P, S.sten, fx, S.sv, S.s_jac, S.usum, dep, S.row, &S.s_V, S.s_dV, S.s_alpha);
+}
+
+// ------------------------------------------------------------------ hill-list bias
+__global__ void __launch_bounds__(256) k_list_cvs(const BiasPlan *__restrict__ Pp, WalkState *ws) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ BiasShared S;
+    stage_plan(Pp, plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    phase_cvs(P, S.smem, S.usum, S.s_sym, S.s_jac, S.sv);
+    WalkState &W = ws[0];
+    for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) W.usum[e / 8][e % 8] = S.usum[e / 8][e % 8];
+    for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
+        W.jac[e / kMaxSymbols][e % kMaxSymbols] = S.s_jac[e / kMaxSymbols][e % kMaxSymbols];
+    if (threadIdx.x < kMaxDim) {
+        const double v = threadIdx.x < P.D ? S.sv[threadIdx.x] : 0.0;
+        W.s[threadIdx.x] = v;
+        if (threadIdx.x < P.D) P.out[threadIdx.x] = v;   // read by the hill-sum / network kernels
+    }
+}
+
+__global__ void __launch_bounds__(256) k_list_finish(const BiasPlan *__restrict__ Pp, long long step,
+                                                     const WalkState *ws, const double *__restrict__ vdv) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ BiasShared S;
+    stage_plan(Pp, plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    const WalkState &W = ws[0];
+    for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) S.usum[e / 8][e % 8] = W.usum[e / 8][e % 8];
+    for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
+        S.s_jac[e / kMaxSymbols][e % kMaxSymbols] = W.jac[e / kMaxSymbols][e % kMaxSymbols];
+    const int dep = (P.pace != 0) && (step % P.pace == 0);
+    if (threadIdx.x < kMaxDim) {
+        S.sv[threadIdx.x] = W.s[threadIdx.x];
+        S.s_dV[threadIdx.x] = threadIdx.x < P.D ? vdv[1 + threadIdx.x] : 0.0;
+    }
+    if (threadIdx.x == 0) {
+        double V = vdv[0];
+        if (dep) {   // WT height from V(s) before the deposit (GH_t0_uniformGrid.cu:195-208)
+            const double w = P.h0 * exp(-(P.wt ? V : 0.0) / (P.temp * P.kb * (P.biasf - 1.0)));
+            record_hill(P, step, W.s, w);
+            V += w;
+        }
+        S.s_V = V;
+    }
+    __syncthreads();
+    phase_coef_from_v(P, S.sv, S.s_jac, S.usum, dep, &S.s_V, S.s_dV, S.s_alpha);
 }
 
 // ------------------------------------------------------------------ multiple walkers
@@ -519,6 +576,17 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st) {
     k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
     prof_mark("bias_step", st);
+}
+
+void launch_list_cvs(const BiasPlan *d_plan, WalkState *ws, cudaStream_t st) {
+    k_list_cvs<<<1, 256, 0, st>>>(d_plan, ws);
+    prof_mark("bias_cvs", st);
+}
+
+void launch_list_finish(const BiasPlan *d_plan, long long step, const WalkState *ws, const double *vdv,
+                        cudaStream_t st) {
+    k_list_finish<<<1, 256, 0, st>>>(d_plan, step, ws, vdv);
+    prof_mark("bias_finish", st);
 }
 
 void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,

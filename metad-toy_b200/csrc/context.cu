@@ -20,6 +20,7 @@
 #include "args.h"
 #include "expr.h"
 #include "kernels.h"
+#include "nnbias.h"
 
 using namespace mtd;
 
@@ -134,6 +135,12 @@ struct mtd_ctx {
     SysDev last_sys{};
     cudaStream_t own_st = nullptr;
     cudaStream_t side_st = nullptr;      // host -> device force upload beside the CV passes
+    // hill-list bias (CV_dim 4 or NN_BIAS 1): hills, exact sum, learned bias
+    mtd_nnbias *nb = nullptr;
+    double *d_vdv = nullptr;             // V, dV/ds at this step's s
+    WalkState *d_ws1 = nullptr;          // CV values and chain factors between the two bias kernels
+    int h_fit = 0;                       // hills the network was fitted on
+    bool nn_usable = false;
     cudaEvent_t f_ready = nullptr;
     Prof prof;
     bool prof_created = false;
@@ -764,8 +771,16 @@ mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, cons
     c->launches = 0;
     mtd_status s = enqueue_values(c, n, x, mask, image);
     if (s != MTD_OK) return s;
-    launch_bias_step(c->d_plan, step, c->st);
-    c->launches += 1;
+    if (c->nb) {   // hill-list bias: CVs, V and dV/ds at s, deposit and coefficients
+        launch_list_cvs(c->d_plan, c->d_ws1, c->st);
+        s = nnbias_enqueue_vdv(c->nb, c->d_out, c->d_vdv, c->nn_usable, c->h_fit, c->st);
+        if (s != MTD_OK) return fail(c, s, mtd_nnbias_last_error(c->nb));
+        launch_list_finish(c->d_plan, step, c->d_ws1, c->d_vdv, c->st);
+        c->launches += 4;
+    } else {
+        launch_bias_step(c->d_plan, step, c->st);
+        c->launches += 1;
+    }
     if (f_ready) MTD_CU(cudaStreamWaitEvent(c->st, f_ready, 0), "force upload");
     return enqueue_forces(c, step, x, mask, fin, fout, virial);
 }
@@ -776,6 +791,31 @@ void write_hill_line(mtd_ctx *c, const HillRec &h) {
     for (int d = 0; d < c->cfg.cv_dim; ++d) std::fprintf(c->f_hills, " %.16g", h.s[d]);
     std::fprintf(c->f_hills, " %.16g %.16g\n", h.w, h.sigma);
     std::fflush(c->f_hills);
+}
+
+// Hill-list bias: new hills join the exact sum; every NN_REFIT hills the
+// network is refitted on the sum and validated against it (the exact sum, plus
+// the network when it passes, is what the next steps use).
+mtd_status list_add_hills(mtd_ctx *c, const std::vector<HillRec> &recs) {
+    const int D = c->cfg.cv_dim;
+    std::vector<double> cen, hgt, sig;
+    for (const HillRec &r : recs) {
+        for (int d = 0; d < D; ++d) cen.push_back(r.s[d]);
+        hgt.push_back(r.w);
+        sig.push_back(r.sigma);
+    }
+    if (!hgt.empty() && mtd_nnbias_add_hills(c->nb, (int)hgt.size(), cen.data(), hgt.data(), sig.data()) != MTD_OK)
+        return fail(c, MTD_ERR_CUDA, mtd_nnbias_last_error(c->nb));
+    const int nh = mtd_nnbias_num_hills(c->nb);
+    if (c->cfg.nn && nh - c->h_fit >= c->cfg.nn_refit) {
+        double loss = 0.0, mx = 0.0, rms = 0.0;
+        if (mtd_nnbias_fit(c->nb, 65536, c->cfg.nn_iters, 4096, 2e-3, 1000 + (unsigned long long)nh, &loss) != MTD_OK ||
+            mtd_nnbias_validate(c->nb, 16384, 7 + (unsigned long long)nh, c->cfg.nn_tol, &mx, &rms) != MTD_OK)
+            return fail(c, MTD_ERR_CUDA, mtd_nnbias_last_error(c->nb));
+        c->h_fit = nh;
+        c->nn_usable = mtd_nnbias_usable(c->nb) != 0;
+    }
+    return MTD_OK;
 }
 
 // Collects the outputs of the last enqueued step (stream already synchronised).
@@ -791,12 +831,18 @@ mtd_status collect(mtd_ctx *c) {
     if (nh > c->hills_written) {
         unsigned long long from = c->hills_written;
         if (nh - from > (unsigned long long)kHillCap) from = nh - kHillCap;
+        std::vector<HillRec> recs;
         for (unsigned long long h = from; h < nh; ++h) {
             HillRec r;
             MTD_CU(cudaMemcpy(&r, c->d_hills + (h % kHillCap), sizeof(HillRec), cudaMemcpyDeviceToHost), "hill record");
             write_hill_line(c, r);
+            recs.push_back(r);
         }
         c->hills_written = nh;
+        if (c->nb) {
+            mtd_status s = list_add_hills(c, recs);
+            if (s != MTD_OK) return s;
+        }
     }
     if (c->f_rec && c->cfg.rec_pace > 0 && c->pending_step % c->cfg.rec_pace == 0) {
         std::fprintf(c->f_rec, "%lld", c->pending_step);
@@ -815,6 +861,7 @@ std::string path_in(const mtd_ctx *c, const std::string &p) {
 
 mtd_status replay_records(mtd_ctx *c, const std::vector<HillRec> &recs) {
     if (recs.empty()) return MTD_OK;
+    if (c->nb) return list_add_hills(c, recs);
     HillRec *d = nullptr;
     MTD_CU(dalloc(&d, sizeof(HillRec) * recs.size()), "replay");
     cudaMemcpy(d, recs.data(), sizeof(HillRec) * recs.size(), cudaMemcpyHostToDevice);
@@ -1004,6 +1051,9 @@ void mtd_destroy(mtd_ctx *c) {
     if (c->h_nhills) cudaFreeHost(c->h_nhills);
     if (c->own_st) cudaStreamDestroy(c->own_st);
     if (c->side_st) cudaStreamDestroy(c->side_st);
+    if (c->nb) mtd_nnbias_destroy(c->nb);
+    dfree(c->d_vdv);
+    dfree(c->d_ws1);
     if (c->f_ready) cudaEventDestroy(c->f_ready);
     if (c->prof_created)
         for (int i = 0; i < kProfMax; ++i) cudaEventDestroy(c->prof.ev[i]);
@@ -1032,10 +1082,23 @@ mtd_status mtd_set_box(mtd_ctx *c, const double lo[3], const double hi[3], const
 mtd_status mtd_init(mtd_ctx *c) {
     if (!c) return MTD_ERR_INVALID_ARG;
     if (c->initialized) return MTD_OK;
-    c->grid_size = 1;
-    for (int d = 0; d < c->cfg.cv_dim; ++d) c->grid_size *= c->cfg.dims[d].nbins;
-    MTD_CU(dalloc(&c->d_grid, sizeof(double) * (size_t)c->grid_size), "bias grid");
-    MTD_CU(cudaMemset(c->d_grid, 0, sizeof(double) * (size_t)c->grid_size), "bias grid");
+    if (c->cfg.hill_list()) {   // hills kept as a list: exact FP64 sum and the learned bias
+        double lo[kMaxDim], hi[kMaxDim];
+        for (int d = 0; d < c->cfg.cv_dim; ++d) {
+            lo[d] = c->cfg.dims[d].lo;
+            hi[d] = c->cfg.dims[d].hi;
+        }
+        if (mtd_nnbias_create(c->cfg.cv_dim, lo, hi, 12345, &c->nb) != MTD_OK)
+            return fail(c, MTD_ERR_CUDA, c->nb ? mtd_nnbias_last_error(c->nb) : "learned bias");
+        MTD_CU(dalloc(&c->d_vdv, sizeof(double) * 8), "bias at s");
+        MTD_CU(dalloc(&c->d_ws1, sizeof(WalkState)), "bias state");
+        c->grid_size = 0;
+    } else {
+        c->grid_size = 1;
+        for (int d = 0; d < c->cfg.cv_dim; ++d) c->grid_size *= c->cfg.dims[d].nbins;
+        MTD_CU(dalloc(&c->d_grid, sizeof(double) * (size_t)c->grid_size), "bias grid");
+        MTD_CU(cudaMemset(c->d_grid, 0, sizeof(double) * (size_t)c->grid_size), "bias grid");
+    }
     c->plan_dirty = true;
     build_plan(c);
     MTD_CU(cudaMemcpy(c->d_plan, &c->plan, sizeof(BiasPlan), cudaMemcpyHostToDevice), "plan");
@@ -1279,6 +1342,14 @@ int mtd_max_neighbors(mtd_ctx *c, const char *name) {
 
 const char *mtd_last_error(const mtd_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
+mtd_status mtd_nn_state(const mtd_ctx *c, int *hills, int *hills_fitted, int *usable) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    if (hills) *hills = c->nb ? mtd_nnbias_num_hills(c->nb) : 0;
+    if (hills_fitted) *hills_fitted = c->h_fit;
+    if (usable) *usable = c->nn_usable ? 1 : 0;
+    return MTD_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------ multiple walkers
@@ -1388,7 +1459,7 @@ mtd_status mtd_walkers_create(int nwalk, int narg, const char *const *arg, const
         const mtd_status s = mtd_create(narg, arg, &o, &c);
         W->w.push_back(c);
         if (s != MTD_OK) return wfail(W, s, c ? c->err : "context creation failed");
-        if (c->cfg.cv_dim > 3) return wfail(W, MTD_ERR_UNSUPPORTED, "walkers share a grid: CV_dim <= 3");
+        if (c->cfg.hill_list()) return wfail(W, MTD_ERR_UNSUPPORTED, "walkers share a grid: CV_dim <= 3, no NN_BIAS");
         if (k > 0) c->cfg.rec_file.clear();   // one RECORD file (walker 0's)
     }
     MTD_WCU(cudaStreamCreateWithFlags(&W->st, cudaStreamNonBlocking), "stream");

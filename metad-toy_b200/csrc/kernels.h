@@ -218,7 +218,7 @@ struct UnitPlan {
 
 struct HillRec {
     long long step;
-    double s[3];
+    double s[kMaxDim];
     double w, sigma;
 };
 
@@ -235,8 +235,8 @@ struct BiasPlan {
     SymPlan sym[kMaxSymbols];
     int nunit;
     UnitPlan unit[kMaxUnits];
-    int ncode[3];
-    ExprInstr code[3][kMaxExprLen];
+    int ncode[kMaxDim];
+    ExprInstr code[kMaxDim][kMaxExprLen];
     double *grid;
     long long grid_size;
     HillRec *hills;
@@ -259,6 +259,15 @@ struct WalkState {
 void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
                       cudaStream_t st);
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
+
+// Hill-list bias (no grid; CV_dim up to 4): the CV values and chain factors
+// into ws[0]; then, with V and dV/ds at s from the hill sum or the learned
+// bias in vdv (V, dV[0..D)), the deposit record, V += the new hill's height
+// (a hill adds its full height and no slope at its own centre) and the force
+// coefficients.
+void launch_list_cvs(const BiasPlan *d_plan, WalkState *ws, cudaStream_t st);
+void launch_list_finish(const BiasPlan *d_plan, long long step, const WalkState *ws, const double *vdv,
+                        cudaStream_t st);
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st);
 
 }  // namespace mtd

@@ -362,15 +362,16 @@ __global__ void __launch_bounds__(256) k_hillsum_batch(int D, int npts, const do
 
 // One point, hills spread over blocks; block partials reduced in block order by the last block.
 constexpr int kPointBlocks = 80;
-__global__ void __launch_bounds__(256) k_hillsum_point(int D, const double *__restrict__ s_in, int nh,
+__global__ void __launch_bounds__(256) k_hillsum_point(int D, const double *__restrict__ s_in, int h_begin, int nh,
                                                        const double *__restrict__ hills, double *part,
-                                                       unsigned int *ticket, double *V, double *dV) {
+                                                       unsigned int *ticket, double *V, double *dV,
+                                                       int accumulate) {
     __shared__ double smem[5 * 32];
     __shared__ bool last;
     double s[kIn] = {0, 0, 0, 0};
     for (int k = 0; k < D; ++k) s[k] = s_in[k];
     double acc[5] = {0, 0, 0, 0, 0};
-    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += gridDim.x * blockDim.x) {
+    for (int h = h_begin + blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += gridDim.x * blockDim.x) {
         const double *c = hills + (size_t)h * 8;
         double r2 = 0.0, d[kIn];
 #pragma unroll
@@ -397,8 +398,8 @@ __global__ void __launch_bounds__(256) k_hillsum_point(int D, const double *__re
         __threadfence();
         double t = 0.0;
         for (int b = 0; b < (int)gridDim.x; ++b) t += *((volatile double *)part + b * 5 + threadIdx.x);
-        if (threadIdx.x == 0) *V = t;
-        else if ((int)threadIdx.x - 1 < D) dV[threadIdx.x - 1] = t;
+        if (threadIdx.x == 0) *V = accumulate ? *V + t : t;
+        else if ((int)threadIdx.x - 1 < D) dV[threadIdx.x - 1] = accumulate ? dV[threadIdx.x - 1] + t : t;
         if (threadIdx.x == 0) *ticket = 0u;
     }
 }
@@ -955,11 +956,35 @@ mtd_status mtd_nnbias_point_device(mtd_nnbias *b, const double *d_s, double *d_V
             NB_CU(cudaMemsetAsync(d_dV, 0, sizeof(double) * b->D, st), "bias");
             return MTD_OK;
         }
-        k_hillsum_point<<<kPointBlocks, 256, 0, st>>>(b->D, d_s, b->nh, b->d_hills, b->d_ppart, b->d_ticket, d_V,
-                                                      d_dV);
+        k_hillsum_point<<<kPointBlocks, 256, 0, st>>>(b->D, d_s, 0, b->nh, b->d_hills, b->d_ppart, b->d_ticket, d_V,
+                                                      d_dV, 0);
     }
     NB_CU(cudaGetLastError(), "bias at a point");
     return MTD_OK;
 }
 
 }  // extern "C"
+
+namespace mtd {
+
+mtd_status nnbias_enqueue_vdv(mtd_nnbias *b, const double *d_s, double *d_vdv, bool nn, int h_from,
+                              cudaStream_t st) {
+    double *d_V = d_vdv, *d_dV = d_vdv + 1;
+    int h0 = 0;
+    if (nn) {
+        double sc[kIn];
+        for (int k = 0; k < kIn; ++k) sc[k] = 2.0 / (b->hi[k] - b->lo[k]);
+        k_mlp_point<<<1, 128, 0, st>>>(nb_dev(b), d_s, b->lo[0], b->lo[1], b->lo[2], b->lo[3], sc[0], sc[1], sc[2],
+                                       sc[3], b->vscale, d_V, d_dV);
+        h0 = std::max(0, std::min(h_from, b->nh));
+    } else if (b->nh == 0 || h_from >= b->nh) {
+        NB_CU(cudaMemsetAsync(d_vdv, 0, sizeof(double) * (1 + b->D), st), "bias");
+    }
+    if (h0 < b->nh)
+        k_hillsum_point<<<kPointBlocks, 256, 0, st>>>(b->D, d_s, h0, b->nh, b->d_hills, b->d_ppart, b->d_ticket, d_V,
+                                                      d_dV, nn ? 1 : 0);
+    NB_CU(cudaGetLastError(), "bias at the CV point");
+    return MTD_OK;
+}
+
+}  // namespace mtd

@@ -31,7 +31,7 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
            "mtd_extract_peratom", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
            "mtd_set_stream", "mtd_profile_enable", "mtd_profile_report",
-           "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc",
+           "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc", "mtd_nn_state",
            "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
            "mtd_nnbias_num_hills", "mtd_nnbias_exact", "mtd_nnbias_eval", "mtd_nnbias_fit", "mtd_nnbias_validate",
            "mtd_nnbias_usable", "mtd_nnbias_point_device", "mtd_nnbias_get_params", "mtd_nnbias_set_params",
@@ -96,6 +96,7 @@ def lib():
         L.mtd_profile_report.argtypes = [vp, C.c_char_p, C.c_int]
         L.mtd_parse_args.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.c_char_p, C.c_int]
         L.mtd_eval_expression.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, dp, dp]
+        L.mtd_nn_state.argtypes = [vp, ip, ip, ip]
         L.mtd_walkers_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_char_p), C.POINTER(Options), C.POINTER(vp)]
         L.mtd_walkers_destroy.argtypes = [vp]
         L.mtd_walkers_last_error.argtypes = [vp]
@@ -286,6 +287,12 @@ class Metad:
 
     def max_neighbors(self, cal):
         return lib().mtd_max_neighbors(self._h, cal.encode())
+
+    def nn_state(self):
+        """(hills, hills fitted, network in use) of the hill-list bias."""
+        h, f, u = C.c_int(), C.c_int(), C.c_int()
+        self._check(lib().mtd_nn_state(self._h, C.byref(h), C.byref(f), C.byref(u)))
+        return h.value, f.value, bool(u.value)
 
     def set_stream(self, stream_ptr):
         """Run on an external cudaStream_t (an int handle, e.g. torch's cuda_stream); 0 = own stream."""

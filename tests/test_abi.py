@@ -63,7 +63,9 @@ def test_reference_configs_parse():
     (C1[:17] + ["SYMBOL", "v1", "Q6.LOC_AVE"], "find the func"),
     (C1[:17] + ["SYMBOL", "v1", "Q6.SW_FUNC.nosw"], "not defined"),
     (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "DIM", "1", "0", "1", "10", "v1"], "CV_dim must be given"),
-    (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "4"], "1D-3D"),
+    (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "5"], "1D-3D"),
+    (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "4"], "DIM 1 is missing"),
+    (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "NN_TOL", "0"], "NN_TOL must be > 0"),
     (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "2", "DIM", "1", "0", "1", "10", "v1"], "DIM 2 is missing"),
     (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "1", "DIM", "1", "0", "1", "10", "v1+w"], "unknown symbol"),
     (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "1", "DIM", "1", "0", "1", "10", "(v1"], "expected ')'"),
