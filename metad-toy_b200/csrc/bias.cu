@@ -309,6 +309,12 @@ __device__ void phase_deposit(const BiasPlan &P, const double *s, double w, cons
     }
 }
 
+// A step whose neighbour lists overflowed is repeated by the host: it must
+// leave no hill and no bias force behind.
+__device__ __forceinline__ bool step_failed(const BiasPlan &P) {
+    return P.status && *(volatile const unsigned *)&P.status->overflow != 0u;
+}
+
 __device__ __forceinline__ void record_hill(const BiasPlan &P, long long step, const double *s, double w) {
     const unsigned long long h = *P.nhills;
     HillRec r;
@@ -350,6 +356,10 @@ __device__ void phase_coef_from_v(const BiasPlan &P, const double *sv, const dou
         P.out[P.D + 1] = dep ? 1.0 : 0.0;
     }
     __syncthreads();
+    if (step_failed(P)) {
+        for (int e = threadIdx.x; e < P.nunit * 8; e += blockDim.x) P.unit[e / 8].coef[e % 8] = 0.0;
+        return;
+    }
     if (threadIdx.x < 2 * P.nunit) {
         const int u = threadIdx.x >> 1, slot = threadIdx.x & 1;
         const UnitPlan &U = P.unit[u];
@@ -411,7 +421,7 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
     stage_plan(Pp, plan_raw);
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
     phase_cvs(P, S.smem, S.usum, S.s_sym, S.s_jac, S.sv);
-    const int dep = (P.pace != 0) && (step % P.pace == 0);
+    const int dep = (P.pace != 0) && (step % P.pace == 0) && !step_failed(P);
     int ix[3] = {1, 1, 1};
     double fx[3] = {0, 0, 0};
     stencil_locate(P, S.sv, ix, fx);
@@ -454,7 +464,7 @@ __global__ void __launch_bounds__(256) k_list_finish(const BiasPlan *__restrict_
     for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) S.usum[e / 8][e % 8] = W.usum[e / 8][e % 8];
     for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
         S.s_jac[e / kMaxSymbols][e % kMaxSymbols] = W.jac[e / kMaxSymbols][e % kMaxSymbols];
-    const int dep = (P.pace != 0) && (step % P.pace == 0);
+    const int dep = (P.pace != 0) && (step % P.pace == 0) && !step_failed(P);
     if (threadIdx.x < kMaxDim) {
         S.sv[threadIdx.x] = W.s[threadIdx.x];
         S.s_dV[threadIdx.x] = threadIdx.x < P.D ? vdv[1 + threadIdx.x] : 0.0;
@@ -487,7 +497,7 @@ __global__ void __launch_bounds__(256) k_walk_cvs(const BiasPlan *const *__restr
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
     const long long step = *d_step;
     phase_cvs(P, S.smem, S.usum, S.s_sym, S.s_jac, S.sv);
-    const int dep = (P.pace != 0) && (step % P.pace == 0);
+    const int dep = (P.pace != 0) && (step % P.pace == 0) && !step_failed(P);
     WalkState &W = ws[blockIdx.x];
     if (dep) {
         int ix[3] = {1, 1, 1};
@@ -505,13 +515,29 @@ __global__ void __launch_bounds__(256) k_walk_cvs(const BiasPlan *const *__restr
     if (threadIdx.x == 0) W.dep = dep;
 }
 
+// True (in every thread) when any walker's neighbour lists overflowed this
+// step: the host repeats the whole group's step, so no walker may deposit or
+// apply a bias force.
+__device__ bool group_failed(const BiasPlan *const *__restrict__ plans, int nwalk) {
+    __shared__ int failed;
+    if (threadIdx.x == 0) failed = 0;
+    __syncthreads();
+    for (int w = threadIdx.x; w < nwalk; w += blockDim.x) {
+        const DevStatus *st = plans[w]->status;
+        if (st && *(volatile const unsigned *)&st->overflow != 0u) failed = 1;
+    }
+    __syncthreads();
+    return failed != 0;
+}
+
 __global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__restrict__ plans, int nwalk,
                                                       const long long *__restrict__ d_step, const WalkState *ws) {
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     stage_plan(plans[0], plan_raw);
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
-    if (!ws[0].dep) return;   // every walker shares PACE
+    if (group_failed(plans, nwalk)) return;
     const long long step = *d_step;
+    if (!(P.pace != 0 && step % P.pace == 0)) return;   // every walker shares PACE
     int ix[3] = {1, 1, 1};
     for (int w = 0; w < nwalk; ++w) {
         phase_deposit(P, ws[w].s, ws[w].hill_w, ix, nullptr);
@@ -520,11 +546,16 @@ __global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__r
     }
 }
 
-__global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__restrict__ plans, const WalkState *ws) {
+__global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__restrict__ plans, int nwalk,
+                                                   const WalkState *ws) {
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
     stage_plan(plans[blockIdx.x], plan_raw);
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    if (group_failed(plans, nwalk)) {
+        for (int e = threadIdx.x; e < P.nunit * 8; e += blockDim.x) P.unit[e / 8].coef[e % 8] = 0.0;
+        return;
+    }
     const WalkState &W = ws[blockIdx.x];
     for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) S.usum[e / 8][e % 8] = W.usum[e / 8][e % 8];
     for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
@@ -593,7 +624,7 @@ void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long
                       cudaStream_t st) {
     k_walk_cvs<<<nwalk, 256, 0, st>>>(d_plans, d_step, ws);
     k_walk_deposit<<<1, 256, 0, st>>>(d_plans, nwalk, d_step, ws);
-    k_walk_coef<<<nwalk, 256, 0, st>>>(d_plans, ws);
+    k_walk_coef<<<nwalk, 256, 0, st>>>(d_plans, nwalk, ws);
     prof_mark("walk_bias", st);
 }
 

@@ -418,6 +418,7 @@ void build_plan(mtd_ctx *c) {
     P.hill_cap = kHillCap;
     P.nhills = c->d_nhills;
     P.out = c->d_out;
+    P.status = c->d_status;
 }
 
 // Neighbour-list and CV-unit layout from the parsed CAL table (env pooling as in

@@ -243,6 +243,8 @@ struct BiasPlan {
     int hill_cap;
     unsigned long long *nhills;
     double *out;           // [0..D) s, D: V, D+1: deposited flag, kOutSymOffset..: symbol values
+    const DevStatus *status;   // a neighbour overflow this step: no deposit, zero force coefficients
+    const void *pad16;         // keeps sizeof a multiple of 16 (staged as 16-byte vectors)
 };
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
 

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import helpers as H
+import mtd
 import oracle as O
 import systems
 
@@ -109,3 +110,51 @@ def test_thin_periodic_box(precision):
     assert H.rel(cv, s) < tcv
     assert H.rel(f, fo) < tf
     assert m.max_neighbors("Q4") == o4["nnb"].max()
+
+
+def _dense_cluster_system():
+    """A compact FCC cluster (a = 3.0 A: ~42 neighbours within 3.9 A) in a
+    sparse gas: the list width estimated from the mean density is far too
+    small, so the first step overflows and is repeated with grown lists."""
+    rng = np.random.default_rng(17)
+    L = np.array([60.0, 60.0, 60.0])
+    cluster = systems.lattice(4, 4, 4, 3.0, systems.FCC_BASIS) + 20.0
+    gas = rng.random((200, 3)) * L
+    gas = gas[np.min(np.linalg.norm(gas[:, None, :] - cluster[None, :, :], axis=2), axis=1) > 3.0]
+    return np.ascontiguousarray(systems.wrap(np.concatenate([cluster, gas]), L)), L
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_neighbour_overflow_is_grown_and_repeated(precision):
+    x, L = _dense_cluster_system()
+    args = H.fix_args_local()
+    m, out = H.run_gpu(args, x, L, [(0, x), (1, x)], precision=precision)
+    o4, o6 = H.oracle_local(x, L, 4), H.oracle_local(x, L, 6)
+    assert m.max_neighbors("Q4") == o4["nnb"].max() > 30
+    g = O.Grid([[0, 1], [0, 1]], [200, 200], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    s = [o4["cv"], o6["cv"]]
+    g.add_hill(s)
+    V, dV = g.value(s)
+    tcv, tf = TOL[precision]
+    for cv, bias, f, _ in out:
+        assert H.rel(cv, s) < tcv
+        assert H.rel(bias, V) < tcv
+        assert H.rel(f, -(dV[0] * o4["grad"] + dV[1] * o6["grad"])) < tf
+
+
+def test_neighbour_overflow_on_the_device_path_asks_for_a_repeat():
+    import torch
+
+    x, L = _dense_cluster_system()
+    m = mtd.Metad(H.fix_args_local(), precision="fp64")
+    m.set_box([0, 0, 0], L)
+    dx = torch.from_numpy(x).cuda()
+    f = torch.zeros_like(dx)
+    m.post_force_device(0, x.shape[0], dx.data_ptr(), f.data_ptr(), f.data_ptr())
+    with pytest.raises(mtd.MetadError, match="NEIGH_OVERFLOW"):
+        m.sync()
+    f.zero_()
+    m.post_force_device(0, x.shape[0], dx.data_ptr(), f.data_ptr(), f.data_ptr())
+    m.sync()
+    o4 = H.oracle_local(x, L, 4)
+    assert abs(m.cv[0] - o4["cv"]) < 1e-9 * abs(o4["cv"])

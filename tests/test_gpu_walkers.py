@@ -87,3 +87,38 @@ def test_walkers_hills_file_in_walker_order(tmp_path):
         assert int(r[0]) == step
         cv = out[step][k][0]
         assert abs(float(r[1]) - cv[0]) < 1e-12 and abs(float(r[2]) - cv[1]) < 1e-12
+
+
+def test_walkers_overflow_leaves_no_hill_and_no_force():
+    """One walker's neighbour lists overflow on the first step: the group step
+    reports it, deposits nothing and leaves every force untouched; the
+    repeated step then matches the oracle."""
+    import torch
+    import test_gpu_parity as P
+
+    syss = [P._dense_cluster_system(), _walker_systems()[0]]
+    W = mtd.Walkers(2, H.fix_args_local(pace=2), precision="fp64")
+    for k, (x, L) in enumerate(syss):
+        W.set_box(k, [0, 0, 0], L)
+    dx = [torch.from_numpy(x).cuda() for x, _ in syss]
+    df = [torch.zeros_like(v) for v in dx]
+    ns = [x.shape[0] for x, _ in syss]
+    W.step_device(0, ns, [v.data_ptr() for v in dx], [v.data_ptr() for v in df])
+    with pytest.raises(mtd.MetadError, match="NEIGH_OVERFLOW"):
+        W.sync()
+    assert all(float(v.abs().max()) == 0.0 for v in df)
+    assert float(np.abs(W.grid(200 * 200)).max()) == 0.0
+    W.step_device(0, ns, [v.data_ptr() for v in dx], [v.data_ptr() for v in df])
+    W.sync()
+    ref = [(H.oracle_local(x, L, 4), H.oracle_local(x, L, 6)) for x, L in syss]
+    g = O.Grid([[0, 1], [0, 1]], [200, 200], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    s = [[o4["cv"], o6["cv"]] for o4, o6 in ref]
+    heights = [0.005 * np.exp(-g.value(sw)[0] / (300.0 * 8.617343e-5 * 8.0)) for sw in s]
+    for sw, w in zip(s, heights):
+        g.deposit(sw, w)
+    for k, (o4, o6) in enumerate(ref):
+        V, dV = g.value(s[k])
+        assert H.rel(W.cv(k, 2), s[k]) < 1e-9
+        assert H.rel(W.bias(k), V) < 1e-9
+        assert H.rel(df[k].cpu().numpy(), -(dV[0] * o4["grad"] + dV[1] * o6["grad"])) < 1e-8
+    W.close()
