@@ -122,7 +122,11 @@ int mtd_cv_dim(const mtd_ctx *ctx);
 
 /* Per-atom export for `compute metad/atom` / Fix::extract
  * ("colvar_peratom:<CAL>.<prop>", props stein_q, dcvdx_x/y/z, stru_f).
- * Copies n values (caller order) into out.
+ * Copies n values (caller order) into out.  dcvdx_* is the exact gradient of
+ * the CV that the first SYMBOL on <CAL> selects, at the last step's positions
+ * (STEINH Q and L, STRU_FACTOR, STRU_FACTOR_K); it re-runs that CAL's force
+ * kernels once per step and CAL and is cached, so dcvdx_x/y/z of one step
+ * cost one pass.
  * Replaces FixMetadynamics::extract (src/core/fix_crystallize.cu:592-613),
  * STEIN_QL::get_peratom_ptr (src/cvs/CVs_Steinhardt.cu:1278-1322),
  * Stru_factor::get_peratom_ptr (src/cvs/CVs_Strufactor.cu:974-979). */

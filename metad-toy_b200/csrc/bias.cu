@@ -332,6 +332,7 @@ __device__ __forceinline__ void record_hill(const BiasPlan &P, long long step, c
 __device__ void phase_coef_from_v(const BiasPlan &P, const double *sv, const double (*s_jac)[kMaxSymbols],
                                   const double (*usum)[8], int dep, const double *s_V, const double *s_dV,
                                   double *s_alpha);
+__device__ void phase_unit_coefs(const BiasPlan &P, const double (*usum)[8], const double *s_alpha);
 
 __device__ void phase_coef(const BiasPlan &P, const double *sten, const double *fx, const double *sv,
                            const double (*s_jac)[kMaxSymbols], const double (*usum)[8], int dep, double (*row)[16],
@@ -356,6 +357,12 @@ __device__ void phase_coef_from_v(const BiasPlan &P, const double *sv, const dou
         P.out[P.D + 1] = dep ? 1.0 : 0.0;
     }
     __syncthreads();
+    phase_unit_coefs(P, usum, s_alpha);
+}
+
+// Per-unit force coefficients from the chain factors alpha (one thread per
+// unit and l slot); zero on a failed step.
+__device__ void phase_unit_coefs(const BiasPlan &P, const double (*usum)[8], const double *s_alpha) {
     if (step_failed(P)) {
         for (int e = threadIdx.x; e < P.nunit * 8; e += blockDim.x) P.unit[e / 8].coef[e % 8] = 0.0;
         return;
@@ -434,6 +441,20 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
         __syncthreads();
     }
     phase_coef(P, S.sten, fx, S.sv, S.s_jac, S.usum, dep, S.row, &S.s_V, S.s_dV, S.s_alpha);
+    if (P.save)
+        for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) P.save->usum[e / 8][e % 8] = S.usum[e / 8][e % 8];
+}
+
+__global__ void __launch_bounds__(256) k_symbol_coef(const BiasPlan *__restrict__ Pp, int sym,
+                                                     const WalkState *ws) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ double usum[kMaxUnits][8], alpha[kMaxSymbols];
+    stage_plan(Pp, plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) usum[e / 8][e % 8] = ws[0].usum[e / 8][e % 8];
+    if (threadIdx.x < kMaxSymbols) alpha[threadIdx.x] = threadIdx.x == sym ? 1.0 : 0.0;
+    __syncthreads();
+    phase_unit_coefs(P, usum, alpha);
 }
 
 // ------------------------------------------------------------------ hill-list bias
@@ -607,6 +628,10 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st) {
     k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
     prof_mark("bias_step", st);
+}
+
+void launch_symbol_coef(const BiasPlan *d_plan, int sym, const WalkState *ws, cudaStream_t st) {
+    k_symbol_coef<<<1, 256, 0, st>>>(d_plan, sym, ws);
 }
 
 void launch_list_cvs(const BiasPlan *d_plan, WalkState *ws, cudaStream_t st) {

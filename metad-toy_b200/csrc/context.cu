@@ -138,10 +138,19 @@ struct mtd_ctx {
     // hill-list bias (CV_dim 4 or NN_BIAS 1): hills, exact sum, learned bias
     mtd_nnbias *nb = nullptr;
     double *d_vdv = nullptr;             // V, dV/ds at this step's s
-    WalkState *d_ws1 = nullptr;          // CV values and chain factors between the two bias kernels
+    WalkState *d_ws1 = nullptr;          // CV values, chain factors and block-sum totals of the last step
     int h_fit = 0;                       // hills the network was fitted on
     bool nn_usable = false;
     cudaEvent_t f_ready = nullptr;
+    // per-atom dCV/dx export (compute metad/atom): last step's inputs, cached result
+    const double *last_x = nullptr;
+    const int *last_mask = nullptr;
+    long long step_gen = 0;              // steps enqueued so far
+    long long dcv_gen = -1;              // step the cached dCV/dx belongs to
+    std::string dcv_cal;
+    std::vector<double> h_dcv;           // [n][3], caller order
+    double *d_dcv = nullptr;             // [2][cap][3]: zero input, gradient output
+    int dcv_cap = 0;
     Prof prof;
     bool prof_created = false;
     std::map<std::string, std::pair<long long, double>> prof_total;
@@ -419,6 +428,7 @@ void build_plan(mtd_ctx *c) {
     P.nhills = c->d_nhills;
     P.out = c->d_out;
     P.status = c->d_status;
+    P.save = c->d_ws1;
 }
 
 // Neighbour-list and CV-unit layout from the parsed CAL table (env pooling as in
@@ -743,6 +753,9 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
     if (c->fp64) run_values<double>(c, g, x, mask);
     else run_values<float>(c, g, x, mask);
     c->last_sys = s;
+    c->last_x = x;
+    c->last_mask = mask;
+    c->step_gen += 1;
     MTD_CU(cudaGetLastError(), "kernel launch");
     return MTD_OK;
 }
@@ -1055,6 +1068,7 @@ void mtd_destroy(mtd_ctx *c) {
     if (c->nb) mtd_nnbias_destroy(c->nb);
     dfree(c->d_vdv);
     dfree(c->d_ws1);
+    dfree(c->d_dcv);
     if (c->f_ready) cudaEventDestroy(c->f_ready);
     if (c->prof_created)
         for (int i = 0; i < kProfMax; ++i) cudaEventDestroy(c->prof.ev[i]);
@@ -1083,6 +1097,8 @@ mtd_status mtd_set_box(mtd_ctx *c, const double lo[3], const double hi[3], const
 mtd_status mtd_init(mtd_ctx *c) {
     if (!c) return MTD_ERR_INVALID_ARG;
     if (c->initialized) return MTD_OK;
+    MTD_CU(dalloc(&c->d_ws1, sizeof(WalkState)), "bias state");
+    MTD_CU(cudaMemset(c->d_ws1, 0, sizeof(WalkState)), "bias state");
     if (c->cfg.hill_list()) {   // hills kept as a list: exact FP64 sum and the learned bias
         double lo[kMaxDim], hi[kMaxDim];
         for (int d = 0; d < c->cfg.cv_dim; ++d) {
@@ -1092,7 +1108,6 @@ mtd_status mtd_init(mtd_ctx *c) {
         if (mtd_nnbias_create(c->cfg.cv_dim, lo, hi, 12345, &c->nb) != MTD_OK)
             return fail(c, MTD_ERR_CUDA, c->nb ? mtd_nnbias_last_error(c->nb) : "learned bias");
         MTD_CU(dalloc(&c->d_vdv, sizeof(double) * 8), "bias at s");
-        MTD_CU(dalloc(&c->d_ws1, sizeof(WalkState)), "bias state");
         c->grid_size = 0;
     } else {
         c->grid_size = 1;
@@ -1228,6 +1243,44 @@ double mtd_compute_vector(const mtd_ctx *c, int k) {
 
 int mtd_cv_dim(const mtd_ctx *c) { return c ? c->cfg.cv_dim : 0; }
 
+// dCV/dx of CAL `cal` at the last step's positions, into c->h_dcv ([n][3],
+// caller order). The CV is the one the first SYMBOL on that CAL selects; the
+// force kernels run once more with chain factor 1 on that symbol, 0 on the
+// others and a zero input force, so their output is -dCV/dx (the exact
+// gradient, every neighbour term included). Cached per step and CAL, as
+// STEIN_QL::get_peratom_ptr caches per timestep (src/cvs/CVs_Steinhardt.cu:1278-1321).
+static mtd_status dcvdx(mtd_ctx *c, const std::string &cal) {
+    if (c->step_gen == 0) return fail(c, MTD_ERR_INVALID_ARG, "no step has run");
+    if (c->dcv_gen == c->step_gen && c->dcv_cal == cal) return MTD_OK;
+    int sym = -1;
+    for (size_t q = 0; q < c->cfg.symbols.size() && sym < 0; ++q)
+        if (c->cfg.symbols[q].cal == cal) sym = (int)q;
+    if (sym < 0) return fail(c, MTD_ERR_INVALID_ARG, "dcvdx: no SYMBOL uses CAL " + cal);
+    const int n = c->n;
+    if (n > c->dcv_cap) {
+        dfree(c->d_dcv);
+        c->dcv_cap = 0;
+        MTD_CU(dalloc(&c->d_dcv, sizeof(double) * 6 * (size_t)n), "dcvdx buffers");
+        c->dcv_cap = n;
+    }
+    double *zero = c->d_dcv, *grad = c->d_dcv + 3 * (size_t)c->dcv_cap;
+    MTD_CU(cudaMemsetAsync(zero, 0, sizeof(double) * 3 * (size_t)n, c->st), "dcvdx");
+    const int launches = c->launches;
+    launch_symbol_coef(c->d_plan, sym, c->d_ws1, c->st);
+    if (c->fp64) run_forces<double>(c, c->last_sys, c->last_grid, c->last_x, c->last_mask, zero, grad, false);
+    else run_forces<float>(c, c->last_sys, c->last_grid, c->last_x, c->last_mask, zero, grad, false);
+    c->launches = launches;
+    MTD_CU(cudaGetLastError(), "kernel launch");
+    c->h_dcv.resize(3 * (size_t)n);
+    MTD_CU(cudaMemcpyAsync(c->h_dcv.data(), grad, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->st),
+           "dcvdx");
+    MTD_CU(cudaStreamSynchronize(c->st), "dcvdx");
+    for (double &v : c->h_dcv) v = -v;
+    c->dcv_gen = c->step_gen;
+    c->dcv_cal = cal;
+    return MTD_OK;
+}
+
 mtd_status mtd_extract_peratom(mtd_ctx *c, const char *key, double *out, int n) {
     if (!c || !key || !out) return MTD_ERR_INVALID_ARG;
     std::string k(key);
@@ -1237,6 +1290,13 @@ mtd_status mtd_extract_peratom(mtd_ctx *c, const char *key, double *out, int n) 
     const std::string cal = k.substr(0, dot), prop = k.substr(dot + 1);
     if (n != c->n) return fail(c, MTD_ERR_INVALID_ARG, "atom count differs from the last step");
     MTD_CU(cudaStreamSynchronize(c->st), "extract");
+    if (prop == "dcvdx_x" || prop == "dcvdx_y" || prop == "dcvdx_z") {
+        mtd_status s = dcvdx(c, cal);
+        if (s != MTD_OK) return s;
+        const int a = prop.back() - 'x';
+        for (int t = 0; t < n; ++t) out[t] = c->h_dcv[3 * (size_t)t + a];
+        return MTD_OK;
+    }
     for (Unit &u : c->units) {
         for (size_t slot = 0; slot < u.calnames.size(); ++slot) {
             if (u.calnames[slot] != cal) continue;

@@ -244,7 +244,7 @@ struct BiasPlan {
     unsigned long long *nhills;
     double *out;           // [0..D) s, D: V, D+1: deposited flag, kOutSymOffset..: symbol values
     const DevStatus *status;   // a neighbour overflow this step: no deposit, zero force coefficients
-    const void *pad16;         // keeps sizeof a multiple of 16 (staged as 16-byte vectors)
+    struct WalkState *save;    // when set, the step's block-sum totals are kept here (per-atom gradients)
 };
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
 
@@ -268,6 +268,9 @@ void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int n
 // (a hill adds its full height and no slope at its own centre) and the force
 // coefficients.
 void launch_list_cvs(const BiasPlan *d_plan, WalkState *ws, cudaStream_t st);
+// Force coefficients of every unit for dCV/dx of one symbol (chain factor 1
+// on it, 0 on the others), from the block-sum totals kept in ws[0].
+void launch_symbol_coef(const BiasPlan *d_plan, int sym, const WalkState *ws, cudaStream_t st);
 void launch_list_finish(const BiasPlan *d_plan, long long step, const WalkState *ws, const double *vdv,
                         cudaStream_t st);
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st);
