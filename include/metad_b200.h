@@ -105,8 +105,12 @@ mtd_status mtd_post_force(mtd_ctx *ctx, int64_t step, int n, const double *x, co
                           const int *image, double *f, double virial[6]);
 
 /* Same step on device-resident arrays, enqueued on the context stream without
- * a host synchronisation.  f_in and f_out may alias.  Completion and device
- * error flags are collected by mtd_sync(). */
+ * a host synchronisation.  f_in and f_out may alias.  Up to four steps may be
+ * in flight: each call collects the outputs of steps that have finished (CVs,
+ * bias, HILLS rows) without waiting, and waits only when four are pending (or,
+ * with the hill-list bias, for the previous step, whose hill joins the list
+ * on the host).  mtd_compute_scalar / _vector report the last collected step;
+ * mtd_sync() collects every step and reports device error flags. */
 mtd_status mtd_post_force_device(mtd_ctx *ctx, int64_t step, int n, const double *d_x, const int *d_mask,
                                  const int *d_image, const double *d_f_in, double *d_f_out);
 

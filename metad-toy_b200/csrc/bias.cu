@@ -323,6 +323,7 @@ __device__ __forceinline__ void record_hill(const BiasPlan &P, long long step, c
     r.w = w;
     r.sigma = P.sigma;
     P.hills[h % (unsigned long long)P.hill_cap] = r;
+    *reinterpret_cast<HillRec *>(P.out + kOutHillOffset) = r;
     *P.nhills = h + 1;
 }
 

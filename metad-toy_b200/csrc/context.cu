@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <string>
 #include <vector>
@@ -78,6 +79,19 @@ template <typename P> void dfree(P *&p) {
 
 }  // namespace
 
+constexpr int kOutSlots = 4;
+struct OutSlot {
+    double out[64];
+    DevStatus status;
+    unsigned long long nhills;
+    double vir[8];
+};
+struct PendingOut {
+    int slot;
+    long long step;
+    bool virial;
+};
+
 struct mtd_ctx {
     int fp64 = 0;
     int device = 0;
@@ -115,6 +129,16 @@ struct mtd_ctx {
     double *d_vpart = nullptr;
     int cap_vpart = 0;
     double *d_vir = nullptr;
+    // Pinned outputs of a step.  A context owns kOutSlots of them: the device
+    // path writes step t into slot t mod kOutSlots and collects it once its
+    // event has completed, so the host never waits for the step it just
+    // enqueued; h_out / h_status / h_vir / h_nhills point at the slot in use.
+    OutSlot *h_slots = nullptr;
+    cudaEvent_t slot_ev[kOutSlots] = {};
+    bool ring = true;                    // false for walkers (fixed slot 0, captured in their graph)
+    int slot_next = 0;
+    std::deque<PendingOut> fifo;         // steps enqueued and not yet collected, oldest first
+    unsigned overflow_seen = 0;          // largest neighbour count of an overflowed step drained since mtd_sync
     double *h_out = nullptr;
     DevStatus *h_status = nullptr;
     double *h_vir = nullptr;
@@ -201,6 +225,14 @@ int record_stride(const mtd_ctx *c, const Unit &u) {
 }
 
 double env_cutoff(const Env &e) { return e.rc; }
+
+void use_slot(mtd_ctx *c, int k) {
+    OutSlot &o = c->h_slots[k];
+    c->h_out = o.out;
+    c->h_status = &o.status;
+    c->h_vir = o.vir;
+    c->h_nhills = &o.nhills;
+}
 
 CellGrid make_grid(const mtd_ctx *c) {
     CellGrid g{};
@@ -767,10 +799,18 @@ mtd_status enqueue_forces(mtd_ctx *c, long long step, const double *x, const int
     else run_forces<float>(c, c->last_sys, c->last_grid, x, mask, fin, fout, virial);
     MTD_CU(cudaGetLastError(), "kernel launch");
     // outputs of this step into pinned host memory
+    const int slot = c->ring ? c->slot_next : 0;
+    use_slot(c, slot);
     MTD_CU(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(double) * 64, cudaMemcpyDeviceToHost, c->st), "outputs");
     MTD_CU(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->st), "status");
     MTD_CU(cudaMemcpyAsync(c->h_nhills, c->d_nhills, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st), "hills");
     if (virial) MTD_CU(cudaMemcpyAsync(c->h_vir, c->d_vir, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->st), "virial");
+    if (c->ring) {
+        MTD_CU(cudaEventRecord(c->slot_ev[slot], c->st), "outputs");
+        c->fifo.push_back(PendingOut{slot, step, virial});
+        c->slot_next = (slot + 1) % kOutSlots;
+        return MTD_OK;
+    }
     c->want_virial = virial;
     c->pending = true;
     c->pending_step = step;
@@ -846,11 +886,19 @@ mtd_status collect(mtd_ctx *c) {
         unsigned long long from = c->hills_written;
         if (nh - from > (unsigned long long)kHillCap) from = nh - kHillCap;
         std::vector<HillRec> recs;
-        for (unsigned long long h = from; h < nh; ++h) {
+        if (nh - from == 1 && c->h_out[D + 1] != 0.0) {   // this step's hill, copied out with its outputs
             HillRec r;
-            MTD_CU(cudaMemcpy(&r, c->d_hills + (h % kHillCap), sizeof(HillRec), cudaMemcpyDeviceToHost), "hill record");
+            std::memcpy(&r, c->h_out + kOutHillOffset, sizeof(HillRec));
             write_hill_line(c, r);
             recs.push_back(r);
+        } else {
+            for (unsigned long long h = from; h < nh; ++h) {
+                HillRec r;
+                MTD_CU(cudaMemcpy(&r, c->d_hills + (h % kHillCap), sizeof(HillRec), cudaMemcpyDeviceToHost),
+                       "hill record");
+                write_hill_line(c, r);
+                recs.push_back(r);
+            }
         }
         c->hills_written = nh;
         if (c->nb) {
@@ -865,6 +913,35 @@ mtd_status collect(mtd_ctx *c) {
         std::fflush(c->f_rec);
     }
     if (c->h_status->nan_force) return fail(c, MTD_ERR_NAN, "STEIN_QL CV error: force is infinity, check your system or cv_value.");
+    return MTD_OK;
+}
+
+// Collects enqueued steps in order: every step whose outputs have arrived
+// (block: every step, waiting for each).  A step that overflowed a neighbour
+// list deposited nothing and applied no bias force; it is not collected, and
+// the overflow is kept for mtd_sync to report.
+mtd_status drain(mtd_ctx *c, bool block) {
+    while (!c->fifo.empty()) {
+        const PendingOut p = c->fifo.front();
+        if (block) {
+            MTD_CU(cudaEventSynchronize(c->slot_ev[p.slot]), "step outputs");
+        } else {
+            const cudaError_t q = cudaEventQuery(c->slot_ev[p.slot]);
+            if (q == cudaErrorNotReady) break;
+            MTD_CU(q, "step outputs");
+        }
+        c->fifo.pop_front();
+        use_slot(c, p.slot);
+        if (c->h_status->overflow) {
+            c->overflow_seen = std::max(c->overflow_seen, c->h_status->overflow);
+            continue;
+        }
+        c->pending = true;
+        c->pending_step = p.step;
+        c->want_virial = p.virial;
+        const mtd_status s = collect(c);
+        if (s != MTD_OK) return s;
+    }
     return MTD_OK;
 }
 
@@ -1033,10 +1110,13 @@ mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, 
         if (ce == cudaSuccess) ce = cudaMemset(c->d_out, 0, sizeof(double) * 64);
         if (ce == cudaSuccess) ce = cudaMemset(c->d_status, 0, sizeof(DevStatus));
         if (ce == cudaSuccess) ce = cudaMemset(c->d_nhills, 0, sizeof(unsigned long long));
-        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_out, sizeof(double) * 64);
-        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_status, sizeof(DevStatus));
-        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_vir, sizeof(double) * 8);
-        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_nhills, sizeof(unsigned long long));
+        if (ce == cudaSuccess) ce = cudaMallocHost((void **)&c->h_slots, sizeof(OutSlot) * kOutSlots);
+        if (ce == cudaSuccess) {
+            std::memset(c->h_slots, 0, sizeof(OutSlot) * kOutSlots);
+            use_slot(c, 0);
+        }
+        for (int k = 0; k < kOutSlots && ce == cudaSuccess; ++k)
+            ce = cudaEventCreateWithFlags(&c->slot_ev[k], cudaEventDisableTiming);
         s = cuda_check(c, ce, "context allocation");
     }
     *out = c;
@@ -1046,6 +1126,7 @@ mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, 
 void mtd_destroy(mtd_ctx *c) {
     if (!c) return;
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->h_slots) drain(c, true);   // hills of steps not yet collected still reach the HILLS file
     for (Env &e : c->envs) {
         dfree(e.list); dfree(e.count); dfree(e.key_r2); dfree(e.key_id); dfree(e.nkept);
     }
@@ -1059,10 +1140,9 @@ void mtd_destroy(mtd_ctx *c) {
     dfree(c->xs); dfree(c->pf); dfree(c->count); dfree(c->start); dfree(c->d_vpart);
     dfree(c->d_plan); dfree(c->d_grid); dfree(c->d_hills); dfree(c->d_nhills); dfree(c->d_out);
     dfree(c->d_status); dfree(c->d_vir);
-    if (c->h_out) cudaFreeHost(c->h_out);
-    if (c->h_status) cudaFreeHost(c->h_status);
-    if (c->h_vir) cudaFreeHost(c->h_vir);
-    if (c->h_nhills) cudaFreeHost(c->h_nhills);
+    if (c->h_slots) cudaFreeHost(c->h_slots);
+    for (int k = 0; k < kOutSlots; ++k)
+        if (c->slot_ev[k]) cudaEventDestroy(c->slot_ev[k]);
     if (c->own_st) cudaStreamDestroy(c->own_st);
     if (c->side_st) cudaStreamDestroy(c->side_st);
     if (c->nb) mtd_nnbias_destroy(c->nb);
@@ -1177,8 +1257,11 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
         s = enqueue_step(c, step, n, c->d_x, mask ? c->d_mask : nullptr, (image && virial) ? c->d_image : nullptr,
                          c->d_fin, c->d_fout, virial != nullptr, c->f_ready);
         if (s != MTD_OK) return s;
+        // the forces go back in the same stream pass (a failed attempt's are overwritten by the retry)
+        MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
         MTD_CU(cudaStreamSynchronize(c->st), "step");
         if (c->h_status->overflow == 0) break;
+        c->fifo.pop_back();   // the failed attempt is not collected
         // neighbour capacity too small: grow and run the step again
         const int need = (int)c->h_status->overflow;
         for (Env &e : c->envs) {
@@ -1189,13 +1272,10 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
             s = alloc_env(c, e, c->cap_n);
             if (s != MTD_OK) return s;
         }
-        c->pending = false;
         if (attempt == 3) return fail(c, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded");
     }
-    s = collect(c);
+    s = drain(c, true);
     if (s != MTD_OK) return s;
-    MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
-    MTD_CU(cudaStreamSynchronize(c->st), "f download");
     if (virial)
         for (int t = 0; t < 6; ++t) virial[t] = c->virial[t];
     return MTD_OK;
@@ -1208,19 +1288,26 @@ mtd_status mtd_post_force_device(mtd_ctx *c, int64_t step, int n, const double *
         mtd_status s = mtd_init(c);
         if (s != MTD_OK) return s;
     }
-    if (c->pending) {   // keep the previous step's outputs
-        MTD_CU(cudaStreamSynchronize(c->st), "step");
-        mtd_status s = collect(c);
-        if (s != MTD_OK) return s;
+    // steps already finished are collected without waiting; the host waits
+    // only when every output slot is in flight, or for the hill-list bias,
+    // whose new hills join the list on the host before the next step
+    mtd_status s = drain(c, c->nb != nullptr);
+    while (s == MTD_OK && (int)c->fifo.size() >= kOutSlots) {
+        MTD_CU(cudaEventSynchronize(c->slot_ev[c->fifo.front().slot]), "step outputs");
+        s = drain(c, false);
     }
+    if (s != MTD_OK) return s;
     return enqueue_step(c, step, n, d_x, d_mask, d_image, d_f_in, d_f_out, false);
 }
 
 mtd_status mtd_sync(mtd_ctx *c) {
     if (!c) return MTD_ERR_INVALID_ARG;
     MTD_CU(cudaStreamSynchronize(c->st), "sync");
-    if (c->h_status && c->h_status->overflow) {
-        const int need = (int)c->h_status->overflow;
+    const mtd_status sd = drain(c, true);
+    if (sd != MTD_OK) return sd;
+    if (c->overflow_seen) {
+        const int need = (int)c->overflow_seen;
+        c->overflow_seen = 0;
         for (Env &e : c->envs)
             if (e.M < need) {
                 e.M = ((need + 8) + 3) & ~3;
@@ -1518,6 +1605,7 @@ mtd_status mtd_walkers_create(int nwalk, int narg, const char *const *arg, const
     for (int k = 0; k < nwalk; ++k) {
         mtd_ctx *c = nullptr;
         const mtd_status s = mtd_create(narg, arg, &o, &c);
+        if (c) c->ring = false;
         W->w.push_back(c);
         if (s != MTD_OK) return wfail(W, s, c ? c->err : "context creation failed");
         if (c->cfg.hill_list()) return wfail(W, MTD_ERR_UNSUPPORTED, "walkers share a grid: CV_dim <= 3, no NN_BIAS");

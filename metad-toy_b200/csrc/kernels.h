@@ -242,11 +242,15 @@ struct BiasPlan {
     HillRec *hills;
     int hill_cap;
     unsigned long long *nhills;
-    double *out;           // [0..D) s, D: V, D+1: deposited flag, kOutSymOffset..: symbol values
+    double *out;           // [0..D) s, D: V, D+1: deposited flag, kOutSymOffset..: symbol values,
+                           // kOutHillOffset..: the hill recorded last (a HillRec)
     const DevStatus *status;   // a neighbour overflow this step: no deposit, zero force coefficients
     struct WalkState *save;    // when set, the step's block-sum totals are kept here (per-atom gradients)
 };
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
+constexpr int kOutHillOffset = 48;  // out[kOutHillOffset ..+7): the last HillRec, copied out with the step's outputs
+static_assert(kOutSymOffset + kMaxSymbols <= kOutHillOffset && kOutHillOffset * 8 + sizeof(HillRec) <= 64 * 8,
+              "output layout");
 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st);
 

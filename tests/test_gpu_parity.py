@@ -158,3 +158,35 @@ def test_neighbour_overflow_on_the_device_path_asks_for_a_repeat():
     m.sync()
     o4 = H.oracle_local(x, L, 4)
     assert abs(m.cv[0] - o4["cv"]) < 1e-9 * abs(o4["cv"])
+
+
+def test_device_path_runs_ahead_and_collects_every_step(tmp_path):
+    """Twelve device steps enqueued with no host wait between them (more steps
+    than output slots in flight), then one mtd_sync: the HILLS file, the last
+    step's CVs and bias and every step's forces equal the host path's."""
+    import torch
+
+    x, L = systems.small_slab(nxy=6, nz_fcc=3, nz_bcc=4, n_liq=300)
+    xs = [np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.05, 100, s), L)) for s in range(12)]
+    args = H.fix_args_local(pace=2)
+    ref = mtd.Metad(args, precision="fp64", hills_path=str(tmp_path / "H1"))
+    ref.set_box([0, 0, 0], L)
+    f_ref = []
+    for s, xv in enumerate(xs):
+        f = np.zeros_like(xv)
+        ref.post_force(s, xv, f)
+        f_ref.append(f)
+    cv_ref, bias_ref = ref.cv.copy(), ref.compute_scalar()
+    ref.close()
+    m = mtd.Metad(args, precision="fp64", hills_path=str(tmp_path / "H2"))
+    m.set_box([0, 0, 0], L)
+    dxs = [torch.from_numpy(xv).cuda() for xv in xs]
+    fs = [torch.zeros_like(d) for d in dxs]
+    for s in range(12):
+        m.post_force_device(s, xs[s].shape[0], dxs[s].data_ptr(), fs[s].data_ptr(), fs[s].data_ptr())
+    m.sync()
+    assert np.array_equal(m.cv, cv_ref) and m.compute_scalar() == bias_ref
+    m.close()
+    assert open(tmp_path / "H1").read() == open(tmp_path / "H2").read()
+    for s in range(12):
+        assert np.array_equal(fs[s].cpu().numpy(), f_ref[s])
