@@ -224,6 +224,28 @@ def secondary_workload(name):
     return args, xs, L, desc
 
 
+def kernel_profile(m, step_fn, flush, steps, stream):
+    """Per-kernel durations from CUDA events recorded between the launches
+    of `steps` steps.  The pass runs on its own stream: event intervals on the
+    legacy default stream came out inflated by several microseconds per
+    kernel, against per-kernel ncu durations of the same build."""
+    import torch
+    ps = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    m.set_stream(ps.cuda_stream)
+    m.profile(True)
+    with torch.cuda.stream(ps):
+        for _ in range(steps):
+            flush.zero_()
+            step_fn()
+    m.sync()
+    prof = m.profile_report()
+    m.profile(False)
+    m.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    return prof
+
+
 def run_secondary(args, local):
     import torch
     import mtd
@@ -244,14 +266,13 @@ def run_secondary(args, local):
         m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
         step += 1
     m.sync()
-    m.profile(True)
-    for _ in range(max(5, args.steps // 3)):
-        flush.zero_()
+
+    def one_step():
+        nonlocal step
         m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
         step += 1
-    m.sync()
-    prof = m.profile_report()
-    m.profile(False)
+
+    prof = kernel_profile(m, one_step, flush, max(5, args.steps // 3), stream)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     hx = [torch.from_numpy(x).pin_memory() for x in xs]
     hf = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
@@ -513,14 +534,7 @@ def main():
     except Exception:
         nbar = 8.0
 
-    # per-kernel durations (separate pass, CUDA events between launches)
-    m.profile(True)
-    for _ in range(max(5, args.steps // 3)):
-        flush.zero_()
-        dev_step()
-    m.sync()
-    prof = m.profile_report()
-    m.profile(False)
+    prof = kernel_profile(m, dev_step, flush, max(5, args.steps // 3), stream)
 
     hx = [torch.from_numpy(x).pin_memory() for x in xs]
     hf = torch.zeros((n, 3), dtype=torch.float64).pin_memory()

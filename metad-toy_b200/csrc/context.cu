@@ -728,12 +728,16 @@ void run_forces(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x,
     }
 }
 
-// Adds the kernel intervals of the last profiled step to the per-name totals.
+// Adds the kernel intervals of the profiled steps in the buffer to the
+// per-name totals (an interval ending at a step's "start" mark spans the gap
+// between two steps and is not counted).  The marks of many steps are kept so
+// that profiling does not make the host wait for every step.
 void prof_collect(mtd_ctx *c) {
     Prof &p = c->prof;
     if (p.n >= 2) {
         cudaEventSynchronize(p.ev[p.n - 1]);
         for (int i = 1; i < p.n; ++i) {
+            if (std::strcmp(p.name[i], "start") == 0) continue;
             float ms = 0.f;
             cudaEventElapsedTime(&ms, p.ev[i - 1], p.ev[i]);
             auto &t = c->prof_total[p.name[i]];
@@ -747,7 +751,7 @@ void prof_collect(mtd_ctx *c) {
 struct ProfScope {
     explicit ProfScope(mtd_ctx *c) {
         if (c->prof.on) {
-            prof_collect(c);
+            if (c->prof.n > kProfMax - 64) prof_collect(c);
             prof_set(&c->prof);
             prof_mark("start", c->st);
         }

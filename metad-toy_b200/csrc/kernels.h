@@ -106,7 +106,7 @@ struct NeighDev {
 // ------------------------------------------------------------------ per-kernel timing
 // When a context enables profiling, every launcher records a CUDA event after
 // each kernel on the launch stream; consecutive events bracket one kernel.
-constexpr int kProfMax = 128;
+constexpr int kProfMax = 1024;   // marks of several steps, read back when the buffer is nearly full
 struct Prof {
     bool on = false;
     int n = 0;

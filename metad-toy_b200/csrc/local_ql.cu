@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
 
 // Pass 2: LQ_lm, LQ, the e1/e2 weights of the adjoint and block partial sums.
 template <int LA, int LB, typename T, bool STEP>
-__global__ void __launch_bounds__(kBlock) k_local_lq(LocalDev<T> d) {
+__global__ void __launch_bounds__(kBlock, 4) k_local_lq(LocalDev<T> d) {
     using S = LSet<LA, LB, T>;
     __shared__ double smem[5 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
 
 // Pass 4: gather forces, f_dst = f_src - dV/dx, plus the virial block partials.
 template <int LA, int LB, typename T, bool STEP>
-__global__ void __launch_bounds__(kBlock) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
+__global__ void __launch_bounds__(kBlock, 4) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
                                                         double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                         double *vpart, DevStatus *status) {
     using S = LSet<LA, LB, T>;

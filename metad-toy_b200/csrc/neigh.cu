@@ -267,8 +267,10 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s,
                 }
                 const float sz = (float)oz * g.hf[2] - a.z;
                 const int jb = __ldg(s.start + col + z), je = __ldg(s.start + col + z + 1);
+                float4 nxt = jb < je ? __ldg(s.pf + jb) : make_float4(0.f, 0.f, 0.f, 0.f);
                 for (int j = jb; j < je; ++j) {
-                    const float4 b = __ldg(s.pf + j);
+                    const float4 b = nxt;
+                    if (j + 1 < je) nxt = __ldg(s.pf + j + 1);
                     const float dx = b.x + sx, dy = b.y + sy, dz = b.z + sz;
                     const float r2f = dx * dx + dy * dy + dz * dz;
                     if (r2f > ns.hi2 || j == k) continue;
