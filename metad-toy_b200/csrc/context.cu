@@ -110,7 +110,7 @@ struct mtd_ctx {
     int n = 0, npad = 0, cap_n = 0, n_plan = -1;
     double *d_x = nullptr, *d_fin = nullptr, *d_fout = nullptr;
     int *d_mask = nullptr, *d_image = nullptr;
-    int *cellof = nullptr, *slot = nullptr, *perm = nullptr, *smask = nullptr;
+    int *cellof = nullptr, *slot = nullptr, *perm = nullptr, *smask = nullptr, *arrival = nullptr;
     double *xs = nullptr;
     float4 *pf = nullptr;
     int *count = nullptr, *start = nullptr;
@@ -363,7 +363,7 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
     if (npad > c->cap_n) {
         const int cap = npad + npad / 4;
         dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
-        dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask);
+        dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask); dfree(c->arrival);
         dfree(c->xs); dfree(c->pf); dfree(c->d_vpart);
         MTD_CU(dalloc(&c->d_x, sizeof(double) * 3 * (size_t)cap), "x");
         MTD_CU(dalloc(&c->d_fin, sizeof(double) * 3 * (size_t)cap), "f");
@@ -373,6 +373,7 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
         MTD_CU(dalloc(&c->cellof, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->slot, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->perm, sizeof(int) * (size_t)cap), "perm");
+        MTD_CU(dalloc(&c->arrival, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->smask, sizeof(int) * (size_t)cap), "mask");
         MTD_CU(dalloc(&c->xs, sizeof(double) * 3 * (size_t)cap), "x sorted");
         MTD_CU(dalloc(&c->pf, sizeof(float4) * (size_t)cap), "x float");
@@ -631,6 +632,7 @@ SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
     s.count = c->count;
     s.start = c->start;
     s.perm = c->perm;
+    s.arrival = c->arrival;
     s.smask = c->smask;
     s.xs = c->xs;
     s.pf = c->pf;
@@ -778,8 +780,7 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
         if (sc != MTD_OK) return sc;
         s.count = c->count;
         s.start = c->start;
-        launch_build_cells(g, s, c->st);
-        c->launches += 6;
+        c->launches += launch_build_cells(g, s, c->st);
         for (Env &e : c->envs) {
             const NeighSpec ns = neigh_spec(e);
             launch_neighbors(g, s, ns, env_dev(e), c->d_status, c->st);
@@ -1140,7 +1141,7 @@ void mtd_destroy(mtd_ctx *c) {
         dfree(u.partials); dfree(u.coef); dfree(u.kvec); dfree(u.rho); dfree(u.skn);
     }
     dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
-    dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask);
+    dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask); dfree(c->arrival);
     dfree(c->xs); dfree(c->pf); dfree(c->count); dfree(c->start); dfree(c->d_vpart);
     dfree(c->d_plan); dfree(c->d_grid); dfree(c->d_hills); dfree(c->d_nhills); dfree(c->d_out);
     dfree(c->d_status); dfree(c->d_vir);

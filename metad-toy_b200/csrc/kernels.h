@@ -70,6 +70,7 @@ struct SysDev {
     const int *mask;      // caller order, may be null (all groups)
     const int *image;     // caller order, may be null
     int *cellof, *slot, *count, *start, *perm, *smask;
+    int *arrival;         // [n] atoms by cell in atomic arrival order (cell-list scratch)
     double *xs;           // sorted raw coordinates AoS npad*3
     float4 *pf;           // sorted cell-relative coordinates + packed cell
 };
@@ -117,7 +118,8 @@ void prof_set(Prof *p);                          // active profiler of this host
 void prof_mark(const char *name, cudaStream_t st);
 
 // ------------------------------------------------------------------ neighbours
-void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st);
+// Returns the number of kernels launched.
+int launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st);
 void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, DevStatus *status,
                       cudaStream_t st);
 

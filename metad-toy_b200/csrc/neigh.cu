@@ -5,8 +5,9 @@
 // get_environment_Steinhardt_LocalQ (src/cvs/CVs_Steinhardt_Local.cu:1210-1285)
 // and get_environment_Strufactor (src/cvs/CVs_Strufactor.cu:1014-1080).
 //
-// Per step: bin atoms to cells (counting sort: histogram, three-pass scan,
-// scatter, per-cell sort by caller index so the order is deterministic), then
+// Per step: bin atoms to cells (counting sort: histogram, scan, scatter in
+// atomic arrival order, then every atom moves to its rank by caller index
+// within its cell, so the order is deterministic), then
 // one thread per sorted atom walks its 9 neighbour-cell columns (z-adjacent
 // cells are contiguous in the sorted order).  A candidate is decided by its
 // FP32 cell-relative distance unless it lies within ~1e-5 of the bound, where
@@ -104,46 +105,60 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add(int *__restrict__ start
     if (i < ncell) start[i] += bsum[blockIdx.x];
 }
 
+// Single-kernel add-back when the block totals fit one block: each block sums
+// the totals of the blocks before it (the last block also writes the total).
+__global__ void __launch_bounds__(kScanBlock) k_scan_add_fused(int *__restrict__ start, const int *__restrict__ bsum,
+                                                               int ncell, int nb) {
+    __shared__ int red[32];
+    const int b = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int v = threadIdx.x < b ? bsum[threadIdx.x] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    int off = 0;
+#pragma unroll 1
+    for (int w = 0; w < (kScanBlock >> 5); ++w) off += red[w];
+    const int i = b * kScanBlock + threadIdx.x;
+    if (i < ncell) start[i] += off;
+    if (b == nb - 1 && threadIdx.x == 0) start[ncell] = off + bsum[b];
+}
+
 __global__ void k_scatter(SysDev s) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
-    s.perm[s.start[s.cellof[i]] + s.slot[i]] = i;
+    s.arrival[s.start[s.cellof[i]] + s.slot[i]] = i;
 }
 
-// Per cell: order members by caller index (removes the atomic arrival order),
-// then write the sorted per-atom arrays.
-__global__ void k_cellsort(CellGrid g, SysDev s) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.ncell) return;
+// One thread per sorted slot: the atom that arrived there takes the place of
+// its rank by caller index among its cell's members (removes the atomic
+// arrival order), and its sorted per-atom arrays are written there.
+__global__ void k_place(CellGrid g, SysDev s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= s.n) return;
+    const int i = s.arrival[k];
+    const int c = s.cellof[i];
     const int b = s.start[c], e = s.start[c + 1];
-    for (int a = b + 1; a < e; ++a) {
-        int v = s.perm[a];
-        int t = a - 1;
-        while (t >= b && s.perm[t] > v) {
-            s.perm[t + 1] = s.perm[t];
-            --t;
-        }
-        s.perm[t + 1] = v;
-    }
+    int rank = 0;
+    for (int t = b; t < e; ++t) rank += s.arrival[t] < i;
+    const int d = b + rank;
+    s.perm[d] = i;
+    const double x0 = s.x[3 * i], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
+    s.xs[3 * d] = x0;
+    s.xs[3 * d + 1] = x1;
+    s.xs[3 * d + 2] = x2;
     const int cz = c % g.nc[2], cy = (c / g.nc[2]) % g.nc[1], cx = c / (g.nc[2] * g.nc[1]);
-    for (int k = b; k < e; ++k) {
-        int i = s.perm[k];
-        const double x0 = s.x[3 * i], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
-        s.xs[3 * k] = x0;
-        s.xs[3 * k + 1] = x1;
-        s.xs[3 * k + 2] = x2;
-        double w0, w1, w2;
-        cell_coord(x0, g, 0, w0);
-        cell_coord(x1, g, 1, w1);
-        cell_coord(x2, g, 2, w2);
-        float4 p;
-        p.x = (float)(w0 - cx * g.h[0]);
-        p.y = (float)(w1 - cy * g.h[1]);
-        p.z = (float)(w2 - cz * g.h[2]);
-        p.w = __int_as_float(pack_cell(cx, cy, cz));
-        s.pf[k] = p;
-        s.smask[k] = s.mask ? s.mask[i] : -1;
-    }
+    double w0, w1, w2;
+    cell_coord(x0, g, 0, w0);
+    cell_coord(x1, g, 1, w1);
+    cell_coord(x2, g, 2, w2);
+    float4 p;
+    p.x = (float)(w0 - cx * g.h[0]);
+    p.y = (float)(w1 - cy * g.h[1]);
+    p.z = (float)(w2 - cz * g.h[2]);
+    p.w = __int_as_float(pack_cell(cx, cy, cz));
+    s.pf[d] = p;
+    s.smask[d] = s.mask ? s.mask[i] : -1;
 }
 
 // FP64 decision on raw coordinates (the oracle's criterion, operation by operation).
@@ -331,7 +346,7 @@ __global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, Nei
 
 }  // namespace
 
-void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
+int launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
     cudaMemsetAsync(s.count, 0, sizeof(int) * (size_t)g.ncell, st);
     const int nb = (s.n + kBlock - 1) / kBlock;
     if (s.n > 0) k_bin<<<nb, kBlock, 0, st>>>(g, s);
@@ -340,14 +355,22 @@ void launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
         const int sb = (g.ncell + kScanBlock - 1) / kScanBlock;
         int *bsum = s.start + g.ncell + 1;   // scratch after the ncell + 1 starts
         k_scan_blocks<<<sb, kScanBlock, 0, st>>>(s.count, s.start, bsum, g.ncell);
-        k_scan_top<<<1, kScanBlock, 0, st>>>(bsum, sb, s.start, g.ncell);
-        k_scan_add<<<sb, kScanBlock, 0, st>>>(s.start, bsum, g.ncell);
+        if (sb <= kScanBlock) {
+            k_scan_add_fused<<<sb, kScanBlock, 0, st>>>(s.start, bsum, g.ncell, sb);
+        } else {
+            k_scan_top<<<1, kScanBlock, 0, st>>>(bsum, sb, s.start, g.ncell);
+            k_scan_add<<<sb, kScanBlock, 0, st>>>(s.start, bsum, g.ncell);
+        }
     }
     prof_mark("cell_scan", st);
-    if (s.n > 0) k_scatter<<<nb, kBlock, 0, st>>>(s);
-    prof_mark("cell_scatter", st);
-    k_cellsort<<<(g.ncell + kBlock - 1) / kBlock, kBlock, 0, st>>>(g, s);
-    prof_mark("cell_sort", st);
+    if (s.n > 0) {
+        k_scatter<<<nb, kBlock, 0, st>>>(s);
+        prof_mark("cell_scatter", st);
+        k_place<<<nb, kBlock, 0, st>>>(g, s);
+        prof_mark("cell_sort", st);
+    }
+    const int sb = (g.ncell + kScanBlock - 1) / kScanBlock;
+    return (s.n > 0 ? 3 : 0) + (sb <= kScanBlock ? 2 : 3);
 }
 
 void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, DevStatus *status,
