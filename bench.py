@@ -224,6 +224,16 @@ def secondary_workload(name):
     return args, xs, L, desc
 
 
+def timing_stream():
+    """A dedicated stream made torch's current one: the L2 flush, the
+    library's kernels (set_stream) and the CUDA events all go to it, so each
+    timed interval holds exactly one step, after the flush has completed."""
+    import torch
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    return st
+
+
 def kernel_profile(m, step_fn, flush, steps, stream):
     """Per-kernel durations from CUDA events recorded between the launches
     of `steps` steps.  The pass runs on its own stream: event intervals on the
@@ -256,7 +266,7 @@ def run_secondary(args, local):
     m = mtd.Metad(fa, precision=prec, device=local)
     m.set_box([0, 0, 0], L)
     m.init()
-    stream = torch.cuda.current_stream()
+    stream = timing_stream()
     m.set_stream(stream.cuda_stream)
     dx = [torch.from_numpy(x).cuda() for x in xs]
     f = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
@@ -338,7 +348,7 @@ def run_nnbias(args, local):
     nb.fit(ntrain=262144, iters=args.nn_iters, batch=8192, lr=3e-3, seed=2)
     fit_s = time.perf_counter() - t0
     mx, rms = nb.validate(npts=65536, seed=7, tol=1e-3)
-    stream = torch.cuda.current_stream()
+    stream = timing_stream()
     d_s = torch.tensor(c[len(c) // 2], dtype=torch.float64, device="cuda")
     d_v = torch.zeros(1, dtype=torch.float64, device="cuda")
     d_g = torch.zeros(4, dtype=torch.float64, device="cuda")
@@ -355,6 +365,26 @@ def run_nnbias(args, local):
         torch.cuda.synchronize()
         res[name] = a.elapsed_time(b) * 1e3 / args.steps
     pts = systems.CV4_LO + (systems.CV4_HI - systems.CV4_LO) * np.random.default_rng(3).random((65536, 4))
+    # V and dV/ds at 65,536 device-resident points: exact FP64 sum vs network,
+    # CUDA events on the launching stream
+    d_p = torch.from_numpy(np.ascontiguousarray(pts)).cuda()
+    b_v = torch.zeros(len(pts), dtype=torch.float64, device="cuda")
+    b_g = torch.zeros((len(pts), 4), dtype=torch.float64, device="cuda")
+    batch = {}
+    for name, use in [("exact", 0), ("nn", 1)]:
+        reps = 3 if use == 0 else 20
+        nb.eval_device(len(pts), d_p.data_ptr(), b_v.data_ptr(), b_g.data_ptr(), use_nn=use, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            nb.eval_device(len(pts), d_p.data_ptr(), b_v.data_ptr(), b_g.data_ptr(), use_nn=use,
+                           stream=stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        batch[name + "_us"] = a.elapsed_time(b) * 1e3 / reps
+    batch["speedup"] = batch["exact_us"] / batch["nn_us"]
+    # the same through the host-array calls (conversions, copies, allocations included)
     t0 = time.perf_counter()
     nb.exact(pts)
     ex_s = time.perf_counter() - t0
@@ -380,7 +410,8 @@ def run_nnbias(args, local):
             "workload": "nn", "unit": "us/step", "higher_is_better": False,
             "exact_us_per_step": res["exact"], "nn_us_per_step": res["nn"],
             "speedup_per_step": res["exact"] / res["nn"], "per_step_vs_hills": scaling,
-            "batch_65536_points_s": {"exact": ex_s, "nn": nn_s},
+            "batch_65536_points_device": batch,
+            "batch_65536_points_host_api_s": {"exact": ex_s, "nn": nn_s},
             "hills": int(len(h)), "vmax_eV": nb.vscale, "max_abs_err_eV": mx, "rms_err_eV": rms,
             "tolerance_eV": 1e-3, "tolerance_met": bool(mx <= 1e-3), "fit_s": fit_s,
             "fit": {"ntrain": 262144, "iters": args.nn_iters, "batch": 8192, "lr": 3e-3},
@@ -443,7 +474,6 @@ def run_walkers(args, local):
             W.sync()
             step += 1
         launches = W.launch_count()
-        stream = torch.cuda.current_stream()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -508,7 +538,7 @@ def main():
     m = mtd.Metad(fix_args(), precision=args.precision, device=local)
     m.set_box([0, 0, 0], L)
     m.init()
-    stream = torch.cuda.current_stream()
+    stream = timing_stream()
     m.set_stream(stream.cuda_stream)
     dx = [torch.from_numpy(x).cuda() for x in xs]
     f_in = torch.zeros((n, 3), dtype=torch.float64, device="cuda")

@@ -282,6 +282,13 @@ int mtd_nnbias_usable(const mtd_nnbias *nb);
 mtd_status mtd_nnbias_point_device(mtd_nnbias *nb, const double *d_s, double *d_V, double *d_dV, int use_nn,
                                    void *stream);
 
+/* Bias at npts device-resident points (rows of D doubles) into d_V (npts) and
+ * d_dV (npts rows of D; NULL = values only), enqueued on `stream`; use_nn as
+ * above.  The network path keeps grow-only scratch in the object (allocated
+ * on the first call of a larger batch).  No counterpart in the reference. */
+mtd_status mtd_nnbias_eval_device(mtd_nnbias *nb, int npts, const double *d_pts, double *d_V, double *d_dV,
+                                  int use_nn, void *stream);
+
 /* Checks: the FP32 master parameters (17,281 floats: W1[128][4], b1[128],
  * W2[128][128], b2[128], w3[128], b3), the output scale, and one gradient of
  * the mean squared error sum_i (V_theta(s_i)/vscale - t_i/vscale)^2 / npts on

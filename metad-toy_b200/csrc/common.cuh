@@ -168,10 +168,15 @@ __device__ __forceinline__ void unpack_image(int img, int &ix, int &iy, int &iz)
 // remainder |r| <= pi/4 goes to FP32, and sin r, cos r come from their Taylor
 // series to degree 9 and 10 (remainders below 2e-9 and 2e-10 on |r| <= pi/4,
 // under the FP32 rounding of the result), rotated back by the quadrant.
+// The nearest multiple comes from adding 1.5 * 2^52 (an FMA rounds ph * 2/pi
+// to an integer held in the low mantissa bits, read back as q), so the
+// reduction needs no rounding or conversion instruction; |ph| < 2^51.
 __device__ __forceinline__ void phase_sincos_f32(double ph, float &s, float &c) {
-    const double n = rint(ph * 0.63661977236758134308);                 // 2 / pi
+    constexpr double kRound = 6755399441055744.0;                        // 1.5 * 2^52
+    const double t = fma(ph, 0.63661977236758134308, kRound);            // 2 / pi
+    const double n = t - kRound;
     const float r = (float)fma(-n, 1.5707963267948966192, ph);          // pi / 2
-    const int q = (int)(long long)n & 3;
+    const int q = __double2loint(t) & 3;
     const float r2 = r * r;
     float sp = fmaf(r2, 1.0f / 362880.0f, -1.0f / 5040.0f);
     sp = fmaf(sp, r2, 1.0f / 120.0f);

@@ -323,13 +323,16 @@ __global__ void k_mlp_gradsum(int ntiles, const float *__restrict__ part, float 
 constexpr int kHillTile = 256;
 constexpr double kExpCut = 40.0;
 
-__global__ void __launch_bounds__(256) k_hillsum_batch(int D, int npts, const double *__restrict__ pts, int nh,
-                                                       const double *__restrict__ hills, double *V, double *dV) {
+// Points and gradients are rows of `ps` / `gs` doubles (kIn, or D for caller
+// layouts); a gradient row of D < gs leaves the rest unwritten.
+__global__ void __launch_bounds__(256) k_hillsum_batch(int D, int npts, const double *__restrict__ pts, int ps, int nh,
+                                                       const double *__restrict__ hills, double *V, double *dV,
+                                                       int gs) {
     __shared__ double sh[kHillTile * 8];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double s[kIn] = {0, 0, 0, 0};
     if (i < npts)
-        for (int k = 0; k < D; ++k) s[k] = pts[(size_t)i * kIn + k];
+        for (int k = 0; k < D; ++k) s[k] = pts[(size_t)i * ps + k];
     double v = 0.0, g[kIn] = {0, 0, 0, 0};
     for (int h0 = 0; h0 < nh; h0 += kHillTile) {
         const int nt = min(kHillTile, nh - h0);
@@ -356,8 +359,30 @@ __global__ void __launch_bounds__(256) k_hillsum_batch(int D, int npts, const do
     if (i < npts) {
         V[i] = v;
         if (dV)
-            for (int k = 0; k < kIn; ++k) dV[(size_t)i * kIn + k] = g[k];
+            for (int k = 0; k < min(gs, kIn); ++k)
+                if (k < D || gs == kIn) dV[(size_t)i * gs + k] = g[k];
     }
+}
+
+// Caller points (rows of D doubles) to the network's normalised FP32 inputs.
+__global__ void k_nb_inputs(int D, int npts, const double *__restrict__ pts, double lo0, double lo1, double lo2,
+                            double lo3, double sc0, double sc1, double sc2, double sc3, float *x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npts) return;
+    const double lo[kIn] = {lo0, lo1, lo2, lo3}, sc[kIn] = {sc0, sc1, sc2, sc3};
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) x[(size_t)i * kIn + k] = k < D ? (float)(sc[k] * (pts[(size_t)i * D + k] - lo[k]) - 1.0) : 0.f;
+}
+
+// Network outputs to V = vscale y and dV/ds = vscale dy/du du/ds (FP64, rows of D).
+__global__ void k_nb_outputs(int D, int npts, const float *__restrict__ y, const float *__restrict__ ds,
+                             double vscale, double sc0, double sc1, double sc2, double sc3, double *V, double *dV) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npts) return;
+    const double sc[kIn] = {sc0, sc1, sc2, sc3};
+    V[i] = vscale * (double)y[i];
+    if (dV)
+        for (int k = 0; k < D; ++k) dV[(size_t)i * D + k] = vscale * (double)ds[(size_t)i * kIn + k] * sc[k];
 }
 
 // One point, hills spread over blocks; block partials reduced in block order by the last block.
@@ -491,6 +516,9 @@ struct mtd_nnbias {
     int adam_t = 0;
     int *d_err = nullptr;
     double *d_pt = nullptr, *d_ppart = nullptr, *d_pout = nullptr;
+    // device batch evaluation scratch (grown on demand)
+    float *d_bx = nullptr, *d_by = nullptr, *d_bds = nullptr;
+    int cap_b = 0;
     unsigned int *d_ticket = nullptr;
     // training pool
     int ntrain = 0;
@@ -580,7 +608,8 @@ mtd_status nb_exact_host(mtd_nnbias *b, int npts, const double *pts, double *V, 
     NB_CU(cudaMalloc(&d_V, sizeof(double) * npts), "values");
     NB_CU(cudaMalloc(&d_dV, sizeof(double) * (size_t)npts * kIn), "gradients");
     cudaMemcpyAsync(d_p, p4.data(), sizeof(double) * p4.size(), cudaMemcpyHostToDevice, b->st);
-    k_hillsum_batch<<<(npts + 255) / 256, 256, 0, b->st>>>(b->D, npts, d_p, b->nh, b->d_hills, d_V, d_dV);
+    k_hillsum_batch<<<(npts + 255) / 256, 256, 0, b->st>>>(b->D, npts, d_p, kIn, b->nh, b->d_hills, d_V, d_dV,
+                                                           kIn);
     std::vector<double> g((size_t)npts * kIn);
     cudaMemcpyAsync(V, d_V, sizeof(double) * npts, cudaMemcpyDeviceToHost, b->st);
     cudaMemcpyAsync(g.data(), d_dV, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, b->st);
@@ -698,7 +727,7 @@ void mtd_nnbias_destroy(mtd_nnbias *b) {
     if (b->st) cudaStreamSynchronize(b->st);
     void *ptrs[] = {b->d_hills, b->d_master, b->d_mom, b->d_vel, b->d_W1, b->d_b1, b->d_b2, b->d_w3, b->d_b3,
                     b->d_W2, b->d_W2t, b->d_part, b->d_loss, b->d_err, b->d_pt, b->d_pout, b->d_ppart,
-                    b->d_ticket, b->d_xt, b->d_tt};
+                    b->d_ticket, b->d_xt, b->d_tt, b->d_bx, b->d_by, b->d_bds};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->st) cudaStreamDestroy(b->st);
@@ -940,6 +969,52 @@ int mtd_nnbias_usable(const mtd_nnbias *b) { return b && b->validated ? 1 : 0; }
 // Bias at one device-resident point (D doubles) into d_V (1) and d_dV (D),
 // enqueued on `stream`: use_nn = 1 the network, 0 the exact hill sum,
 // -1 the network when the last validation passed, else the exact sum.
+mtd_status mtd_nnbias_eval_device(mtd_nnbias *b, int npts, const double *d_pts, double *d_V, double *d_dV,
+                                  int use_nn, void *stream) {
+    if (!b || npts < 0 || (npts > 0 && (!d_pts || !d_V))) return MTD_ERR_INVALID_ARG;
+    if (npts == 0) return MTD_OK;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->st;
+    const bool nn = use_nn > 0 || (use_nn < 0 && b->validated);
+    const int nb = (npts + 255) / 256;
+    if (!nn) {
+        if (b->nh == 0) {
+            NB_CU(cudaMemsetAsync(d_V, 0, sizeof(double) * npts, st), "bias");
+            if (d_dV) NB_CU(cudaMemsetAsync(d_dV, 0, sizeof(double) * npts * b->D, st), "bias");
+            return MTD_OK;
+        }
+        k_hillsum_batch<<<nb, 256, 0, st>>>(b->D, npts, d_pts, b->D, b->nh, b->d_hills, d_V, d_dV, b->D);
+        NB_CU(cudaGetLastError(), "exact hill sum");
+        return MTD_OK;
+    }
+    if (npts > b->cap_b) {
+        cudaFree(b->d_bx);
+        cudaFree(b->d_by);
+        cudaFree(b->d_bds);
+        b->d_bx = b->d_by = b->d_bds = nullptr;
+        b->cap_b = 0;
+        NB_CU(cudaMalloc(&b->d_bx, sizeof(float) * (size_t)npts * kIn), "points");
+        NB_CU(cudaMalloc(&b->d_by, sizeof(float) * (size_t)npts), "values");
+        NB_CU(cudaMalloc(&b->d_bds, sizeof(float) * (size_t)npts * kIn), "gradients");
+        b->cap_b = npts;
+    }
+    double sc[kIn];
+    for (int k = 0; k < kIn; ++k) sc[k] = 2.0 / (b->hi[k] - b->lo[k]);
+    k_nb_inputs<<<nb, 256, 0, st>>>(b->D, npts, d_pts, b->lo[0], b->lo[1], b->lo[2], b->lo[3], sc[0], sc[1], sc[2],
+                                    sc[3], b->d_bx);
+    mtd_status s = nb_tile_attr(b);
+    if (s != MTD_OK) return s;
+    const int ntiles = (npts + kH - 1) / kH;
+    if (d_dV)
+        k_mlp_tile<MODE_GRAD_S><<<ntiles, 128, kTileSmem, st>>>(nb_dev(b), npts, b->d_bx, nullptr, b->d_by, b->d_bds,
+                                                                nullptr, nullptr, 0.f, b->d_err);
+    else
+        k_mlp_tile<MODE_FWD><<<ntiles, 128, kTileSmem, st>>>(nb_dev(b), npts, b->d_bx, nullptr, b->d_by, nullptr,
+                                                             nullptr, nullptr, 0.f, b->d_err);
+    k_nb_outputs<<<nb, 256, 0, st>>>(b->D, npts, b->d_by, b->d_bds, b->vscale, sc[0], sc[1], sc[2], sc[3], d_V, d_dV);
+    NB_CU(cudaGetLastError(), "network");
+    return MTD_OK;
+}
+
 mtd_status mtd_nnbias_point_device(mtd_nnbias *b, const double *d_s, double *d_V, double *d_dV, int use_nn,
                                    void *stream) {
     if (!b || !d_s || !d_V || !d_dV) return MTD_ERR_INVALID_ARG;

@@ -130,27 +130,25 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
 constexpr int kSkChunk = 16;       // reals per register tile (8 k-vectors per pass over the atoms)
 constexpr int kSkBlocks = 148 * 8;  // grid for the partial sums (8 blocks per SM)
 
-template <bool FP64> __device__ __forceinline__ void phase_sincos(double ph, double &s, double &c) {
-    if (FP64) {
-        sincos(ph, &s, &c);
-    } else {
-        float sf, cf;
-        phase_sincos_f32(ph, sf, cf);
-        s = sf;
-        c = cf;
-    }
-}
 
+// k-vectors (and, in the force pass, rho) staged in dynamic shared memory
+// sized to K, so a small K leaves room for more resident blocks.
 template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
     __shared__ double smem[kSkChunk * 32];
-    __shared__ double kk[3 * 1024];
+    extern __shared__ double kk[];   // 3K
     for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
     __syncthreads();
     double cnt = 0.0;
     for (int k0 = 0; k0 < d.K; k0 += kSkChunk / 2) {
         double acc[kSkChunk];
+        // mixed precision: a thread's few atoms (grid-stride, about n / (1184 * 256))
+        // are summed in FP32, every sum across threads and blocks in FP64
+        float facc[kSkChunk];
 #pragma unroll
-        for (int t = 0; t < kSkChunk; ++t) acc[t] = 0.0;
+        for (int t = 0; t < kSkChunk; ++t) {
+            acc[t] = 0.0;
+            facc[t] = 0.f;
+        }
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
             if (d.mask && !(d.mask[i] & d.groupbit)) continue;
             if (k0 == 0) cnt += 1.0;
@@ -160,12 +158,23 @@ template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d
                 const int kq = k0 + q;
                 if (kq < d.K) {
                     const double ph = kk[3 * kq] * x + kk[3 * kq + 1] * y + kk[3 * kq + 2] * z;
-                    double s, c;
-                    phase_sincos<FP64>(ph, s, c);
-                    acc[2 * q] += c;
-                    acc[2 * q + 1] += s;
+                    if (FP64) {
+                        double s, c;
+                        sincos(ph, &s, &c);
+                        acc[2 * q] += c;
+                        acc[2 * q + 1] += s;
+                    } else {
+                        float s, c;
+                        phase_sincos_f32(ph, s, c);
+                        facc[2 * q] += c;
+                        facc[2 * q + 1] += s;
+                    }
                 }
             }
+        }
+        if (!FP64) {
+#pragma unroll
+            for (int t = 0; t < kSkChunk; ++t) acc[t] = facc[t];
         }
         block_sum<kSkChunk>(acc, smem);
         if (threadIdx.x == 0)
@@ -198,10 +207,20 @@ template <bool FP64>
 __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restrict__ f_src, double *__restrict__ f_dst,
                                                   SysDev s, CellGrid g, double *vpart) {
     __shared__ double smem[6 * 32];
-    __shared__ double kk[3 * 1024];
-    __shared__ double rr[2 * 1024];
-    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
-    for (int t = threadIdx.x; t < 2 * d.K; t += blockDim.x) rr[t] = d.rho[t];
+    extern __shared__ double kk[];   // 3K doubles, then 2K doubles (FP64) or 5K floats (FP32)
+    // FP64: rho as doubles; FP32: rho and k as floats (the per-atom gradient
+    // is accumulated in FP32, the phase stays FP64)
+    float *aux = reinterpret_cast<float *>(kk + 3 * d.K);
+    double *rr = kk + 3 * d.K;
+    float *rrf = aux, *kkf = aux + 2 * d.K;
+    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) {
+        kk[t] = d.k[t];
+        if (!FP64) kkf[t] = (float)d.k[t];
+    }
+    for (int t = threadIdx.x; t < 2 * d.K; t += blockDim.x) {
+        if (FP64) rr[t] = d.rho[t];
+        else rrf[t] = (float)d.rho[t];
+    }
     __syncthreads();
     const double a = d.coef[0];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -210,14 +229,30 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
         double gx = 0, gy = 0, gz = 0;
         if (!d.mask || (d.mask[i] & d.groupbit)) {
             const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
-            for (int q = 0; q < d.K; ++q) {
-                const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
-                double sn, cs;
-                phase_sincos<FP64>(ph, sn, cs);
-                const double w = -rr[2 * q] * sn + rr[2 * q + 1] * cs;
-                gx += w * kk[3 * q];
-                gy += w * kk[3 * q + 1];
-                gz += w * kk[3 * q + 2];
+            if (FP64) {
+                for (int q = 0; q < d.K; ++q) {
+                    const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
+                    double sn, cs;
+                    sincos(ph, &sn, &cs);
+                    const double w = -rr[2 * q] * sn + rr[2 * q + 1] * cs;
+                    gx += w * kk[3 * q];
+                    gy += w * kk[3 * q + 1];
+                    gz += w * kk[3 * q + 2];
+                }
+            } else {
+                float fx = 0.f, fy = 0.f, fz = 0.f;
+                for (int q = 0; q < d.K; ++q) {
+                    const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
+                    float sn, cs;
+                    phase_sincos_f32(ph, sn, cs);
+                    const float w = fmaf(rrf[2 * q + 1], cs, -rrf[2 * q] * sn);
+                    fx = fmaf(w, kkf[3 * q], fx);
+                    fy = fmaf(w, kkf[3 * q + 1], fy);
+                    fz = fmaf(w, kkf[3 * q + 2], fz);
+                }
+                gx = fx;
+                gy = fy;
+                gz = fz;
             }
         }
         const double fx = -a * gx, fy = -a * gy, fz = -a * gz;
@@ -271,8 +306,9 @@ int sk_blocks(int n) {
 }
 
 void launch_sk_values(const SkDev &d, cudaStream_t st) {
-    if (d.fp64) k_sk_partial<true><<<d.nblocks, 256, 0, st>>>(d);
-    else k_sk_partial<false><<<d.nblocks, 256, 0, st>>>(d);
+    const size_t sm = sizeof(double) * 3 * (size_t)d.K;
+    if (d.fp64) k_sk_partial<true><<<d.nblocks, 256, sm, st>>>(d);
+    else k_sk_partial<false><<<d.nblocks, 256, sm, st>>>(d);
     prof_mark("sk_partial", st);
     k_sk_reduce<<<2 * d.K + 1, 256, 0, st>>>(d);
     prof_mark("sk_reduce", st);
@@ -282,8 +318,9 @@ void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const 
                       double *vpart, cudaStream_t st) {
     if (d.n == 0) return;
     const int nb = (d.n + 255) / 256;
-    if (d.fp64) k_sk_force<true><<<nb, 256, 0, st>>>(d, f_src, f_dst, s, g, vpart);
-    else k_sk_force<false><<<nb, 256, 0, st>>>(d, f_src, f_dst, s, g, vpart);
+    const size_t sm = sizeof(double) * 3 * (size_t)d.K + (d.fp64 ? sizeof(double) * 2 : sizeof(float) * 5) * (size_t)d.K;
+    if (d.fp64) k_sk_force<true><<<nb, 256, sm, st>>>(d, f_src, f_dst, s, g, vpart);
+    else k_sk_force<false><<<nb, 256, sm, st>>>(d, f_src, f_dst, s, g, vpart);
     prof_mark("sk_force", st);
 }
 

@@ -34,7 +34,7 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc", "mtd_nn_state",
            "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
            "mtd_nnbias_num_hills", "mtd_nnbias_exact", "mtd_nnbias_eval", "mtd_nnbias_fit", "mtd_nnbias_validate",
-           "mtd_nnbias_usable", "mtd_nnbias_point_device", "mtd_nnbias_get_params", "mtd_nnbias_set_params",
+           "mtd_nnbias_usable", "mtd_nnbias_point_device", "mtd_nnbias_eval_device", "mtd_nnbias_get_params", "mtd_nnbias_set_params",
            "mtd_nnbias_vscale", "mtd_nnbias_loss_grad",
            "mtd_walkers_create", "mtd_walkers_destroy", "mtd_walkers_last_error", "mtd_walkers_count",
            "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
@@ -125,6 +125,7 @@ def lib():
         L.mtd_nnbias_validate.argtypes = [vp, C.c_int, C.c_uint64, C.c_double, dp, dp]
         L.mtd_nnbias_usable.argtypes = [vp]
         L.mtd_nnbias_point_device.argtypes = [vp, vp, vp, vp, C.c_int, vp]
+        L.mtd_nnbias_eval_device.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, vp]
         L.mtd_nnbias_get_params.argtypes = [vp, C.POINTER(C.c_float)]
         L.mtd_nnbias_set_params.argtypes = [vp, C.POINTER(C.c_float), C.c_double]
         L.mtd_nnbias_vscale.argtypes = [vp]
@@ -394,6 +395,11 @@ class NNBias:
     def point_device(self, s_ptr, v_ptr, dv_ptr, use_nn=-1, stream=0):
         self._check(lib().mtd_nnbias_point_device(self._h, C.c_void_p(s_ptr), C.c_void_p(v_ptr),
                                                   C.c_void_p(dv_ptr), int(use_nn), C.c_void_p(stream or None)))
+
+    def eval_device(self, npts, pts_ptr, v_ptr, dv_ptr=0, use_nn=-1, stream=0):
+        """Device pointers (ints): npts rows of D doubles in, V (and dV/ds rows) out."""
+        self._check(lib().mtd_nnbias_eval_device(self._h, int(npts), C.c_void_p(pts_ptr), C.c_void_p(v_ptr),
+                                                 C.c_void_p(dv_ptr or None), int(use_nn), C.c_void_p(stream or None)))
 
     def get_params(self):
         w = np.zeros(NN_PARAMS, dtype=np.float32)

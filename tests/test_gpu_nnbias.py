@@ -131,3 +131,29 @@ def test_fit_on_hill_sum_and_fallback():
     nb.validate(npts=4096, seed=8, tol=0.0)
     assert not nb.usable
     nb.close()
+
+
+def test_device_batch_equals_host_batch():
+    """mtd_nnbias_eval_device on device-resident points: the exact path equals
+    mtd_nnbias_exact bit for bit, the network path equals mtd_nnbias_eval up
+    to the input normalisation's last-bit rounding (1e-5 of max|V|)."""
+    import torch
+
+    c, h, s = systems.cv4_hills(n=500, seed=3)
+    nb = mtd.NNBias(systems.CV4_LO, systems.CV4_HI)
+    nb.set_params(_random_params(13), 0.7)
+    nb.add_hills(c, h, s)
+    p = _box_points(1000, 6)
+    d_p = torch.from_numpy(np.ascontiguousarray(p)).cuda()
+    for use_nn, ref in [(0, nb.exact(p)), (1, nb.eval(p))]:
+        v = torch.zeros(len(p), dtype=torch.float64, device="cuda")
+        g = torch.zeros((len(p), 4), dtype=torch.float64, device="cuda")
+        nb.eval_device(len(p), d_p.data_ptr(), v.data_ptr(), g.data_ptr(), use_nn=use_nn)
+        torch.cuda.synchronize()
+        V, dV = v.cpu().numpy(), g.cpu().numpy()
+        if use_nn == 0:
+            assert np.array_equal(V, ref[0]) and np.array_equal(dV, ref[1])
+        else:
+            assert np.abs(V - ref[0]).max() <= 1e-5 * np.abs(ref[0]).max()
+            assert np.abs(dV - ref[1]).max() <= 1e-4 * np.abs(ref[1]).max()
+    nb.close()
