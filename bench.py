@@ -468,6 +468,7 @@ def run_walkers(args, local):
         dx = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x, _ in syss]
         df = [torch.zeros_like(v) for v in dx]
         xp, fp = [v.data_ptr() for v in dx], [v.data_ptr() for v in df]
+        picks = W.autotune(ns, xp, reps=5)   # kernel shapes per walker (results do not depend on them)
         step = 0
         for _ in range(max(3, args.warmup)):
             W.step_device(step, ns, xp, fp)
@@ -482,8 +483,13 @@ def run_walkers(args, local):
             step += 1
         torch.cuda.synchronize()
         wall = (time.perf_counter() - t0) / args.steps
+        shapes = {}
+        for p in picks:
+            key = "nbr%d/q%d/l%d" % p
+            shapes[key] = shapes.get(key, 0) + 1
         res["graph" if graph else "plain"] = {"ms_per_step": wall * 1e3,
-                                              "atom_steps_per_s": sum(ns) / wall, "launches_per_step": launches}
+                                              "atom_steps_per_s": sum(ns) / wall, "launches_per_step": launches,
+                                              "autotuned_shapes": shapes}
         cvs = [W.cv(k, 2).tolist() for k in range(3)]
         W.close()
     line = {"metric": "multi-walker CV+bias+force atom-steps/s (all walkers)", "workload": "walkers",
@@ -552,6 +558,11 @@ def main():
         step += 1
 
     for _ in range(args.warmup):
+        dev_step()
+    m.sync()
+    # kernel shapes from the autotuner (every shape gives bitwise-identical steps)
+    tuned = m.autotune(n, dx[0].data_ptr(), reps=5)
+    for _ in range(2):
         dev_step()
     m.sync()
     torch.cuda.synchronize()
@@ -636,6 +647,8 @@ def main():
                        "max_neighbors": m.max_neighbors("Q4"), "cap_cutoff_Natoms": 18,
                        "precision": args.precision, "l2": "flushed (256 MB write) before each timed step",
                        "parallelism": "replicas" if world > 1 else "single GPU",
+                       "autotuned_shapes": {"neighbors": ["fast/256", "fast/128", "flat/128"][tuned[0]],
+                                            "q_block": tuned[1], "lambda_block": tuned[2]},
                        "cv": [float(v) for v in m.cv]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps},

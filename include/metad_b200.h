@@ -160,6 +160,18 @@ mtd_status mtd_set_stream(mtd_ctx *ctx, void *cuda_stream);
 mtd_status mtd_profile_enable(mtd_ctx *ctx, int enable);
 int mtd_profile_report(mtd_ctx *ctx, char *buf, int len);
 
+/* Autotuner: times the interchangeable kernel shapes on device positions
+ * d_x (n x 3, caller order; d_mask may be NULL) over `reps` launches each and
+ * keeps the fastest -- the neighbour search (0: 256-thread blocks, 1:
+ * 128-thread blocks, 2: flat per-thread candidate loop) and the threads per
+ * block of the q and lambda passes (256 or 128).  Every shape gives
+ * bitwise-identical results, so tuning never changes a step's output; it
+ * records no step and deposits nothing.  choice (may be NULL) receives the
+ * three picks.  mtd_set_tuning sets them directly (q/lambda 0 = 256).
+ * No counterpart in the reference (fixed launch shapes). */
+mtd_status mtd_autotune(mtd_ctx *ctx, int n, const double *d_x, const int *d_mask, int reps, int choice[3]);
+mtd_status mtd_set_tuning(mtd_ctx *ctx, int neighbor_shape, int q_block, int lambda_block);
+
 /* Largest neighbour count seen by the last step for CAL `name` (cap reporting). */
 int mtd_max_neighbors(mtd_ctx *ctx, const char *name);
 
@@ -230,6 +242,10 @@ mtd_status mtd_walkers_enable_graph(mtd_walkers *W, int enable);
 mtd_status mtd_walkers_step_device(mtd_walkers *W, int64_t step, const int *n, const double *const *d_x,
                                    double *const *d_f);
 mtd_status mtd_walkers_sync(mtd_walkers *W);
+/* Runs mtd_autotune on every walker with its own positions (walker k's three
+ * picks into choices[3k..3k+2], may be NULL); the next step re-captures the
+ * CUDA graph with the chosen shapes. */
+mtd_status mtd_walkers_autotune(mtd_walkers *W, const int *n, const double *const *d_x, int reps, int *choices);
 double mtd_walkers_cv(const mtd_walkers *W, int k, int d);
 double mtd_walkers_bias(const mtd_walkers *W, int k);
 mtd_status mtd_walkers_get_grid(mtd_walkers *W, double *out, int64_t count);

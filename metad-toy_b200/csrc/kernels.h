@@ -93,6 +93,7 @@ struct NeighSpec {
     SwParams sw;
     float lo2, hi2;     // FP32 accept-below / reject-above
     int cap;            // STEINH Q cutoff_Natoms, 0 = none
+    int variant;        // kernel shape of the fast path (0, 1, 2: see launch_neighbors); same lists
 };
 
 struct NeighDev {
@@ -136,6 +137,7 @@ template <typename T> struct LocalDev {
     T *q, *nf, *lq, *lqs, *e12, *lam, *g, *tu;
     double *partials;           // [nblocks][8]: S1A S0A S1B S0B N
     const double *coef;         // c1A c2A c1B c2B (written by the bias kernel)
+    int qblock, lblock;         // threads per block of the q and lambda passes (0: kBlock); same results
 };
 template <typename T> void launch_local_values(const LocalDev<T> &d, cudaStream_t st);
 // Reals per STEINH L record (both orders): a multiple of 32 bytes.

@@ -402,13 +402,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_local_force(LocalDev<T> d, const 
 
 template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cudaStream_t st) {
     const int nb = (d.n + kBlock - 1) / kBlock;
+    const int qb = d.qblock > 0 ? d.qblock : kBlock, qg = (d.n + qb - 1) / qb;   // no block reduction in q
     if (d.sw_r.type == SW_STEP) {
-        k_local_q<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
+        k_local_q<LA, LB, T, true><<<qg, qb, 0, st>>>(d);
         prof_mark("local_q", st);
         k_local_lq<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
         prof_mark("local_lq", st);
     } else {
-        k_local_q<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
+        k_local_q<LA, LB, T, false><<<qg, qb, 0, st>>>(d);
         prof_mark("local_q", st);
         k_local_lq<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
         prof_mark("local_lq", st);
@@ -419,13 +420,14 @@ template <int LA, int LB, typename T>
 void run_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                 double *vpart, DevStatus *status, cudaStream_t st) {
     const int nb = (d.n + kBlock - 1) / kBlock;
+    const int lb = d.lblock > 0 ? d.lblock : kBlock, lg = (d.n + lb - 1) / lb;   // no block reduction in lambda
     if (d.sw_r.type == SW_STEP) {
-        k_local_lambda<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
+        k_local_lambda<LA, LB, T, true><<<lg, lb, 0, st>>>(d);
         prof_mark("local_lambda", st);
         k_local_force<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
         prof_mark("local_force", st);
     } else {
-        k_local_lambda<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
+        k_local_lambda<LA, LB, T, false><<<lg, lb, 0, st>>>(d);
         prof_mark("local_lambda", st);
         k_local_force<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
         prof_mark("local_force", st);

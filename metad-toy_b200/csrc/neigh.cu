@@ -308,6 +308,107 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s,
     if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
 }
 
+// Same lists as k_neighbors_fast (same cells in the same order, same tests),
+// with the warp's divergence taken out of the cell loop: each thread first
+// records the non-empty cells of its 27-cell stencil in shared memory (a
+// uniform pass), then walks all its candidates in one flat loop, moving to the
+// next recorded cell when one runs out.  A warp then runs as many trips as
+// its busiest lane has candidates, instead of, for each of 27 cells, as many
+// as the fullest lane's cell holds.
+constexpr int kFlatBlock = 128;
+template <int KIND>
+__global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
+                                                               DevStatus *status) {
+    // [cell][thread]: a lane's entry sits in the same bank whatever cell it reads
+    __shared__ int2 rng[27][kFlatBlock];
+    const int tid = threadIdx.x;
+    const int k = blockIdx.x * blockDim.x + tid;
+    if (k >= s.n) return;   // no block-wide synchronisation below
+    const GeoD gd = geo_d(g, s.xs);
+    const float4 a = s.pf[k];
+    const int w = __float_as_int(a.w);
+    const int cx = w & 1023, cy = (w >> 10) & 1023, cz = w >> 20;
+    const int nx = g.nc[0], ny = g.nc[1], nz = g.nc[2];
+    // the cell shift o h - offset for o = -1, 0, 1 per dimension (as k_neighbors_fast forms it)
+    const float shx[3] = {-g.hf[0] - a.x, 0.f * g.hf[0] - a.x, g.hf[0] - a.x};
+    const float shy[3] = {-g.hf[1] - a.y, 0.f * g.hf[1] - a.y, g.hf[1] - a.y};
+    const float shz[3] = {-g.hf[2] - a.z, 0.f * g.hf[2] - a.z, g.hf[2] - a.z};
+    int nr = 0;
+#pragma unroll 1
+    for (int ox = 0; ox < 3; ++ox) {
+        int x = cx + ox - 1;
+        if (x < 0 || x >= nx) {
+            if (!g.periodic[0]) continue;
+            x += x < 0 ? nx : -nx;
+        }
+#pragma unroll 1
+        for (int oy = 0; oy < 3; ++oy) {
+            int y = cy + oy - 1;
+            if (y < 0 || y >= ny) {
+                if (!g.periodic[1]) continue;
+                y += y < 0 ? ny : -ny;
+            }
+            const int col = (x * ny + y) * nz;
+#pragma unroll
+            for (int oz = 0; oz < 3; ++oz) {
+                int z = cz + oz - 1;
+                if (z < 0 || z >= nz) {
+                    if (!g.periodic[2]) continue;
+                    z += z < 0 ? nz : -nz;
+                }
+                const int b0 = __ldg(s.start + col + z), b1 = __ldg(s.start + col + z + 1);
+                // end < 2^26, the stencil offsets (2 bits each) above it
+                const unsigned code = (unsigned)ox | ((unsigned)oy << 2) | ((unsigned)oz << 4);
+                if (b0 < b1) rng[nr++][tid] = make_int2(b0, (int)((unsigned)b1 | (code << 26)));
+            }
+        }
+    }
+    int cnt = 0;
+    int r = 0, j = 0, je = 0;
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    auto open = [&]() {
+        const int2 e = rng[r++][tid];
+        const unsigned code = (unsigned)e.y >> 26;
+        j = e.x;
+        je = e.y & ((1 << 26) - 1);
+        const unsigned qx = code & 3u, qy = (code >> 2) & 3u, qz = code >> 4;
+        sx = qx == 0 ? shx[0] : (qx == 1 ? shx[1] : shx[2]);
+        sy = qy == 0 ? shy[0] : (qy == 1 ? shy[1] : shy[2]);
+        sz = qz == 0 ? shz[0] : (qz == 1 ? shz[1] : shz[2]);
+    };
+    bool live = nr > 0;
+    float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (live) {
+        open();
+        nxt = __ldg(s.pf + j);
+    }
+    while (live) {
+        const float4 b = nxt;
+        const int jj = j;
+        const float dx = b.x + sx, dy = b.y + sy, dz = b.z + sz;
+        if (++j == je) {
+            live = r < nr;
+            if (live) open();
+        }
+        if (live) nxt = __ldg(s.pf + j);
+        const float r2f = dx * dx + dy * dy + dz * dz;
+        if (r2f > ns.hi2 || jj == k) continue;
+        bool in;
+        if (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f) {
+            in = true;
+        } else {
+            const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
+            const double xj[3] = {s.xs[3 * jj], s.xs[3 * jj + 1], s.xs[3 * jj + 2]};
+            in = exact_decide<KIND>(gd, ns, xk, xj);
+        }
+        if (!in) continue;
+        if (cnt < nd.M) nd.list[(size_t)cnt * s.npad + k] = jj;
+        ++cnt;
+    }
+    nd.count[k] = cnt;
+    if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
+}
+
 constexpr int kMaxCapList = 64;
 
 // STEINH Q cap: keep the `cap` nearest by (r2, caller index), the order of the
@@ -380,10 +481,19 @@ void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, N
     bool fast = true;
     for (int c = 0; c < 3; ++c)
         if (g.periodic[c] && g.nc[c] < 3) fast = false;
-    if (fast) {
-        if (ns.kind == NK_RANGE) k_neighbors_fast<NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
-        else if (ns.kind == NK_STEP) k_neighbors_fast<NK_STEP><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
-        else k_neighbors_fast<NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+    // the fast path has three interchangeable shapes (identical lists): 256- or
+    // 128-thread blocks of k_neighbors_fast, or k_neighbors_flat (autotuned)
+    if (fast && ns.variant == 2 && s.n < (1 << 26)) {
+        const int fb = (s.n + kFlatBlock - 1) / kFlatBlock;
+        if (ns.kind == NK_RANGE) k_neighbors_flat<NK_RANGE><<<fb, kFlatBlock, 0, st>>>(g, s, ns, nd, status);
+        else if (ns.kind == NK_STEP) k_neighbors_flat<NK_STEP><<<fb, kFlatBlock, 0, st>>>(g, s, ns, nd, status);
+        else k_neighbors_flat<NK_SWITCH><<<fb, kFlatBlock, 0, st>>>(g, s, ns, nd, status);
+    } else if (fast) {
+        const int tb = ns.variant == 1 ? 128 : kBlock;
+        const int gb = (s.n + tb - 1) / tb;
+        if (ns.kind == NK_RANGE) k_neighbors_fast<NK_RANGE><<<gb, tb, 0, st>>>(g, s, ns, nd, status);
+        else if (ns.kind == NK_STEP) k_neighbors_fast<NK_STEP><<<gb, tb, 0, st>>>(g, s, ns, nd, status);
+        else k_neighbors_fast<NK_SWITCH><<<gb, tb, 0, st>>>(g, s, ns, nd, status);
     } else if (ns.kind == NK_RANGE) k_neighbors<NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
     else if (ns.kind == NK_STEP) k_neighbors<NK_STEP><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
     else k_neighbors<NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);

@@ -39,7 +39,7 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_walkers_create", "mtd_walkers_destroy", "mtd_walkers_last_error", "mtd_walkers_count",
            "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
            "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
-           "mtd_walkers_last_launch_count"]
+           "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune"]
 
 
 class MetadError(RuntimeError):
@@ -88,6 +88,10 @@ def lib():
         L.mtd_get_grid.argtypes = [vp, dp, C.c_int64]
         L.mtd_last_launch_count.argtypes = [vp]
         L.mtd_max_neighbors.argtypes = [vp, C.c_char_p]
+        L.mtd_autotune.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
+        L.mtd_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.mtd_walkers_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_int,
+                                           C.POINTER(C.c_int)]
         L.mtd_last_error.argtypes = [vp]
         L.mtd_last_error.restype = C.c_char_p
         L.mtd_abi_version.restype = C.c_int
@@ -288,6 +292,16 @@ class Metad:
 
     def max_neighbors(self, cal):
         return lib().mtd_max_neighbors(self._h, cal.encode())
+
+    def autotune(self, n, x_ptr, mask_ptr=0, reps=5):
+        """Device pointers (ints); returns (neighbour shape, q block, lambda block)."""
+        ch = (C.c_int * 3)()
+        self._check(lib().mtd_autotune(self._h, int(n), C.c_void_p(x_ptr), C.c_void_p(mask_ptr or None), int(reps),
+                                       ch))
+        return tuple(ch)
+
+    def set_tuning(self, neighbor_shape=0, q_block=0, lambda_block=0):
+        self._check(lib().mtd_set_tuning(self._h, int(neighbor_shape), int(q_block), int(lambda_block)))
 
     def nn_state(self):
         """(hills, hills fitted, network in use) of the hill-list bias."""
@@ -491,3 +505,12 @@ class Walkers:
 
     def launch_count(self):
         return lib().mtd_walkers_last_launch_count(self._h)
+
+    def autotune(self, ns, x_ptrs, reps=5):
+        """Per walker (neighbour shape, q block, lambda block), tuned on its own device positions."""
+        k = len(ns)
+        na = (C.c_int * k)(*[int(v) for v in ns])
+        xa = (C.c_void_p * k)(*[C.c_void_p(p) for p in x_ptrs])
+        ch = (C.c_int * (3 * k))()
+        self._check(lib().mtd_walkers_autotune(self._h, na, xa, int(reps), ch))
+        return [tuple(ch[3 * i:3 * i + 3]) for i in range(k)]
