@@ -1,0 +1,12 @@
+// Test stand-in for LAMMPS's Domain (orthogonal box).
+#ifndef STUB_DOMAIN_H
+#define STUB_DOMAIN_H
+namespace LAMMPS_NS {
+class Domain {
+ public:
+  double boxlo[3] = {0, 0, 0}, boxhi[3] = {1, 1, 1};
+  int xperiodic = 1, yperiodic = 1, zperiodic = 1;
+  int triclinic = 0;
+};
+}  // namespace LAMMPS_NS
+#endif
