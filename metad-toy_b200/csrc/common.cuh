@@ -188,8 +188,9 @@ __device__ __forceinline__ void phase_sincos_f32(double ph, float &s, float &c) 
     cp = fmaf(cp, r2, -0.5f);
     const float c0 = fmaf(cp, r2, 1.0f);
     const float ss = (q & 1) ? c0 : s0, cc = (q & 1) ? s0 : c0;
-    s = (q & 2) ? -ss : ss;
-    c = ((q + 1) & 2) ? -cc : cc;
+    // rotation by q quarter turns: sign bits from q (bit 1 for sin, bit 1 of q + 1 for cos)
+    s = __int_as_float(__float_as_int(ss) ^ ((q & 2) << 30));
+    c = __int_as_float(__float_as_int(cc) ^ (((q + 1) & 2) << 30));
 }
 
 }  // namespace mtd

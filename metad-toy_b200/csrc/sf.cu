@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
 
 // ------------------------------------------------------------------ S(k)
 constexpr int kSkChunk = 16;       // reals per register tile (8 k-vectors per pass over the atoms)
-constexpr int kSkBlocks = 148 * 8;  // grid for the partial sums (8 blocks per SM)
+constexpr int kSkBlocks = 148 * 4;  // grid for the partial sums (4 blocks per SM: more atoms per thread, fewer block sums)
 
 
 // k-vectors (and, in the force pass, rho) staged in dynamic shared memory
