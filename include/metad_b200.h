@@ -130,7 +130,8 @@ int mtd_cv_dim(const mtd_ctx *ctx);
  * the CV that the first SYMBOL on <CAL> selects, at the last step's positions
  * (STEINH Q and L, STRU_FACTOR, STRU_FACTOR_K); it re-runs that CAL's force
  * kernels once per step and CAL and is cached, so dcvdx_x/y/z of one step
- * cost one pass.
+ * cost one pass.  After mtd_post_force_device it reads the caller's position
+ * buffer of that step, which must still hold those positions.
  * Replaces FixMetadynamics::extract (src/core/fix_crystallize.cu:592-613),
  * STEIN_QL::get_peratom_ptr (src/cvs/CVs_Steinhardt.cu:1278-1322),
  * Stru_factor::get_peratom_ptr (src/cvs/CVs_Strufactor.cu:974-979). */
