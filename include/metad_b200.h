@@ -173,6 +173,17 @@ int mtd_profile_report(mtd_ctx *ctx, char *buf, int len);
 mtd_status mtd_autotune(mtd_ctx *ctx, int n, const double *d_x, const int *d_mask, int reps, int choice[3]);
 mtd_status mtd_set_tuning(mtd_ctx *ctx, int neighbor_shape, int q_block, int lambda_block);
 
+/* Atom types (caller order, n values, host array) for `STRU_FACTOR ...
+ * Chemical`, whose pair terms are weighted by w(type_i) w(type_j): w from the
+ * CAL's Chem_map pairs, else exp(-(type - Chem_ctarget)^2 / (2 Chem_sigma^2)),
+ * type 0 weighing 0.  Call it before the first step and whenever types or
+ * atom order change; a step with a Chemical CAL and no types for its n atoms
+ * fails.  mtd_needs_types tells whether the context has such a CAL.
+ * Replaces the type upload of Stru_fact_chem_env::refresh_lmpbox and its
+ * weight table (src/cvs/CVs_Strufactor_chem.cu:33-55, :77-100). */
+mtd_status mtd_set_types(mtd_ctx *ctx, int n, const int *types);
+int mtd_needs_types(const mtd_ctx *ctx);
+
 /* Largest neighbour count seen by the last step for CAL `name` (cap reporting). */
 int mtd_max_neighbors(mtd_ctx *ctx, const char *name);
 

@@ -164,12 +164,49 @@ bool parse_sf(Cursor &c, int &i, const GroupTable &groups, CalDef &d) {
             if (!parse_switch(c, kk, d.sf_sw)) return false;
             d.sf_use_sw = true;
             k = kk;
-        } else if (!std::strcmp(c.arg[k], "Chemical") || !std::strcmp(c.arg[k], "Chem_ctarget") ||
-                   !std::strcmp(c.arg[k], "Chem_sigma") || !std::strcmp(c.arg[k], "Chem_map")) {
-            return c.fail("Error: STRU_FACTOR Chemical (multi-species) is not supported by this library.");
+        } else if (!std::strcmp(c.arg[k], "Chemical")) {
+            d.chem = true;
+            k += 1;
+        } else if (!std::strcmp(c.arg[k], "Chem_ctarget")) {
+            if (k + 1 >= c.narg) return c.fail("Error: 'Chem_ctarget' keyword requires a number");
+            if (!need_double(c, k + 1, d.chem_ctarget, "Chem_ctarget")) return false;
+            k += 2;
+        } else if (!std::strcmp(c.arg[k], "Chem_sigma")) {
+            if (k + 1 >= c.narg) return c.fail("Error: 'sigma' keyword requires a number");
+            if (!need_double(c, k + 1, d.chem_sigma, "Chem_sigma")) return false;
+            k += 2;
+        } else if (!std::strcmp(c.arg[k], "Chem_map")) {
+            // (type weight) pairs: one token "(1,0.5)" / "(1 0.5)", or two tokens "(1" "0.5)"
+            k += 1;
+            while (k < c.narg && c.arg[k][0] == '(') {
+                std::string a = c.arg[k];
+                std::string type_s, w_s;
+                if (a.size() >= 2 && a.back() == ')') {
+                    const std::string body = a.substr(1, a.size() - 2);
+                    const size_t sep = body.find_first_of(" ,");
+                    if (sep == std::string::npos) return c.fail("Error: Chem_map pairs must be formatted as (type weight)");
+                    type_s = body.substr(0, sep);
+                    w_s = body.substr(sep + 1);
+                } else {
+                    if (k + 1 >= c.narg) return c.fail("Error: Invalid Chem_map format near " + a);
+                    const std::string b = c.arg[k + 1];
+                    if (b.empty() || b.back() != ')') return c.fail("Error: Chem_map pairs must be formatted as (type weight)");
+                    type_s = a.substr(1);
+                    w_s = b.substr(0, b.size() - 1);
+                    k += 1;
+                }
+                char *e1 = nullptr, *e2 = nullptr;
+                const long t = std::strtol(type_s.c_str(), &e1, 10);
+                const double w = std::strtod(w_s.c_str(), &e2);
+                if (e1 == type_s.c_str() || e2 == w_s.c_str() || t < 0)
+                    return c.fail("Error: Chem_map pairs must be formatted as (type weight)");
+                d.chem_map.emplace_back((int)t, w);
+                k += 1;
+            }
         } else break;
     }
     if (!d.has_q_factor) return c.fail("Error: STRU_FACTOR requires 'q_factor' (it has no default).");
+    if (d.chem && !(d.chem_sigma > 0.0)) return c.fail("Error: STRU_FACTOR 'Chem_sigma' must be > 0.");
     i = k;
     return true;
 }

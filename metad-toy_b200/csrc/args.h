@@ -35,6 +35,12 @@ struct CalDef {
     bool has_q_factor = false;
     bool sf_use_sw = false;
     SwParams sf_sw{SW_RATIONAL, 1.25, 0.0, 20.0, 6, 12};
+    // STRU_FACTOR Chemical: pair terms weighted by w(type_i) w(type_j), w from
+    // Chem_map (type weight) pairs, else exp(-(type - Chem_ctarget)^2 / (2 Chem_sigma^2)), w(0) = 0
+    // (StruFactorRequest defaults, include/CVsets/CV_Stru_factor.h:28-33)
+    bool chem = false;
+    double chem_ctarget = 0.0, chem_sigma = 1.0;
+    std::vector<std::pair<int, double>> chem_map;
     // STRU_FACTOR_K (k-vector S(k), no reference counterpart)
     int nk = 96;
     double kmag = 0.0;

@@ -66,6 +66,14 @@ struct Unit {
     double *coef = nullptr;
     int K = 0;
     double *kvec = nullptr, *rho = nullptr, *skn = nullptr;
+    // STRU_FACTOR Chemical: type-weight parameters, the table built from the
+    // types of mtd_set_types, and the per-atom weights (sorted order)
+    bool chem = false;
+    double chem_ctarget = 0.0, chem_sigma = 1.0;
+    std::vector<std::pair<int, double>> chem_map;
+    double *d_wtab = nullptr;
+    int ntab = 0;
+    void *w = nullptr;
 };
 
 template <typename P> cudaError_t dalloc(P **p, size_t bytes) {
@@ -166,6 +174,9 @@ struct mtd_ctx {
     int h_fit = 0;                       // hills the network was fitted on
     bool nn_usable = false;
     cudaEvent_t f_ready = nullptr;
+    // atom types (caller order) for STRU_FACTOR Chemical, from mtd_set_types
+    int *d_types = nullptr;
+    int types_cap = 0, types_n = -1;
     // kernel shapes chosen by mtd_autotune (every choice gives bitwise-identical results)
     int tune_nbr = 0;                    // neighbour search: 0 fast/256, 1 fast/128, 2 flat/128
     int tune_q = 0, tune_l = 0;          // threads per block of the q and lambda passes (0: 256)
@@ -322,7 +333,7 @@ mtd_status alloc_unit(mtd_ctx *c, Unit &u, int npad) {
     const size_t R = real_size(c);
     const int SQ = record_stride(c, u);
     const int nb = (npad + kBlock - 1) / kBlock;
-    void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S};
+    void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S, &u.w};
     for (void **a : arrs) dfree(*a);
     dfree(u.partials);
     if (u.kind == CAL_STEINH_L) {
@@ -345,6 +356,7 @@ mtd_status alloc_unit(mtd_ctx *c, Unit &u, int npad) {
         MTD_CU(dalloc(&u.partials, sizeof(double) * 8 * (size_t)nb), "partials");
     } else if (u.kind == CAL_STRU_FACTOR) {
         MTD_CU(dalloc(&u.S, R * (size_t)npad), "S");
+        if (u.chem) MTD_CU(dalloc(&u.w, R * (size_t)npad), "type weights");
         u.nblocks = nb;
         MTD_CU(dalloc(&u.partials, sizeof(double) * 8 * (size_t)nb), "partials");
     } else {
@@ -544,6 +556,10 @@ mtd_status plan_units(mtd_ctx *c) {
         u.rc = d.cutoff_r;
         u.qf = d.q_factor;
         u.sf_sw = d.sf_sw;
+        u.chem = d.kind == CAL_STRU_FACTOR && d.chem;
+        u.chem_ctarget = d.chem_ctarget;
+        u.chem_sigma = d.chem_sigma;
+        u.chem_map = d.chem_map;
         u.used = used;
         unit_of[d.name] = (int)c->units.size();
         slot_of[d.name] = 0;
@@ -670,6 +686,10 @@ template <typename T> DebyeDev<T> debye_dev(mtd_ctx *c, Unit &u, const CellGrid 
     d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
     d.S = (T *)u.S; d.partials = u.partials; d.coef = u.coef;
+    d.w = u.chem ? (T *)u.w : nullptr;
+    d.types = c->d_types;
+    d.wtab = u.d_wtab;
+    d.ntab = u.ntab;
     return d;
 }
 
@@ -692,7 +712,7 @@ template <typename T> void run_values(mtd_ctx *c, const CellGrid &g, const doubl
             c->launches += 1;
         } else if (u.kind == CAL_STRU_FACTOR) {
             launch_debye_values<T>(debye_dev<T>(c, u, g), st);
-            c->launches += 1;
+            c->launches += u.chem ? 2 : 1;
         } else {
             launch_sk_values(sk_dev(c, u, x, mask), st);
             c->launches += 2;
@@ -793,6 +813,11 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
             c->launches += ns.cap > 0 ? 2 : 1;
         }
     }
+    for (const Unit &u : c->units)
+        if (u.chem && c->types_n != n)
+            return fail(c, MTD_ERR_INVALID_ARG,
+                        "STRU_FACTOR Chemical needs the atom types of these " + std::to_string(n) +
+                            " atoms: call mtd_set_types first");
     if (c->fp64) run_values<double>(c, g, x, mask);
     else run_values<float>(c, g, x, mask);
     c->last_sys = s;
@@ -1142,9 +1167,9 @@ void mtd_destroy(mtd_ctx *c) {
         dfree(e.list); dfree(e.count); dfree(e.key_r2); dfree(e.key_id); dfree(e.nkept);
     }
     for (Unit &u : c->units) {
-        void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S};
+        void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S, &u.w};
         for (void **a : arrs) dfree(*a);
-        dfree(u.partials); dfree(u.coef); dfree(u.kvec); dfree(u.rho); dfree(u.skn);
+        dfree(u.partials); dfree(u.coef); dfree(u.kvec); dfree(u.rho); dfree(u.skn); dfree(u.d_wtab);
     }
     dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
     dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask); dfree(c->arrival);
@@ -1159,6 +1184,7 @@ void mtd_destroy(mtd_ctx *c) {
     if (c->nb) mtd_nnbias_destroy(c->nb);
     dfree(c->d_vdv);
     dfree(c->d_ws1);
+    dfree(c->d_types);
     dfree(c->d_dcv);
     if (c->f_ready) cudaEventDestroy(c->f_ready);
     if (c->prof_created)
@@ -1614,6 +1640,52 @@ int mtd_profile_report(mtd_ctx *c, char *buf, int len) {
         buf[len - 1] = '\0';
     }
     return (int)s.size() + 1;
+}
+
+mtd_status mtd_set_types(mtd_ctx *c, int n, const int *types) {
+    if (!c || n < 0 || (n > 0 && !types)) return MTD_ERR_INVALID_ARG;
+    if (n > c->types_cap) {
+        dfree(c->d_types);
+        c->types_cap = 0;
+        MTD_CU(dalloc(&c->d_types, sizeof(int) * (size_t)(n + n / 4 + 1)), "atom types");
+        c->types_cap = n + n / 4 + 1;
+    }
+    int maxt = 0;
+    for (int i = 0; i < n; ++i) {
+        if (types[i] < 0) return fail(c, MTD_ERR_INVALID_ARG, "atom types must be >= 0");
+        maxt = std::max(maxt, types[i]);
+    }
+    MTD_CU(cudaStreamSynchronize(c->st), "atom types");   // no step in flight reads the old types
+    if (n > 0) MTD_CU(cudaMemcpy(c->d_types, types, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice), "atom types");
+    // type-weight tables (Stru_fact_chem_env constructor, src/cvs/CVs_Strufactor_chem.cu:33-55):
+    // Chem_map value, else a Gaussian in the type index around Chem_ctarget; type 0 weighs 0
+    for (Unit &u : c->units) {
+        if (!u.chem) continue;
+        std::vector<double> tab((size_t)maxt + 1);
+        for (int t = 0; t <= maxt; ++t) {
+            const double dt = t - u.chem_ctarget;
+            tab[t] = std::exp(-dt * dt / (2.0 * u.chem_sigma * u.chem_sigma));
+            for (const auto &kv : u.chem_map)
+                if (kv.first == t) tab[t] = kv.second;
+        }
+        tab[0] = 0.0;
+        if ((int)tab.size() > u.ntab) {
+            dfree(u.d_wtab);
+            u.ntab = 0;
+            MTD_CU(dalloc(&u.d_wtab, sizeof(double) * tab.size()), "type weights");
+        }
+        u.ntab = (int)tab.size();
+        MTD_CU(cudaMemcpy(u.d_wtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice), "type weights");
+    }
+    c->types_n = n;
+    return MTD_OK;
+}
+
+int mtd_needs_types(const mtd_ctx *c) {
+    if (!c) return 0;
+    for (const Unit &u : c->units)
+        if (u.chem) return 1;
+    return 0;
 }
 
 int mtd_max_neighbors(mtd_ctx *c, const char *name) {

@@ -176,6 +176,10 @@ template <typename T> struct DebyeDev {
     T *S;
     double *partials;           // [nblocks][4]: sumS, sum f(S), N
     const double *coef;         // c_ave, c_count
+    T *w;                       // STRU_FACTOR Chemical: per-atom type weight, sorted order (null: all 1)
+    const int *types;           // caller-order atom types (Chemical)
+    const double *wtab;         // weight of each type 0..ntab-1 (Chemical)
+    int ntab;
 };
 template <typename T> void launch_debye_values(const DebyeDev<T> &d, cudaStream_t st);
 template <typename T>

@@ -35,6 +35,15 @@ template <typename T> __device__ __forceinline__ void debye_g(T r2, T rc2, T qf,
     dg = (cs / th - sn / (th * th)) * s * qf + ds * sn / th;
 }
 
+// STRU_FACTOR Chemical: the type weight of every sorted atom (types outside
+// the table weigh 0, as type 0 does).
+template <typename T> __global__ void k_chem_weights(DebyeDev<T> d) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const int t = d.types[d.perm[k]];
+    d.w[k] = (T)(t >= 0 && t < d.ntab ? d.wtab[t] : 0.0);
+}
+
 template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(DebyeDev<T> d) {
     __shared__ double smem[4 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -45,12 +54,14 @@ template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(D
             const int c = min(d.nb.count[k], d.nb.M);
             const T rc2 = (T)d.rc2, qf = (T)d.qf;
             const auto a = d.geo.load(k);
+            const T wk = d.w ? d.w[k] : T(1);
             for (int t = 0; t < c; ++t) {
+                const int j = d.nb.list[(size_t)t * d.npad + k];
                 T dx, dy, dz;
-                d.geo.disp(a, d.geo.load(d.nb.list[(size_t)t * d.npad + k]), dx, dy, dz);
+                d.geo.disp(a, d.geo.load(j), dx, dy, dz);
                 T gv, dg;
                 debye_g<T>(dx * dx + dy * dy + dz * dz, rc2, qf, gv, dg);
-                S += gv;
+                S += d.w ? wk * d.w[j] * gv : gv;
             }
             S += T(1);
             part[0] = (double)S;
@@ -86,9 +97,11 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
         T gx = T(0), gy = T(0), gz = T(0);
         const int c = min(d.nb.count[k], d.nb.M);
         const auto a = d.geo.load(k);
+        const T wk = d.w ? d.w[k] : T(1);
         for (int t = 0; t < c; ++t) {
             const int j = d.nb.list[(size_t)t * d.npad + k];
-            const T w = ak + debye_a<T>(d, j, c0, c1);
+            T w = ak + debye_a<T>(d, j, c0, c1);
+            if (d.w) w *= wk * d.w[j];
             if (w == T(0)) continue;
             T dx, dy, dz;
             d.geo.disp(a, d.geo.load(j), dx, dy, dz);
@@ -283,6 +296,7 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
 
 template <typename T> void launch_debye_values(const DebyeDev<T> &d, cudaStream_t st) {
     if (d.n == 0) return;
+    if (d.w) k_chem_weights<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d);
     k_debye_values<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d);
     prof_mark("debye_values", st);
 }

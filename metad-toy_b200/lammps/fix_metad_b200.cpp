@@ -36,6 +36,7 @@ FixMetadB200::FixMetadB200(LAMMPS *lmp, int narg, char **arg) : Fix(lmp, narg, a
   // the tokens after the style name, as the reference parses them (fix_crystallize.cu:32-302)
   const mtd_status s = mtd_create(narg - 3, arg + 3, &opt, &ctx_);
   if (s != MTD_OK) error->all(FLERR, std::string("fix metad: ") + mtd_last_error(ctx_));
+  needs_types_ = mtd_needs_types(ctx_) != 0;
   scalar_flag = 1;
   vector_flag = 1;
   size_vector = mtd_cv_dim(ctx_);
@@ -92,6 +93,7 @@ void FixMetadB200::post_force(int vflag)
   set_box();   // the box may change between steps (NPT)
   double vir[6] = {0, 0, 0, 0, 0, 0};
   const int n = atom->nlocal;
+  if (needs_types_) check(mtd_set_types(ctx_, n, atom->type));   // types follow LAMMPS's atom sorting
   check(mtd_post_force(ctx_, (int64_t) update->ntimestep, n, n ? &atom->x[0][0] : nullptr, atom->mask,
                        atom->image, n ? &atom->f[0][0] : nullptr, vflag_global ? vir : nullptr));
   if (vflag_global)

@@ -32,6 +32,7 @@ class FixMetadB200 : public Fix {
 
  private:
   mtd_ctx *ctx_ = nullptr;
+  bool needs_types_ = false;   // a STRU_FACTOR Chemical CAL reads atom->type every step
   std::vector<double> peratom_;
   void set_box();
   void check(mtd_status s);

@@ -39,7 +39,7 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_walkers_create", "mtd_walkers_destroy", "mtd_walkers_last_error", "mtd_walkers_count",
            "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
            "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
-           "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune"]
+           "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types"]
 
 
 class MetadError(RuntimeError):
@@ -88,6 +88,8 @@ def lib():
         L.mtd_get_grid.argtypes = [vp, dp, C.c_int64]
         L.mtd_last_launch_count.argtypes = [vp]
         L.mtd_max_neighbors.argtypes = [vp, C.c_char_p]
+        L.mtd_set_types.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
+        L.mtd_needs_types.argtypes = [vp]
         L.mtd_autotune.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
         L.mtd_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.mtd_walkers_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_int,
@@ -299,6 +301,15 @@ class Metad:
         self._check(lib().mtd_autotune(self._h, int(n), C.c_void_p(x_ptr), C.c_void_p(mask_ptr or None), int(reps),
                                        ch))
         return tuple(ch)
+
+    def set_types(self, types):
+        """Atom types (caller order) for STRU_FACTOR Chemical."""
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        self._check(lib().mtd_set_types(self._h, int(t.shape[0]), t.ctypes.data_as(C.POINTER(C.c_int))))
+
+    @property
+    def needs_types(self):
+        return bool(lib().mtd_needs_types(self._h))
 
     def set_tuning(self, neighbor_shape=0, q_block=0, lambda_block=0):
         self._check(lib().mtd_set_tuning(self._h, int(neighbor_shape), int(q_block), int(lambda_block)))

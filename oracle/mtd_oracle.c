@@ -653,6 +653,14 @@ static void debye_g(double r2, double rc2, double qf, double *g, double *dg) {
 int orc_debye(int n, const double *x, const orc_box *box, const int *ingroup,
               double rc, double qf, int mode, const orc_sw *sw,
               double *S, double *cv, double *grad) {
+    return orc_debye_w(n, x, box, ingroup, rc, qf, mode, sw, NULL, S, cv, grad);
+}
+
+/* STRU_FACTOR Chemical (src/cvs/CVs_Strufactor_chem.cu:137-175, :204-265): every
+ * pair term times w_i w_j, the per-atom type weights (w = NULL: all 1). */
+int orc_debye_w(int n, const double *x, const orc_box *box, const int *ingroup,
+                double rc, double qf, int mode, const orc_sw *sw, const double *w,
+                double *S, double *cv, double *grad) {
     int64_t *off; int *nbr;
     orc_pairs(n, x, box, rc, &off, &nbr);
     double rc2 = rc * rc;
@@ -668,7 +676,7 @@ int orc_debye(int n, const double *x, const orc_box *box, const int *ingroup,
             if (r2 > rc2 || r2 < 1e-12) continue;
             double g, dg;
             debye_g(r2, rc2, qf, &g, &dg);
-            acc += g;
+            acc += w ? w[i] * w[nbr[p]] * g : g;
         }
         S[i] = acc + 1.0;
     }
@@ -695,7 +703,8 @@ int orc_debye(int n, const double *x, const orc_box *box, const int *ingroup,
                     double gv, dg;
                     debye_g(r2, rc2, qf, &gv, &dg);
                     double r = sqrt(r2);
-                    for (int c = 0; c < 3; c++) { double v = a * dg * d[c] / r; g[3 * j + c] += v; g[3 * i + c] -= v; }
+                    double aw = w ? a * w[i] * w[j] : a;
+                    for (int c = 0; c < 3; c++) { double v = aw * dg * d[c] / r; g[3 * j + c] += v; g[3 * i + c] -= v; }
                 }
             }
         }

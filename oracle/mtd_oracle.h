@@ -75,6 +75,9 @@ int orc_steinh_l(int l, int n, const double *x, const orc_box *box, const int *i
 int orc_debye(int n, const double *x, const orc_box *box, const int *ingroup,
               double rc, double qf, int mode, const orc_sw *sw,
               double *S, double *cv, double *grad);
+int orc_debye_w(int n, const double *x, const orc_box *box, const int *ingroup,
+                double rc, double qf, int mode, const orc_sw *sw, const double *w,
+                double *S, double *cv, double *grad);
 
 /* k-vector structure factor: rho_k = sum_{j in group} exp(i k.x_j), S(k) = |rho_k|^2/N,
  * CV = mean_k S(k).  No reference counterpart. */

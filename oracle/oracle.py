@@ -85,6 +85,8 @@ def lib():
                                    C.c_double, C.POINTER(Sw), C.c_int, dp, dp, dp, dp, ip, dp, dp, dp]
         L.orc_debye.argtypes = [C.c_int, dp, C.POINTER(Box), ip, C.c_double, C.c_double, C.c_int,
                                 C.POINTER(Sw), dp, dp, dp]
+        L.orc_debye_w.argtypes = [C.c_int, dp, C.POINTER(Box), ip, C.c_double, C.c_double, C.c_int,
+                                  C.POINTER(Sw), dp, dp, dp, dp]
         L.orc_sk.argtypes = [C.c_int, dp, ip, C.c_int, dp, dp, dp, dp, dp]
         L.orc_grid_deposit.argtypes = [C.c_int, ip, dp, dp, dp, C.c_double, C.c_double, C.c_double]
         L.orc_grid_value.restype = C.c_double
@@ -207,7 +209,20 @@ def steinh_l(l, x, L, rlist, swr, eps=1e-6, swcv=None, mode="MEAN_SOLID", ingrou
     return out
 
 
-def debye(x, L, rc, qf, mode="AVE", sw=None, ingroup=None, periodic=(1, 1, 1), grad=True):
+def chem_type_weights(types, ctarget=0.0, sigma=1.0, cmap=None):
+    """Per-atom STRU_FACTOR Chemical weights: Chem_map value of the atom's type,
+    else exp(-(type - ctarget)^2 / (2 sigma^2)); type 0 weighs 0
+    (Stru_fact_chem_env constructor, src/cvs/CVs_Strufactor_chem.cu:33-55)."""
+    cmap = dict(cmap or {})
+    t = np.asarray(types, dtype=np.int64)
+    w = np.exp(-(t - ctarget) ** 2 / (2.0 * sigma ** 2))
+    for k, v in cmap.items():
+        w[t == k] = v
+    w[t == 0] = 0.0
+    return np.ascontiguousarray(w, dtype=np.float64)
+
+
+def debye(x, L, rc, qf, mode="AVE", sw=None, ingroup=None, periodic=(1, 1, 1), grad=True, weights=None):
     x = np.ascontiguousarray(x, dtype=np.float64)
     n = x.shape[0]
     g = _group(n, ingroup)
@@ -216,8 +231,9 @@ def debye(x, L, rc, qf, mode="AVE", sw=None, ingroup=None, periodic=(1, 1, 1), g
     gr = np.zeros(3 * n) if grad else None
     s = sw if sw is not None else make_sw("LINE")
     box = make_box(L, periodic)
-    lib().orc_debye(n, _dp(x), C.byref(box), _ip(g), float(rc), float(qf), 0 if mode == "AVE" else 1,
-                    C.byref(s), _dp(S), _dp(cv), _dp(gr) if grad else None)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    lib().orc_debye_w(n, _dp(x), C.byref(box), _ip(g), float(rc), float(qf), 0 if mode == "AVE" else 1,
+                      C.byref(s), _dp(w) if w is not None else None, _dp(S), _dp(cv), _dp(gr) if grad else None)
     out = dict(S=S, cv=cv[0])
     if grad:
         out["grad"] = gr.reshape(n, 3)

@@ -7,6 +7,7 @@ class Atom {
  public:
   double **x = nullptr, **f = nullptr;
   int *mask = nullptr;
+  int *type = nullptr;
   imageint *image = nullptr;
   int nlocal = 0, nmax = 0;
 };

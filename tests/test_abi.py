@@ -46,6 +46,10 @@ def test_reference_configs_parse():
     g = {"all": 1, "metad_group": 2}
     assert mtd.parse_args(deck1, groups=g) == ""
     assert mtd.parse_args(deck2, groups=g) == ""
+    # STRU_FACTOR Chemical with both Chem_map spellings (CVs_Strufactor.cu:125-183)
+    chem = deck2[:20] + ["Chemical", "Chem_ctarget", "2", "Chem_sigma", "0.5", "Chem_map", "(1,0.5)", "(3", "0.2)"] + \
+        deck2[20:]
+    assert mtd.parse_args(chem, groups=g) == ""
 
 
 @pytest.mark.parametrize("args,needle", [
@@ -69,6 +73,11 @@ def test_reference_configs_parse():
     (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "2", "DIM", "1", "0", "1", "10", "v1"], "DIM 2 is missing"),
     (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "1", "DIM", "1", "0", "1", "10", "v1+w"], "unknown symbol"),
     (C1[:17] + ["SYMBOL", "v1", "Q6.AVE", "CV_dim", "1", "DIM", "1", "0", "1", "10", "(v1"], "expected ')'"),
+    (["CAL", "NAME", "S", "STRU_FACTOR", "all", "q_factor", "2.8", "Chemical", "Chem_sigma", "0"], "Chem_sigma"),
+    (["CAL", "NAME", "S", "STRU_FACTOR", "all", "q_factor", "2.8", "Chemical", "Chem_map", "(2"],
+     "Invalid Chem_map format"),
+    (["CAL", "NAME", "S", "STRU_FACTOR", "all", "q_factor", "2.8", "Chemical", "Chem_map", "(2;1)"],
+     "(type weight)"),
     (["PACE", "ten"], "expects an integer"),
     (["GAUSSIAN", "0.01", "x", "10"], "expects a number"),
 ])

@@ -42,6 +42,39 @@ def test_debye_structure_factor(precision, mode):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chemical_structure_factor(precision):
+    """STRU_FACTOR Chemical: three atom types, Gaussian type weights around
+    type 2 with a Chem_map override for type 3; CV, forces and S_i against
+    the oracle.  Without types the step is refused."""
+    import mtd
+
+    x, L = _fcc_jit(nc=7)
+    types = (np.arange(x.shape[0]) * 7 % 3) + 1
+    args = ["GAUSSIAN", 0.01, 0.005, 10.0, "PACE", 10,
+            "CAL", "NAME", "SF", "STRU_FACTOR", "all", "cutoff_r", 6.0, "q_factor", 2.8,
+            "Chemical", "Chem_ctarget", 2, "Chem_sigma", 0.8, "Chem_map", "(3,0.4)",
+            "SYMBOL", "v1", "SF.AVE", "CV_dim", 1, "DIM", 1, 0.0, 2.0, 400, "v1", "WT", 0]
+    m = mtd.Metad(args, precision=precision)
+    m.set_box([0, 0, 0], L)
+    assert m.needs_types
+    with pytest.raises(mtd.MetadError, match="mtd_set_types"):
+        m.post_force(0, x, np.zeros_like(x))
+    m.set_types(types)
+    f = np.zeros_like(x)
+    m.post_force(0, x, f)
+    w = O.chem_type_weights(types, 2.0, 0.8, {3: 0.4})
+    o = O.debye(x, L, 6.0, 2.8, weights=w)
+    g = O.Grid([[0.0, 2.0]], [400], 0.01, 0.005, 10.0, 300.0, 8.617343e-5, False)
+    g.add_hill([o["cv"]])
+    V, dV = g.value([o["cv"]])
+    tcv, tf = (1e-9, 1e-8) if precision == "fp64" else (2e-5, 2e-3)
+    assert H.rel(m.cv[0], o["cv"]) < tcv
+    assert H.rel(f, -dV[0] * o["grad"]) < tf
+    assert H.rel(m.extract("SF.stru_f", x.shape[0]), o["S"]) < tcv * 10
+    m.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_kvector_structure_factor(precision):
     x, L = _fcc_jit(nc=8, sigma=0.2)
     kvec = systems.kvectors(24, systems.KMAG_111, 99)

@@ -135,6 +135,20 @@ def test_debye_gradient_fd(mode):
     assert np.max(np.abs(g - o["grad"][IDX])) < 1e-7 * max(1.0, np.abs(g).max())
 
 
+def test_chemical_debye_gradient_fd_and_unit_weights():
+    """STRU_FACTOR Chemical: pair terms times w(type_i) w(type_j); with all
+    weights 1 it is the plain Debye CV exactly."""
+    types = (np.arange(X0.shape[0]) % 3) + 1
+    w = O.chem_type_weights(types, ctarget=2.0, sigma=0.8, cmap={3: 0.4})
+    assert w[types == 3].max() == 0.4 and abs(w[types == 1][0] - np.exp(-1 / 1.28)) < 1e-15
+    plain = O.debye(X0, L0, 6.0, 2.8)
+    ones = O.debye(X0, L0, 6.0, 2.8, weights=np.ones(X0.shape[0]))
+    assert ones["cv"] == plain["cv"] and np.array_equal(ones["grad"], plain["grad"])
+    o = O.debye(X0, L0, 6.0, 2.8, weights=w)
+    g = _fd(lambda x: O.debye(x, L0, 6.0, 2.8, weights=w, grad=False)["cv"], X0, IDX)
+    assert np.max(np.abs(g - o["grad"][IDX])) < 1e-7 * max(1.0, np.abs(g).max())
+
+
 def test_sk_gradient_fd_and_bragg_peak():
     k = systems.kvectors(8, systems.KMAG_111, 5)
     o = O.sk(X0, k)
