@@ -125,7 +125,8 @@ double mtd_compute_vector(const mtd_ctx *ctx, int k);
 int mtd_cv_dim(const mtd_ctx *ctx);
 
 /* Per-atom export for `compute metad/atom` / Fix::extract
- * ("colvar_peratom:<CAL>.<prop>", props stein_q, dcvdx_x/y/z, stru_f).
+ * ("colvar_peratom:<CAL>.<prop>", props stein_q, dcvdx_x/y/z, stru_f,
+ * chem_pair_r for WEIGHT_CHEM).
  * Copies n values (caller order) into out.  dcvdx_* is the exact gradient of
  * the CV that the first SYMBOL on <CAL> selects, at the last step's positions
  * (STEINH Q and L, STRU_FACTOR, STRU_FACTOR_K); it re-runs that CAL's force
@@ -174,7 +175,8 @@ mtd_status mtd_autotune(mtd_ctx *ctx, int n, const double *d_x, const int *d_mas
 mtd_status mtd_set_tuning(mtd_ctx *ctx, int neighbor_shape, int q_block, int lambda_block);
 
 /* Atom types (caller order, n values, host array) for `STRU_FACTOR ...
- * Chemical`, whose pair terms are weighted by w(type_i) w(type_j): w from the
+ * Chemical` and `WEIGHT_CHEM`, whose pair terms are weighted by
+ * w(type_i) w(type_j): w from the
  * CAL's Chem_map pairs, else exp(-(type - Chem_ctarget)^2 / (2 Chem_sigma^2)),
  * type 0 weighing 0.  Call it before the first step and whenever types or
  * atom order change; a step with a Chemical CAL and no types for its n atoms
@@ -183,6 +185,43 @@ mtd_status mtd_set_tuning(mtd_ctx *ctx, int neighbor_shape, int q_block, int lam
  * weight table (src/cvs/CVs_Strufactor_chem.cu:33-55, :77-100). */
 mtd_status mtd_set_types(mtd_ctx *ctx, int n, const int *types);
 int mtd_needs_types(const mtd_ctx *ctx);
+
+/* Domain decomposition across ranks (one context per rank).  After
+ * mtd_set_domain, the n atoms of every step are this rank's nlocal owned
+ * atoms followed by ghosts (images of other ranks' atoms and periodic images,
+ * supplied by the caller): ghosts are neighbours only, never centres of a CV
+ * sum.  The box is the caller's subdomain grown by mtd_ghost_cutoff() on each
+ * side, normally with periodic = {0,0,0} (the ghosts carry the images).
+ * Once per step, between the CV passes and the bias, the library calls
+ * fn(buf, count, user) with this rank's totals (unit sums, S(k) sums, an
+ * overflow flag; count is the same on every rank); fn must replace buf with
+ * the element-wise sum over all ranks, the same bits on every rank
+ * (MPI_Allreduce(MPI_IN_PLACE, buf, count, MPI_DOUBLE, MPI_SUM, world)), and
+ * return 0.  Every rank then holds the same CVs, deposits the same hill and
+ * keeps the same grid; rank 0 alone writes HILLS and the record file.  The
+ * forces written to f cover all n rows: a ghost row holds the bias force of
+ * this rank's centres on that image, which the caller adds to the owning
+ * atom (LAMMPS reverse communication).  The virial is this rank's share.  A
+ * neighbour overflow on any rank makes every rank retry the step together.
+ * Call before the first step; mtd_set_nlocal updates nlocal when atoms
+ * migrate.  Needs the grid bias (not the hill-list bias).
+ * Replaces the per-rank reductions of the reference's CVs under LAMMPS's
+ * decomposition: MPI_Allreduce of the local sums over nlocal atoms
+ * (src/cvs/CVs_Steinhardt.cu:836, src/cvs/CVs_Strufactor.cu:653, :671,
+ * src/cvs/CV_Weighted_Chemical_Pair_Order.cu:306, :324) with ghosts
+ * nlocal..nlocal+nghost (src/cvs/CVs_Steinhardt.cu:595).  The reference's
+ * forward communication of per-atom CV values to ghosts before the gradient
+ * (src/cvs/CVs_Strufactor.cu:805-808) is not needed: each rank applies only
+ * its own centres' terms, to owned and ghost rows alike, and the ghost rows
+ * go back through the fix's reverse communication
+ * (src/core/fix_crystallize.cu:510-520). */
+typedef int (*mtd_allreduce_fn)(double *buf, int count, void *user);
+mtd_status mtd_set_domain(mtd_ctx *ctx, int nlocal, int rank, mtd_allreduce_fn fn, void *user);
+mtd_status mtd_set_nlocal(mtd_ctx *ctx, int nlocal);
+/* Ghost shell the caller must supply under domain decomposition: cutoff_r of
+ * STEINH Q and STRU_FACTOR, 2 x the cutoff of STEINH L (its centres read q_lm
+ * of neighbours, which need their own neighbours), 0 for S(k) alone. */
+double mtd_ghost_cutoff(const mtd_ctx *ctx);
 
 /* Largest neighbour count seen by the last step for CAL `name` (cap reporting). */
 int mtd_max_neighbors(mtd_ctx *ctx, const char *name);

@@ -135,10 +135,21 @@ bool parse_steinh(Cursor &c, int &i, const GroupTable &groups, Config &cfg, CalD
     return true;
 }
 
-// Stru_factor::create: `STRU_FACTOR group [cutoff_r x] [q_factor x] [d_block_size n] [SW_func TYPE ...]`.
-bool parse_sf(Cursor &c, int &i, const GroupTable &groups, CalDef &d) {
-    if (i + 1 >= c.narg) return c.fail("Error: STRU_FACTOR command requires at least \"STRU_FACTOR <group> \".");
+// Stru_factor::create: `STRU_FACTOR group [cutoff_r x] [q_factor x] [d_block_size n] [SW_func TYPE ...]
+// [Chemical] [Chem_ctarget c] [Chem_sigma s] [Chem_map (t w) ...]`; with wchem, Weighted_chem_pair::create
+// (src/cvs/CV_Weighted_Chemical_Pair_Order.cu:33-210): `WEIGHT_CHEM group [cutoff_r x] [d_block_size n]
+// [SW_func ...] [Chem_map ...] [Chem_ctarget c] [Chem_sigma s]`, always type-weighted, no q_factor.
+bool parse_sf(Cursor &c, int &i, const GroupTable &groups, CalDef &d, bool wchem) {
+    if (i + 1 >= c.narg)
+        return c.fail(wchem ? "Error: CHEM_PAIR command requires at least \"CHEM_PAIR <group> \"."
+                            : "Error: STRU_FACTOR command requires at least \"STRU_FACTOR <group> \".");
     d.kind = CAL_STRU_FACTOR;
+    if (wchem) {
+        d.wchem = true;
+        d.chem = true;
+        d.q_factor = 0.0;
+        d.has_q_factor = true;
+    }
     d.group = c.arg[i + 1];
     d.groupbit = groups.find(d.group);
     if (d.groupbit < 0) return c.fail("Error: group name " + d.group + " not found.");
@@ -146,7 +157,7 @@ bool parse_sf(Cursor &c, int &i, const GroupTable &groups, CalDef &d) {
     int k = i + 2;
     while (k < c.narg) {
         if (!std::strcmp(c.arg[k], "cutoff_r")) { if (!need_double(c, k + 1, d.cutoff_r, "cutoff_r")) return false; k += 2; }
-        else if (!std::strcmp(c.arg[k], "q_factor")) {
+        else if (!wchem && !std::strcmp(c.arg[k], "q_factor")) {
             if (!need_double(c, k + 1, d.q_factor, "q_factor")) return false;
             if (d.q_factor <= 0) return c.fail("Error: 'q_factor' must be > 0");
             d.has_q_factor = true;
@@ -164,7 +175,7 @@ bool parse_sf(Cursor &c, int &i, const GroupTable &groups, CalDef &d) {
             if (!parse_switch(c, kk, d.sf_sw)) return false;
             d.sf_use_sw = true;
             k = kk;
-        } else if (!std::strcmp(c.arg[k], "Chemical")) {
+        } else if (!wchem && !std::strcmp(c.arg[k], "Chemical")) {
             d.chem = true;
             k += 1;
         } else if (!std::strcmp(c.arg[k], "Chem_ctarget")) {
@@ -257,7 +268,8 @@ std::string resolve_symbol(Config &cfg, const SymbolDef &s) {
         d.sw_cv = cfg.sws[s.sub];
     }
     if (d.kind == CAL_STRU_FACTOR && s.func == "COUNT" && !d.sf_use_sw)
-        return "Error: STRU_FACTOR COUNT needs 'SW_func' on the CAL.";
+        return d.wchem ? "Error: WEIGHT_CHEM COUNT needs 'SW_func' on the CAL."
+                       : "Error: STRU_FACTOR COUNT needs 'SW_func' on the CAL.";
     return "";
 }
 
@@ -366,7 +378,8 @@ std::string parse_fix_args(int narg, const char *const *arg, const GroupTable &g
                 d.name = name;
                 bool ok;
                 if (type == "STEINH") ok = parse_steinh(c, i, groups, cfg, d);
-                else if (type == "STRU_FACTOR") ok = parse_sf(c, i, groups, d);
+                else if (type == "STRU_FACTOR") ok = parse_sf(c, i, groups, d, false);
+                else if (type == "WEIGHT_CHEM" || type == "CHEM_PAIR") ok = parse_sf(c, i, groups, d, true);
                 else if (type == "STRU_FACTOR_K") ok = parse_sk(c, i, groups, d);
                 else
                     return "Metad-toy Error: Unknown or unregistered object type '" + type + "' specified in CAL '" + name +

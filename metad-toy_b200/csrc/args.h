@@ -39,6 +39,7 @@ struct CalDef {
     // Chem_map (type weight) pairs, else exp(-(type - Chem_ctarget)^2 / (2 Chem_sigma^2)), w(0) = 0
     // (StruFactorRequest defaults, include/CVsets/CV_Stru_factor.h:28-33)
     bool chem = false;
+    bool wchem = false;           // WEIGHT_CHEM: the same pair sum with the taper alone as pair term (q_factor 0)
     double chem_ctarget = 0.0, chem_sigma = 1.0;
     std::vector<std::pair<int, double>> chem_map;
     // STRU_FACTOR_K (k-vector S(k), no reference counterpart)

@@ -204,39 +204,48 @@ __device__ __forceinline__ void stage_plan(const BiasPlan *__restrict__ Pp, unsi
     __syncthreads();
 }
 
-// Phases 1-3: deterministic reductions of every unit's block partials (rows
-// of 8 doubles, four rows in flight per thread), symbol values (one thread
-// each), DIM expressions with exact chain factors (one thread per dimension).
-__device__ void phase_cvs(const BiasPlan &P, double *smem, double (*usum)[8], double *s_sym,
-                          double (*s_jac)[kMaxSymbols], double *sv) {
-    for (int u = 0; u < P.nunit; ++u) {
-        const UnitPlan &U = P.unit[u];
-        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (U.partials && U.pstride != 8) {
-            for (int b = threadIdx.x; b < U.nparts; b += blockDim.x)
-                for (int t = 0; t < U.nvals && t < 8; ++t) v[t] += U.partials[(size_t)b * U.pstride + t];
-        } else if (U.partials) {
-            const double4 *rows = reinterpret_cast<const double4 *>(U.partials);
-            const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
-            for (int b0 = 0; b0 < U.nparts; b0 += 4 * blockDim.x) {
-                double4 r[8];
+// Deterministic reduction of one unit's block partials (rows of 8 doubles,
+// four rows in flight per thread); the totals land in usum_u on thread 0.
+__device__ void unit_total(const UnitPlan &U, double *smem, double *usum_u) {
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (U.partials && U.pstride != 8) {
+        for (int b = threadIdx.x; b < U.nparts; b += blockDim.x)
+            for (int t = 0; t < U.nvals && t < 8; ++t) v[t] += U.partials[(size_t)b * U.pstride + t];
+    } else if (U.partials) {
+        const double4 *rows = reinterpret_cast<const double4 *>(U.partials);
+        const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int b0 = 0; b0 < U.nparts; b0 += 4 * blockDim.x) {
+            double4 r[8];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int b = b0 + threadIdx.x + q * blockDim.x;
-                    r[2 * q] = b < U.nparts ? rows[2 * (size_t)b] : zero;
-                    r[2 * q + 1] = b < U.nparts ? rows[2 * (size_t)b + 1] : zero;
-                }
+            for (int q = 0; q < 4; ++q) {
+                const int b = b0 + threadIdx.x + q * blockDim.x;
+                r[2 * q] = b < U.nparts ? rows[2 * (size_t)b] : zero;
+                r[2 * q + 1] = b < U.nparts ? rows[2 * (size_t)b + 1] : zero;
+            }
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    v[0] += r[2 * q].x; v[1] += r[2 * q].y; v[2] += r[2 * q].z; v[3] += r[2 * q].w;
-                    v[4] += r[2 * q + 1].x; v[5] += r[2 * q + 1].y; v[6] += r[2 * q + 1].z; v[7] += r[2 * q + 1].w;
-                }
+            for (int q = 0; q < 4; ++q) {
+                v[0] += r[2 * q].x; v[1] += r[2 * q].y; v[2] += r[2 * q].z; v[3] += r[2 * q].w;
+                v[4] += r[2 * q + 1].x; v[5] += r[2 * q + 1].y; v[6] += r[2 * q + 1].z; v[7] += r[2 * q + 1].w;
             }
         }
-        block_sum<8>(v, smem);
-        if (threadIdx.x == 0)
-            for (int t = 0; t < 8; ++t) usum[u][t] = t < U.nvals ? v[t] : 0.0;
+    }
+    block_sum<8>(v, smem);
+    if (threadIdx.x == 0)
+        for (int t = 0; t < 8; ++t) usum_u[t] = t < U.nvals ? v[t] : 0.0;
+    __syncthreads();
+}
+
+// Phases 1-3: every unit's totals (this context's block partials, or the
+// totals over all ranks under domain decomposition), symbol values (one
+// thread each), DIM expressions with exact chain factors (one thread per
+// dimension).
+__device__ void phase_cvs(const BiasPlan &P, double *smem, double (*usum)[8], double *s_sym,
+                          double (*s_jac)[kMaxSymbols], double *sv) {
+    if (P.gsum) {
+        for (int e = threadIdx.x; e < P.nunit * 8; e += blockDim.x) usum[e / 8][e % 8] = P.gsum[e];
         __syncthreads();
+    } else {
+        for (int u = 0; u < P.nunit; ++u) unit_total(P.unit[u], smem, usum[u]);
     }
     if (threadIdx.x < P.nsym) {
         const int q = threadIdx.x;
@@ -625,6 +634,35 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 }
 
 }  // namespace
+
+__global__ void __launch_bounds__(256) k_unit_sums(const BiasPlan *__restrict__ Pp, double *out) {
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ double smem[8 * 32];
+    stage_plan(Pp, plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    for (int u = 0; u < P.nunit; ++u) unit_total(P.unit[u], smem, out + 8 * u);
+    int off = 8 * P.nunit;
+    for (int u = 0; u < P.nunit; ++u) {
+        const UnitPlan &U = P.unit[u];
+        if (!U.rho) continue;
+        for (int t = threadIdx.x; t < 2 * U.K; t += blockDim.x) out[off + t] = U.rho[t];
+        if (threadIdx.x == 0) out[off + 2 * U.K] = *U.sk_n;
+        off += 2 * U.K + 1;
+    }
+    if (threadIdx.x == 0) out[off] = P.status ? (double)P.status->overflow : 0.0;
+}
+
+int unit_sums_count(const BiasPlan &P) {
+    int c = 8 * P.nunit + 1;   // + the neighbour-overflow flag
+    for (int u = 0; u < P.nunit; ++u)
+        if (P.unit[u].rho) c += 2 * P.unit[u].K + 1;
+    return c;
+}
+
+void launch_unit_sums(const BiasPlan *d_plan, double *out, cudaStream_t st) {
+    k_unit_sums<<<1, 256, 0, st>>>(d_plan, out);
+    prof_mark("unit_sums", st);
+}
 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st) {
     k_bias_step<<<1, 256, 0, st>>>(d_plan, step);

@@ -121,6 +121,13 @@ struct DevStatus {
     unsigned int pad;
 };
 
+// A centre of the CV sums: in the CAL's group and owned by this context
+// (caller index below nown; under domain decomposition the atoms from nown
+// on are ghosts, which only serve as neighbours).
+__device__ __forceinline__ bool is_centre(const int *smask, const int *perm, int k, int groupbit, int nown) {
+    return (smask[k] & groupbit) && perm[k] < nown;
+}
+
 // Deterministic block sum of up to NV doubles per thread (fixed shuffle tree,
 // then warp 0 over the warp partials).  Result valid in thread 0.
 template <int NV>

@@ -68,7 +68,7 @@ struct Unit {
     double *kvec = nullptr, *rho = nullptr, *skn = nullptr;
     // STRU_FACTOR Chemical: type-weight parameters, the table built from the
     // types of mtd_set_types, and the per-atom weights (sorted order)
-    bool chem = false;
+    bool chem = false, wchem = false;
     double chem_ctarget = 0.0, chem_sigma = 1.0;
     std::vector<std::pair<int, double>> chem_map;
     double *d_wtab = nullptr;
@@ -192,6 +192,14 @@ struct mtd_ctx {
     Prof prof;
     bool prof_created = false;
     std::map<std::string, std::pair<long long, double>> prof_total;
+    // domain decomposition (mtd_set_domain): caller indices from nown on are ghosts
+    int nown = -1;                       // -1: off, every atom is owned
+    int dom_rank = 0;
+    mtd_allreduce_fn dom_fn = nullptr;
+    void *dom_user = nullptr;
+    double *d_xchg = nullptr;            // this rank's unit totals, then the totals over all ranks
+    double *h_xchg = nullptr;            // pinned staging of the same
+    int xchg_n = 0;
 };
 
 namespace {
@@ -477,6 +485,7 @@ void build_plan(mtd_ctx *c) {
     P.out = c->d_out;
     P.status = c->d_status;
     P.save = c->d_ws1;
+    P.gsum = c->nown >= 0 ? c->d_xchg : nullptr;
 }
 
 // Neighbour-list and CV-unit layout from the parsed CAL table (env pooling as in
@@ -557,6 +566,7 @@ mtd_status plan_units(mtd_ctx *c) {
         u.qf = d.q_factor;
         u.sf_sw = d.sf_sw;
         u.chem = d.kind == CAL_STRU_FACTOR && d.chem;
+        u.wchem = d.kind == CAL_STRU_FACTOR && d.wchem;
         u.chem_ctarget = d.chem_ctarget;
         u.chem_sigma = d.chem_sigma;
         u.chem_map = d.chem_map;
@@ -628,6 +638,10 @@ mtd_status plan_units(mtd_ctx *c) {
     return MTD_OK;
 }
 
+// Atoms that are centres of the CV sums: all of them, or under domain
+// decomposition the caller's first nlocal (the rest are ghosts).
+int owned(const mtd_ctx *c) { return c->nown >= 0 ? std::min(c->nown, c->n) : c->n; }
+
 NeighDev env_dev(const Env &e) {
     NeighDev nd;
     nd.list = e.list;
@@ -663,6 +677,7 @@ template <typename T> LocalDev<T> local_dev(mtd_ctx *c, Unit &u, const CellGrid 
     d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(c, u); d.LA = u.LA; d.LB = u.LB;
     d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
+    d.nown = owned(c);
     d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
     d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
     d.qblock = c->tune_q;
@@ -677,6 +692,7 @@ template <typename T> GlobalDev<T> global_dev(mtd_ctx *c, Unit &u, const CellGri
     for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.exact = geo_d(g, c->xs);
     d.nb = env_dev(c->envs[u.env]);
+    d.nown = owned(c);
     d.q = (T *)u.q; d.Q = (T *)u.Q; d.partials = u.partials; d.coef = u.coef;
     return d;
 }
@@ -686,6 +702,7 @@ template <typename T> DebyeDev<T> debye_dev(mtd_ctx *c, Unit &u, const CellGrid 
     d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
     d.S = (T *)u.S; d.partials = u.partials; d.coef = u.coef;
+    d.nown = owned(c);
     d.w = u.chem ? (T *)u.w : nullptr;
     d.types = c->d_types;
     d.wtab = u.d_wtab;
@@ -698,6 +715,7 @@ SkDev sk_dev(mtd_ctx *c, Unit &u, const double *x, const int *mask) {
     d.n = c->n; d.K = u.K; d.groupbit = u.groupbit; d.x = x; d.mask = mask; d.k = u.kvec;
     d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
     d.fp64 = c->fp64;
+    d.nown = owned(c);
     return d;
 }
 
@@ -791,6 +809,17 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
     if (!c->box_set) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_box must be called before the first step");
     mtd_status s0 = ensure_capacity(c, n);
     if (s0 != MTD_OK) return s0;
+    if (c->nown > n)
+        return fail(c, MTD_ERR_INVALID_ARG, "domain decomposition: nlocal " + std::to_string(c->nown) +
+                                                " exceeds the " + std::to_string(n) + " atoms of this step");
+    if (c->nown >= 0 && !c->d_xchg) {
+        build_plan(c);
+        c->xchg_n = unit_sums_count(c->plan);
+        MTD_CU(dalloc(&c->d_xchg, sizeof(double) * (size_t)c->xchg_n), "domain totals");
+        MTD_CU(cudaHostAlloc((void **)&c->h_xchg, sizeof(double) * (size_t)c->xchg_n, cudaHostAllocDefault),
+               "domain totals");
+        c->plan_dirty = true;
+    }
     CellGrid g = make_grid(c);
     c->last_grid = g;
     if (c->plan_dirty) {
@@ -853,6 +882,34 @@ mtd_status enqueue_forces(mtd_ctx *c, long long step, const double *x, const int
     return MTD_OK;
 }
 
+// Domain decomposition, between the CV passes and the bias kernel: this
+// rank's unit totals (and S(k) sums, and its neighbour-overflow flag) go to
+// the caller's allreduce; the totals over all ranks come back for the bias
+// kernel (P.gsum) and the S(k) arrays.  A step that overflowed on any rank
+// counts as overflowed on every rank, so all ranks skip the deposit and, in
+// mtd_post_force, retry together.
+mtd_status exchange_totals(mtd_ctx *c) {
+    const int cnt = c->xchg_n;
+    launch_unit_sums(c->d_plan, c->d_xchg, c->st);
+    c->launches += 1;
+    MTD_CU(cudaMemcpyAsync(c->h_xchg, c->d_xchg, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st), "domain totals");
+    MTD_CU(cudaStreamSynchronize(c->st), "domain totals");
+    const double own_overflow = c->h_xchg[cnt - 1];
+    if (c->dom_fn(c->h_xchg, cnt, c->dom_user) != 0)
+        return fail(c, MTD_ERR_INVALID_ARG, "domain decomposition: the allreduce callback failed");
+    MTD_CU(cudaMemcpyAsync(c->d_xchg, c->h_xchg, sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st), "domain totals");
+    int off = 8 * (int)c->units.size();
+    for (Unit &u : c->units) {
+        if (u.kind != CAL_STRU_FACTOR_K) continue;
+        MTD_CU(cudaMemcpyAsync(u.rho, c->d_xchg + off, sizeof(double) * 2 * u.K, cudaMemcpyDeviceToDevice, c->st), "rho(k)");
+        MTD_CU(cudaMemcpyAsync(u.skn, c->d_xchg + off + 2 * u.K, sizeof(double), cudaMemcpyDeviceToDevice, c->st), "rho(k)");
+        off += 2 * u.K + 1;
+    }
+    if (c->h_xchg[cnt - 1] != 0.0 && own_overflow == 0.0)   // another rank overflowed: a flag of 1 (no growth here)
+        MTD_CU(cudaMemsetAsync(&c->d_status->overflow, 1, 1, c->st), "status");
+    return MTD_OK;
+}
+
 // f_ready (may be null): an event the force kernels wait for (forces uploaded
 // on the side stream while the CV passes run).
 mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, const int *mask, const int *image,
@@ -861,6 +918,10 @@ mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, cons
     c->launches = 0;
     mtd_status s = enqueue_values(c, n, x, mask, image);
     if (s != MTD_OK) return s;
+    if (c->nown >= 0) {
+        s = exchange_totals(c);
+        if (s != MTD_OK) return s;
+    }
     if (c->nb) {   // hill-list bias: CVs, V and dV/ds at s, deposit and coefficients
         launch_list_cvs(c->d_plan, c->d_ws1, c->st);
         s = nnbias_enqueue_vdv(c->nb, c->d_out, c->d_vdv, c->nn_usable, c->h_fit, c->st);
@@ -1186,6 +1247,8 @@ void mtd_destroy(mtd_ctx *c) {
     dfree(c->d_ws1);
     dfree(c->d_types);
     dfree(c->d_dcv);
+    dfree(c->d_xchg);
+    if (c->h_xchg) cudaFreeHost(c->h_xchg);
     if (c->f_ready) cudaEventDestroy(c->f_ready);
     if (c->prof_created)
         for (int i = 0; i < kProfMax; ++i) cudaEventDestroy(c->prof.ev[i]);
@@ -1249,6 +1312,12 @@ mtd_status mtd_init(mtd_ctx *c) {
             c->f_hills = std::fopen(hp.c_str(), "a");
             appended = true;
         }
+    }
+    if (c->dom_rank != 0) {   // domain decomposition: rank 0 alone writes HILLS and the record file
+        if (c->f_hills) std::fclose(c->f_hills);
+        c->f_hills = nullptr;
+        c->initialized = true;
+        return MTD_OK;
     }
     if (!hp.empty() && !appended) {
         c->f_hills = std::fopen(hp.c_str(), "w");
@@ -1567,7 +1636,8 @@ mtd_status mtd_extract_peratom(mtd_ctx *c, const char *key, double *out, int n) 
             const void *src = nullptr;
             if (prop == "stein_q" && u.kind == CAL_STEINH_Q) { src = u.Q; }
             else if (prop == "stein_q" && u.kind == CAL_STEINH_L) { src = u.lqs; stride = 2; off = (int)slot; }
-            else if (prop == "stru_f" && u.kind == CAL_STRU_FACTOR) { src = u.S; }
+            else if (prop == "stru_f" && u.kind == CAL_STRU_FACTOR && !u.wchem) { src = u.S; }
+            else if (prop == "chem_pair_r" && u.kind == CAL_STRU_FACTOR && u.wchem) { src = u.S; }
             else return fail(c, MTD_ERR_INVALID_ARG, "unknown per-atom property " + prop + " for CAL " + cal);
             raw.resize(R * stride * (size_t)n);
             MTD_CU(cudaMemcpy(raw.data(), src, R * stride * (size_t)n, cudaMemcpyDeviceToHost), "extract");
@@ -1679,6 +1749,36 @@ mtd_status mtd_set_types(mtd_ctx *c, int n, const int *types) {
     }
     c->types_n = n;
     return MTD_OK;
+}
+
+mtd_status mtd_set_domain(mtd_ctx *c, int nlocal, int rank, mtd_allreduce_fn fn, void *user) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    if (c->initialized)
+        return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_domain must be called before the first step");
+    if (nlocal < 0 || rank < 0 || !fn)
+        return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_domain needs nlocal >= 0, rank >= 0 and an allreduce callback");
+    if (c->cfg.hill_list())
+        return fail(c, MTD_ERR_UNSUPPORTED, "domain decomposition needs the grid bias (CV_dim 1-3, no NN_BIAS)");
+    c->nown = nlocal;
+    c->dom_rank = rank;
+    c->dom_fn = fn;
+    c->dom_user = user;
+    c->plan_dirty = true;
+    return MTD_OK;
+}
+
+mtd_status mtd_set_nlocal(mtd_ctx *c, int nlocal) {
+    if (!c || nlocal < 0) return MTD_ERR_INVALID_ARG;
+    if (c->nown < 0) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_nlocal: domain decomposition is not enabled");
+    c->nown = nlocal;
+    return MTD_OK;
+}
+
+double mtd_ghost_cutoff(const mtd_ctx *c) {
+    if (!c) return 0.0;
+    double g = 0.0;
+    for (const Env &e : c->envs) g = std::fmax(g, e.kind == ENV_L ? 2.0 * e.rc : e.rc);
+    return g;
 }
 
 int mtd_needs_types(const mtd_ctx *c) {

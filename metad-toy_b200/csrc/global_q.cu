@@ -60,7 +60,7 @@ template <int L, typename T> __global__ void __launch_bounds__(kBlock) k_global_
 #pragma unroll
         for (int t = 0; t < Z::SQ; ++t) d.q[(size_t)k * Z::SQ + t] = acc[t];
         d.Q[k] = Q;
-        if (d.smask[k] & d.groupbit) {
+        if (is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) {
             part[0] = (double)Q;
             if (d.nsw > 0) part[1] = sw_f<double>(d.sw[0], (double)Q);
             if (d.nsw > 1) part[2] = sw_f<double>(d.sw[1], (double)Q);
@@ -74,7 +74,7 @@ template <int L, typename T> __global__ void __launch_bounds__(kBlock) k_global_
 
 template <int L, typename T>
 __device__ __forceinline__ T lambda_scale(const GlobalDev<T> &d, int k, const double *c) {
-    if (!(d.smask[k] & d.groupbit)) return T(0);
+    if (!is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) return T(0);
     const int n = d.nb.nkept[k];
     const double Q = (double)d.Q[k];
     if (n <= 0 || !(Q > 0.0)) return T(0);

@@ -132,6 +132,7 @@ template <typename T> struct LocalDev {
     SwParams sw_r, sw_cvA, sw_cvB;
     const int *smask;
     const int *perm;
+    int nown;                   // caller indices >= nown are ghosts: neighbours, never centres
     Geo<T> geo;
     NeighDev nb;
     T *q, *nf, *lq, *lqs, *e12, *lam, *g, *tu;
@@ -152,6 +153,7 @@ template <typename T> struct GlobalDev {
     int groupbit, nsw;
     SwParams sw[2];             // SW_FUNC symbols of this CAL
     const int *smask, *perm;
+    int nown;                   // caller indices >= nown are ghosts
     Geo<T> geo;
     GeoD exact;                 // FP64 raw coordinates for the cap-membership test
     NeighDev nb;
@@ -171,6 +173,7 @@ template <typename T> struct DebyeDev {
     double rc2, qf;
     SwParams sw;
     const int *smask, *perm;
+    int nown;                   // caller indices >= nown are ghosts
     Geo<T> geo;
     NeighDev nb;
     T *S;
@@ -188,6 +191,7 @@ void launch_debye_forces(const DebyeDev<T> &d, const double *f_src, double *f_ds
 
 struct SkDev {
     int n, K, groupbit;
+    int nown;                   // caller indices >= nown are ghosts (no S(k) term)
     const double *x;            // caller order AoS
     const int *mask;
     const double *k;            // K*3
@@ -232,7 +236,7 @@ struct HillRec {
 
 constexpr int kMaxUnits = 16;
 
-struct BiasPlan {
+struct alignas(16) BiasPlan {
     int D;
     int nbin[3];
     double lo[3], hi[3], dcv[3];
@@ -254,6 +258,8 @@ struct BiasPlan {
                            // kOutHillOffset..: the hill recorded last (a HillRec)
     const DevStatus *status;   // a neighbour overflow this step: no deposit, zero force coefficients
     struct WalkState *save;    // when set, the step's block-sum totals are kept here (per-atom gradients)
+    const double *gsum;        // domain decomposition: every unit's totals summed over the ranks
+                               // ([nunit][8]), used in place of this rank's block partials
 };
 constexpr int kOutSymOffset = 8;   // out[kOutSymOffset + sym]
 constexpr int kOutHillOffset = 48;  // out[kOutHillOffset ..+7): the last HillRec, copied out with the step's outputs
@@ -261,6 +267,12 @@ static_assert(kOutSymOffset + kMaxSymbols <= kOutHillOffset && kOutHillOffset * 
               "output layout");
 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st);
+// Domain decomposition: this rank's totals of every unit ([nunit][8], the
+// block partials reduced in the order the bias kernel uses), the rho(k) (2K)
+// and atom count of each S(k) unit in unit order, and last this step's
+// neighbour-overflow count (0: none).
+void launch_unit_sums(const BiasPlan *d_plan, double *out, cudaStream_t st);
+int unit_sums_count(const BiasPlan &P);
 
 // Per-walker state handed between the multi-walker bias kernels.
 struct WalkState {

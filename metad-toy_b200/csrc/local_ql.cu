@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_local_lq(LocalDev<T> d) {
     const bool valid = k < d.n;
     double part[5] = {0, 0, 0, 0, 0};
     if (valid) {
-        const bool ing = (d.smask[k] & d.groupbit) != 0;
+        const bool ing = is_centre(d.smask, d.perm, k, d.groupbit, d.nown);
         const T nfk = d.nf[k];
         T A[S::SQ];
         T lqA = T(0), lqB = T(0);

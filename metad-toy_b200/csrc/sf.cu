@@ -29,6 +29,11 @@ template <typename T> __device__ __forceinline__ void debye_g(T r2, T rc2, T qf,
         s = T(1) - t * t * t;
         ds = T(-3) * t * t * (T(2) * r) / (rc2 - r_on);
     }
+    if (qf == T(0)) {   // WEIGHT_CHEM: the taper alone is the pair term
+        gv = s;
+        dg = ds;
+        return;
+    }
     T sn, cs;
     t_sincos<T>(th, &sn, &cs);
     gv = sn / th * s;
@@ -50,7 +55,7 @@ template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(D
     double part[4] = {0, 0, 0, 0};
     if (k < d.n) {
         T S = T(0);
-        if (d.smask[k] & d.groupbit) {
+        if (is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) {
             const int c = min(d.nb.count[k], d.nb.M);
             const T rc2 = (T)d.rc2, qf = (T)d.qf;
             const auto a = d.geo.load(k);
@@ -77,7 +82,7 @@ template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(D
 
 template <typename T>
 __device__ __forceinline__ T debye_a(const DebyeDev<T> &d, int k, double c0, double c1) {
-    if (!(d.smask[k] & d.groupbit)) return T(0);
+    if (!is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) return T(0);
     double a = c0;
     if (c1 != 0.0) a += c1 * sw_df<double>(d.sw, (double)d.S[k]);
     return (T)a;
@@ -162,7 +167,7 @@ template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d
             acc[t] = 0.0;
             facc[t] = 0.f;
         }
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.nown; i += gridDim.x * blockDim.x) {
             if (d.mask && !(d.mask[i] & d.groupbit)) continue;
             if (k0 == 0) cnt += 1.0;
             const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
     double vir[6] = {0, 0, 0, 0, 0, 0};
     if (i < d.n) {
         double gx = 0, gy = 0, gz = 0;
-        if (!d.mask || (d.mask[i] & d.groupbit)) {
+        if (i < d.nown && (!d.mask || (d.mask[i] & d.groupbit))) {
             const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
             if (FP64) {
                 for (int q = 0; q < d.K; ++q) {

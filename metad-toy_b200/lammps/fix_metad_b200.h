@@ -5,7 +5,10 @@
 // grammar (passed to mtd_create verbatim), same thermo scalar (bias energy)
 // and vector (the CVs), the same `colvar_peratom:<CAL>.<prop>` extract keys,
 // energy and virial contributions.  Compiled with the plugin against LAMMPS's
-// headers; everything it computes is done by the library.
+// headers; everything it computes is done by the library.  On several MPI
+// ranks each rank's context takes its local atoms as centres and its ghosts
+// as neighbours, sums its totals with MPI_Allreduce, and the ghost rows of
+// the bias force return to their owners through reverse communication.
 #ifndef LMP_FIX_METAD_B200_H
 #define LMP_FIX_METAD_B200_H
 
@@ -29,11 +32,15 @@ class FixMetadB200 : public Fix {
   double compute_scalar() override;
   double compute_vector(int) override;
   void *extract(const char *, int &) override;
+  int pack_reverse_comm(int, int, double *) override;
+  void unpack_reverse_comm(int, int *, double *) override;
 
  private:
   mtd_ctx *ctx_ = nullptr;
   bool needs_types_ = false;   // a STRU_FACTOR Chemical CAL reads atom->type every step
+  bool multi_ = false;         // more than one MPI rank: domain decomposition
   std::vector<double> peratom_;
+  std::vector<double> fbuf_;   // bias force of local and ghost rows (several ranks)
   void set_box();
   void check(mtd_status s);
 };

@@ -39,7 +39,8 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_walkers_create", "mtd_walkers_destroy", "mtd_walkers_last_error", "mtd_walkers_count",
            "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
            "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
-           "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types"]
+           "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types",
+           "mtd_set_domain", "mtd_set_nlocal", "mtd_ghost_cutoff"]
 
 
 class MetadError(RuntimeError):
@@ -55,6 +56,9 @@ class Options(C.Structure):
 
 
 _lib = None
+
+# int (*)(double *buf, int count, void *user): in-place sum of buf over the ranks
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.c_void_p)
 
 
 def build(jobs=8):
@@ -90,6 +94,10 @@ def lib():
         L.mtd_max_neighbors.argtypes = [vp, C.c_char_p]
         L.mtd_set_types.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.mtd_needs_types.argtypes = [vp]
+        L.mtd_set_domain.argtypes = [vp, C.c_int, C.c_int, ALLREDUCE_FN, vp]
+        L.mtd_set_nlocal.argtypes = [vp, C.c_int]
+        L.mtd_ghost_cutoff.argtypes = [vp]
+        L.mtd_ghost_cutoff.restype = C.c_double
         L.mtd_autotune.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
         L.mtd_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.mtd_walkers_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_int,
@@ -310,6 +318,29 @@ class Metad:
     @property
     def needs_types(self):
         return bool(lib().mtd_needs_types(self._h))
+
+    def set_domain(self, nlocal, rank, allreduce):
+        """Domain decomposition: the first nlocal atoms of each step are owned,
+        the rest ghosts.  allreduce(buf) must replace the float64 array buf, in
+        place, with its element-wise sum over all ranks (identical on every
+        rank); it is called once per step from inside post_force."""
+        def cb(ptr, count, _user):
+            try:
+                allreduce(np.ctypeslib.as_array(ptr, shape=(count,)))
+                return 0
+            except Exception as e:  # reported through the step's status
+                self._domain_error = e
+                return 1
+        self._domain_error = None
+        self._domain_cb = ALLREDUCE_FN(cb)   # kept alive as long as the context
+        self._check(lib().mtd_set_domain(self._h, int(nlocal), int(rank), self._domain_cb, None))
+
+    def set_nlocal(self, nlocal):
+        self._check(lib().mtd_set_nlocal(self._h, int(nlocal)))
+
+    @property
+    def ghost_cutoff(self):
+        return lib().mtd_ghost_cutoff(self._h)
 
     def set_tuning(self, neighbor_shape=0, q_block=0, lambda_block=0):
         self._check(lib().mtd_set_tuning(self._h, int(neighbor_shape), int(q_block), int(lambda_block)))

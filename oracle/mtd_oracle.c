@@ -645,6 +645,11 @@ static void debye_g(double r2, double rc2, double qf, double *g, double *dg) {
         s = 1.0 - t * t * t;
         ds = -3.0 * t * t * (2.0 * r) / (rc2 - r_on);
     }
+    if (qf == 0.0) {   /* WEIGHT_CHEM pair term (CV_Weighted_Chemical_Pair_Order.cu:647-690) */
+        *g = s;
+        *dg = ds;
+        return;
+    }
     double sn = sin(th), cs = cos(th);
     *g = sn / th * s;
     *dg = (cs / th - sn / (th * th)) * s * qf + ds * sn / th;

@@ -9,7 +9,7 @@ class Atom {
   int *mask = nullptr;
   int *type = nullptr;
   imageint *image = nullptr;
-  int nlocal = 0, nmax = 0;
+  int nlocal = 0, nghost = 0, nmax = 0;
 };
 }  // namespace LAMMPS_NS
 #endif

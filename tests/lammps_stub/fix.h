@@ -15,6 +15,7 @@ class Fix : protected Pointers {
   int extscalar = 0, extvector = 0;
   int energy_global_flag = 0, virial_global_flag = 0, thermo_energy = 0, thermo_virial = 0;
   int vflag_global = 0;
+  int comm_reverse = 0;
   double virial[6] = {0, 0, 0, 0, 0, 0};
   Fix(LAMMPS *lmp, int, char **arg) : Pointers(lmp), id(arg[0]), style(arg[2]) {
     igroup = group->find(arg[1]);
@@ -30,6 +31,8 @@ class Fix : protected Pointers {
   virtual double compute_scalar() { return 0.0; }
   virtual double compute_vector(int) { return 0.0; }
   virtual void *extract(const char *, int &) { return nullptr; }
+  virtual int pack_reverse_comm(int, int, double *) { return 0; }
+  virtual void unpack_reverse_comm(int, int *, double *) {}
 
  protected:
   void v_init(int vflag) {

@@ -1,6 +1,7 @@
 // Test stand-in for LAMMPS's top-level class: owns the sub-objects the shim reads.
 #ifndef STUB_LAMMPS_H
 #define STUB_LAMMPS_H
+#include "mpi.h"
 namespace LAMMPS_NS {
 class Memory;
 class Error;
@@ -22,6 +23,7 @@ class LAMMPS {
   Modify *modify;
   Group *group;
   Comm *comm;
+  MPI_Comm world = 0;
   LAMMPS();
   ~LAMMPS();
 };

@@ -8,7 +8,8 @@ class Pointers {
  public:
   explicit Pointers(LAMMPS *ptr) :
       lmp(ptr), memory(ptr->memory), error(ptr->error), atom(ptr->atom), update(ptr->update),
-      domain(ptr->domain), force(ptr->force), modify(ptr->modify), group(ptr->group), comm(ptr->comm) {}
+      domain(ptr->domain), force(ptr->force), modify(ptr->modify), group(ptr->group), comm(ptr->comm),
+      world(ptr->world) {}
   virtual ~Pointers() = default;
 
  protected:
@@ -22,6 +23,7 @@ class Pointers {
   Modify *&modify;
   Group *&group;
   Comm *&comm;
+  MPI_Comm &world;
 };
 }  // namespace LAMMPS_NS
 #endif

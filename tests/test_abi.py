@@ -50,6 +50,11 @@ def test_reference_configs_parse():
     chem = deck2[:20] + ["Chemical", "Chem_ctarget", "2", "Chem_sigma", "0.5", "Chem_map", "(1,0.5)", "(3", "0.2)"] + \
         deck2[20:]
     assert mtd.parse_args(chem, groups=g) == ""
+    # WEIGHT_CHEM as the user manual writes it (docs/manuals/User_Manual.zh.md:156)
+    wchem = ["GAUSSIAN", "0.01", "0.01", "10.0", "PACE", "50", "CAL", "NAME", "CP", "WEIGHT_CHEM", "metad_group",
+             "cutoff_r", "3", "Chem_map", "(1,0.1)", "(2,3.0)", "SYMBOL", "v1", "CP.AVE", "CV_dim", "1",
+             "DIM", "1", "0", "10", "1000", "v1"]
+    assert mtd.parse_args(wchem, groups=g) == ""
 
 
 @pytest.mark.parametrize("args,needle", [

@@ -75,6 +75,38 @@ def test_chemical_structure_factor(precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("mode", ["AVE", "COUNT"])
+def test_weight_chem(precision, mode):
+    """WEIGHT_CHEM (type-weighted tapered pair count) against the oracle,
+    with the per-atom chem_pair_r export."""
+    import mtd
+
+    x, L = _fcc_jit(nc=7)
+    types = (np.arange(x.shape[0]) * 5 % 2) + 1
+    sym = "CP.%s" % mode
+    lo, hi, sig = (0.0, 40.0, 0.2) if mode == "AVE" else (0.0, 1000.0, 10.0)
+    args = ["GAUSSIAN", sig, 0.005, 10.0, "PACE", 10,
+            "CAL", "NAME", "CP", "WEIGHT_CHEM", "all", "cutoff_r", 4.5, "Chem_map", "(1,0.1)", "(2", "3.0)",
+            "SW_func", "FERMI", "r_0", 30.0, "alpha", 0.1,
+            "SYMBOL", "v1", sym, "CV_dim", 1, "DIM", 1, lo, hi, 400, "v1", "WT", 0]
+    m = mtd.Metad(args, precision=precision)
+    m.set_box([0, 0, 0], L)
+    m.set_types(types)
+    f = np.zeros_like(x)
+    m.post_force(0, x, f)
+    w = O.chem_type_weights(types, cmap={1: 0.1, 2: 3.0})
+    o = O.debye(x, L, 4.5, 0.0, mode=mode, sw=O.make_sw("FERMI", r0=30.0, alpha=0.1), weights=w)
+    g = O.Grid([[lo, hi]], [400], sig, 0.005, 10.0, 300.0, 8.617343e-5, False)
+    g.add_hill([o["cv"]])
+    V, dV = g.value([o["cv"]])
+    tcv, tf = (1e-9, 1e-8) if precision == "fp64" else (2e-5, 2e-3)
+    assert H.rel(m.cv[0], o["cv"]) < tcv
+    assert H.rel(f, -dV[0] * o["grad"]) < tf
+    assert H.rel(m.extract("CP.chem_pair_r", x.shape[0]), o["S"]) < tcv * 10
+    m.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_kvector_structure_factor(precision):
     x, L = _fcc_jit(nc=8, sigma=0.2)
     kvec = systems.kvectors(24, systems.KMAG_111, 99)

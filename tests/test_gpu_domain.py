@@ -1,0 +1,173 @@
+"""Domain decomposition through the C ABI on one GPU: two ranks emulated as
+two contexts driven by two host threads (each with its own stream; they meet
+only on the host, in the allreduce callback), against one context holding the
+whole periodic system.  Forces are compared after the ghost rows have been
+added to their owners; CVs, bias and the grid must agree with the single
+domain, and bit for bit between the ranks."""
+import threading
+
+import numpy as np
+import pytest
+
+import domain
+import helpers as H
+import mtd
+import systems
+
+pytestmark = pytest.mark.gpu
+
+
+def _fcc(nc=7, seed=4, sigma=0.15):
+    x, L = systems.fcc(nc, 5.26), np.array([nc * 5.26] * 3)
+    return systems.wrap(systems.jitter(x, sigma, seed), L), L
+
+
+def _args_q():
+    return ["GAUSSIAN", 0.01, 0.005, 10.0, "PACE", 1, "TEMP", 300.0,
+            "CAL", "NAME", "SWC", "SW_FUNC", "FERMI", "r_0", 0.45, "alpha", 20.0,
+            "CAL", "NAME", "Q6", "STEINH", "Q", 6, "all", "cutoff_r", 4.5, "cutoff_Natoms", 12,
+            "SYMBOL", "v1", "Q6.AVE", "SYMBOL", "v2", "Q6.SW_FUNC.SWC", "CV_dim", 2,
+            "DIM", 1, 0.0, 1.0, 200, "v1", "DIM", 2, 0.0, 2000.0, 200, "v2", "WT", 1]
+
+
+def _args_sf():
+    return ["GAUSSIAN", 20.0, 0.005, 10.0, "PACE", 1,
+            "CAL", "NAME", "SF", "STRU_FACTOR", "all", "cutoff_r", 6.0, "q_factor", 2.8, "Chemical",
+            "Chem_ctarget", 2.0, "Chem_sigma", 0.8, "Chem_map", "(3,0.4)",
+            "SW_func", "FERMI", "r_0", 1.0, "alpha", 5.0,
+            "SYMBOL", "v1", "SF.COUNT", "CV_dim", 1, "DIM", 1, 0.0, 2000.0, 400, "v1", "WT", 0]
+
+
+def _args_sk(nk=24):
+    return ["GAUSSIAN", 0.01, 0.005, 10.0, "PACE", 1,
+            "CAL", "NAME", "SK", "STRU_FACTOR_K", "all", "nk", nk, "kmag", systems.KMAG_111, "seed", 3,
+            "SYMBOL", "v1", "SK.AVE", "CV_dim", 1, "DIM", 1, 0.0, 2.0, 400, "v1", "WT", 0]
+
+
+CASES = {
+    "steinh_l_step": lambda: H.fix_args_local(pace=1),
+    "steinh_l_fermi": lambda: H.fix_args_local(pace=1, sw="FERMI"),
+    "steinh_q": _args_q,
+    "stru_factor_chem": _args_sf,
+    "sk": _args_sk,
+}
+
+
+def _run_single(args, x, L, steps, precision, types, tmp):
+    m = mtd.Metad(args, precision=precision, hills_path="HILLS", work_dir=str(tmp))
+    m.set_box([0, 0, 0], L)
+    if m.needs_types:
+        m.set_types(types)
+    out = []
+    for step, xs in steps:
+        f = np.zeros_like(xs)
+        m.post_force(step, xs, f)
+        out.append((m.cv, m.compute_scalar(), f))
+    grid = m.grid(_grid_size(args))
+    m.close()
+    return out, grid
+
+
+def _grid_size(args):
+    a = [str(t) for t in args]
+    size, i = 1, 0
+    while i < len(a):
+        if a[i] == "DIM":
+            size *= int(a[i + 4])
+            i += 5
+        else:
+            i += 1
+    return size
+
+
+def _run_ranks(args, x, L, steps, precision, types, tmp, grid=(2, 1, 1)):
+    probe = mtd.Metad(args, precision=precision)
+    cut = probe.ghost_cutoff
+    probe.close()
+    nr = int(np.prod(grid))
+    red = domain.LocalAllreduce(nr, timeout=120)
+    ctx = []
+    for r in range(nr):
+        m = mtd.Metad(args, precision=precision, hills_path="HILLS", work_dir=str(tmp))
+        m.set_domain(0, r, red.for_rank(r))
+        ctx.append(m)
+    res = [[None] * len(steps) for _ in range(nr)]
+    errs = []
+
+    def run(r):
+        try:
+            m = ctx[r]
+            for s, (step, xs) in enumerate(steps):
+                rk = domain.decompose(xs, [0, 0, 0], L, grid, max(cut, 1e-9))[r]
+                m.set_box(rk["lo"], rk["hi"], (0, 0, 0))
+                m.set_nlocal(rk["owned"].size)
+                if m.needs_types:
+                    m.set_types(types[rk["ids"]])
+                f = np.zeros_like(rk["x"])
+                m.post_force(step, rk["x"], f)
+                res[r][s] = (m.cv, m.compute_scalar(), f, rk)
+        except BaseException as e:   # the other rank's barrier gives up instead of waiting
+            errs.append(e)
+            red.abort()
+
+    ts = [threading.Thread(target=run, args=(r,)) for r in range(nr)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if errs:
+        raise errs[0]
+    grids = [m.grid(_grid_size(args)) for m in ctx]
+    for m in ctx:
+        m.close()
+    return res, grids, cut
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", list(CASES))
+def test_two_ranks_equal_one_domain(case, precision, tmp_path):
+    args = CASES[case]()
+    x, L = _fcc()
+    n = x.shape[0]
+    types = (np.arange(n) * 7 % 4).astype(np.int32)
+    steps = [(s, np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.03, 90, s), L))) for s in range(3)]
+    (tmp_path / "one").mkdir()
+    (tmp_path / "two").mkdir()
+    single, grid1 = _run_single(args, x, L, steps, precision, types, tmp_path / "one")
+    ranks, grids, cut = _run_ranks(args, x, L, steps, precision, types, tmp_path / "two")
+    assert cut == pytest.approx({"steinh_l_step": 7.8, "steinh_l_fermi": 7.8, "steinh_q": 4.5,
+                                 "stru_factor_chem": 6.0, "sk": 0.0}[case])
+    tcv, tf = (1e-10, 1e-8) if precision == "fp64" else (2e-5, 3e-3)
+    for s in range(len(steps)):
+        cv1, b1, f1 = single[s]
+        for r in range(2):
+            cv, b, _, _ = ranks[r][s]
+            assert np.array_equal(cv, ranks[0][s][0]) and b == ranks[0][s][1]
+            assert H.rel(cv, cv1) < tcv
+            assert H.rel(b, b1) < max(tcv, 1e-9)
+        f = domain.reverse_sum(n, [ranks[r][s][3] for r in range(2)], [ranks[r][s][2] for r in range(2)])
+        assert H.rel(f, f1) < tf
+    assert np.array_equal(grids[0], grids[1])
+    assert H.rel(grids[0], grid1) < max(tcv, 1e-9)
+    rows = [l for l in (tmp_path / "two" / "HILLS").read_text().splitlines() if not l.startswith("#")]
+    assert len(rows) == len(steps)   # rank 0 alone writes HILLS
+
+
+def test_domain_api_errors():
+    m = mtd.Metad(H.fix_args_local())
+    with pytest.raises(mtd.MetadError, match="domain decomposition is not enabled"):
+        m.set_nlocal(10)
+    red = domain.LocalAllreduce(1)
+    m.set_domain(5, 0, red.for_rank(0))
+    x, L = _fcc(nc=3)
+    m.set_box([0, 0, 0], L, (0, 0, 0))
+    m.set_nlocal(x.shape[0] + 1)
+    with pytest.raises(mtd.MetadError, match="exceeds"):
+        m.post_force(0, x, np.zeros_like(x))
+    m.close()
+    m = mtd.Metad(H.fix_args_local())
+    m.set_box([0, 0, 0], L)
+    m.post_force(0, x, np.zeros_like(x))
+    with pytest.raises(mtd.MetadError, match="before the first step"):
+        m.set_domain(5, 0, red.for_rank(0))
+    m.close()

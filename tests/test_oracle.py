@@ -149,6 +149,18 @@ def test_chemical_debye_gradient_fd_and_unit_weights():
     assert np.max(np.abs(g - o["grad"][IDX])) < 1e-7 * max(1.0, np.abs(g).max())
 
 
+@pytest.mark.parametrize("mode", ["AVE", "COUNT"])
+def test_weight_chem_gradient_fd(mode):
+    """WEIGHT_CHEM: P_i = 1 + sum_j w_i w_j s(r_ij) with the taper s alone as
+    pair term (q_factor 0 in the shared Debye restatement)."""
+    types = (np.arange(X0.shape[0]) % 2) + 1
+    w = O.chem_type_weights(types, cmap={1: 0.1, 2: 3.0})
+    sw = O.make_sw("FERMI", r0=12.0, alpha=2.0)
+    o = O.debye(X0, L0, 3.0, 0.0, mode=mode, sw=sw, weights=w)
+    g = _fd(lambda x: O.debye(x, L0, 3.0, 0.0, mode=mode, sw=sw, weights=w, grad=False)["cv"], X0, IDX)
+    assert np.max(np.abs(g - o["grad"][IDX])) < 1e-7 * max(1.0, np.abs(g).max())
+
+
 def test_sk_gradient_fd_and_bragg_peak():
     k = systems.kvectors(8, systems.KMAG_111, 5)
     o = O.sk(X0, k)
