@@ -433,6 +433,7 @@ struct BiasShared {
 
 // One context, one step: all phases in one block.
 __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
     stage_plan(Pp, plan_raw);
@@ -457,6 +458,7 @@ __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ 
 
 __global__ void __launch_bounds__(256) k_symbol_coef(const BiasPlan *__restrict__ Pp, int sym,
                                                      const WalkState *ws) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ double usum[kMaxUnits][8], alpha[kMaxSymbols];
     stage_plan(Pp, plan_raw);
@@ -469,6 +471,7 @@ __global__ void __launch_bounds__(256) k_symbol_coef(const BiasPlan *__restrict_
 
 // ------------------------------------------------------------------ hill-list bias
 __global__ void __launch_bounds__(256) k_list_cvs(const BiasPlan *__restrict__ Pp, WalkState *ws) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
     stage_plan(Pp, plan_raw);
@@ -487,6 +490,7 @@ __global__ void __launch_bounds__(256) k_list_cvs(const BiasPlan *__restrict__ P
 
 __global__ void __launch_bounds__(256) k_list_finish(const BiasPlan *__restrict__ Pp, long long step,
                                                      const WalkState *ws, const double *__restrict__ vdv) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
     stage_plan(Pp, plan_raw);
@@ -522,6 +526,7 @@ __global__ void __launch_bounds__(256) k_list_finish(const BiasPlan *__restrict_
 // memory so the three launches can sit in a CUDA graph.
 __global__ void __launch_bounds__(256) k_walk_cvs(const BiasPlan *const *__restrict__ plans,
                                                   const long long *__restrict__ d_step, WalkState *ws) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
     stage_plan(plans[blockIdx.x], plan_raw);
@@ -563,6 +568,7 @@ __device__ bool group_failed(const BiasPlan *const *__restrict__ plans, int nwal
 
 __global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__restrict__ plans, int nwalk,
                                                       const long long *__restrict__ d_step, const WalkState *ws) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     stage_plan(plans[0], plan_raw);
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
@@ -579,6 +585,7 @@ __global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__r
 
 __global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__restrict__ plans, int nwalk,
                                                    const WalkState *ws) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
     stage_plan(plans[blockIdx.x], plan_raw);
@@ -604,6 +611,7 @@ __global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__rest
 // HILLS replay: every thread owns grid bins and adds the hills in file order,
 // so the FP64 sum order per bin is the file order.
 __global__ void k_hills_replay(const BiasPlan *__restrict__ Pp, const HillRec *__restrict__ h, int nh, int ncell) {
+    pdl_entry();
     const BiasPlan &P = *Pp;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ncell; g += gridDim.x * blockDim.x) {
         int idx[3] = {0, 0, 0}, rem = g;
@@ -624,6 +632,7 @@ __global__ void k_hills_replay(const BiasPlan *__restrict__ Pp, const HillRec *_
 }
 
 __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, double *out6) {
+    pdl_entry();
     __shared__ double smem[6 * 32];
     double v[6] = {0, 0, 0, 0, 0, 0};
     for (int b = threadIdx.x; b < nparts; b += blockDim.x)
@@ -636,6 +645,7 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 }  // namespace
 
 __global__ void __launch_bounds__(256) k_unit_sums(const BiasPlan *__restrict__ Pp, double *out) {
+    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ double smem[8 * 32];
     stage_plan(Pp, plan_raw);
@@ -660,35 +670,35 @@ int unit_sums_count(const BiasPlan &P) {
 }
 
 void launch_unit_sums(const BiasPlan *d_plan, double *out, cudaStream_t st) {
-    k_unit_sums<<<1, 256, 0, st>>>(d_plan, out);
+    launch_k(k_unit_sums, 1, 256, 0, st, d_plan, out);
     prof_mark("unit_sums", st);
 }
 
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st) {
-    k_bias_step<<<1, 256, 0, st>>>(d_plan, step);
+    launch_k(k_bias_step, 1, 256, 0, st, d_plan, step);
     prof_mark("bias_step", st);
 }
 
 void launch_symbol_coef(const BiasPlan *d_plan, int sym, const WalkState *ws, cudaStream_t st) {
-    k_symbol_coef<<<1, 256, 0, st>>>(d_plan, sym, ws);
+    launch_k(k_symbol_coef, 1, 256, 0, st, d_plan, sym, ws);
 }
 
 void launch_list_cvs(const BiasPlan *d_plan, WalkState *ws, cudaStream_t st) {
-    k_list_cvs<<<1, 256, 0, st>>>(d_plan, ws);
+    launch_k(k_list_cvs, 1, 256, 0, st, d_plan, ws);
     prof_mark("bias_cvs", st);
 }
 
 void launch_list_finish(const BiasPlan *d_plan, long long step, const WalkState *ws, const double *vdv,
                         cudaStream_t st) {
-    k_list_finish<<<1, 256, 0, st>>>(d_plan, step, ws, vdv);
+    launch_k(k_list_finish, 1, 256, 0, st, d_plan, step, ws, vdv);
     prof_mark("bias_finish", st);
 }
 
 void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
                       cudaStream_t st) {
-    k_walk_cvs<<<nwalk, 256, 0, st>>>(d_plans, d_step, ws);
-    k_walk_deposit<<<1, 256, 0, st>>>(d_plans, nwalk, d_step, ws);
-    k_walk_coef<<<nwalk, 256, 0, st>>>(d_plans, nwalk, ws);
+    launch_k(k_walk_cvs, nwalk, 256, 0, st, d_plans, d_step, ws);
+    launch_k(k_walk_deposit, 1, 256, 0, st, d_plans, nwalk, d_step, ws);
+    launch_k(k_walk_coef, nwalk, 256, 0, st, d_plans, nwalk, ws);
     prof_mark("walk_bias", st);
 }
 
@@ -696,11 +706,11 @@ void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int n
     if (nh <= 0 || ncell <= 0) return;
     int blocks = (ncell + 255) / 256;
     if (blocks > 4096) blocks = 4096;
-    k_hills_replay<<<blocks, 256, 0, st>>>(d_plan, h, nh, ncell);
+    launch_k(k_hills_replay, blocks, 256, 0, st, d_plan, h, nh, ncell);
 }
 
 void launch_virial_finalize(const double *vpart, int nparts, double *out6, cudaStream_t st) {
-    k_virial_finalize<<<1, 256, 0, st>>>(vpart, nparts, out6);
+    launch_k(k_virial_finalize, 1, 256, 0, st, vpart, nparts, out6);
     prof_mark("virial", st);
 }
 

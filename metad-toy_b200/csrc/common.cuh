@@ -121,11 +121,12 @@ struct DevStatus {
     unsigned int pad;
 };
 
-// A centre of the CV sums: in the CAL's group and owned by this context
-// (caller index below nown; under domain decomposition the atoms from nown
-// on are ghosts, which only serve as neighbours).
-__device__ __forceinline__ bool is_centre(const int *smask, const int *perm, int k, int groupbit, int nown) {
-    return (smask[k] & groupbit) && perm[k] < nown;
+// First statement of every step kernel: wait until the previous kernel of the
+// stream has completed and its writes are visible, then let the next kernel's
+// blocks be scheduled as this one's drain (no-ops without the PDL attribute).
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // Deterministic block sum of up to NV doubles per thread (fixed shuffle tree,

@@ -204,9 +204,12 @@ struct mtd_ctx {
 
 namespace {
 thread_local Prof *g_prof = nullptr;
+thread_local bool g_pdl = false;
 }
 
 namespace mtd {
+void pdl_set(bool on) { g_pdl = on; }
+bool pdl_on() { return g_pdl; }
 void prof_set(Prof *p) { g_prof = p; }
 void prof_mark(const char *name, cudaStream_t st) {
     Prof *p = g_prof;
@@ -669,6 +672,7 @@ SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
     s.smask = c->smask;
     s.xs = c->xs;
     s.pf = c->pf;
+    s.nown = owned(c);
     return s;
 }
 
@@ -677,7 +681,6 @@ template <typename T> LocalDev<T> local_dev(mtd_ctx *c, Unit &u, const CellGrid 
     d.n = c->n; d.npad = c->cap_n; d.SQ = record_stride(c, u); d.LA = u.LA; d.LB = u.LB;
     d.groupbit = u.groupbit; d.sw_r = u.sw_r; d.sw_cvA = u.sw_cvA; d.sw_cvB = u.sw_cvB;
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
-    d.nown = owned(c);
     d.q = (T *)u.q; d.nf = (T *)u.nf; d.lq = (T *)u.lq; d.lqs = (T *)u.lqs; d.e12 = (T *)u.e12;
     d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
     d.qblock = c->tune_q;
@@ -692,7 +695,6 @@ template <typename T> GlobalDev<T> global_dev(mtd_ctx *c, Unit &u, const CellGri
     for (int t = 0; t < d.nsw; ++t) d.sw[t] = u.qsw[t];
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.exact = geo_d(g, c->xs);
     d.nb = env_dev(c->envs[u.env]);
-    d.nown = owned(c);
     d.q = (T *)u.q; d.Q = (T *)u.Q; d.partials = u.partials; d.coef = u.coef;
     return d;
 }
@@ -702,7 +704,6 @@ template <typename T> DebyeDev<T> debye_dev(mtd_ctx *c, Unit &u, const CellGrid 
     d.n = c->n; d.npad = c->cap_n; d.groupbit = u.groupbit; d.rc2 = u.rc * u.rc; d.qf = u.qf; d.sw = u.sf_sw;
     d.smask = c->smask; d.perm = c->perm; d.geo = make_geo<T>(g, c->pf, c->xs); d.nb = env_dev(c->envs[u.env]);
     d.S = (T *)u.S; d.partials = u.partials; d.coef = u.coef;
-    d.nown = owned(c);
     d.w = u.chem ? (T *)u.w : nullptr;
     d.types = c->d_types;
     d.wtab = u.d_wtab;
@@ -792,6 +793,12 @@ void prof_collect(mtd_ctx *c) {
     }
     p.n = 0;
 }
+
+// The step's kernels use programmatic dependent launch (kernels.h).
+struct PdlScope {
+    PdlScope() { pdl_set(true); }
+    ~PdlScope() { pdl_set(false); }
+};
 
 struct ProfScope {
     explicit ProfScope(mtd_ctx *c) {
@@ -915,6 +922,7 @@ mtd_status exchange_totals(mtd_ctx *c) {
 mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, const int *mask, const int *image,
                         const double *fin, double *fout, bool virial, cudaEvent_t f_ready = nullptr) {
     ProfScope prof_scope(c);
+    PdlScope pdl_scope;
     c->launches = 0;
     mtd_status s = enqueue_values(c, n, x, mask, image);
     if (s != MTD_OK) return s;

@@ -30,6 +30,7 @@ template <int L> struct QSize {
 };
 
 template <int L, typename T> __global__ void __launch_bounds__(kBlock) k_global_values(GlobalDev<T> d) {
+    pdl_entry();
     using Z = QSize<L>;
     __shared__ double smem[4 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -60,7 +61,7 @@ template <int L, typename T> __global__ void __launch_bounds__(kBlock) k_global_
 #pragma unroll
         for (int t = 0; t < Z::SQ; ++t) d.q[(size_t)k * Z::SQ + t] = acc[t];
         d.Q[k] = Q;
-        if (is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) {
+        if (d.smask[k] & d.groupbit) {
             part[0] = (double)Q;
             if (d.nsw > 0) part[1] = sw_f<double>(d.sw[0], (double)Q);
             if (d.nsw > 1) part[2] = sw_f<double>(d.sw[1], (double)Q);
@@ -74,7 +75,7 @@ template <int L, typename T> __global__ void __launch_bounds__(kBlock) k_global_
 
 template <int L, typename T>
 __device__ __forceinline__ T lambda_scale(const GlobalDev<T> &d, int k, const double *c) {
-    if (!is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) return T(0);
+    if (!(d.smask[k] & d.groupbit)) return T(0);
     const int n = d.nb.nkept[k];
     const double Q = (double)d.Q[k];
     if (n <= 0 || !(Q > 0.0)) return T(0);
@@ -88,6 +89,7 @@ template <int L, typename T>
 __global__ void __launch_bounds__(kBlock) k_global_force(GlobalDev<T> d, const double *__restrict__ f_src,
                                                          double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                          double *vpart, DevStatus *status) {
+    pdl_entry();
     using Z = QSize<L>;
     __shared__ double smem[6 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -165,9 +167,9 @@ template <typename T> void launch_global_values(const GlobalDev<T> &d, cudaStrea
     if (d.n == 0) return;
     const int nb = (d.n + kBlock - 1) / kBlock;
     switch (d.L) {
-    case 3: k_global_values<3, T><<<nb, kBlock, 0, st>>>(d); break;
-    case 4: k_global_values<4, T><<<nb, kBlock, 0, st>>>(d); break;
-    case 6: k_global_values<6, T><<<nb, kBlock, 0, st>>>(d); break;
+    case 3: launch_k(k_global_values<3, T>, nb, kBlock, 0, st, d); break;
+    case 4: launch_k(k_global_values<4, T>, nb, kBlock, 0, st, d); break;
+    case 6: launch_k(k_global_values<6, T>, nb, kBlock, 0, st, d); break;
     }
     prof_mark("global_values", st);
 }
@@ -178,9 +180,9 @@ void launch_global_forces(const GlobalDev<T> &d, const double *f_src, double *f_
     if (d.n == 0) return;
     const int nb = (d.n + kBlock - 1) / kBlock;
     switch (d.L) {
-    case 3: k_global_force<3, T><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status); break;
-    case 4: k_global_force<4, T><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status); break;
-    case 6: k_global_force<6, T><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status); break;
+    case 3: launch_k(k_global_force<3, T>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status); break;
+    case 4: launch_k(k_global_force<4, T>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status); break;
+    case 6: launch_k(k_global_force<6, T>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status); break;
     }
     prof_mark("global_force", st);
 }

@@ -71,6 +71,8 @@ struct SysDev {
     const int *image;     // caller order, may be null
     int *cellof, *slot, *count, *start, *perm, *smask;
     int *arrival;         // [n] atoms by cell in atomic arrival order (cell-list scratch)
+    int nown;             // caller indices >= nown are ghosts (domain decomposition): their
+                          // sorted group mask is 0, so they are neighbours and never centres
     double *xs;           // sorted raw coordinates AoS npad*3
     float4 *pf;           // sorted cell-relative coordinates + packed cell
 };
@@ -118,6 +120,35 @@ struct Prof {
 void prof_set(Prof *p);                          // active profiler of this host thread (null: off)
 void prof_mark(const char *name, cudaStream_t st);
 
+// ------------------------------------------------------------------ programmatic dependent launch
+// Inside a context's step the kernels are launched with the programmatic-
+// stream-serialisation attribute: a kernel's blocks may be scheduled while
+// the previous kernel's last wave drains, and each kernel waits (pdl_entry)
+// for the previous one to complete before reading anything.  Outside a step
+// (walkers' graph capture, autotuning) kernels launch plainly and the wait is
+// a no-op.
+void pdl_set(bool on);                           // this host thread's launches use the attribute
+bool pdl_on();
+template <typename... KArgs, typename... Args>
+void launch_k(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+              Args &&...args) {
+    if (!pdl_on()) {
+        kernel<<<grid, block, smem, st>>>(static_cast<KArgs>(args)...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // ------------------------------------------------------------------ neighbours
 // Returns the number of kernels launched.
 int launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st);
@@ -132,7 +163,6 @@ template <typename T> struct LocalDev {
     SwParams sw_r, sw_cvA, sw_cvB;
     const int *smask;
     const int *perm;
-    int nown;                   // caller indices >= nown are ghosts: neighbours, never centres
     Geo<T> geo;
     NeighDev nb;
     T *q, *nf, *lq, *lqs, *e12, *lam, *g, *tu;
@@ -153,7 +183,6 @@ template <typename T> struct GlobalDev {
     int groupbit, nsw;
     SwParams sw[2];             // SW_FUNC symbols of this CAL
     const int *smask, *perm;
-    int nown;                   // caller indices >= nown are ghosts
     Geo<T> geo;
     GeoD exact;                 // FP64 raw coordinates for the cap-membership test
     NeighDev nb;
@@ -173,7 +202,6 @@ template <typename T> struct DebyeDev {
     double rc2, qf;
     SwParams sw;
     const int *smask, *perm;
-    int nown;                   // caller indices >= nown are ghosts
     Geo<T> geo;
     NeighDev nb;
     T *S;

@@ -132,6 +132,7 @@ __device__ __forceinline__ int nb_index(const NeighDev &nb, int npad, int t, int
 // Pass 1: q_lm and NF for every atom.
 template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
+    pdl_entry();
     using S = LSet<LA, LB, T>;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
@@ -159,13 +160,14 @@ __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
 // Pass 2: LQ_lm, LQ, the e1/e2 weights of the adjoint and block partial sums.
 template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock, 4) k_local_lq(LocalDev<T> d) {
+    pdl_entry();
     using S = LSet<LA, LB, T>;
     __shared__ double smem[5 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = k < d.n;
     double part[5] = {0, 0, 0, 0, 0};
     if (valid) {
-        const bool ing = is_centre(d.smask, d.perm, k, d.groupbit, d.nown);
+        const bool ing = (d.smask[k] & d.groupbit) != 0;
         const T nfk = d.nf[k];
         T A[S::SQ];
         T lqA = T(0), lqB = T(0);
@@ -244,6 +246,7 @@ __device__ __forceinline__ void add_g(T *acc, const T *lq, T w, T s) {
 // Pass 3 (after the bias kernel): lam_k / NF_k, and for smooth switches G_k, t_k, u_k.
 template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
+    pdl_entry();
     using S = LSet<LA, LB, T>;
     constexpr bool DSIG = !STEP;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -313,6 +316,7 @@ template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock, 4) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
                                                         double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                         double *vpart, DevStatus *status) {
+    pdl_entry();
     using S = LSet<LA, LB, T>;
     constexpr bool DSIG = !STEP;
     __shared__ double smem[6 * 32];
@@ -404,14 +408,14 @@ template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cuda
     const int nb = (d.n + kBlock - 1) / kBlock;
     const int qb = d.qblock > 0 ? d.qblock : kBlock, qg = (d.n + qb - 1) / qb;   // no block reduction in q
     if (d.sw_r.type == SW_STEP) {
-        k_local_q<LA, LB, T, true><<<qg, qb, 0, st>>>(d);
+        launch_k(k_local_q<LA, LB, T, true>, qg, qb, 0, st, d);
         prof_mark("local_q", st);
-        k_local_lq<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d);
+        launch_k(k_local_lq<LA, LB, T, true>, nb, kBlock, 0, st, d);
         prof_mark("local_lq", st);
     } else {
-        k_local_q<LA, LB, T, false><<<qg, qb, 0, st>>>(d);
+        launch_k(k_local_q<LA, LB, T, false>, qg, qb, 0, st, d);
         prof_mark("local_q", st);
-        k_local_lq<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d);
+        launch_k(k_local_lq<LA, LB, T, false>, nb, kBlock, 0, st, d);
         prof_mark("local_lq", st);
     }
 }
@@ -422,14 +426,14 @@ void run_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const 
     const int nb = (d.n + kBlock - 1) / kBlock;
     const int lb = d.lblock > 0 ? d.lblock : kBlock, lg = (d.n + lb - 1) / lb;   // no block reduction in lambda
     if (d.sw_r.type == SW_STEP) {
-        k_local_lambda<LA, LB, T, true><<<lg, lb, 0, st>>>(d);
+        launch_k(k_local_lambda<LA, LB, T, true>, lg, lb, 0, st, d);
         prof_mark("local_lambda", st);
-        k_local_force<LA, LB, T, true><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+        launch_k(k_local_force<LA, LB, T, true>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
         prof_mark("local_force", st);
     } else {
-        k_local_lambda<LA, LB, T, false><<<lg, lb, 0, st>>>(d);
+        launch_k(k_local_lambda<LA, LB, T, false>, lg, lb, 0, st, d);
         prof_mark("local_lambda", st);
-        k_local_force<LA, LB, T, false><<<nb, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+        launch_k(k_local_force<LA, LB, T, false>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
         prof_mark("local_force", st);
     }
 }

@@ -35,6 +35,7 @@ __device__ __forceinline__ int cell_coord(double v, const CellGrid &g, int c, do
 }
 
 __global__ void k_bin(CellGrid g, SysDev s) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
     double w;
@@ -79,6 +80,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int &total) {
 // block totals, add-back.  The totals live in start[ncell + 1 ...].
 __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int *__restrict__ count, int *__restrict__ start,
                                                             int *__restrict__ bsum, int ncell) {
+    pdl_entry();
     const int i = blockIdx.x * kScanBlock + threadIdx.x;
     int total;
     const int e = block_excl_scan(i < ncell ? count[i] : 0, total);
@@ -88,6 +90,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int *__restric
 
 __global__ void __launch_bounds__(kScanBlock) k_scan_top(int *__restrict__ bsum, int nb, int *__restrict__ start,
                                                          int ncell) {
+    pdl_entry();
     int carry = 0;
     for (int base = 0; base < nb; base += kScanBlock) {
         const int i = base + threadIdx.x;
@@ -101,6 +104,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_top(int *__restrict__ bsum,
 
 __global__ void __launch_bounds__(kScanBlock) k_scan_add(int *__restrict__ start, const int *__restrict__ bsum,
                                                          int ncell) {
+    pdl_entry();
     const int i = blockIdx.x * kScanBlock + threadIdx.x;
     if (i < ncell) start[i] += bsum[blockIdx.x];
 }
@@ -109,6 +113,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add(int *__restrict__ start
 // the totals of the blocks before it (the last block also writes the total).
 __global__ void __launch_bounds__(kScanBlock) k_scan_add_fused(int *__restrict__ start, const int *__restrict__ bsum,
                                                                int ncell, int nb) {
+    pdl_entry();
     __shared__ int red[32];
     const int b = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int v = threadIdx.x < b ? bsum[threadIdx.x] : 0;
@@ -125,6 +130,7 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add_fused(int *__restrict__
 }
 
 __global__ void k_scatter(SysDev s) {
+    pdl_entry();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
     s.arrival[s.start[s.cellof[i]] + s.slot[i]] = i;
@@ -134,6 +140,7 @@ __global__ void k_scatter(SysDev s) {
 // its rank by caller index among its cell's members (removes the atomic
 // arrival order), and its sorted per-atom arrays are written there.
 __global__ void k_place(CellGrid g, SysDev s) {
+    pdl_entry();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
     const int i = s.arrival[k];
@@ -158,7 +165,7 @@ __global__ void k_place(CellGrid g, SysDev s) {
     p.z = (float)(w2 - cz * g.h[2]);
     p.w = __int_as_float(pack_cell(cx, cy, cz));
     s.pf[d] = p;
-    s.smask[d] = s.mask ? s.mask[i] : -1;
+    s.smask[d] = i < s.nown ? (s.mask ? s.mask[i] : -1) : 0;
 }
 
 // FP64 decision on raw coordinates (the oracle's criterion, operation by operation).
@@ -174,6 +181,7 @@ __device__ __noinline__ bool exact_decide(const GeoD &gd, const NeighSpec &ns, c
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
                                                       DevStatus *status) {
+    pdl_entry();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
     const GeoF gf = geo_f(g, s.pf);
@@ -248,6 +256,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, Neig
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
                                                            DevStatus *status) {
+    pdl_entry();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
     const GeoD gd = geo_d(g, s.xs);
@@ -319,6 +328,7 @@ constexpr int kFlatBlock = 128;
 template <int KIND>
 __global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
                                                                DevStatus *status) {
+    pdl_entry();
     // [cell][thread]: a lane's entry sits in the same bank whatever cell it reads
     __shared__ int2 rng[27][kFlatBlock];
     const int tid = threadIdx.x;
@@ -414,6 +424,7 @@ constexpr int kMaxCapList = 64;
 // STEINH Q cap: keep the `cap` nearest by (r2, caller index), the order of the
 // reference's strict-'>' insertion with ties resolved canonically.
 __global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd) {
+    pdl_entry();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
     const GeoD gd = geo_d(g, s.xs);
@@ -450,24 +461,24 @@ __global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, Nei
 int launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
     cudaMemsetAsync(s.count, 0, sizeof(int) * (size_t)g.ncell, st);
     const int nb = (s.n + kBlock - 1) / kBlock;
-    if (s.n > 0) k_bin<<<nb, kBlock, 0, st>>>(g, s);
+    if (s.n > 0) launch_k(k_bin, nb, kBlock, 0, st, g, s);
     prof_mark("cell_bin", st);
     {
         const int sb = (g.ncell + kScanBlock - 1) / kScanBlock;
         int *bsum = s.start + g.ncell + 1;   // scratch after the ncell + 1 starts
-        k_scan_blocks<<<sb, kScanBlock, 0, st>>>(s.count, s.start, bsum, g.ncell);
+        launch_k(k_scan_blocks, sb, kScanBlock, 0, st, s.count, s.start, bsum, g.ncell);
         if (sb <= kScanBlock) {
-            k_scan_add_fused<<<sb, kScanBlock, 0, st>>>(s.start, bsum, g.ncell, sb);
+            launch_k(k_scan_add_fused, sb, kScanBlock, 0, st, s.start, bsum, g.ncell, sb);
         } else {
-            k_scan_top<<<1, kScanBlock, 0, st>>>(bsum, sb, s.start, g.ncell);
-            k_scan_add<<<sb, kScanBlock, 0, st>>>(s.start, bsum, g.ncell);
+            launch_k(k_scan_top, 1, kScanBlock, 0, st, bsum, sb, s.start, g.ncell);
+            launch_k(k_scan_add, sb, kScanBlock, 0, st, s.start, bsum, g.ncell);
         }
     }
     prof_mark("cell_scan", st);
     if (s.n > 0) {
-        k_scatter<<<nb, kBlock, 0, st>>>(s);
+        launch_k(k_scatter, nb, kBlock, 0, st, s);
         prof_mark("cell_scatter", st);
-        k_place<<<nb, kBlock, 0, st>>>(g, s);
+        launch_k(k_place, nb, kBlock, 0, st, g, s);
         prof_mark("cell_sort", st);
     }
     const int sb = (g.ncell + kScanBlock - 1) / kScanBlock;
@@ -485,21 +496,21 @@ void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, N
     // 128-thread blocks of k_neighbors_fast, or k_neighbors_flat (autotuned)
     if (fast && ns.variant == 2 && s.n < (1 << 26)) {
         const int fb = (s.n + kFlatBlock - 1) / kFlatBlock;
-        if (ns.kind == NK_RANGE) k_neighbors_flat<NK_RANGE><<<fb, kFlatBlock, 0, st>>>(g, s, ns, nd, status);
-        else if (ns.kind == NK_STEP) k_neighbors_flat<NK_STEP><<<fb, kFlatBlock, 0, st>>>(g, s, ns, nd, status);
-        else k_neighbors_flat<NK_SWITCH><<<fb, kFlatBlock, 0, st>>>(g, s, ns, nd, status);
+        if (ns.kind == NK_RANGE) launch_k(k_neighbors_flat<NK_RANGE>, fb, kFlatBlock, 0, st, g, s, ns, nd, status);
+        else if (ns.kind == NK_STEP) launch_k(k_neighbors_flat<NK_STEP>, fb, kFlatBlock, 0, st, g, s, ns, nd, status);
+        else launch_k(k_neighbors_flat<NK_SWITCH>, fb, kFlatBlock, 0, st, g, s, ns, nd, status);
     } else if (fast) {
         const int tb = ns.variant == 1 ? 128 : kBlock;
         const int gb = (s.n + tb - 1) / tb;
-        if (ns.kind == NK_RANGE) k_neighbors_fast<NK_RANGE><<<gb, tb, 0, st>>>(g, s, ns, nd, status);
-        else if (ns.kind == NK_STEP) k_neighbors_fast<NK_STEP><<<gb, tb, 0, st>>>(g, s, ns, nd, status);
-        else k_neighbors_fast<NK_SWITCH><<<gb, tb, 0, st>>>(g, s, ns, nd, status);
-    } else if (ns.kind == NK_RANGE) k_neighbors<NK_RANGE><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
-    else if (ns.kind == NK_STEP) k_neighbors<NK_STEP><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
-    else k_neighbors<NK_SWITCH><<<nb, kBlock, 0, st>>>(g, s, ns, nd, status);
+        if (ns.kind == NK_RANGE) launch_k(k_neighbors_fast<NK_RANGE>, gb, tb, 0, st, g, s, ns, nd, status);
+        else if (ns.kind == NK_STEP) launch_k(k_neighbors_fast<NK_STEP>, gb, tb, 0, st, g, s, ns, nd, status);
+        else launch_k(k_neighbors_fast<NK_SWITCH>, gb, tb, 0, st, g, s, ns, nd, status);
+    } else if (ns.kind == NK_RANGE) launch_k(k_neighbors<NK_RANGE>, nb, kBlock, 0, st, g, s, ns, nd, status);
+    else if (ns.kind == NK_STEP) launch_k(k_neighbors<NK_STEP>, nb, kBlock, 0, st, g, s, ns, nd, status);
+    else launch_k(k_neighbors<NK_SWITCH>, nb, kBlock, 0, st, g, s, ns, nd, status);
     prof_mark("neighbors", st);
     if (ns.cap > 0) {
-        k_select_cap<<<nb, kBlock, 0, st>>>(g, s, ns, nd);
+        launch_k(k_select_cap, nb, kBlock, 0, st, g, s, ns, nd);
         prof_mark("select_cap", st);
     }
 }

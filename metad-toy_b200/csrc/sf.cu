@@ -43,6 +43,7 @@ template <typename T> __device__ __forceinline__ void debye_g(T r2, T rc2, T qf,
 // STRU_FACTOR Chemical: the type weight of every sorted atom (types outside
 // the table weigh 0, as type 0 does).
 template <typename T> __global__ void k_chem_weights(DebyeDev<T> d) {
+    pdl_entry();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
     const int t = d.types[d.perm[k]];
@@ -50,12 +51,13 @@ template <typename T> __global__ void k_chem_weights(DebyeDev<T> d) {
 }
 
 template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(DebyeDev<T> d) {
+    pdl_entry();
     __shared__ double smem[4 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double part[4] = {0, 0, 0, 0};
     if (k < d.n) {
         T S = T(0);
-        if (is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) {
+        if (d.smask[k] & d.groupbit) {
             const int c = min(d.nb.count[k], d.nb.M);
             const T rc2 = (T)d.rc2, qf = (T)d.qf;
             const auto a = d.geo.load(k);
@@ -82,7 +84,7 @@ template <typename T> __global__ void __launch_bounds__(kBlock) k_debye_values(D
 
 template <typename T>
 __device__ __forceinline__ T debye_a(const DebyeDev<T> &d, int k, double c0, double c1) {
-    if (!is_centre(d.smask, d.perm, k, d.groupbit, d.nown)) return T(0);
+    if (!(d.smask[k] & d.groupbit)) return T(0);
     double a = c0;
     if (c1 != 0.0) a += c1 * sw_df<double>(d.sw, (double)d.S[k]);
     return (T)a;
@@ -92,6 +94,7 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const double *__restrict__ f_src,
                                                         double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                         double *vpart, DevStatus *status) {
+    pdl_entry();
     __shared__ double smem[6 * 32];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double vir[6] = {0, 0, 0, 0, 0, 0};
@@ -152,6 +155,7 @@ constexpr int kSkBlocks = 148 * 4;  // grid for the partial sums (4 blocks per S
 // k-vectors (and, in the force pass, rho) staged in dynamic shared memory
 // sized to K, so a small K leaves room for more resident blocks.
 template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
+    pdl_entry();
     __shared__ double smem[kSkChunk * 32];
     extern __shared__ double kk[];   // 3K
     for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
@@ -210,6 +214,7 @@ template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d
 
 // One block per output value (2K rho components + the group count).
 __global__ void __launch_bounds__(256) k_sk_reduce(SkDev d) {
+    pdl_entry();
     __shared__ double smem[32];
     const int v = blockIdx.x;
     double acc[1] = {0.0};
@@ -224,6 +229,7 @@ __global__ void __launch_bounds__(256) k_sk_reduce(SkDev d) {
 template <bool FP64>
 __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restrict__ f_src, double *__restrict__ f_dst,
                                                   SysDev s, CellGrid g, double *vpart) {
+    pdl_entry();
     __shared__ double smem[6 * 32];
     extern __shared__ double kk[];   // 3K doubles, then 2K doubles (FP64) or 5K floats (FP32)
     // FP64: rho as doubles; FP32: rho and k as floats (the per-atom gradient
@@ -301,15 +307,15 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
 
 template <typename T> void launch_debye_values(const DebyeDev<T> &d, cudaStream_t st) {
     if (d.n == 0) return;
-    if (d.w) k_chem_weights<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d);
-    k_debye_values<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d);
+    if (d.w) launch_k(k_chem_weights<T>, (d.n + kBlock - 1) / kBlock, kBlock, 0, st, d);
+    launch_k(k_debye_values<T>, (d.n + kBlock - 1) / kBlock, kBlock, 0, st, d);
     prof_mark("debye_values", st);
 }
 template <typename T>
 void launch_debye_forces(const DebyeDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                          double *vpart, DevStatus *status, cudaStream_t st) {
     if (d.n == 0) return;
-    k_debye_force<T><<<(d.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(d, f_src, f_dst, s, g, vpart, status);
+    launch_k(k_debye_force<T>, (d.n + kBlock - 1) / kBlock, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
     prof_mark("debye_force", st);
 }
 template void launch_debye_values<float>(const DebyeDev<float> &, cudaStream_t);
@@ -326,10 +332,10 @@ int sk_blocks(int n) {
 
 void launch_sk_values(const SkDev &d, cudaStream_t st) {
     const size_t sm = sizeof(double) * 3 * (size_t)d.K;
-    if (d.fp64) k_sk_partial<true><<<d.nblocks, 256, sm, st>>>(d);
-    else k_sk_partial<false><<<d.nblocks, 256, sm, st>>>(d);
+    if (d.fp64) launch_k(k_sk_partial<true>, d.nblocks, 256, sm, st, d);
+    else launch_k(k_sk_partial<false>, d.nblocks, 256, sm, st, d);
     prof_mark("sk_partial", st);
-    k_sk_reduce<<<2 * d.K + 1, 256, 0, st>>>(d);
+    launch_k(k_sk_reduce, 2 * d.K + 1, 256, 0, st, d);
     prof_mark("sk_reduce", st);
 }
 
@@ -338,8 +344,8 @@ void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const 
     if (d.n == 0) return;
     const int nb = (d.n + 255) / 256;
     const size_t sm = sizeof(double) * 3 * (size_t)d.K + (d.fp64 ? sizeof(double) * 2 : sizeof(float) * 5) * (size_t)d.K;
-    if (d.fp64) k_sk_force<true><<<nb, 256, sm, st>>>(d, f_src, f_dst, s, g, vpart);
-    else k_sk_force<false><<<nb, 256, sm, st>>>(d, f_src, f_dst, s, g, vpart);
+    if (d.fp64) launch_k(k_sk_force<true>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
+    else launch_k(k_sk_force<false>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
     prof_mark("sk_force", st);
 }
 

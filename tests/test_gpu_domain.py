@@ -12,6 +12,7 @@ import pytest
 import domain
 import helpers as H
 import mtd
+import oracle as O
 import systems
 
 pytestmark = pytest.mark.gpu
@@ -135,7 +136,9 @@ def test_two_ranks_equal_one_domain(case, precision, tmp_path):
     (tmp_path / "two").mkdir()
     single, grid1 = _run_single(args, x, L, steps, precision, types, tmp_path / "one")
     ranks, grids, cut = _run_ranks(args, x, L, steps, precision, types, tmp_path / "two")
-    assert cut == pytest.approx({"steinh_l_step": 7.8, "steinh_l_fermi": 7.8, "steinh_q": 4.5,
+    # 2 x the STEINH L list radius: r_0 for STEP, sigma(r) = cutoff_eps for FERMI
+    rl = O.sw_invert_for_eps(O.make_sw("FERMI", r0=3.9, alpha=-8.0), 1e-6)
+    assert cut == pytest.approx({"steinh_l_step": 7.8, "steinh_l_fermi": 2 * rl, "steinh_q": 4.5,
                                  "stru_factor_chem": 6.0, "sk": 0.0}[case])
     tcv, tf = (1e-10, 1e-8) if precision == "fp64" else (2e-5, 3e-3)
     for s in range(len(steps)):
