@@ -118,6 +118,33 @@ mtd_status mtd_post_force_device(mtd_ctx *ctx, int64_t step, int n, const double
  * overflow, NaN forces, timeouts) raised by earlier asynchronous calls. */
 mtd_status mtd_sync(mtd_ctx *ctx);
 
+/* The same step in two calls, for callers that hand over positions before
+ * the force array (the interface shape of a `mtd_step` driver):
+ * mtd_set_positions_f64 copies x (AoS n*3), mask (NULL = every atom in every
+ * group) and, when a CAL needs them, type (NULL otherwise) to the device
+ * before it returns, so the arrays are borrowed for the call only; groupbit
+ * is the fix's own group bit, which the reference's post_force does not
+ * apply either (src/core/fix_crystallize.cu:386-472): it is checked to be
+ * non-zero and recorded.  mtd_step then runs the step on those positions and
+ * f_inout (AoS n*3, -= bias force), writes the CV_dim values to cv_out and
+ * the bias energy to bias_energy_out (either may be NULL) and the virial
+ * (may be NULL; x taken as unwrapped).  Results equal mtd_post_force on the
+ * same arrays bit for bit.  mtd_get_peratom is mtd_extract_peratom for the
+ * last step's n atoms. */
+mtd_status mtd_set_positions_f64(mtd_ctx *ctx, const double *x, const int *type, const int *mask, int n,
+                                 int groupbit);
+mtd_status mtd_step(mtd_ctx *ctx, int64_t step, double *f_inout, double *cv_out, double *bias_energy_out,
+                    double virial_out[6]);
+mtd_status mtd_get_peratom(mtd_ctx *ctx, const char *key, double *out);
+
+/* mtd_create with the deck and options in one struct. */
+typedef struct {
+    int narg;
+    const char *const *arg;           /* the tokens after "metad" */
+    mtd_options opt;
+} mtd_config;
+mtd_status mtd_create_from_config(const mtd_config *cfg, mtd_ctx **out);
+
 /* Thermo output.  Replaces FixMetadynamics::compute_scalar / compute_vector
  * (src/core/fix_crystallize.cu:484-494): bias energy V_b(s) and CV k (0-based). */
 double mtd_compute_scalar(const mtd_ctx *ctx);

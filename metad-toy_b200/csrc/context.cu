@@ -200,6 +200,10 @@ struct mtd_ctx {
     double *d_xchg = nullptr;            // this rank's unit totals, then the totals over all ranks
     double *h_xchg = nullptr;            // pinned staging of the same
     int xchg_n = 0;
+    // two-call step (mtd_set_positions_f64, then mtd_step)
+    int staged_n = -1;                   // atoms uploaded and not yet stepped (-1: none)
+    bool staged_mask = false;
+    int fix_groupbit = 1;
 };
 
 namespace {
@@ -1347,20 +1351,14 @@ mtd_status mtd_init(mtd_ctx *c) {
     return MTD_OK;
 }
 
-mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, const int *mask, const int *image,
-                          double *f, double virial[6]) {
-    if (!c || n < 0 || (n > 0 && (!x || !f))) return MTD_ERR_INVALID_ARG;
-    if (!c->initialized) {
-        mtd_status s = mtd_init(c);
-        if (s != MTD_OK) return s;
-    }
-    mtd_status s = ensure_capacity(c, n);
-    if (s != MTD_OK) return s;
+namespace {
+// The part of mtd_post_force after x (and mask) are on the device: f upload
+// beside the CV passes, the step with its overflow retries, f download.
+mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const int *image, double *f,
+                         double virial[6]) {
     const size_t b3 = sizeof(double) * 3 * (size_t)n;
-    // x (and mask) first on the step's stream; f (and image, read by the force
-    // kernels only) on the side stream, overlapping the CV passes
-    MTD_CU(cudaMemcpyAsync(c->d_x, x, b3, cudaMemcpyHostToDevice, c->st), "x upload");
-    if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
+    const int *mask = has_mask ? c->d_mask : nullptr;
+    mtd_status s = MTD_OK;
     MTD_CU(cudaEventRecord(c->f_ready, c->st), "force upload");   // the side copies start after the previous step
     MTD_CU(cudaStreamWaitEvent(c->side_st, c->f_ready, 0), "force upload");
     MTD_CU(cudaMemcpyAsync(c->d_fin, f, b3, cudaMemcpyHostToDevice, c->side_st), "f upload");
@@ -1368,7 +1366,7 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
     MTD_CU(cudaEventRecord(c->f_ready, c->side_st), "force upload");
     for (int attempt = 0; attempt < 4; ++attempt) {
         MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
-        s = enqueue_step(c, step, n, c->d_x, mask ? c->d_mask : nullptr, (image && virial) ? c->d_image : nullptr,
+        s = enqueue_step(c, step, n, c->d_x, mask, (image && virial) ? c->d_image : nullptr,
                          c->d_fin, c->d_fout, virial != nullptr, c->f_ready);
         if (s != MTD_OK) return s;
         // the forces go back in the same stream pass (a failed attempt's are overwritten by the retry)
@@ -1393,6 +1391,73 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
     if (virial)
         for (int t = 0; t < 6; ++t) virial[t] = c->virial[t];
     return MTD_OK;
+}
+}  // namespace
+
+mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, const int *mask, const int *image,
+                          double *f, double virial[6]) {
+    if (!c || n < 0 || (n > 0 && (!x || !f))) return MTD_ERR_INVALID_ARG;
+    if (!c->initialized) {
+        mtd_status s = mtd_init(c);
+        if (s != MTD_OK) return s;
+    }
+    mtd_status s = ensure_capacity(c, n);
+    if (s != MTD_OK) return s;
+    const size_t b3 = sizeof(double) * 3 * (size_t)n;
+    // x (and mask) first on the step's stream; f (and image, read by the force
+    // kernels only) on the side stream, overlapping the CV passes
+    MTD_CU(cudaMemcpyAsync(c->d_x, x, b3, cudaMemcpyHostToDevice, c->st), "x upload");
+    if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
+    return step_uploaded(c, step, n, mask != nullptr, image, f, virial);
+}
+
+mtd_status mtd_set_positions_f64(mtd_ctx *c, const double *x, const int *type, const int *mask, int n, int groupbit) {
+    if (!c || n < 0 || (n > 0 && !x)) return MTD_ERR_INVALID_ARG;
+    if (groupbit == 0) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_positions_f64: groupbit must be non-zero");
+    if (!c->initialized) {
+        mtd_status s = mtd_init(c);
+        if (s != MTD_OK) return s;
+    }
+    mtd_status s = ensure_capacity(c, n);
+    if (s != MTD_OK) return s;
+    if (type && mtd_needs_types(c)) {
+        s = mtd_set_types(c, n, type);
+        if (s != MTD_OK) return s;
+    }
+    MTD_CU(cudaMemcpyAsync(c->d_x, x, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, c->st), "x upload");
+    if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
+    MTD_CU(cudaStreamSynchronize(c->st), "x upload");   // the caller's arrays are borrowed for this call only
+    c->staged_n = n;
+    c->staged_mask = mask != nullptr;
+    c->fix_groupbit = groupbit;
+    return MTD_OK;
+}
+
+mtd_status mtd_step(mtd_ctx *c, int64_t step, double *f_inout, double *cv_out, double *bias_energy_out,
+                    double virial_out[6]) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    if (c->staged_n < 0) return fail(c, MTD_ERR_INVALID_ARG, "mtd_step: call mtd_set_positions_f64 first");
+    if (c->staged_n > 0 && !f_inout) return MTD_ERR_INVALID_ARG;
+    const int n = c->staged_n;
+    c->staged_n = -1;
+    mtd_status s = ensure_capacity(c, n);
+    if (s != MTD_OK) return s;
+    s = step_uploaded(c, step, n, c->staged_mask, nullptr, f_inout, virial_out);
+    if (s != MTD_OK) return s;
+    if (cv_out)
+        for (int d = 0; d < c->cfg.cv_dim; ++d) cv_out[d] = c->cv[d];
+    if (bias_energy_out) *bias_energy_out = c->bias;
+    return MTD_OK;
+}
+
+mtd_status mtd_get_peratom(mtd_ctx *c, const char *key, double *out) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    return mtd_extract_peratom(c, key, out, c->n);
+}
+
+mtd_status mtd_create_from_config(const mtd_config *cfg, mtd_ctx **out) {
+    if (!cfg || !out) return MTD_ERR_INVALID_ARG;
+    return mtd_create(cfg->narg, cfg->arg, &cfg->opt, out);
 }
 
 mtd_status mtd_post_force_device(mtd_ctx *c, int64_t step, int n, const double *d_x, const int *d_mask,

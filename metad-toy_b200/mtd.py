@@ -40,7 +40,8 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
            "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
            "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types",
-           "mtd_set_domain", "mtd_set_nlocal", "mtd_ghost_cutoff"]
+           "mtd_set_domain", "mtd_set_nlocal", "mtd_ghost_cutoff",
+           "mtd_set_positions_f64", "mtd_step", "mtd_get_peratom", "mtd_create_from_config"]
 
 
 class MetadError(RuntimeError):
@@ -53,6 +54,10 @@ class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("boltz", C.c_double), ("n_groups", C.c_int),
                 ("group_names", C.POINTER(C.c_char_p)), ("group_bits", C.POINTER(C.c_int)),
                 ("hills_path", C.c_char_p), ("work_dir", C.c_char_p)]
+
+
+class Config(C.Structure):
+    _fields_ = [("narg", C.c_int), ("arg", C.POINTER(C.c_char_p)), ("opt", Options)]
 
 
 _lib = None
@@ -98,6 +103,10 @@ def lib():
         L.mtd_set_nlocal.argtypes = [vp, C.c_int]
         L.mtd_ghost_cutoff.argtypes = [vp]
         L.mtd_ghost_cutoff.restype = C.c_double
+        L.mtd_set_positions_f64.argtypes = [vp, dp, ip, ip, C.c_int, C.c_int]
+        L.mtd_step.argtypes = [vp, C.c_int64, dp, dp, dp, dp]
+        L.mtd_get_peratom.argtypes = [vp, C.c_char_p, dp]
+        L.mtd_create_from_config.argtypes = [C.POINTER(Config), C.POINTER(vp)]
         L.mtd_autotune.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
         L.mtd_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.mtd_walkers_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.c_int,
@@ -318,6 +327,35 @@ class Metad:
     @property
     def needs_types(self):
         return bool(lib().mtd_needs_types(self._h))
+
+    def set_positions(self, x, types=None, mask=None, groupbit=1):
+        """First call of the two-call step: x (n x 3 float64) and optional
+        types / mask, copied to the device before returning."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        t = np.ascontiguousarray(types, dtype=np.int32) if types is not None else None
+        m = np.ascontiguousarray(mask, dtype=np.int32) if mask is not None else None
+        ip = C.POINTER(C.c_int)
+        self._check(lib().mtd_set_positions_f64(self._h, x.ctypes.data_as(C.POINTER(C.c_double)),
+                                                t.ctypes.data_as(ip) if t is not None else None,
+                                                m.ctypes.data_as(ip) if m is not None else None,
+                                                int(x.shape[0]), int(groupbit)))
+
+    def step(self, step, f, virial=False):
+        """Second call: f (n x 3 float64) -= bias force in place; returns
+        (cv, bias energy, virial or None)."""
+        assert f.dtype == np.float64 and f.flags.c_contiguous
+        cv = np.zeros(self.cv_dim)
+        b = np.zeros(1)
+        v = np.zeros(6) if virial else None
+        dp = C.POINTER(C.c_double)
+        self._check(lib().mtd_step(self._h, int(step), f.ctypes.data_as(dp), cv.ctypes.data_as(dp),
+                                   b.ctypes.data_as(dp), v.ctypes.data_as(dp) if v is not None else None))
+        return cv, b[0], v
+
+    def get_peratom(self, key, n):
+        out = np.zeros(n)
+        self._check(lib().mtd_get_peratom(self._h, key.encode(), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
 
     def set_domain(self, nlocal, rank, allreduce):
         """Domain decomposition: the first nlocal atoms of each step are owned,
