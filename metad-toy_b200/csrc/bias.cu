@@ -433,10 +433,12 @@ struct BiasShared {
 
 // One context, one step: all phases in one block.
 __global__ void __launch_bounds__(256) k_bias_step(const BiasPlan *__restrict__ Pp, long long step) {
-    pdl_entry();
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
+    // the plan is uploaded (and the stream synchronised) before a step's first
+    // kernel, so it is staged while the CV kernel before this one drains
     stage_plan(Pp, plan_raw);
+    pdl_entry();
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
     phase_cvs(P, S.smem, S.usum, S.s_sym, S.s_jac, S.sv);
     const int dep = (P.pace != 0) && (step % P.pace == 0) && !step_failed(P);

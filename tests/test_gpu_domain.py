@@ -156,6 +156,31 @@ def test_two_ranks_equal_one_domain(case, precision, tmp_path):
     assert len(rows) == len(steps)   # rank 0 alone writes HILLS
 
 
+@pytest.mark.parametrize("case", ["steinh_l_step", "stru_factor_chem"])
+def test_four_ranks_in_a_2x2_grid(case, tmp_path):
+    """Four thread ranks over a 2 x 2 x 1 brick grid (ghosts from two
+    neighbouring bricks and their corner), FP64, against one domain."""
+    args = CASES[case]()
+    x, L = _fcc(nc=8)
+    n = x.shape[0]
+    types = (np.arange(n) * 7 % 4).astype(np.int32)
+    steps = [(s, np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.03, 91, s), L))) for s in range(2)]
+    (tmp_path / "one").mkdir()
+    (tmp_path / "four").mkdir()
+    single, grid1 = _run_single(args, x, L, steps, "fp64", types, tmp_path / "one")
+    ranks, grids, _ = _run_ranks(args, x, L, steps, "fp64", types, tmp_path / "four", grid=(2, 2, 1))
+    for s in range(len(steps)):
+        cv1, b1, f1 = single[s]
+        for r in range(4):
+            assert np.array_equal(ranks[r][s][0], ranks[0][s][0]) and ranks[r][s][1] == ranks[0][s][1]
+        assert H.rel(ranks[0][s][0], cv1) < 1e-10 and H.rel(ranks[0][s][1], b1) < 1e-9
+        f = domain.reverse_sum(n, [ranks[r][s][3] for r in range(4)], [ranks[r][s][2] for r in range(4)])
+        assert H.rel(f, f1) < 1e-8
+    for g in grids[1:]:
+        assert np.array_equal(g, grids[0])
+    assert H.rel(grids[0], grid1) < 1e-9
+
+
 def test_domain_api_errors():
     m = mtd.Metad(H.fix_args_local())
     with pytest.raises(mtd.MetadError, match="domain decomposition is not enabled"):
