@@ -1947,6 +1947,7 @@ void walkers_drop_graph(mtd_walkers *W) {
 mtd_status walkers_enqueue(mtd_walkers *W, long long step, const int *n, const double *const *d_x,
                            double *const *d_f) {
     const int nw = (int)W->w.size();
+    PdlScope pdl_scope;   // each walker's kernel chain uses dependent launch (captured as programmatic edges)
     MTD_WCU(cudaMemcpyAsync(W->d_step, W->h_step, sizeof(long long), cudaMemcpyHostToDevice, W->st), "step");
     MTD_WCU(cudaEventRecord(W->ev_start, W->st), "fork");
     W->launches = 3;
