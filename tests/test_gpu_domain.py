@@ -181,6 +181,33 @@ def test_four_ranks_in_a_2x2_grid(case, tmp_path):
     assert H.rel(grids[0], grid1) < 1e-9
 
 
+def test_overflow_on_one_rank_retries_on_every_rank(tmp_path):
+    """A dense cluster inside rank 0's brick overflows its neighbour lists on
+    the first step while rank 1's do not: the overflow flag travels with the
+    totals, both ranks skip the deposit and retry together, and the result
+    equals the single domain (which overflows and retries too)."""
+    x, L = _fcc(nc=7)
+    rng = np.random.default_rng(5)
+    c = np.array([0.25, 0.5, 0.5]) * L
+    blob = c + rng.uniform(-1.2, 1.2, size=(40, 3))
+    x = np.ascontiguousarray(np.concatenate([x, blob]))
+    n = x.shape[0]
+    types = np.ones(n, dtype=np.int32)
+    args = CASES["steinh_l_step"]()
+    steps = [(s, x) for s in range(2)]
+    (tmp_path / "one").mkdir()
+    (tmp_path / "two").mkdir()
+    single, grid1 = _run_single(args, x, L, steps, "fp64", types, tmp_path / "one")
+    ranks, grids, _ = _run_ranks(args, x, L, steps, "fp64", types, tmp_path / "two")
+    for s in range(len(steps)):
+        cv1, b1, f1 = single[s]
+        assert np.array_equal(ranks[0][s][0], ranks[1][s][0])
+        assert H.rel(ranks[0][s][0], cv1) < 1e-10 and H.rel(ranks[0][s][1], b1) < 1e-9
+        f = domain.reverse_sum(n, [ranks[r][s][3] for r in range(2)], [ranks[r][s][2] for r in range(2)])
+        assert H.rel(f, f1) < 1e-8
+    assert np.array_equal(grids[0], grids[1]) and H.rel(grids[0], grid1) < 1e-9
+
+
 def test_domain_api_errors():
     m = mtd.Metad(H.fix_args_local())
     with pytest.raises(mtd.MetadError, match="domain decomposition is not enabled"):
