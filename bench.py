@@ -334,7 +334,7 @@ def run_secondary(args, local):
 
 def run_nnbias(args, local):
     """Learned 4D bias: 20,000 seeded hills (sigma 0.02, h 0.005 eV) along a 4D
-    CV trajectory; the MLP is fitted on the device, judged on 65,536 sampled
+    CV trajectory; the MLP is fitted on the device, checked on 65,536 sampled
     points, and the per-step bias (V and dV/ds at one CV point) is timed for
     the exact FP64 hill sum and for the network."""
     import torch

@@ -333,7 +333,7 @@ int mtd_walkers_last_launch_count(const mtd_walkers *W);
  * V_theta(s) for CV_dim >= 3, where the grid blows up: an MLP D -> 128 -> 128
  * -> 1 (SiLU, BF16 weights, FP32 accumulation, the 128 x 128 layer and its
  * backward contractions on the tensor cores), trained on the device on the
- * FP64 hill sum of the hills deposited so far.  The exact sum stays the judge
+ * FP64 hill sum of the hills deposited so far.  The exact sum stays the check
  * of its error (mtd_nnbias_validate) and the fallback (use_nn = -1 below).
  * No counterpart in the reference, whose only bias representations are the
  * grids (src/grids/GH_t0_uniformGrid.cu, src/grids/GH_t1_sparseGrid.cu).

@@ -74,7 +74,7 @@ struct Config {
     bool restart = false;
     bool wt = false;
     // hill-list bias (no grid): CV_dim 4, or any CV_dim with NN_BIAS 1
-    bool nn = false;              // NN_BIAS 1: learned bias judged by, and falling back to, the exact hill sum
+    bool nn = false;              // NN_BIAS 1: learned bias checked against, and falling back to, the exact hill sum
     double nn_tol = 1e-3;         // NN_TOL: max |V_theta - V_exact| on validation points
     int nn_refit = 1000;          // NN_REFIT: new hills between fits
     int nn_iters = 2000;          // NN_ITERS: Adam steps per fit

@@ -1,6 +1,6 @@
 // mlp.cu -- learned bias V_theta(s) for CV_dim >= 3: an MLP D -> 128 -> 128 -> 1
 // with SiLU activations, BF16 weights and FP32 accumulation, trained on the GPU
-// on the FP64 hill sum the method deposits, which stays the judge of its error
+// on the FP64 hill sum the method deposits, which stays the measure of its error
 // and the fallback.  No counterpart in the reference (its grids are the only
 // bias representation: src/grids/GH_t0_uniformGrid.cu, GH_t1_sparseGrid.cu).
 //
@@ -938,7 +938,7 @@ mtd_status mtd_nnbias_fit(mtd_nnbias *b, int ntrain, int iters, int batch, doubl
     return MTD_OK;
 }
 
-// Max and RMS of |V_theta - V_exact| on npts sampled points (the judge of the
+// Max and RMS of |V_theta - V_exact| on npts sampled points (the measure of the
 // network's error); marks the network usable when max <= tol.
 mtd_status mtd_nnbias_validate(mtd_nnbias *b, int npts, unsigned long long seed, double tol, double *max_err,
                                double *rms_err) {

@@ -417,7 +417,7 @@ def _dp(a):
 
 class NNBias:
     """Learned bias V_theta(s) (MLP D -> 128 -> 128 -> 1, BF16 weights, trained
-    on the device on the FP64 hill sum, which stays its judge and fallback)."""
+    on the device on the FP64 hill sum, which stays its check and fallback)."""
 
     def __init__(self, lo, hi, seed=1):
         lo = np.ascontiguousarray(lo, dtype=np.float64)

@@ -6,7 +6,7 @@ largest component (the device uses SFU exp in SiLU and FP32 tensor-core
 accumulation; a BF16 rounding of h1 can flip by one unit); the parameter
 gradient within 2e-2 of each block's largest entry; exact hill sum 1e-12
 relative plus the skipped far hills (each below h e^-40).  The fitted
-network is judged on 65,536 sampled points.
+network is checked on 65,536 sampled points.
 """
 import numpy as np
 import pytest
@@ -111,7 +111,7 @@ def test_point_evaluation_matches_batch():
 
 def test_fit_on_hill_sum_and_fallback():
     """20,000 hills (sigma 0.02, h 0.005 eV) along a seeded 4D CV trajectory:
-    the fitted network is judged on 65,536 sampled points.  Measured on B200:
+    the fitted network is checked on 65,536 sampled points.  Measured on B200:
     RMS error ~0.017 eV and max ~0.10 eV on a 0.56 eV landscape after 20,000
     Adam steps -- above the 1e-3 eV tolerance, so `usable` stays false and the
     exact FP64 sum stays in charge; a loose tolerance hands over to the network."""
