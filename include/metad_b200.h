@@ -244,6 +244,15 @@ int mtd_needs_types(const mtd_ctx *ctx);
  * (src/core/fix_crystallize.cu:510-520). */
 typedef int (*mtd_allreduce_fn)(double *buf, int count, void *user);
 mtd_status mtd_set_domain(mtd_ctx *ctx, int nlocal, int rank, mtd_allreduce_fn fn, void *user);
+/* The same with the exchange kept on the device: fn(d_buf, count, stream,
+ * user) receives the totals in device memory and must enqueue, on `stream`
+ * (the context's cudaStream_t), their in-place sum over the ranks, e.g.
+ * ncclAllReduce(d_buf, d_buf, count, ncclFloat64, ncclSum, comm, stream),
+ * and return 0.  The step then continues on the stream with no host
+ * synchronisation (the host callback costs one device-to-host and one
+ * host-to-device copy and a stream synchronisation per step). */
+typedef int (*mtd_allreduce_device_fn)(double *d_buf, int count, void *stream, void *user);
+mtd_status mtd_set_domain_device(mtd_ctx *ctx, int nlocal, int rank, mtd_allreduce_device_fn fn, void *user);
 mtd_status mtd_set_nlocal(mtd_ctx *ctx, int nlocal);
 /* Ghost shell the caller must supply under domain decomposition: cutoff_r of
  * STEINH Q and STRU_FACTOR, 2 x the cutoff of STEINH L (its centres read q_lm

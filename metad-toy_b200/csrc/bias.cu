@@ -676,6 +676,17 @@ void launch_unit_sums(const BiasPlan *d_plan, double *out, cudaStream_t st) {
     prof_mark("unit_sums", st);
 }
 
+// Domain decomposition with a device-side allreduce: the summed overflow
+// counts of all ranks mark this rank's step failed too (flag 1: nothing to grow).
+__global__ void k_domain_flag(const double *gflag, DevStatus *status) {
+    pdl_entry();
+    if (threadIdx.x == 0 && *gflag != 0.0 && status->overflow == 0u) status->overflow = 1u;
+}
+
+void launch_domain_flag(const double *gflag, DevStatus *status, cudaStream_t st) {
+    launch_k(k_domain_flag, 1, 32, 0, st, gflag, status);
+}
+
 void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st) {
     launch_k(k_bias_step, 1, 256, 0, st, d_plan, step);
     prof_mark("bias_step", st);

@@ -196,6 +196,7 @@ struct mtd_ctx {
     int nown = -1;                       // -1: off, every atom is owned
     int dom_rank = 0;
     mtd_allreduce_fn dom_fn = nullptr;
+    mtd_allreduce_device_fn dom_dev_fn = nullptr;   // stream-ordered variant (no host round trip)
     void *dom_user = nullptr;
     double *d_xchg = nullptr;            // this rank's unit totals, then the totals over all ranks
     double *h_xchg = nullptr;            // pinned staging of the same
@@ -903,6 +904,21 @@ mtd_status exchange_totals(mtd_ctx *c) {
     const int cnt = c->xchg_n;
     launch_unit_sums(c->d_plan, c->d_xchg, c->st);
     c->launches += 1;
+    if (c->dom_dev_fn) {   // the caller enqueues the sum over ranks on the step's stream
+        if (c->dom_dev_fn(c->d_xchg, cnt, (void *)c->st, c->dom_user) != 0)
+            return fail(c, MTD_ERR_INVALID_ARG, "domain decomposition: the device allreduce callback failed");
+        MTD_CU(cudaGetLastError(), "domain allreduce");
+        int off = 8 * (int)c->units.size();
+        for (Unit &u : c->units) {
+            if (u.kind != CAL_STRU_FACTOR_K) continue;
+            MTD_CU(cudaMemcpyAsync(u.rho, c->d_xchg + off, sizeof(double) * 2 * u.K, cudaMemcpyDeviceToDevice, c->st), "rho(k)");
+            MTD_CU(cudaMemcpyAsync(u.skn, c->d_xchg + off + 2 * u.K, sizeof(double), cudaMemcpyDeviceToDevice, c->st), "rho(k)");
+            off += 2 * u.K + 1;
+        }
+        launch_domain_flag(c->d_xchg + cnt - 1, c->d_status, c->st);   // any rank overflowed: every rank retries
+        c->launches += 1;
+        return MTD_OK;
+    }
     MTD_CU(cudaMemcpyAsync(c->h_xchg, c->d_xchg, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st), "domain totals");
     MTD_CU(cudaStreamSynchronize(c->st), "domain totals");
     const double own_overflow = c->h_xchg[cnt - 1];
@@ -1837,6 +1853,15 @@ mtd_status mtd_set_domain(mtd_ctx *c, int nlocal, int rank, mtd_allreduce_fn fn,
     c->dom_fn = fn;
     c->dom_user = user;
     c->plan_dirty = true;
+    return MTD_OK;
+}
+
+mtd_status mtd_set_domain_device(mtd_ctx *c, int nlocal, int rank, mtd_allreduce_device_fn fn, void *user) {
+    if (!c || !fn) return MTD_ERR_INVALID_ARG;
+    const mtd_status s = mtd_set_domain(c, nlocal, rank, reinterpret_cast<mtd_allreduce_fn>(fn), user);
+    if (s != MTD_OK) return s;
+    c->dom_fn = nullptr;
+    c->dom_dev_fn = fn;
     return MTD_OK;
 }
 

@@ -301,6 +301,7 @@ void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st);
 // neighbour-overflow count (0: none).
 void launch_unit_sums(const BiasPlan *d_plan, double *out, cudaStream_t st);
 int unit_sums_count(const BiasPlan &P);
+void launch_domain_flag(const double *gflag, DevStatus *status, cudaStream_t st);
 
 // Per-walker state handed between the multi-walker bias kernels.
 struct WalkState {

@@ -13,8 +13,10 @@ src/core/fix_crystallize.cu:510-520).
 
 ``decompose`` builds the per-rank atom sets, ``reverse_sum`` gathers forces
 onto owners, ``LocalAllreduce`` sums over ranks that are host threads of one
-process (one context per thread), and ``TorchAllreduce`` over the processes
-of a ``torch.distributed`` group (gloo on CPU tensors, NCCL on CUDA tensors).
+process (one context per thread), ``TorchAllreduce`` over the processes of a
+``torch.distributed`` group (gloo on CPU tensors, NCCL on CUDA tensors), and
+``TorchDeviceAllreduce`` enqueues the sum on the library's stream with NCCL,
+for ``Metad.set_domain_device`` (no host round trip per step).
 """
 from __future__ import annotations
 
@@ -123,3 +125,28 @@ class TorchAllreduce:
         t = torch.from_numpy(np.array(buf, copy=True)).to(self.device)
         dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
         buf[:] = t.cpu().numpy()
+
+
+class _DeviceView:
+    """A float64 vector at a raw device address, for torch.as_tensor."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                         "strides": None, "stream": None}
+
+
+class TorchDeviceAllreduce:
+    """Device-side allreduce for Metad.set_domain_device: sums the totals in
+    place over a torch.distributed NCCL group, enqueued on the library's
+    stream (the step goes on without a host synchronisation)."""
+
+    def __init__(self, group=None):
+        self.group = group
+
+    def __call__(self, ptr, count, stream):
+        import torch
+        import torch.distributed as dist
+
+        t = torch.as_tensor(_DeviceView(ptr, count), device="cuda")
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)

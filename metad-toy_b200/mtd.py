@@ -41,7 +41,8 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
            "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types",
            "mtd_set_domain", "mtd_set_nlocal", "mtd_ghost_cutoff",
-           "mtd_set_positions_f64", "mtd_step", "mtd_get_peratom", "mtd_create_from_config"]
+           "mtd_set_positions_f64", "mtd_step", "mtd_get_peratom", "mtd_create_from_config",
+           "mtd_set_domain_device"]
 
 
 class MetadError(RuntimeError):
@@ -64,6 +65,8 @@ _lib = None
 
 # int (*)(double *buf, int count, void *user): in-place sum of buf over the ranks
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.c_void_p)
+# int (*)(double *d_buf, int count, void *stream, void *user): enqueue that sum on the stream
+ALLREDUCE_DEVICE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p)
 
 
 def build(jobs=8):
@@ -100,6 +103,7 @@ def lib():
         L.mtd_set_types.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.mtd_needs_types.argtypes = [vp]
         L.mtd_set_domain.argtypes = [vp, C.c_int, C.c_int, ALLREDUCE_FN, vp]
+        L.mtd_set_domain_device.argtypes = [vp, C.c_int, C.c_int, ALLREDUCE_DEVICE_FN, vp]
         L.mtd_set_nlocal.argtypes = [vp, C.c_int]
         L.mtd_ghost_cutoff.argtypes = [vp]
         L.mtd_ghost_cutoff.restype = C.c_double
@@ -372,6 +376,23 @@ class Metad:
         self._domain_error = None
         self._domain_cb = ALLREDUCE_FN(cb)   # kept alive as long as the context
         self._check(lib().mtd_set_domain(self._h, int(nlocal), int(rank), self._domain_cb, None))
+
+    def set_domain_device(self, nlocal, rank, allreduce):
+        """Domain decomposition with the exchange on the device:
+        allreduce(ptr, count, stream) gets the device address of count float64
+        totals and the context's cudaStream_t (ints) and must enqueue their
+        in-place sum over all ranks on that stream (domain.TorchDeviceAllreduce
+        does it with torch.distributed / NCCL)."""
+        def cb(ptr, count, stream, _user):
+            try:
+                allreduce(int(ptr or 0), int(count), int(stream or 0))
+                return 0
+            except Exception as e:  # reported through the step's status
+                self._domain_error = e
+                return 1
+        self._domain_error = None
+        self._domain_cb = ALLREDUCE_DEVICE_FN(cb)
+        self._check(lib().mtd_set_domain_device(self._h, int(nlocal), int(rank), self._domain_cb, None))
 
     def set_nlocal(self, nlocal):
         self._check(lib().mtd_set_nlocal(self._h, int(nlocal)))

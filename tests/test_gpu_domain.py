@@ -208,6 +208,51 @@ def test_overflow_on_one_rank_retries_on_every_rank(tmp_path):
     assert np.array_equal(grids[0], grids[1]) and H.rel(grids[0], grid1) < 1e-9
 
 
+def _one_rank_vs_plain(setup, precision="mixed"):
+    """A single rank owning every atom of the periodic box, exchange through
+    `setup(m)`, against the plain context: the same bits (the one-rank sum
+    is the rank's own totals, reduced in the bias kernel's order)."""
+    x, L = _fcc(nc=6)
+    args = H.fix_args_local(pace=1)
+    a = mtd.Metad(args, precision=precision)
+    b = mtd.Metad(args, precision=precision)
+    setup(b, x.shape[0])
+    for m in (a, b):
+        m.set_box([0, 0, 0], L)
+    for s in range(3):
+        xs = np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.03, 95, s), L))
+        fa, fb = np.zeros_like(xs), np.zeros_like(xs)
+        a.post_force(s, xs, fa)
+        b.post_force(s, xs, fb)
+        assert np.array_equal(fa, fb) and np.array_equal(a.cv, b.cv) and a.compute_scalar() == b.compute_scalar()
+    a.close()
+    b.close()
+
+
+def test_device_exchange_one_rank_identity():
+    """Device-side exchange with a callback that enqueues nothing (the sum
+    over one rank): no host round trip, same bits as the plain step."""
+    calls = []
+    _one_rank_vs_plain(lambda m, n: m.set_domain_device(n, 0, lambda p, c, s: calls.append((c, s))))
+    assert len(calls) == 3 and all(c == calls[0][0] for c, _ in calls)
+
+
+def test_device_exchange_one_rank_nccl():
+    """Device-side exchange through torch.distributed NCCL (world size 1),
+    enqueued on the library's stream."""
+    import socket
+
+    import torch.distributed as dist
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        _one_rank_vs_plain(lambda m, n: m.set_domain_device(n, 0, domain.TorchDeviceAllreduce()))
+    finally:
+        dist.destroy_process_group()
+
+
 def test_domain_api_errors():
     m = mtd.Metad(H.fix_args_local())
     with pytest.raises(mtd.MetadError, match="domain decomposition is not enabled"):
