@@ -7,8 +7,11 @@
  * reference interface it replaces (paths inside the Metad-toy project).
  *
  * Threading: one host thread per context; calls on one context are not
- * thread-safe.  Each context owns one CUDA stream and all of its device
- * memory.  Caller arrays are borrowed for the duration of a call only.
+ * thread-safe, while different contexts may be driven from different host
+ * threads at the same time (the library keeps no shared mutable state
+ * between contexts).  Each context owns one CUDA stream and all of its
+ * device memory.  Caller arrays are borrowed for the duration of a call
+ * only.
  */
 #ifndef METAD_B200_H
 #define METAD_B200_H
