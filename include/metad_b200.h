@@ -321,6 +321,26 @@ int mtd_walkers_count(const mtd_walkers *W);
 mtd_status mtd_walkers_set_box(mtd_walkers *W, int k, const double lo[3], const double hi[3], const int periodic[3]);
 mtd_status mtd_walkers_init(mtd_walkers *W);
 
+/* Walkers sharded over ranks (one walkers object per rank and GPU, each with
+ * the same number of walkers nwalk; global walker id = rank * nwalk + k).
+ * Every step, after the CVs, each rank's hills (kWalkRec = 8 doubles per
+ * walker: s[4], height, deposit flag, overflow flag, 0) are gathered from
+ * all ranks in rank order by the caller's allgather -- fn(send, count,
+ * recv, user) on host buffers (recv holds nranks * count doubles), or the
+ * device variant that enqueues it on the walkers' stream (e.g.
+ * ncclAllGather(d_send, d_recv, count, ncclFloat64, comm, stream)) -- and
+ * every rank deposits all hills in global walker order, so every rank keeps
+ * the same grid.  A neighbour overflow of any walker on any rank makes every
+ * rank report the step for repetition.  Rank 0 alone writes HILLS.  Call
+ * before the first step; the CUDA graph is not used while sharded.
+ * Replaces nothing in the reference (no multi-walker mode); the shape is the
+ * hill allgather per PACE step of a walker-sharded run. */
+typedef int (*mtd_allgather_fn)(const double *send, int count, double *recv, void *user);
+typedef int (*mtd_allgather_device_fn)(const double *d_send, int count, double *d_recv, void *stream, void *user);
+mtd_status mtd_walkers_set_ranks(mtd_walkers *W, int rank, int nranks, mtd_allgather_fn fn, void *user);
+mtd_status mtd_walkers_set_ranks_device(mtd_walkers *W, int rank, int nranks, mtd_allgather_device_fn fn,
+                                        void *user);
+
 /* Capture the step in a CUDA graph (one graph launch per MD step once the
  * atom counts and array pointers repeat); 0 = plain launches. */
 mtd_status mtd_walkers_enable_graph(mtd_walkers *W, int enable);

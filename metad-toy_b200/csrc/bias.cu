@@ -610,6 +610,78 @@ __global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__rest
     phase_coef(P, S.sten, fx, S.sv, S.s_jac, S.usum, W.dep, S.row, &S.s_V, S.s_dV, S.s_alpha);
 }
 
+// ---- walkers sharded over ranks: each rank steps its own walkers; their
+// hills are exchanged (kWalkRec doubles per walker: s[kMaxDim], height,
+// deposit flag, neighbour-overflow flag, 0) and every rank deposits all
+// ranks' hills in global walker order, so every grid stays the same.
+__global__ void k_walk_pack(const BiasPlan *const *__restrict__ plans, int nwalk, const WalkState *ws, double *out) {
+    pdl_entry();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nwalk) return;
+    double *r = out + (size_t)k * kWalkRec;
+    for (int d = 0; d < kMaxDim; ++d) r[d] = ws[k].s[d];
+    r[kMaxDim] = ws[k].hill_w;
+    r[kMaxDim + 1] = ws[k].dep ? 1.0 : 0.0;
+    const DevStatus *st = plans[k]->status;
+    r[kMaxDim + 2] = (st && *(volatile const unsigned *)&st->overflow != 0u) ? 1.0 : 0.0;
+    r[kMaxDim + 3] = 0.0;
+}
+
+// Any walker of any rank overflowed its neighbour lists this step.
+__device__ bool all_failed(const double *__restrict__ recs, int nrec) {
+    __shared__ int failed;
+    if (threadIdx.x == 0) failed = 0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < nrec; r += blockDim.x)
+        if (recs[(size_t)r * kWalkRec + kMaxDim + 2] != 0.0) failed = 1;
+    __syncthreads();
+    return failed != 0;
+}
+
+__global__ void __launch_bounds__(256) k_walk_deposit_all(const BiasPlan *const *__restrict__ plans,
+                                                          const long long *__restrict__ d_step,
+                                                          const double *__restrict__ recs, int nrec) {
+    pdl_entry();
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    stage_plan(plans[0], plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    if (all_failed(recs, nrec)) return;
+    const long long step = *d_step;
+    if (!(P.pace != 0 && step % P.pace == 0)) return;   // every walker shares PACE
+    int ix[3] = {1, 1, 1};
+    for (int r = 0; r < nrec; ++r) {
+        const double *rec = recs + (size_t)r * kWalkRec;
+        phase_deposit(P, rec, rec[kMaxDim], ix, nullptr);
+        if (threadIdx.x == 0) record_hill(P, step, rec, rec[kMaxDim]);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_walk_coef_all(const BiasPlan *const *__restrict__ plans, const WalkState *ws,
+                                                       const double *__restrict__ recs, int nrec) {
+    pdl_entry();
+    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
+    __shared__ BiasShared S;
+    stage_plan(plans[blockIdx.x], plan_raw);
+    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+    if (all_failed(recs, nrec)) {
+        for (int e = threadIdx.x; e < P.nunit * 8; e += blockDim.x) P.unit[e / 8].coef[e % 8] = 0.0;
+        return;
+    }
+    const WalkState &W = ws[blockIdx.x];
+    for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) S.usum[e / 8][e % 8] = W.usum[e / 8][e % 8];
+    for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
+        S.s_jac[e / kMaxSymbols][e % kMaxSymbols] = W.jac[e / kMaxSymbols][e % kMaxSymbols];
+    if (threadIdx.x < kMaxDim) S.sv[threadIdx.x] = W.s[threadIdx.x];
+    __syncthreads();
+    int ix[3] = {1, 1, 1};
+    double fx[3] = {0, 0, 0};
+    stencil_locate(P, S.sv, ix, fx);
+    stencil_load(P, ix, S.sten);
+    __syncthreads();
+    phase_coef(P, S.sten, fx, S.sv, S.s_jac, S.usum, W.dep, S.row, &S.s_V, S.s_dV, S.s_alpha);
+}
+
 // HILLS replay: every thread owns grid bins and adds the hills in file order,
 // so the FP64 sum order per bin is the file order.
 __global__ void k_hills_replay(const BiasPlan *__restrict__ Pp, const HillRec *__restrict__ h, int nh, int ncell) {
@@ -712,6 +784,19 @@ void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long
     launch_k(k_walk_cvs, nwalk, 256, 0, st, d_plans, d_step, ws);
     launch_k(k_walk_deposit, 1, 256, 0, st, d_plans, nwalk, d_step, ws);
     launch_k(k_walk_coef, nwalk, 256, 0, st, d_plans, nwalk, ws);
+    prof_mark("walk_bias", st);
+}
+
+void launch_walk_cvs_pack(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
+                          double *out, cudaStream_t st) {
+    launch_k(k_walk_cvs, nwalk, 256, 0, st, d_plans, d_step, ws);
+    launch_k(k_walk_pack, (nwalk + 127) / 128, 128, 0, st, d_plans, nwalk, (const WalkState *)ws, out);
+}
+
+void launch_walk_finish(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, const WalkState *ws,
+                        const double *recs, int nrec, cudaStream_t st) {
+    launch_k(k_walk_deposit_all, 1, 256, 0, st, d_plans, d_step, recs, nrec);
+    launch_k(k_walk_coef_all, nwalk, 256, 0, st, d_plans, ws, recs, nrec);
     prof_mark("walk_bias", st);
 }
 

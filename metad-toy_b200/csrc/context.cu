@@ -1946,6 +1946,14 @@ struct mtd_walkers {
     bool pending = false;
     long long pending_step = 0;
     int launches = 0;
+    // sharded over ranks (mtd_walkers_set_ranks*): this object's walkers are
+    // the global walkers rank * nwalk .. rank * nwalk + nwalk - 1
+    int rank = 0, nranks = 0;                 // nranks 0: not sharded
+    mtd_allgather_fn ag = nullptr;
+    mtd_allgather_device_fn ag_dev = nullptr;
+    void *ag_user = nullptr;
+    double *d_xloc = nullptr, *d_xall = nullptr;   // [nwalk][kWalkRec], [nranks * nwalk][kWalkRec]
+    double *h_xloc = nullptr, *h_xall = nullptr;   // pinned staging of the same
 };
 
 namespace {
@@ -1985,7 +1993,29 @@ mtd_status walkers_enqueue(mtd_walkers *W, long long step, const int *n, const d
         MTD_WCU(cudaEventRecord(W->ev_done[k], c->st), "join");
         MTD_WCU(cudaStreamWaitEvent(W->st, W->ev_done[k], 0), "join");
     }
-    launch_walk_bias(W->d_plans, nw, W->d_step, W->d_ws, W->st);
+    if (W->nranks > 0) {   // this rank's hills out, every rank's hills in, all deposited in global order
+        const int cnt = nw * kWalkRec, nall = W->nranks * nw;
+        launch_walk_cvs_pack(W->d_plans, nw, W->d_step, W->d_ws, W->d_xloc, W->st);
+        if (W->ag_dev) {
+            if (W->ag_dev(W->d_xloc, cnt, W->d_xall, (void *)W->st, W->ag_user) != 0)
+                return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks: the device allgather callback failed");
+            MTD_WCU(cudaGetLastError(), "walker allgather");
+        } else {
+            MTD_WCU(cudaMemcpyAsync(W->h_xloc, W->d_xloc, sizeof(double) * cnt, cudaMemcpyDeviceToHost, W->st), "hills out");
+            MTD_WCU(cudaStreamSynchronize(W->st), "hills out");
+            if (W->ag(W->h_xloc, cnt, W->h_xall, W->ag_user) != 0)
+                return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks: the allgather callback failed");
+            MTD_WCU(cudaMemcpyAsync(W->d_xall, W->h_xall, sizeof(double) * nall * kWalkRec, cudaMemcpyHostToDevice,
+                                    W->st), "hills in");
+        }
+        launch_walk_finish(W->d_plans, nw, W->d_step, W->d_ws, W->d_xall, nall, W->st);
+        if (W->ag_dev)   // every rank's overflow flag, for mtd_walkers_sync
+            MTD_WCU(cudaMemcpyAsync(W->h_xall, W->d_xall, sizeof(double) * nall * kWalkRec, cudaMemcpyDeviceToHost,
+                                    W->st), "hills in");
+        W->launches += 4;
+    } else {
+        launch_walk_bias(W->d_plans, nw, W->d_step, W->d_ws, W->st);
+    }
     MTD_WCU(cudaGetLastError(), "walker bias");
     MTD_WCU(cudaEventRecord(W->ev_bias, W->st), "fork");
     for (int k = 0; k < nw; ++k) {
@@ -2058,6 +2088,10 @@ void mtd_walkers_destroy(mtd_walkers *W) {
     if (W->d_ws) cudaFree(W->d_ws);
     if (W->d_step) cudaFree(W->d_step);
     if (W->h_step) cudaFreeHost(W->h_step);
+    if (W->d_xloc) cudaFree(W->d_xloc);
+    if (W->d_xall) cudaFree(W->d_xall);
+    if (W->h_xloc) cudaFreeHost(W->h_xloc);
+    if (W->h_xall) cudaFreeHost(W->h_xall);
     if (W->st) cudaStreamDestroy(W->st);
     if (W->f_hills) std::fclose(W->f_hills);
     delete W;
@@ -2098,7 +2132,15 @@ mtd_status mtd_walkers_init(mtd_walkers *W) {
     }
     W->initialized = true;
     MTD_WCU(cudaMemcpy(W->d_plans, plans.data(), sizeof(BiasPlan *) * nw, cudaMemcpyHostToDevice), "plans");
-    if (!W->hills_path.empty()) {
+    if (W->nranks > 0) {
+        const size_t loc = sizeof(double) * nw * kWalkRec, all = loc * W->nranks;
+        MTD_WCU(cudaMalloc((void **)&W->d_xloc, loc), "walker ranks");
+        MTD_WCU(cudaMalloc((void **)&W->d_xall, all), "walker ranks");
+        MTD_WCU(cudaHostAlloc((void **)&W->h_xloc, loc, cudaHostAllocDefault), "walker ranks");
+        MTD_WCU(cudaHostAlloc((void **)&W->h_xall, all, cudaHostAllocDefault), "walker ranks");
+        std::memset(W->h_xall, 0, all);
+    }
+    if (!W->hills_path.empty() && W->rank == 0) {   // sharded: rank 0 alone writes the group's HILLS
         W->f_hills = std::fopen(W->hills_path.c_str(), "w");
         if (!W->f_hills) return wfail(W, MTD_ERR_IO, "Cannot open HILLS file for writing/appending.");
         if (c0->cfg.cv_dim == 2) std::fprintf(W->f_hills, "# step cv1 cv2 height sigma\n");
@@ -2108,11 +2150,35 @@ mtd_status mtd_walkers_init(mtd_walkers *W) {
     return MTD_OK;
 }
 
+static mtd_status walkers_set_ranks(mtd_walkers *W, int rank, int nranks, mtd_allgather_fn fn,
+                             mtd_allgather_device_fn fn_dev, void *user) {
+    if (!W) return MTD_ERR_INVALID_ARG;
+    if (W->initialized) return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks must be set before the first step");
+    if (nranks < 1 || rank < 0 || rank >= nranks || (!fn && !fn_dev))
+        return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks need 0 <= rank < nranks and an allgather callback");
+    W->rank = rank;
+    W->nranks = nranks;
+    W->ag = fn;
+    W->ag_dev = fn_dev;
+    W->ag_user = user;
+    W->use_graph = false;   // the exchange sits between the captured phases
+    return MTD_OK;
+}
+
+mtd_status mtd_walkers_set_ranks(mtd_walkers *W, int rank, int nranks, mtd_allgather_fn fn, void *user) {
+    return walkers_set_ranks(W, rank, nranks, fn, nullptr, user);
+}
+
+mtd_status mtd_walkers_set_ranks_device(mtd_walkers *W, int rank, int nranks, mtd_allgather_device_fn fn,
+                                        void *user) {
+    return walkers_set_ranks(W, rank, nranks, nullptr, fn, user);
+}
+
 mtd_status mtd_walkers_enable_graph(mtd_walkers *W, int enable) {
     if (!W) return MTD_ERR_INVALID_ARG;
     if (W->st) cudaStreamSynchronize(W->st);
     walkers_drop_graph(W);
-    W->use_graph = enable != 0;
+    W->use_graph = enable != 0 && W->nranks == 0;
     return MTD_OK;
 }
 
@@ -2208,6 +2274,9 @@ mtd_status mtd_walkers_sync(mtd_walkers *W) {
             overflow = true;
         }
     }
+    if (W->nranks > 0)   // sharded: a walker of any rank overflowed, so every rank repeats the step
+        for (int r = 0; r < W->nranks * (int)W->w.size(); ++r)
+            if (W->h_xall[(size_t)r * kWalkRec + kMaxDim + 2] != 0.0) overflow = true;
     if (overflow) {
         walkers_drop_graph(W);
         W->g_n.clear();

@@ -313,6 +313,15 @@ struct WalkState {
 };
 void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
                       cudaStream_t st);
+// Walkers sharded over ranks: CVs and heights of this rank's walkers packed
+// into kWalkRec-double records (out[nwalk][kWalkRec]); then, with every
+// rank's records gathered in rank order (recs[nrec][kWalkRec]), the deposit
+// of all hills and this rank's force coefficients.
+constexpr int kWalkRec = kMaxDim + 4;
+void launch_walk_cvs_pack(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
+                          double *out, cudaStream_t st);
+void launch_walk_finish(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, const WalkState *ws,
+                        const double *recs, int nrec, cudaStream_t st);
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
 
 // Hill-list bias (no grid; CV_dim up to 4): the CV values and chain factors

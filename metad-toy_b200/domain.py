@@ -17,6 +17,8 @@ process (one context per thread), ``TorchAllreduce`` over the processes of a
 ``torch.distributed`` group (gloo on CPU tensors, NCCL on CUDA tensors), and
 ``TorchDeviceAllreduce`` enqueues the sum on the library's stream with NCCL,
 for ``Metad.set_domain_device`` (no host round trip per step).
+``LocalAllgather`` and ``TorchDeviceAllgather`` do the same for walkers
+sharded over ranks (``Walkers.set_ranks`` / ``set_ranks_device``).
 """
 from __future__ import annotations
 
@@ -150,3 +152,42 @@ class TorchDeviceAllreduce:
         t = torch.as_tensor(_DeviceView(ptr, count), device="cuda")
         with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
             dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+
+
+class LocalAllgather:
+    """Allgather across ranks that are host threads of one process (one
+    walkers object per thread); ``for_rank(r)`` is the callback of rank r."""
+
+    def __init__(self, nranks, timeout=120.0):
+        self.n = nranks
+        self._bufs = [None] * nranks
+        self._barrier = threading.Barrier(nranks, timeout=timeout)
+
+    def for_rank(self, r):
+        def allgather(send, recv):
+            self._bufs[r] = np.array(send, copy=True)
+            self._barrier.wait()
+            recv[:] = np.concatenate(self._bufs)
+            self._barrier.wait()
+        return allgather
+
+    def abort(self):
+        self._barrier.abort()
+
+
+class TorchDeviceAllgather:
+    """Device-side allgather for Walkers.set_ranks_device over a
+    torch.distributed NCCL group, enqueued on the walkers' stream."""
+
+    def __init__(self, nranks, group=None):
+        self.n = nranks
+        self.group = group
+
+    def __call__(self, send_ptr, count, recv_ptr, stream):
+        import torch
+        import torch.distributed as dist
+
+        send = torch.as_tensor(_DeviceView(send_ptr, count), device="cuda")
+        recv = torch.as_tensor(_DeviceView(recv_ptr, count * self.n), device="cuda")
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            dist.all_gather_into_tensor(recv, send, group=self.group)

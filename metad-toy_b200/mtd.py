@@ -42,7 +42,7 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types",
            "mtd_set_domain", "mtd_set_nlocal", "mtd_ghost_cutoff",
            "mtd_set_positions_f64", "mtd_step", "mtd_get_peratom", "mtd_create_from_config",
-           "mtd_set_domain_device"]
+           "mtd_set_domain_device", "mtd_walkers_set_ranks", "mtd_walkers_set_ranks_device"]
 
 
 class MetadError(RuntimeError):
@@ -67,6 +67,11 @@ _lib = None
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.c_void_p)
 # int (*)(double *d_buf, int count, void *stream, void *user): enqueue that sum on the stream
 ALLREDUCE_DEVICE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p)
+# int (*)(const double *send, int count, double *recv, void *user): every rank's send, in rank order
+ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_void_p)
+# int (*)(const double *d_send, int count, double *d_recv, void *stream, void *user)
+ALLGATHER_DEVICE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+WALK_REC = 8   # doubles per walker in the exchange: s[4], height, deposit flag, overflow flag, 0
 
 
 def build(jobs=8):
@@ -105,6 +110,8 @@ def lib():
         L.mtd_set_domain.argtypes = [vp, C.c_int, C.c_int, ALLREDUCE_FN, vp]
         L.mtd_set_domain_device.argtypes = [vp, C.c_int, C.c_int, ALLREDUCE_DEVICE_FN, vp]
         L.mtd_set_nlocal.argtypes = [vp, C.c_int]
+        L.mtd_walkers_set_ranks.argtypes = [vp, C.c_int, C.c_int, ALLGATHER_FN, vp]
+        L.mtd_walkers_set_ranks_device.argtypes = [vp, C.c_int, C.c_int, ALLGATHER_DEVICE_FN, vp]
         L.mtd_ghost_cutoff.argtypes = [vp]
         L.mtd_ghost_cutoff.restype = C.c_double
         L.mtd_set_positions_f64.argtypes = [vp, dp, ip, ip, C.c_int, C.c_int]
@@ -583,6 +590,35 @@ class Walkers:
 
     def enable_graph(self, on=True):
         self._check(lib().mtd_walkers_enable_graph(self._h, 1 if on else 0))
+
+    def set_ranks(self, rank, nranks, allgather):
+        """Shard walkers over ranks: allgather(send, recv) fills the float64
+        array recv (nranks * len(send)) with every rank's send in rank order."""
+        def cb(sp, count, rp, _user):
+            try:
+                allgather(np.ctypeslib.as_array(sp, shape=(count,)),
+                          np.ctypeslib.as_array(rp, shape=(count * nranks,)))
+                return 0
+            except Exception as e:
+                self._rank_error = e
+                return 1
+        self._rank_error = None
+        self._rank_cb = ALLGATHER_FN(cb)
+        self._check(lib().mtd_walkers_set_ranks(self._h, int(rank), int(nranks), self._rank_cb, None))
+
+    def set_ranks_device(self, rank, nranks, allgather):
+        """Device variant: allgather(send_ptr, count, recv_ptr, stream) enqueues
+        the gather on the walkers' stream (ints: device addresses, cudaStream_t)."""
+        def cb(sp, count, rp, stream, _user):
+            try:
+                allgather(int(sp or 0), int(count), int(rp or 0), int(stream or 0))
+                return 0
+            except Exception as e:
+                self._rank_error = e
+                return 1
+        self._rank_error = None
+        self._rank_cb = ALLGATHER_DEVICE_FN(cb)
+        self._check(lib().mtd_walkers_set_ranks_device(self._h, int(rank), int(nranks), self._rank_cb, None))
 
     def step_device(self, step, ns, x_ptrs, f_ptrs):
         n = (C.c_int * self.n)(*[int(v) for v in ns])

@@ -122,3 +122,112 @@ def test_walkers_overflow_leaves_no_hill_and_no_force():
         assert H.rel(W.bias(k), V) < 1e-9
         assert H.rel(df[k].cpu().numpy(), -(dV[0] * o4["grad"] + dV[1] * o6["grad"])) < 1e-8
     W.close()
+
+
+def _run_ranks(args, syss, steps, nranks):
+    """The same walkers split over nranks thread ranks (equal shares), hills
+    exchanged by a host allgather."""
+    import threading
+
+    import domain
+    import torch
+
+    per = len(syss) // nranks
+    red = domain.LocalAllgather(nranks, timeout=120)
+    objs = []
+    for r in range(nranks):
+        W = mtd.Walkers(per, args, precision="fp64")
+        W.set_ranks(r, nranks, red.for_rank(r))
+        for k in range(per):
+            W.set_box(k, [0, 0, 0], syss[r * per + k][1])
+        objs.append(W)
+    out = [[None] * len(steps) for _ in range(nranks)]
+    errs = []
+
+    def run(r):
+        try:
+            W = objs[r]
+            mine = syss[r * per:(r + 1) * per]
+            dx = [torch.from_numpy(x).cuda() for x, _ in mine]
+            df = [torch.zeros_like(v) for v in dx]
+            for i, step in enumerate(steps):
+                for v in df:
+                    v.zero_()
+                W.step_device(step, [x.shape[0] for x, _ in mine], [v.data_ptr() for v in dx],
+                              [v.data_ptr() for v in df])
+                W.sync()
+                out[r][i] = [(W.cv(k, 2), W.bias(k), df[k].cpu().numpy()) for k in range(per)]
+        except BaseException as e:
+            errs.append(e)
+            red.abort()
+
+    th = [threading.Thread(target=run, args=(r,)) for r in range(nranks)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    if errs:
+        raise errs[0]
+    grids = [W.grid(200 * 200) for W in objs]
+    for W in objs:
+        W.close()
+    return out, grids
+
+
+def test_walkers_sharded_over_two_ranks_equal_one_group():
+    """Four walkers as one group against the same four split 2 + 2 over two
+    thread ranks: CVs, bias, forces and the grid bit for bit (each rank
+    deposits every rank's hills in global walker order)."""
+    base = _walker_systems()
+    syss = base + [(np.ascontiguousarray(systems.wrap(systems.jitter(base[0][0], 0.05, 77), base[0][1])),
+                    base[0][1])]
+    steps = [0, 1, 2, 3]
+    args = H.fix_args_local(pace=2)
+    one, grid1 = _run(args, syss, steps, graph=False)
+    two, grids = _run_ranks(args, syss, steps, 2)
+    for i in range(len(steps)):
+        for r in range(2):
+            for k in range(2):
+                cv, b, f = two[r][i][k]
+                cv1, b1, f1 = one[i][2 * r + k]
+                assert np.array_equal(cv, cv1) and b == b1 and np.array_equal(f, f1)
+    assert np.array_equal(grids[0], grids[1]) and np.array_equal(grids[0], grid1)
+
+
+def test_walkers_sharded_device_allgather_one_rank_nccl():
+    """The device-side gather (torch.distributed NCCL all_gather on the
+    walkers' stream, world size 1) against the unsharded group, bit for bit."""
+    import socket
+
+    import domain
+    import torch
+    import torch.distributed as dist
+
+    syss = _walker_systems()
+    steps = [0, 1, 2]
+    args = H.fix_args_local(pace=2)
+    one, grid1 = _run(args, syss, steps, graph=False)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        W = mtd.Walkers(len(syss), args, precision="fp64")
+        W.set_ranks_device(0, 1, domain.TorchDeviceAllgather(1))
+        for k, (x, L) in enumerate(syss):
+            W.set_box(k, [0, 0, 0], L)
+        dx = [torch.from_numpy(x).cuda() for x, _ in syss]
+        df = [torch.zeros_like(v) for v in dx]
+        for i, step in enumerate(steps):
+            for v in df:
+                v.zero_()
+            W.step_device(step, [x.shape[0] for x, _ in syss], [v.data_ptr() for v in dx], [v.data_ptr() for v in df])
+            W.sync()
+            for k in range(len(syss)):
+                cv1, b1, f1 = one[i][k]
+                assert np.array_equal(W.cv(k, 2), cv1) and W.bias(k) == b1
+                assert np.array_equal(df[k].cpu().numpy(), f1)
+        assert np.array_equal(W.grid(200 * 200), grid1)
+        W.close()
+    finally:
+        dist.destroy_process_group()
