@@ -165,3 +165,18 @@ def test_two_gloo_ranks_match_the_single_domain_oracle():
             scale = max(1e-30, np.abs(o["grad"]).max())
             assert np.abs(grad - o["grad"]).max() / scale < 1e-10, name
         assert res[0][name][0] == res[1][name][0]
+
+
+def test_local_allgather_orders_by_rank():
+    n = 3
+    red = domain.LocalAllgather(n, timeout=30)
+    sends = [np.full(4, float(r + 1)) for r in range(n)]
+    recvs = [np.zeros(4 * n) for _ in range(n)]
+    ts = [threading.Thread(target=red.for_rank(r), args=(sends[r], recvs[r])) for r in range(n)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    want = np.concatenate(sends)
+    for rv in recvs:
+        assert np.array_equal(rv, want)
