@@ -320,9 +320,10 @@ __device__ void phase_deposit(const BiasPlan &P, const double *s, double w, cons
 
 // A step whose neighbour lists overflowed is repeated by the host: it must
 // leave no hill and no bias force behind.
-__device__ __forceinline__ bool step_failed(const BiasPlan &P) {
-    return P.status && *(volatile const unsigned *)&P.status->overflow != 0u;
+__device__ __forceinline__ bool status_failed(const DevStatus *st) {
+    return st && (*(volatile const unsigned *)&st->overflow != 0u || *(volatile const unsigned *)&st->bad_pos != 0u);
 }
+__device__ __forceinline__ bool step_failed(const BiasPlan &P) { return status_failed(P.status); }
 
 __device__ __forceinline__ void record_hill(const BiasPlan &P, long long step, const double *s, double w) {
     const unsigned long long h = *P.nhills;
@@ -562,7 +563,7 @@ __device__ bool group_failed(const BiasPlan *const *__restrict__ plans, int nwal
     __syncthreads();
     for (int w = threadIdx.x; w < nwalk; w += blockDim.x) {
         const DevStatus *st = plans[w]->status;
-        if (st && *(volatile const unsigned *)&st->overflow != 0u) failed = 1;
+        if (status_failed(st)) failed = 1;
     }
     __syncthreads();
     return failed != 0;
@@ -623,7 +624,7 @@ __global__ void k_walk_pack(const BiasPlan *const *__restrict__ plans, int nwalk
     r[kMaxDim] = ws[k].hill_w;
     r[kMaxDim + 1] = ws[k].dep ? 1.0 : 0.0;
     const DevStatus *st = plans[k]->status;
-    r[kMaxDim + 2] = (st && *(volatile const unsigned *)&st->overflow != 0u) ? 1.0 : 0.0;
+    r[kMaxDim + 2] = status_failed(st) ? 1.0 : 0.0;
     r[kMaxDim + 3] = 0.0;
 }
 

@@ -118,7 +118,7 @@ struct DevStatus {
     unsigned int overflow;        // max neighbour count seen when above capacity
     unsigned int nan_force;       // a force component was not finite
     unsigned int timeout;         // a bounded wait gave up
-    unsigned int pad;
+    unsigned int bad_pos;         // an atom position was not finite (NaN or Inf)
 };
 
 // First statement of every step kernel: wait until the previous kernel of the

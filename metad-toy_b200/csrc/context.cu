@@ -678,6 +678,7 @@ SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
     s.xs = c->xs;
     s.pf = c->pf;
     s.nown = owned(c);
+    s.status = c->d_status;
     return s;
 }
 
@@ -1037,6 +1038,8 @@ mtd_status collect(mtd_ctx *c) {
         std::fprintf(c->f_rec, " %.16g\n", c->bias);
         std::fflush(c->f_rec);
     }
+    if (c->h_status->bad_pos)
+        return fail(c, MTD_ERR_NAN, "non-finite atom position (NaN or Inf): the step deposited nothing and applied no bias force");
     if (c->h_status->nan_force) return fail(c, MTD_ERR_NAN, "STEIN_QL CV error: force is infinity, check your system or cv_value.");
     return MTD_OK;
 }

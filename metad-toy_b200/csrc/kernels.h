@@ -75,6 +75,7 @@ struct SysDev {
                           // sorted group mask is 0, so they are neighbours and never centres
     double *xs;           // sorted raw coordinates AoS npad*3
     float4 *pf;           // sorted cell-relative coordinates + packed cell
+    DevStatus *status;    // k_bin flags non-finite positions (bad_pos)
 };
 
 // Neighbour criteria (the reference's per-CV filters).

@@ -39,9 +39,14 @@ __global__ void k_bin(CellGrid g, SysDev s) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
     double w;
-    const int cx = cell_coord(s.x[3 * i + 0], g, 0, w);
-    const int cy = cell_coord(s.x[3 * i + 1], g, 1, w);
-    const int cz = cell_coord(s.x[3 * i + 2], g, 2, w);
+    const double x0 = s.x[3 * i + 0], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
+    // a non-finite coordinate is binned into a valid cell (cell_coord clamps),
+    // matches no neighbour test (every comparison with NaN is false), and
+    // fails the step: no deposit, no bias force, an error on the host
+    if (!(isfinite(x0) && isfinite(x1) && isfinite(x2)) && s.status) atomicOr(&s.status->bad_pos, 1u);
+    const int cx = cell_coord(x0, g, 0, w);
+    const int cy = cell_coord(x1, g, 1, w);
+    const int cz = cell_coord(x2, g, 2, w);
     const int cell = (cx * g.nc[1] + cy) * g.nc[2] + cz;
     s.cellof[i] = cell;
     s.slot[i] = atomicAdd(&s.count[cell], 1);

@@ -1,7 +1,7 @@
 """Edge cases through the C ABI against the FP64 oracle: pairs sitting on the
 cutoff to the last bit, two atoms in an open box (the reference's two-atom
-toy deck), an empty group, zero atoms, a non-periodic dimension and a 3D
-bias grid.  Tolerances as in the parity tests: FP64 1e-9 relative on CVs and
+toy deck), an empty group, zero atoms, a non-periodic dimension, a 3D
+bias grid and a non-finite position.  Tolerances as in the parity tests: FP64 1e-9 relative on CVs and
 bias, 1e-8 on forces; mixed 2e-5 and 2e-3 of the largest force component."""
 import numpy as np
 import pytest
@@ -153,4 +153,29 @@ def test_three_dimensional_grid(precision):
         assert H.rel(bias, V) < tcv * 10
         fo = -(dV[0] * o4["grad"] + dV[1] * o6["grad"] + dV[2] * oq["grad"])
         assert H.rel(f, fo) < tf
+    m.close()
+
+
+def test_non_finite_position_fails_the_step_cleanly():
+    """A NaN coordinate is flagged while binning (the atom lands in a valid
+    cell and matches no neighbour test): the step deposits nothing, applies
+    no bias force and reports MTD_ERR_NAN; the next good step runs normally."""
+    x, L = systems.fcc(5, 5.26), np.array([5 * 5.26] * 3)
+    x = np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.1, 3), L))
+    m = mtd.Metad(H.fix_args_local(pace=1), precision="mixed")
+    m.set_box([0, 0, 0], L)
+    f0 = np.full_like(x, 0.5)
+    f = f0.copy()
+    m.post_force(0, x, f)
+    g0 = m.grid(200 * 200)
+    xb = x.copy()
+    xb[3, 1] = np.nan
+    f = f0.copy()
+    with pytest.raises(mtd.MetadError, match="non-finite"):
+        m.post_force(1, xb, f)
+    assert np.array_equal(f, f0)
+    assert np.array_equal(m.grid(200 * 200), g0)
+    f = f0.copy()
+    m.post_force(2, x, f)
+    assert np.all(np.isfinite(f)) and not np.array_equal(m.grid(200 * 200), g0)
     m.close()
