@@ -195,6 +195,20 @@ def test_hills_file_and_restart(tmp_path):
     assert len(lines2) == len(lines) + 1 and lines2[-1].startswith("25 ")
 
 
+@pytest.mark.parametrize("bad", ["10 0.25 0.005\n", "10 0.25 abc 0.01\n"])
+def test_corrupt_hills_line_is_an_error(tmp_path, bad):
+    """A truncated or non-numeric HILLS row stops the restart with
+    MTD_ERR_IO and the offending line, before any step (comment and blank
+    lines are skipped)."""
+    hills = tmp_path / "HILLS"
+    hills.write_text("# step cv_values height sigma\n\n0 0.20 0.005 0.01\n" + bad)
+    m = mtd.Metad(H.fix_args_q(wt=1, pace=5) + ["METAD_RESTART", 1], precision="fp64", hills_path=str(hills))
+    m.set_box([0, 0, 0], [20.0, 20.0, 20.0])
+    with pytest.raises(mtd.MetadError, match="malformed HILLS line"):
+        m.init()
+    m.close()
+
+
 def test_reference_hills_fixture_replays():
     """The reference's own 1D HILLS (test/test_cvset/HILLS: 238 hills, h 0.005,
     sigma 0.01), committed under tests/golden, replays like the oracle's sum."""
