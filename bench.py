@@ -503,6 +503,70 @@ def run_walkers(args, local):
     return 0
 
 
+def run_domain(args, local):
+    """Per-step cost of the domain-decomposition exchange on the headline
+    workload with one rank owning every atom (so the results equal the plain
+    step): plain, host allreduce callback, device callback that enqueues
+    nothing, device callback through a one-rank NCCL group.  Wall clock per
+    synchronised step after an L2 flush (the exchange is host latency, which
+    CUDA events on the device would not show)."""
+    import socket
+    import time
+
+    import torch
+    import torch.distributed as dist
+
+    import domain
+    import mtd
+    torch.cuda.set_device(local)
+    xs, L = load_system()
+    n = xs[0].shape[0]
+    dx = [torch.from_numpy(x).cuda() for x in xs]
+    f = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    res, cvs = {}, {}
+    try:
+        for mode in ("plain", "host", "device", "device_nccl"):
+            m = mtd.Metad(fix_args(), precision=args.precision, device=local)
+            if mode == "host":
+                m.set_domain(n, 0, domain.LocalAllreduce(1).for_rank(0))
+            elif mode == "device":
+                m.set_domain_device(n, 0, lambda p, c, s: None)
+            elif mode == "device_nccl":
+                m.set_domain_device(n, 0, domain.TorchDeviceAllreduce())
+            m.set_box([0, 0, 0], L)
+            step = 0
+            for _ in range(args.warmup):
+                m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
+                step += 1
+            m.sync()
+            tot = 0.0
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
+                m.sync()
+                tot += time.perf_counter() - t0
+                step += 1
+            res[mode] = tot * 1e3 / args.steps
+            cvs[mode] = m.cv.tolist()
+            m.close()
+    finally:
+        dist.destroy_process_group()
+    print(json.dumps({"metric": "domain-decomposition exchange cost", "workload": "domain", "unit": "ms/step",
+                      "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": res, "exchange_us": {k: (v - res["plain"]) * 1e3 for k, v in res.items()},
+                      "cv_equal": all(c == cvs["plain"] for c in cvs.values()),
+                      "config": {"workload": WORKLOAD, "atoms": n, "ranks": 1,
+                                 "timing": "wall clock per synchronised step after a 256 MB L2 flush"}}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -511,10 +575,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="local", choices=["local", "sk", "q", "nn", "walkers"],
+    ap.add_argument("--workload", default="local", choices=["local", "sk", "q", "nn", "walkers", "domain"],
                     help="local: the headline 256k-atom STEINH L workload; sk: 1M-atom k-vector S(k); "
                          "q: 4,000-atom STEINH Q (FP64); nn: learned 4D bias vs exact hill sum; "
-                         "walkers: 32 walkers sharing one grid")
+                         "walkers: 32 walkers sharing one grid; domain: cost of the decomposition exchange")
     ap.add_argument("--nn-iters", type=int, default=20000, help="Adam steps of the learned-bias fit (--workload nn)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -527,6 +591,8 @@ def main():
         return run_nnbias(args, local)
     if args.workload == "walkers":
         return run_walkers(args, local)
+    if args.workload == "domain":
+        return run_domain(args, local)
     if args.workload != "local":
         return run_secondary(args, local)
 
