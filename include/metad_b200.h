@@ -223,8 +223,9 @@ int mtd_needs_types(const mtd_ctx *ctx);
  * sum.  The box is the caller's subdomain grown by mtd_ghost_cutoff() on each
  * side, normally with periodic = {0,0,0} (the ghosts carry the images).
  * Once per step, between the CV passes and the bias, the library calls
- * fn(buf, count, user) with this rank's totals (unit sums, S(k) sums, an
- * overflow flag; count is the same on every rank); fn must replace buf with
+ * fn(buf, count, user) with this rank's totals (unit sums, S(k) sums, a
+ * neighbour-overflow flag and a non-finite-position flag; count is the same
+ * on every rank); fn must replace buf with
  * the element-wise sum over all ranks, the same bits on every rank
  * (MPI_Allreduce(MPI_IN_PLACE, buf, count, MPI_DOUBLE, MPI_SUM, world)), and
  * return 0.  Every rank then holds the same CVs, deposits the same hill and
@@ -232,7 +233,9 @@ int mtd_needs_types(const mtd_ctx *ctx);
  * forces written to f cover all n rows: a ghost row holds the bias force of
  * this rank's centres on that image, which the caller adds to the owning
  * atom (LAMMPS reverse communication).  The virial is this rank's share.  A
- * neighbour overflow on any rank makes every rank retry the step together.
+ * neighbour overflow on any rank makes every rank retry the step together; a
+ * NaN or Inf position on any rank makes every rank skip the deposit and the
+ * bias force and return MTD_ERR_NAN, so the ranks stay in step.
  * Call before the first step; mtd_set_nlocal updates nlocal when atoms
  * migrate.  Needs the grid bias (not the hill-list bias).
  * Replaces the per-rank reductions of the reference's CVs under LAMMPS's
@@ -275,15 +278,14 @@ mtd_status mtd_nn_state(const mtd_ctx *ctx, int *hills, int *hills_fitted, int *
 int mtd_abi_version(void);
 
 /* k-vector structure factor of a group, computed with NO device allocation.
- * No counterpart in the reference (its structure factor lives in
- * Stru_factor, src/cvs/CVs_Strufactor.cu, and allocates per call); this is an
+ * This entry point has no counterpart in the reference.  It is an
  * allocation-free variant of the STRU_FACTOR_K unit of a context:
  *   rho(k) = sum_{i in group} exp(i k.x_i),   S = sum_k |rho(k)|^2 / (N K).
  * For callers that cannot allocate device memory at the point of the call:
  * an MD engine that computes this CV between its own kernels on several
  * streams (cudaMalloc / cudaFree synchronise the device and would serialise
  * them) or that runs with all device memory reserved up front by its own pool.
- *   n, d_x      atoms, device FP64 AoS n*3 (caller order)
+ *   n, d_x      0 <= n <= INT_MAX atoms, device FP64 AoS n*3 (caller order)
  *   d_mask      device group bitmask per atom, NULL = every atom; groupbit as in mtd_options
  *   nk, d_k     1 <= nk <= 1024 k-vectors, device FP64 AoS nk*3
  *   precision   MTD_PREC_FP64, or MTD_PREC_MIXED: FP32 sincos of the reduced FP64 phase
@@ -419,6 +421,23 @@ mtd_status mtd_nnbias_eval_device(mtd_nnbias *nb, int npts, const double *d_pts,
  * W2[128][128], b2[128], w3[128], b3), the output scale, and one gradient of
  * the mean squared error sum_i (V_theta(s_i)/vscale - t_i/vscale)^2 / npts on
  * given points and targets, without an update. */
+/* Waits for the object's stream and reports MTD_ERR_TIMEOUT when a network
+ * tile enqueued since the last check (mtd_nnbias_eval_device) gave up a
+ * tensor-core wait; work enqueued on another stream must have completed
+ * first (synchronise that stream).  Clears the flag. */
+mtd_status mtd_nnbias_sync(mtd_nnbias *nb);
+
+/* Diagnostics of the tensor-core waits of the network's tile kernel: every
+ * mbarrier wait polls at most `tries` times (0: the default, 2^20) before the
+ * tile gives up -- it issues no further MMA, waits once more with the same
+ * limit for the batch in flight, releases its tensor memory and the call
+ * returns MTD_ERR_TIMEOUT.  stall = 1 makes every tile, after its first
+ * tensor-core batch has completed, wait on a barrier phase that nothing
+ * completes, so the next batched call takes that path (a check of it that
+ * leaves no work in flight); stall = 0 restores normal operation.  No
+ * counterpart in the reference. */
+mtd_status mtd_nnbias_set_wait(mtd_nnbias *nb, int tries, int stall);
+
 mtd_status mtd_nnbias_get_params(mtd_nnbias *nb, float *out);
 mtd_status mtd_nnbias_set_params(mtd_nnbias *nb, const float *in, double vscale);
 double mtd_nnbias_vscale(const mtd_nnbias *nb);

@@ -734,11 +734,14 @@ __global__ void __launch_bounds__(256) k_unit_sums(const BiasPlan *__restrict__ 
         if (threadIdx.x == 0) out[off + 2 * U.K] = *U.sk_n;
         off += 2 * U.K + 1;
     }
-    if (threadIdx.x == 0) out[off] = P.status ? (double)P.status->overflow : 0.0;
+    if (threadIdx.x == 0) {
+        out[off] = P.status ? (double)P.status->overflow : 0.0;
+        out[off + 1] = P.status ? (double)P.status->bad_pos : 0.0;
+    }
 }
 
 int unit_sums_count(const BiasPlan &P) {
-    int c = 8 * P.nunit + 1;   // + the neighbour-overflow flag
+    int c = 8 * P.nunit + 2;   // + the neighbour-overflow and non-finite-position flags
     for (int u = 0; u < P.nunit; ++u)
         if (P.unit[u].rho) c += 2 * P.unit[u].K + 1;
     return c;
@@ -750,10 +753,15 @@ void launch_unit_sums(const BiasPlan *d_plan, double *out, cudaStream_t st) {
 }
 
 // Domain decomposition with a device-side allreduce: the summed overflow
-// counts of all ranks mark this rank's step failed too (flag 1: nothing to grow).
+// counts of all ranks mark this rank's step failed too (flag 1: nothing to
+// grow), and so does a non-finite position on any rank (no rank deposits,
+// every rank reports it).  gflag[0]: overflow sum, gflag[1]: bad-position sum.
 __global__ void k_domain_flag(const double *gflag, DevStatus *status) {
     pdl_entry();
-    if (threadIdx.x == 0 && *gflag != 0.0 && status->overflow == 0u) status->overflow = 1u;
+    if (threadIdx.x == 0) {
+        if (gflag[0] != 0.0 && status->overflow == 0u) status->overflow = 1u;
+        if (gflag[1] != 0.0) status->bad_pos = 1u;
+    }
 }
 
 void launch_domain_flag(const double *gflag, DevStatus *status, cudaStream_t st) {

@@ -1,6 +1,7 @@
 // context.cu -- the C ABI of libmetad_b200.so: context set-up from the
 // `fix metad` arguments, device memory, the per-step launch sequence and the
-// HILLS / rec.log files.
+// collection of each step's outputs (the other parts of the context live in
+// decomp.cu, hills.cu, autotune.cu, peratom.cu and walkers.cu; context.h).
 //
 // Per step (one CUDA stream, no host synchronisation inside the step):
 //   cells -> neighbour lists (one per distinct environment) -> CV value
@@ -8,204 +9,7 @@
 //   kernels (f_out = f_in - dV/dx) -> virial reduction.
 // This is FixMetadynamics::post_force (src/core/fix_crystallize.cu:386-472)
 // without its host loops, PCIe round trips and per-call synchronisations.
-#include "../../include/metad_b200.h"
-
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <deque>
-#include <map>
-#include <string>
-#include <vector>
-
-#include "args.h"
-#include "expr.h"
-#include "kernels.h"
-#include "nnbias.h"
-
-using namespace mtd;
-
-namespace {
-
-enum EnvKind { ENV_Q = 0, ENV_L = 1, ENV_R = 2 };
-
-struct Env {
-    int kind = ENV_R;
-    double rc = 0;
-    int cap = 0;
-    SwParams sw{};
-    double eps = 0;
-    int M = 0;
-    int cap_n = 0;
-    int *list = nullptr;
-    int *count = nullptr;
-    double *key_r2 = nullptr;
-    int *key_id = nullptr;
-    int *nkept = nullptr;
-    std::vector<int> cals;
-};
-
-struct Unit {
-    int kind = 0;                 // CalKind
-    std::vector<std::string> calnames;
-    int env = -1;
-    int LA = 0, LB = 0;
-    int groupbit = 1;
-    SwParams sw_r{}, sw_cvA{}, sw_cvB{};
-    std::vector<SwParams> qsw;
-    std::vector<std::string> qswnames;
-    double rc = 0, qf = 0;
-    SwParams sf_sw{};
-    bool dsig = false;
-    bool used = false;
-    int cap_n = 0;
-    void *q = nullptr, *nf = nullptr, *lq = nullptr, *lqs = nullptr, *e12 = nullptr, *lam = nullptr, *g = nullptr,
-         *tu = nullptr, *Q = nullptr, *S = nullptr;
-    double *partials = nullptr;
-    int nblocks = 0;
-    double *coef = nullptr;
-    int K = 0;
-    double *kvec = nullptr, *rho = nullptr, *skn = nullptr;
-    // STRU_FACTOR Chemical: type-weight parameters, the table built from the
-    // types of mtd_set_types, and the per-atom weights (sorted order)
-    bool chem = false, wchem = false;
-    double chem_ctarget = 0.0, chem_sigma = 1.0;
-    std::vector<std::pair<int, double>> chem_map;
-    double *d_wtab = nullptr;
-    int ntab = 0;
-    void *w = nullptr;
-};
-
-template <typename P> cudaError_t dalloc(P **p, size_t bytes) {
-    *p = nullptr;
-    return cudaMalloc((void **)p, bytes < 16 ? 16 : bytes);
-}
-template <typename P> void dfree(P *&p) {
-    if (p) cudaFree((void *)p);
-    p = nullptr;
-}
-
-}  // namespace
-
-constexpr int kOutSlots = 4;
-struct OutSlot {
-    double out[64];
-    DevStatus status;
-    unsigned long long nhills;
-    double vir[8];
-};
-struct PendingOut {
-    int slot;
-    long long step;
-    bool virial;
-};
-
-struct mtd_ctx {
-    int fp64 = 0;
-    int device = 0;
-    double boltz = 8.617343e-5;
-    GroupTable groups;
-    std::string hills_path = "HILLS";
-    std::string work_dir;
-    Config cfg;
-    std::vector<std::string> symnames;
-    std::vector<std::vector<ExprInstr>> code;
-    cudaStream_t st = nullptr;
-    bool box_set = false;
-    double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
-    int periodic[3] = {1, 1, 1};
-    bool initialized = false;
-    int n = 0, npad = 0, cap_n = 0, n_plan = -1;
-    double *d_x = nullptr, *d_fin = nullptr, *d_fout = nullptr;
-    int *d_mask = nullptr, *d_image = nullptr;
-    int *cellof = nullptr, *slot = nullptr, *perm = nullptr, *smask = nullptr, *arrival = nullptr;
-    double *xs = nullptr;
-    float4 *pf = nullptr;
-    int *count = nullptr, *start = nullptr;
-    int cap_cell = 0;
-    std::vector<Env> envs;
-    std::vector<Unit> units;
-    BiasPlan plan{};
-    BiasPlan *d_plan = nullptr;
-    bool plan_dirty = true;
-    double *d_grid = nullptr;
-    long long grid_size = 0;
-    HillRec *d_hills = nullptr;
-    unsigned long long *d_nhills = nullptr;
-    double *d_out = nullptr;
-    DevStatus *d_status = nullptr;
-    double *d_vpart = nullptr;
-    int cap_vpart = 0;
-    double *d_vir = nullptr;
-    // Pinned outputs of a step.  A context owns kOutSlots of them: the device
-    // path writes step t into slot t mod kOutSlots and collects it once its
-    // event has completed, so the host never waits for the step it just
-    // enqueued; h_out / h_status / h_vir / h_nhills point at the slot in use.
-    OutSlot *h_slots = nullptr;
-    cudaEvent_t slot_ev[kOutSlots] = {};
-    bool ring = true;                    // false for walkers (fixed slot 0, captured in their graph)
-    int slot_next = 0;
-    std::deque<PendingOut> fifo;         // steps enqueued and not yet collected, oldest first
-    unsigned overflow_seen = 0;          // largest neighbour count of an overflowed step drained since mtd_sync
-    double *h_out = nullptr;
-    DevStatus *h_status = nullptr;
-    double *h_vir = nullptr;
-    HillRec *h_hills = nullptr;
-    unsigned long long *h_nhills = nullptr;
-    unsigned long long hills_written = 0;
-    std::vector<double> cv;
-    double bias = 0.0;
-    double virial[6] = {0, 0, 0, 0, 0, 0};
-    FILE *f_hills = nullptr;
-    FILE *f_rec = nullptr;
-    std::string err;
-    int launches = 0;
-    bool want_virial = false;
-    bool pending = false;
-    long long pending_step = 0;
-    CellGrid last_grid{};
-    SysDev last_sys{};
-    cudaStream_t own_st = nullptr;
-    cudaStream_t side_st = nullptr;      // host -> device force upload beside the CV passes
-    // hill-list bias (CV_dim 4 or NN_BIAS 1): hills, exact sum, learned bias
-    mtd_nnbias *nb = nullptr;
-    double *d_vdv = nullptr;             // V, dV/ds at this step's s
-    WalkState *d_ws1 = nullptr;          // CV values, chain factors and block-sum totals of the last step
-    int h_fit = 0;                       // hills the network was fitted on
-    bool nn_usable = false;
-    cudaEvent_t f_ready = nullptr;
-    // atom types (caller order) for STRU_FACTOR Chemical, from mtd_set_types
-    int *d_types = nullptr;
-    int types_cap = 0, types_n = -1;
-    // kernel shapes chosen by mtd_autotune (every choice gives bitwise-identical results)
-    int tune_nbr = 0;                    // neighbour search: 0 fast/256, 1 fast/128, 2 flat/128
-    int tune_q = 0, tune_l = 0;          // threads per block of the q and lambda passes (0: 256)
-    // per-atom dCV/dx export (compute metad/atom): last step's inputs, cached result
-    const double *last_x = nullptr;
-    const int *last_mask = nullptr;
-    long long step_gen = 0;              // steps enqueued so far
-    long long dcv_gen = -1;              // step the cached dCV/dx belongs to
-    std::string dcv_cal;
-    std::vector<double> h_dcv;           // [n][3], caller order
-    double *d_dcv = nullptr;             // [2][cap][3]: zero input, gradient output
-    int dcv_cap = 0;
-    Prof prof;
-    bool prof_created = false;
-    std::map<std::string, std::pair<long long, double>> prof_total;
-    // domain decomposition (mtd_set_domain): caller indices from nown on are ghosts
-    int nown = -1;                       // -1: off, every atom is owned
-    int dom_rank = 0;
-    mtd_allreduce_fn dom_fn = nullptr;
-    mtd_allreduce_device_fn dom_dev_fn = nullptr;   // stream-ordered variant (no host round trip)
-    void *dom_user = nullptr;
-    double *d_xchg = nullptr;            // this rank's unit totals, then the totals over all ranks
-    double *h_xchg = nullptr;            // pinned staging of the same
-    int xchg_n = 0;
-    // two-call step (mtd_set_positions_f64, then mtd_step)
-    int staged_n = -1;                   // atoms uploaded and not yet stepped (-1: none)
-    bool staged_mask = false;
-    int fix_groupbit = 1;
-};
+#include "context.h"
 
 namespace {
 thread_local Prof *g_prof = nullptr;
@@ -225,9 +29,8 @@ void prof_mark(const char *name, cudaStream_t st) {
 }
 }  // namespace mtd
 
-namespace {
-
-constexpr int kHillCap = 4096;
+namespace mtd {
+namespace ctx {
 
 mtd_status fail(mtd_ctx *c, mtd_status s, const std::string &m) {
     if (c) c->err = m;
@@ -239,12 +42,6 @@ mtd_status cuda_check(mtd_ctx *c, cudaError_t e, const char *what) {
     if (e == cudaErrorMemoryAllocation) return fail(c, MTD_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
     return fail(c, MTD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-#define MTD_CU(expr, what)                                        \
-    do {                                                          \
-        mtd_status _s = cuda_check(c, (expr), what);              \
-        if (_s != MTD_OK) return _s;                              \
-    } while (0)
 
 size_t real_size(const mtd_ctx *c) { return c->fp64 ? sizeof(double) : sizeof(float); }
 
@@ -800,22 +597,6 @@ void prof_collect(mtd_ctx *c) {
     p.n = 0;
 }
 
-// The step's kernels use programmatic dependent launch (kernels.h).
-struct PdlScope {
-    PdlScope() { pdl_set(true); }
-    ~PdlScope() { pdl_set(false); }
-};
-
-struct ProfScope {
-    explicit ProfScope(mtd_ctx *c) {
-        if (c->prof.on) {
-            if (c->prof.n > kProfMax - 64) prof_collect(c);
-            prof_set(&c->prof);
-            prof_mark("start", c->st);
-        }
-    }
-    ~ProfScope() { prof_set(nullptr); }
-};
 
 // Stage 1 of a step: capacity, plan, cell list, neighbour lists, CV values.
 mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, const int *image) {
@@ -895,53 +676,10 @@ mtd_status enqueue_forces(mtd_ctx *c, long long step, const double *x, const int
     return MTD_OK;
 }
 
-// Domain decomposition, between the CV passes and the bias kernel: this
-// rank's unit totals (and S(k) sums, and its neighbour-overflow flag) go to
-// the caller's allreduce; the totals over all ranks come back for the bias
-// kernel (P.gsum) and the S(k) arrays.  A step that overflowed on any rank
-// counts as overflowed on every rank, so all ranks skip the deposit and, in
-// mtd_post_force, retry together.
-mtd_status exchange_totals(mtd_ctx *c) {
-    const int cnt = c->xchg_n;
-    launch_unit_sums(c->d_plan, c->d_xchg, c->st);
-    c->launches += 1;
-    if (c->dom_dev_fn) {   // the caller enqueues the sum over ranks on the step's stream
-        if (c->dom_dev_fn(c->d_xchg, cnt, (void *)c->st, c->dom_user) != 0)
-            return fail(c, MTD_ERR_INVALID_ARG, "domain decomposition: the device allreduce callback failed");
-        MTD_CU(cudaGetLastError(), "domain allreduce");
-        int off = 8 * (int)c->units.size();
-        for (Unit &u : c->units) {
-            if (u.kind != CAL_STRU_FACTOR_K) continue;
-            MTD_CU(cudaMemcpyAsync(u.rho, c->d_xchg + off, sizeof(double) * 2 * u.K, cudaMemcpyDeviceToDevice, c->st), "rho(k)");
-            MTD_CU(cudaMemcpyAsync(u.skn, c->d_xchg + off + 2 * u.K, sizeof(double), cudaMemcpyDeviceToDevice, c->st), "rho(k)");
-            off += 2 * u.K + 1;
-        }
-        launch_domain_flag(c->d_xchg + cnt - 1, c->d_status, c->st);   // any rank overflowed: every rank retries
-        c->launches += 1;
-        return MTD_OK;
-    }
-    MTD_CU(cudaMemcpyAsync(c->h_xchg, c->d_xchg, sizeof(double) * cnt, cudaMemcpyDeviceToHost, c->st), "domain totals");
-    MTD_CU(cudaStreamSynchronize(c->st), "domain totals");
-    const double own_overflow = c->h_xchg[cnt - 1];
-    if (c->dom_fn(c->h_xchg, cnt, c->dom_user) != 0)
-        return fail(c, MTD_ERR_INVALID_ARG, "domain decomposition: the allreduce callback failed");
-    MTD_CU(cudaMemcpyAsync(c->d_xchg, c->h_xchg, sizeof(double) * cnt, cudaMemcpyHostToDevice, c->st), "domain totals");
-    int off = 8 * (int)c->units.size();
-    for (Unit &u : c->units) {
-        if (u.kind != CAL_STRU_FACTOR_K) continue;
-        MTD_CU(cudaMemcpyAsync(u.rho, c->d_xchg + off, sizeof(double) * 2 * u.K, cudaMemcpyDeviceToDevice, c->st), "rho(k)");
-        MTD_CU(cudaMemcpyAsync(u.skn, c->d_xchg + off + 2 * u.K, sizeof(double), cudaMemcpyDeviceToDevice, c->st), "rho(k)");
-        off += 2 * u.K + 1;
-    }
-    if (c->h_xchg[cnt - 1] != 0.0 && own_overflow == 0.0)   // another rank overflowed: a flag of 1 (no growth here)
-        MTD_CU(cudaMemsetAsync(&c->d_status->overflow, 1, 1, c->st), "status");
-    return MTD_OK;
-}
-
 // f_ready (may be null): an event the force kernels wait for (forces uploaded
 // on the side stream while the CV passes run).
 mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, const int *mask, const int *image,
-                        const double *fin, double *fout, bool virial, cudaEvent_t f_ready = nullptr) {
+                        const double *fin, double *fout, bool virial, cudaEvent_t f_ready) {
     ProfScope prof_scope(c);
     PdlScope pdl_scope;
     c->launches = 0;
@@ -963,39 +701,6 @@ mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, cons
     }
     if (f_ready) MTD_CU(cudaStreamWaitEvent(c->st, f_ready, 0), "force upload");
     return enqueue_forces(c, step, x, mask, fin, fout, virial);
-}
-
-void write_hill_line(mtd_ctx *c, const HillRec &h) {
-    if (!c->f_hills) return;
-    std::fprintf(c->f_hills, "%lld", h.step);   // GH_t0_uniformGrid.cu:211-220
-    for (int d = 0; d < c->cfg.cv_dim; ++d) std::fprintf(c->f_hills, " %.16g", h.s[d]);
-    std::fprintf(c->f_hills, " %.16g %.16g\n", h.w, h.sigma);
-    std::fflush(c->f_hills);
-}
-
-// Hill-list bias: new hills join the exact sum; every NN_REFIT hills the
-// network is refitted on the sum and validated against it (the exact sum, plus
-// the network when it passes, is what the next steps use).
-mtd_status list_add_hills(mtd_ctx *c, const std::vector<HillRec> &recs) {
-    const int D = c->cfg.cv_dim;
-    std::vector<double> cen, hgt, sig;
-    for (const HillRec &r : recs) {
-        for (int d = 0; d < D; ++d) cen.push_back(r.s[d]);
-        hgt.push_back(r.w);
-        sig.push_back(r.sigma);
-    }
-    if (!hgt.empty() && mtd_nnbias_add_hills(c->nb, (int)hgt.size(), cen.data(), hgt.data(), sig.data()) != MTD_OK)
-        return fail(c, MTD_ERR_CUDA, mtd_nnbias_last_error(c->nb));
-    const int nh = mtd_nnbias_num_hills(c->nb);
-    if (c->cfg.nn && nh - c->h_fit >= c->cfg.nn_refit) {
-        double loss = 0.0, mx = 0.0, rms = 0.0;
-        if (mtd_nnbias_fit(c->nb, 65536, c->cfg.nn_iters, 4096, 2e-3, 1000 + (unsigned long long)nh, &loss) != MTD_OK ||
-            mtd_nnbias_validate(c->nb, 16384, 7 + (unsigned long long)nh, c->cfg.nn_tol, &mx, &rms) != MTD_OK)
-            return fail(c, MTD_ERR_CUDA, mtd_nnbias_last_error(c->nb));
-        c->h_fit = nh;
-        c->nn_usable = mtd_nnbias_usable(c->nb) != 0;
-    }
-    return MTD_OK;
 }
 
 // Collects the outputs of the last enqueued step (stream already synchronised).
@@ -1073,65 +778,15 @@ mtd_status drain(mtd_ctx *c, bool block) {
     return MTD_OK;
 }
 
-std::string path_in(const mtd_ctx *c, const std::string &p) {
-    if (p.empty() || p[0] == '/' || c->work_dir.empty()) return p;
-    return c->work_dir + "/" + p;
-}
+template void run_values<float>(mtd_ctx *, const CellGrid &, const double *, const int *);
+template void run_values<double>(mtd_ctx *, const CellGrid &, const double *, const int *);
+template void run_forces<float>(mtd_ctx *, const SysDev &, const CellGrid &, const double *, const int *,
+                                const double *, double *, bool);
+template void run_forces<double>(mtd_ctx *, const SysDev &, const CellGrid &, const double *, const int *,
+                                 const double *, double *, bool);
 
-mtd_status replay_records(mtd_ctx *c, const std::vector<HillRec> &recs) {
-    if (recs.empty()) return MTD_OK;
-    if (c->nb) return list_add_hills(c, recs);
-    HillRec *d = nullptr;
-    MTD_CU(dalloc(&d, sizeof(HillRec) * recs.size()), "replay");
-    cudaMemcpy(d, recs.data(), sizeof(HillRec) * recs.size(), cudaMemcpyHostToDevice);
-    if (c->plan_dirty) {
-        build_plan(c);
-        cudaMemcpy(c->d_plan, &c->plan, sizeof(BiasPlan), cudaMemcpyHostToDevice);
-        c->plan_dirty = false;
-    }
-    launch_hills_replay(c->d_plan, d, (int)recs.size(), (int)c->grid_size, c->st);
-    cudaError_t e = cudaStreamSynchronize(c->st);
-    cudaFree(d);
-    return cuda_check(c, e, "HILLS replay");
-}
-
-// HILLS rows `step cv[D] height sigma`; '#' and blank lines skipped
-// (GH_t0_uniformGrid.cu:101-192 on one rank).
-mtd_status read_hills(mtd_ctx *c, const std::string &path, std::vector<HillRec> &recs, bool *exists) {
-    FILE *f = std::fopen(path.c_str(), "r");
-    if (exists) *exists = f != nullptr;
-    if (!f) return MTD_OK;
-    char line[1024];
-    const int D = c->cfg.cv_dim;
-    while (std::fgets(line, sizeof(line), f)) {
-        if (line[0] == '#' || line[0] == '\n' || line[0] == '\r') continue;
-        char *p = line, *e = nullptr;
-        HillRec r{};
-        r.step = std::strtoll(p, &e, 10);
-        if (e == p) continue;
-        p = e;
-        bool ok = true;
-        for (int d = 0; d < D; ++d) {
-            r.s[d] = std::strtod(p, &e);
-            ok = ok && e != p;
-            p = e;
-        }
-        r.w = std::strtod(p, &e);
-        ok = ok && e != p;
-        p = e;
-        r.sigma = std::strtod(p, &e);
-        ok = ok && e != p;
-        if (!ok) {
-            std::fclose(f);
-            return fail(c, MTD_ERR_IO, "malformed HILLS line: " + std::string(line));
-        }
-        recs.push_back(r);
-    }
-    std::fclose(f);
-    return MTD_OK;
-}
-
-}  // namespace
+}  // namespace ctx
+}  // namespace mtd
 
 extern "C" {
 
@@ -1337,6 +992,19 @@ mtd_status mtd_init(mtd_ctx *c) {
         bool exists = false;
         mtd_status s = read_hills(c, hp, recs, &exists);
         if (s != MTD_OK) return s;
+        // an empty file counts as absent: it is rewritten with the header
+        // (the reference restarts only from a file of non-zero size,
+        // GH_t0_uniformGrid.cu:118, :175-181)
+        if (exists) {
+            FILE *f = std::fopen(hp.c_str(), "rb");
+            long size = 0;
+            if (f) {
+                std::fseek(f, 0, SEEK_END);
+                size = std::ftell(f);
+                std::fclose(f);
+            }
+            exists = size > 0;
+        }
         if (exists) {
             s = replay_records(c, recs);
             if (s != MTD_OK) return s;
@@ -1469,11 +1137,6 @@ mtd_status mtd_step(mtd_ctx *c, int64_t step, double *f_inout, double *cv_out, d
     return MTD_OK;
 }
 
-mtd_status mtd_get_peratom(mtd_ctx *c, const char *key, double *out) {
-    if (!c) return MTD_ERR_INVALID_ARG;
-    return mtd_extract_peratom(c, key, out, c->n);
-}
-
 mtd_status mtd_create_from_config(const mtd_config *cfg, mtd_ctx **out) {
     if (!cfg || !out) return MTD_ERR_INVALID_ARG;
     return mtd_create(cfg->narg, cfg->arg, &cfg->opt, out);
@@ -1519,140 +1182,6 @@ mtd_status mtd_sync(mtd_ctx *c) {
     return collect(c);
 }
 
-namespace {
-
-// Grows every list that a step reported too small (as mtd_sync does).
-void grow_lists(mtd_ctx *c, unsigned need) {
-    for (Env &e : c->envs)
-        if (e.M < (int)need) {
-            e.M = (((int)need + 8) + 3) & ~3;
-            alloc_env(c, e, c->cap_n);
-        }
-}
-
-// The tuning passes of one idle context: a values pass on the given
-// positions (lists grown until they fit), then each interchangeable kernel
-// shape timed over `reps` launches with CUDA events on the context stream,
-// the fastest kept.  The passes write only scratch (lists, per-atom records,
-// d_fout); no step is recorded, no hill deposited.
-mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask, int reps, int *choice) {
-    const bool prof = c->prof.on;
-    c->prof.on = false;
-    mtd_status s = MTD_OK;
-    for (int attempt = 0;; ++attempt) {
-        MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
-        s = enqueue_values(c, n, d_x, d_mask, nullptr);
-        if (s != MTD_OK) break;
-        DevStatus hs{};
-        MTD_CU(cudaMemcpyAsync(&hs, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->st), "status");
-        MTD_CU(cudaStreamSynchronize(c->st), "autotune");
-        if (hs.overflow == 0) break;
-        if (attempt == 3) {
-            s = fail(c, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded");
-            break;
-        }
-        grow_lists(c, hs.overflow);
-    }
-    if (s != MTD_OK) {
-        c->prof.on = prof;
-        return s;
-    }
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    MTD_CU(cudaEventCreate(&e0), "autotune");
-    MTD_CU(cudaEventCreate(&e1), "autotune");
-    auto timed = [&](auto &&fn) {
-        fn();
-        cudaEventRecord(e0, c->st);
-        for (int r = 0; r < reps; ++r) fn();
-        cudaEventRecord(e1, c->st);
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        return ms;
-    };
-    const CellGrid g = c->last_grid;
-    const SysDev sd = c->last_sys;
-    float best = 1e30f;
-    for (int v = 0; v < 3; ++v) {
-        const float t = timed([&] {
-            for (Env &e : c->envs) {
-                NeighSpec ns = neigh_spec(e);
-                ns.variant = v;
-                launch_neighbors(g, sd, ns, env_dev(e), c->d_status, c->st);
-            }
-        });
-        if (t < best) {
-            best = t;
-            c->tune_nbr = v;
-        }
-    }
-    const int shapes[2] = {256, 128};
-    best = 1e30f;
-    int bq = 256;
-    for (int qb : shapes) {
-        c->tune_q = qb;
-        const float t = timed([&] {
-            if (c->fp64) run_values<double>(c, g, d_x, d_mask);
-            else run_values<float>(c, g, d_x, d_mask);
-        });
-        if (t < best) {
-            best = t;
-            bq = qb;
-        }
-    }
-    c->tune_q = bq;
-    best = 1e30f;
-    int bl = 256;
-    for (int lb : shapes) {
-        c->tune_l = lb;
-        const float t = timed([&] {
-            if (c->fp64) run_forces<double>(c, sd, g, d_x, d_mask, c->d_fin, c->d_fout, false);
-            else run_forces<float>(c, sd, g, d_x, d_mask, c->d_fin, c->d_fout, false);
-        });
-        if (t < best) {
-            best = t;
-            bl = lb;
-        }
-    }
-    c->tune_l = bl;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
-    MTD_CU(cudaStreamSynchronize(c->st), "autotune");
-    c->prof.on = prof;
-    if (choice) {
-        choice[0] = c->tune_nbr;
-        choice[1] = c->tune_q;
-        choice[2] = c->tune_l;
-    }
-    return MTD_OK;
-}
-
-}  // namespace
-
-mtd_status mtd_autotune(mtd_ctx *c, int n, const double *d_x, const int *d_mask, int reps, int choice[3]) {
-    if (!c || n < 1 || !d_x || reps < 1) return MTD_ERR_INVALID_ARG;
-    if (!c->initialized) {
-        const mtd_status s = mtd_init(c);
-        if (s != MTD_OK) return s;
-    }
-    if (!c->box_set) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_box must be called before mtd_autotune");
-    const mtd_status s = mtd_sync(c);
-    if (s != MTD_OK) return s;
-    return autotune_idle(c, n, d_x, d_mask, reps, choice);
-}
-
-mtd_status mtd_set_tuning(mtd_ctx *c, int neighbor_shape, int q_block, int lambda_block) {
-    if (!c || neighbor_shape < 0 || neighbor_shape > 2) return MTD_ERR_INVALID_ARG;
-    if ((q_block != 0 && q_block != 128 && q_block != 256) || (lambda_block != 0 && lambda_block != 128 &&
-                                                               lambda_block != 256))
-        return MTD_ERR_INVALID_ARG;
-    c->tune_nbr = neighbor_shape;
-    c->tune_q = q_block;
-    c->tune_l = lambda_block;
-    return MTD_OK;
-}
-
 double mtd_compute_scalar(const mtd_ctx *c) { return c ? c->bias : 0.0; }
 
 double mtd_compute_vector(const mtd_ctx *c, int k) {
@@ -1661,110 +1190,6 @@ double mtd_compute_vector(const mtd_ctx *c, int k) {
 }
 
 int mtd_cv_dim(const mtd_ctx *c) { return c ? c->cfg.cv_dim : 0; }
-
-// dCV/dx of CAL `cal` at the last step's positions, into c->h_dcv ([n][3],
-// caller order). The CV is the one the first SYMBOL on that CAL selects; the
-// force kernels run once more with chain factor 1 on that symbol, 0 on the
-// others and a zero input force, so their output is -dCV/dx (the exact
-// gradient, every neighbour term included). Cached per step and CAL, as
-// STEIN_QL::get_peratom_ptr caches per timestep (src/cvs/CVs_Steinhardt.cu:1278-1321).
-static mtd_status dcvdx(mtd_ctx *c, const std::string &cal) {
-    if (c->step_gen == 0) return fail(c, MTD_ERR_INVALID_ARG, "no step has run");
-    if (c->dcv_gen == c->step_gen && c->dcv_cal == cal) return MTD_OK;
-    int sym = -1;
-    for (size_t q = 0; q < c->cfg.symbols.size() && sym < 0; ++q)
-        if (c->cfg.symbols[q].cal == cal) sym = (int)q;
-    if (sym < 0) return fail(c, MTD_ERR_INVALID_ARG, "dcvdx: no SYMBOL uses CAL " + cal);
-    const int n = c->n;
-    if (n > c->dcv_cap) {
-        dfree(c->d_dcv);
-        c->dcv_cap = 0;
-        MTD_CU(dalloc(&c->d_dcv, sizeof(double) * 6 * (size_t)n), "dcvdx buffers");
-        c->dcv_cap = n;
-    }
-    double *zero = c->d_dcv, *grad = c->d_dcv + 3 * (size_t)c->dcv_cap;
-    MTD_CU(cudaMemsetAsync(zero, 0, sizeof(double) * 3 * (size_t)n, c->st), "dcvdx");
-    const int launches = c->launches;
-    launch_symbol_coef(c->d_plan, sym, c->d_ws1, c->st);
-    if (c->fp64) run_forces<double>(c, c->last_sys, c->last_grid, c->last_x, c->last_mask, zero, grad, false);
-    else run_forces<float>(c, c->last_sys, c->last_grid, c->last_x, c->last_mask, zero, grad, false);
-    c->launches = launches;
-    MTD_CU(cudaGetLastError(), "kernel launch");
-    c->h_dcv.resize(3 * (size_t)n);
-    MTD_CU(cudaMemcpyAsync(c->h_dcv.data(), grad, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->st),
-           "dcvdx");
-    MTD_CU(cudaStreamSynchronize(c->st), "dcvdx");
-    for (double &v : c->h_dcv) v = -v;
-    c->dcv_gen = c->step_gen;
-    c->dcv_cal = cal;
-    return MTD_OK;
-}
-
-mtd_status mtd_extract_peratom(mtd_ctx *c, const char *key, double *out, int n) {
-    if (!c || !key || !out) return MTD_ERR_INVALID_ARG;
-    std::string k(key);
-    if (k.rfind("colvar_peratom:", 0) == 0) k = k.substr(15);
-    size_t dot = k.find('.');
-    if (dot == std::string::npos) return fail(c, MTD_ERR_INVALID_ARG, "key must be <CAL>.<prop>");
-    const std::string cal = k.substr(0, dot), prop = k.substr(dot + 1);
-    if (n != c->n) return fail(c, MTD_ERR_INVALID_ARG, "atom count differs from the last step");
-    MTD_CU(cudaStreamSynchronize(c->st), "extract");
-    if (prop == "dcvdx_x" || prop == "dcvdx_y" || prop == "dcvdx_z") {
-        mtd_status s = dcvdx(c, cal);
-        if (s != MTD_OK) return s;
-        const int a = prop.back() - 'x';
-        for (int t = 0; t < n; ++t) out[t] = c->h_dcv[3 * (size_t)t + a];
-        return MTD_OK;
-    }
-    for (Unit &u : c->units) {
-        for (size_t slot = 0; slot < u.calnames.size(); ++slot) {
-            if (u.calnames[slot] != cal) continue;
-            std::vector<int> perm(n);
-            MTD_CU(cudaMemcpy(perm.data(), c->perm, sizeof(int) * n, cudaMemcpyDeviceToHost), "perm");
-            std::vector<double> v(n, 0.0);
-            const size_t R = real_size(c);
-            std::vector<unsigned char> raw;
-            int stride = 1, off = 0;
-            const void *src = nullptr;
-            if (prop == "stein_q" && u.kind == CAL_STEINH_Q) { src = u.Q; }
-            else if (prop == "stein_q" && u.kind == CAL_STEINH_L) { src = u.lqs; stride = 2; off = (int)slot; }
-            else if (prop == "stru_f" && u.kind == CAL_STRU_FACTOR && !u.wchem) { src = u.S; }
-            else if (prop == "chem_pair_r" && u.kind == CAL_STRU_FACTOR && u.wchem) { src = u.S; }
-            else return fail(c, MTD_ERR_INVALID_ARG, "unknown per-atom property " + prop + " for CAL " + cal);
-            raw.resize(R * stride * (size_t)n);
-            MTD_CU(cudaMemcpy(raw.data(), src, R * stride * (size_t)n, cudaMemcpyDeviceToHost), "extract");
-            for (int t = 0; t < n; ++t) {
-                double val = c->fp64 ? ((const double *)raw.data())[t * stride + off]
-                                     : (double)((const float *)raw.data())[t * stride + off];
-                out[perm[t]] = val;
-            }
-            return MTD_OK;
-        }
-    }
-    return fail(c, MTD_ERR_INVALID_ARG, "unknown CAL " + cal);
-}
-
-mtd_status mtd_hills_replay(mtd_ctx *c, const char *path) {
-    if (!c || !path) return MTD_ERR_INVALID_ARG;
-    if (!c->initialized) {
-        mtd_status s = mtd_init(c);
-        if (s != MTD_OK) return s;
-    }
-    std::vector<HillRec> recs;
-    bool exists = false;
-    mtd_status s = read_hills(c, path_in(c, path), recs, &exists);
-    if (s != MTD_OK) return s;
-    if (!exists) return fail(c, MTD_ERR_IO, std::string("cannot open ") + path);
-    return replay_records(c, recs);
-}
-
-mtd_status mtd_get_grid(mtd_ctx *c, double *out, int64_t count) {
-    if (!c || !out) return MTD_ERR_INVALID_ARG;
-    if (!c->initialized || count != c->grid_size) return fail(c, MTD_ERR_INVALID_ARG, "grid not allocated or size mismatch");
-    MTD_CU(cudaStreamSynchronize(c->st), "grid");
-    MTD_CU(cudaMemcpy(out, c->d_grid, sizeof(double) * (size_t)count, cudaMemcpyDeviceToHost), "grid");
-    return MTD_OK;
-}
 
 int mtd_last_launch_count(const mtd_ctx *c) { return c ? c->launches : 0; }
 
@@ -1804,531 +1229,6 @@ int mtd_profile_report(mtd_ctx *c, char *buf, int len) {
     return (int)s.size() + 1;
 }
 
-mtd_status mtd_set_types(mtd_ctx *c, int n, const int *types) {
-    if (!c || n < 0 || (n > 0 && !types)) return MTD_ERR_INVALID_ARG;
-    if (n > c->types_cap) {
-        dfree(c->d_types);
-        c->types_cap = 0;
-        MTD_CU(dalloc(&c->d_types, sizeof(int) * (size_t)(n + n / 4 + 1)), "atom types");
-        c->types_cap = n + n / 4 + 1;
-    }
-    int maxt = 0;
-    for (int i = 0; i < n; ++i) {
-        if (types[i] < 0) return fail(c, MTD_ERR_INVALID_ARG, "atom types must be >= 0");
-        maxt = std::max(maxt, types[i]);
-    }
-    MTD_CU(cudaStreamSynchronize(c->st), "atom types");   // no step in flight reads the old types
-    if (n > 0) MTD_CU(cudaMemcpy(c->d_types, types, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice), "atom types");
-    // type-weight tables (Stru_fact_chem_env constructor, src/cvs/CVs_Strufactor_chem.cu:33-55):
-    // Chem_map value, else a Gaussian in the type index around Chem_ctarget; type 0 weighs 0
-    for (Unit &u : c->units) {
-        if (!u.chem) continue;
-        std::vector<double> tab((size_t)maxt + 1);
-        for (int t = 0; t <= maxt; ++t) {
-            const double dt = t - u.chem_ctarget;
-            tab[t] = std::exp(-dt * dt / (2.0 * u.chem_sigma * u.chem_sigma));
-            for (const auto &kv : u.chem_map)
-                if (kv.first == t) tab[t] = kv.second;
-        }
-        tab[0] = 0.0;
-        if ((int)tab.size() > u.ntab) {
-            dfree(u.d_wtab);
-            u.ntab = 0;
-            MTD_CU(dalloc(&u.d_wtab, sizeof(double) * tab.size()), "type weights");
-        }
-        u.ntab = (int)tab.size();
-        MTD_CU(cudaMemcpy(u.d_wtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice), "type weights");
-    }
-    c->types_n = n;
-    return MTD_OK;
-}
-
-mtd_status mtd_set_domain(mtd_ctx *c, int nlocal, int rank, mtd_allreduce_fn fn, void *user) {
-    if (!c) return MTD_ERR_INVALID_ARG;
-    if (c->initialized)
-        return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_domain must be called before the first step");
-    if (nlocal < 0 || rank < 0 || !fn)
-        return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_domain needs nlocal >= 0, rank >= 0 and an allreduce callback");
-    if (c->cfg.hill_list())
-        return fail(c, MTD_ERR_UNSUPPORTED, "domain decomposition needs the grid bias (CV_dim 1-3, no NN_BIAS)");
-    c->nown = nlocal;
-    c->dom_rank = rank;
-    c->dom_fn = fn;
-    c->dom_user = user;
-    c->plan_dirty = true;
-    return MTD_OK;
-}
-
-mtd_status mtd_set_domain_device(mtd_ctx *c, int nlocal, int rank, mtd_allreduce_device_fn fn, void *user) {
-    if (!c || !fn) return MTD_ERR_INVALID_ARG;
-    const mtd_status s = mtd_set_domain(c, nlocal, rank, reinterpret_cast<mtd_allreduce_fn>(fn), user);
-    if (s != MTD_OK) return s;
-    c->dom_fn = nullptr;
-    c->dom_dev_fn = fn;
-    return MTD_OK;
-}
-
-mtd_status mtd_set_nlocal(mtd_ctx *c, int nlocal) {
-    if (!c || nlocal < 0) return MTD_ERR_INVALID_ARG;
-    if (c->nown < 0) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_nlocal: domain decomposition is not enabled");
-    c->nown = nlocal;
-    return MTD_OK;
-}
-
-double mtd_ghost_cutoff(const mtd_ctx *c) {
-    if (!c) return 0.0;
-    double g = 0.0;
-    for (const Env &e : c->envs) g = std::fmax(g, e.kind == ENV_L ? 2.0 * e.rc : e.rc);
-    return g;
-}
-
-int mtd_needs_types(const mtd_ctx *c) {
-    if (!c) return 0;
-    for (const Unit &u : c->units)
-        if (u.chem) return 1;
-    return 0;
-}
-
-int mtd_max_neighbors(mtd_ctx *c, const char *name) {
-    if (!c || !name) return -1;
-    for (Unit &u : c->units)
-        for (auto &cn : u.calnames)
-            if (cn == name && u.env >= 0) {
-                const Env &e = c->envs[u.env];
-                if (c->n == 0) return 0;
-                std::vector<int> cnt(c->n);
-                cudaStreamSynchronize(c->st);
-                if (cudaMemcpy(cnt.data(), e.count, sizeof(int) * c->n, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
-                int m = 0;
-                for (int v : cnt) m = v > m ? v : m;
-                return m;
-            }
-    return -1;
-}
-
 const char *mtd_last_error(const mtd_ctx *c) { return c ? c->err.c_str() : "null context"; }
-
-mtd_status mtd_nn_state(const mtd_ctx *c, int *hills, int *hills_fitted, int *usable) {
-    if (!c) return MTD_ERR_INVALID_ARG;
-    if (hills) *hills = c->nb ? mtd_nnbias_num_hills(c->nb) : 0;
-    if (hills_fitted) *hills_fitted = c->h_fit;
-    if (usable) *usable = c->nn_usable ? 1 : 0;
-    return MTD_OK;
-}
-
-}  // extern "C"
-
-// ------------------------------------------------------------------ multiple walkers
-// W contexts built from the same `fix metad` arguments share walker 0's bias
-// grid.  A step enqueues every walker's cell list, neighbour lists and CV
-// values on its own stream, joins them for the three multi-walker bias
-// kernels (WT heights from the grid at the start of the step, deposits in
-// walker order, per-walker V, dV/ds and force coefficients), and forks again
-// for the forces.  With the CUDA graph enabled the whole step is captured
-// once per (atom counts, array pointers) and replayed; the step number
-// travels through device memory.
-struct mtd_walkers {
-    std::vector<mtd_ctx *> w;
-    std::string err;
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_bias = nullptr;
-    std::vector<cudaEvent_t> ev_done;
-    BiasPlan **d_plans = nullptr;
-    WalkState *d_ws = nullptr;
-    long long *d_step = nullptr, *h_step = nullptr;
-    std::string hills_path = "HILLS";
-    FILE *f_hills = nullptr;
-    unsigned long long hills_written = 0;
-    bool initialized = false;
-    bool use_graph = false;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    std::vector<int> g_n;
-    std::vector<const double *> g_x;
-    std::vector<double *> g_f;
-    bool pending = false;
-    long long pending_step = 0;
-    int launches = 0;
-    // sharded over ranks (mtd_walkers_set_ranks*): this object's walkers are
-    // the global walkers rank * nwalk .. rank * nwalk + nwalk - 1
-    int rank = 0, nranks = 0;                 // nranks 0: not sharded
-    mtd_allgather_fn ag = nullptr;
-    mtd_allgather_device_fn ag_dev = nullptr;
-    void *ag_user = nullptr;
-    double *d_xloc = nullptr, *d_xall = nullptr;   // [nwalk][kWalkRec], [nranks * nwalk][kWalkRec]
-    double *h_xloc = nullptr, *h_xall = nullptr;   // pinned staging of the same
-};
-
-namespace {
-
-mtd_status wfail(mtd_walkers *W, mtd_status s, const std::string &m) {
-    W->err = m;
-    return s;
-}
-
-#define MTD_WCU(expr, what)                                                                          \
-    do {                                                                                             \
-        cudaError_t e_ = (expr);                                                                     \
-        if (e_ != cudaSuccess) return wfail(W, MTD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-void walkers_drop_graph(mtd_walkers *W) {
-    if (W->gexec) cudaGraphExecDestroy(W->gexec);
-    if (W->graph) cudaGraphDestroy(W->graph);
-    W->gexec = nullptr;
-    W->graph = nullptr;
-}
-
-// The step's work on the group stream and the walker streams.
-mtd_status walkers_enqueue(mtd_walkers *W, long long step, const int *n, const double *const *d_x,
-                           double *const *d_f) {
-    const int nw = (int)W->w.size();
-    PdlScope pdl_scope;   // each walker's kernel chain uses dependent launch (captured as programmatic edges)
-    MTD_WCU(cudaMemcpyAsync(W->d_step, W->h_step, sizeof(long long), cudaMemcpyHostToDevice, W->st), "step");
-    MTD_WCU(cudaEventRecord(W->ev_start, W->st), "fork");
-    W->launches = 3;
-    for (int k = 0; k < nw; ++k) {
-        mtd_ctx *c = W->w[k];
-        MTD_WCU(cudaStreamWaitEvent(c->st, W->ev_start, 0), "fork");
-        c->launches = 0;
-        mtd_status s = enqueue_values(c, n[k], d_x[k], nullptr, nullptr);
-        if (s != MTD_OK) return wfail(W, s, "walker " + std::to_string(k) + ": " + c->err);
-        MTD_WCU(cudaEventRecord(W->ev_done[k], c->st), "join");
-        MTD_WCU(cudaStreamWaitEvent(W->st, W->ev_done[k], 0), "join");
-    }
-    if (W->nranks > 0) {   // this rank's hills out, every rank's hills in, all deposited in global order
-        const int cnt = nw * kWalkRec, nall = W->nranks * nw;
-        launch_walk_cvs_pack(W->d_plans, nw, W->d_step, W->d_ws, W->d_xloc, W->st);
-        if (W->ag_dev) {
-            if (W->ag_dev(W->d_xloc, cnt, W->d_xall, (void *)W->st, W->ag_user) != 0)
-                return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks: the device allgather callback failed");
-            MTD_WCU(cudaGetLastError(), "walker allgather");
-        } else {
-            MTD_WCU(cudaMemcpyAsync(W->h_xloc, W->d_xloc, sizeof(double) * cnt, cudaMemcpyDeviceToHost, W->st), "hills out");
-            MTD_WCU(cudaStreamSynchronize(W->st), "hills out");
-            if (W->ag(W->h_xloc, cnt, W->h_xall, W->ag_user) != 0)
-                return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks: the allgather callback failed");
-            MTD_WCU(cudaMemcpyAsync(W->d_xall, W->h_xall, sizeof(double) * nall * kWalkRec, cudaMemcpyHostToDevice,
-                                    W->st), "hills in");
-        }
-        launch_walk_finish(W->d_plans, nw, W->d_step, W->d_ws, W->d_xall, nall, W->st);
-        if (W->ag_dev)   // every rank's overflow flag, for mtd_walkers_sync
-            MTD_WCU(cudaMemcpyAsync(W->h_xall, W->d_xall, sizeof(double) * nall * kWalkRec, cudaMemcpyDeviceToHost,
-                                    W->st), "hills in");
-        W->launches += 4;
-    } else {
-        launch_walk_bias(W->d_plans, nw, W->d_step, W->d_ws, W->st);
-    }
-    MTD_WCU(cudaGetLastError(), "walker bias");
-    MTD_WCU(cudaEventRecord(W->ev_bias, W->st), "fork");
-    for (int k = 0; k < nw; ++k) {
-        mtd_ctx *c = W->w[k];
-        MTD_WCU(cudaStreamWaitEvent(c->st, W->ev_bias, 0), "fork");
-        mtd_status s = enqueue_forces(c, step, d_x[k], nullptr, d_f[k], d_f[k], false);
-        if (s != MTD_OK) return wfail(W, s, "walker " + std::to_string(k) + ": " + c->err);
-        W->launches += c->launches;
-        MTD_WCU(cudaEventRecord(W->ev_done[k], c->st), "join");
-        MTD_WCU(cudaStreamWaitEvent(W->st, W->ev_done[k], 0), "join");
-    }
-    return MTD_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-mtd_status mtd_walkers_create(int nwalk, int narg, const char *const *arg, const mtd_options *opt,
-                              mtd_walkers **out) {
-    if (!out) return MTD_ERR_INVALID_ARG;
-    *out = nullptr;
-    mtd_walkers *W = new mtd_walkers();
-    *out = W;
-    if (nwalk < 1 || nwalk > 1024) return wfail(W, MTD_ERR_INVALID_ARG, "nwalk must be in [1, 1024]");
-    mtd_options o;
-    mtd_options_default(&o);
-    if (opt) o = *opt;
-    if (o.hills_path) W->hills_path = o.hills_path;
-    const std::string wd = o.work_dir ? o.work_dir : "";
-    if (!W->hills_path.empty() && W->hills_path[0] != '/' && !wd.empty()) W->hills_path = wd + "/" + W->hills_path;
-    o.hills_path = "";   // the group writes one HILLS file
-    for (int k = 0; k < nwalk; ++k) {
-        mtd_ctx *c = nullptr;
-        const mtd_status s = mtd_create(narg, arg, &o, &c);
-        if (c) c->ring = false;
-        W->w.push_back(c);
-        if (s != MTD_OK) return wfail(W, s, c ? c->err : "context creation failed");
-        if (c->cfg.hill_list()) return wfail(W, MTD_ERR_UNSUPPORTED, "walkers share a grid: CV_dim <= 3, no NN_BIAS");
-        if (k > 0) c->cfg.rec_file.clear();   // one RECORD file (walker 0's)
-    }
-    MTD_WCU(cudaStreamCreateWithFlags(&W->st, cudaStreamNonBlocking), "stream");
-    MTD_WCU(cudaEventCreateWithFlags(&W->ev_start, cudaEventDisableTiming), "event");
-    MTD_WCU(cudaEventCreateWithFlags(&W->ev_bias, cudaEventDisableTiming), "event");
-    W->ev_done.resize(nwalk);
-    for (int k = 0; k < nwalk; ++k)
-        MTD_WCU(cudaEventCreateWithFlags(&W->ev_done[k], cudaEventDisableTiming), "event");
-    MTD_WCU(cudaMalloc(&W->d_plans, sizeof(BiasPlan *) * nwalk), "plans");
-    MTD_WCU(cudaMalloc(&W->d_ws, sizeof(WalkState) * nwalk), "walker state");
-    MTD_WCU(cudaMemset(W->d_ws, 0, sizeof(WalkState) * nwalk), "walker state");
-    MTD_WCU(cudaMalloc(&W->d_step, sizeof(long long)), "step");
-    MTD_WCU(cudaMallocHost(&W->h_step, sizeof(long long)), "step");
-    return MTD_OK;
-}
-
-void mtd_walkers_destroy(mtd_walkers *W) {
-    if (!W) return;
-    if (W->st) cudaStreamSynchronize(W->st);
-    walkers_drop_graph(W);
-    for (size_t k = 0; k < W->w.size(); ++k) {
-        if (!W->w[k]) continue;
-        if (k > 0 && W->initialized) W->w[k]->d_grid = nullptr;   // walker 0 owns the shared grid
-        mtd_destroy(W->w[k]);
-    }
-    for (cudaEvent_t e : W->ev_done)
-        if (e) cudaEventDestroy(e);
-    if (W->ev_start) cudaEventDestroy(W->ev_start);
-    if (W->ev_bias) cudaEventDestroy(W->ev_bias);
-    if (W->d_plans) cudaFree(W->d_plans);
-    if (W->d_ws) cudaFree(W->d_ws);
-    if (W->d_step) cudaFree(W->d_step);
-    if (W->h_step) cudaFreeHost(W->h_step);
-    if (W->d_xloc) cudaFree(W->d_xloc);
-    if (W->d_xall) cudaFree(W->d_xall);
-    if (W->h_xloc) cudaFreeHost(W->h_xloc);
-    if (W->h_xall) cudaFreeHost(W->h_xall);
-    if (W->st) cudaStreamDestroy(W->st);
-    if (W->f_hills) std::fclose(W->f_hills);
-    delete W;
-}
-
-const char *mtd_walkers_last_error(const mtd_walkers *W) { return W ? W->err.c_str() : "null object"; }
-
-int mtd_walkers_count(const mtd_walkers *W) { return W ? (int)W->w.size() : 0; }
-
-mtd_status mtd_walkers_set_box(mtd_walkers *W, int k, const double lo[3], const double hi[3],
-                               const int periodic[3]) {
-    if (!W || k < 0 || k >= (int)W->w.size()) return MTD_ERR_INVALID_ARG;
-    walkers_drop_graph(W);
-    const mtd_status s = mtd_set_box(W->w[k], lo, hi, periodic);
-    return s == MTD_OK ? s : wfail(W, s, W->w[k]->err);
-}
-
-mtd_status mtd_walkers_init(mtd_walkers *W) {
-    if (!W) return MTD_ERR_INVALID_ARG;
-    if (W->initialized) return MTD_OK;
-    const int nw = (int)W->w.size();
-    for (int k = 0; k < nw; ++k) {
-        const mtd_status s = mtd_init(W->w[k]);
-        if (s != MTD_OK) return wfail(W, s, W->w[k]->err);
-    }
-    mtd_ctx *c0 = W->w[0];
-    std::vector<BiasPlan *> plans(nw);
-    for (int k = 0; k < nw; ++k) {
-        mtd_ctx *c = W->w[k];
-        if (k > 0) {
-            cudaFree(c->d_grid);
-            c->d_grid = c0->d_grid;   // one grid for the group
-        }
-        build_plan(c);
-        MTD_WCU(cudaMemcpy(c->d_plan, &c->plan, sizeof(BiasPlan), cudaMemcpyHostToDevice), "plan");
-        c->plan_dirty = false;
-        plans[k] = c->d_plan;
-    }
-    W->initialized = true;
-    MTD_WCU(cudaMemcpy(W->d_plans, plans.data(), sizeof(BiasPlan *) * nw, cudaMemcpyHostToDevice), "plans");
-    if (W->nranks > 0) {
-        const size_t loc = sizeof(double) * nw * kWalkRec, all = loc * W->nranks;
-        MTD_WCU(cudaMalloc((void **)&W->d_xloc, loc), "walker ranks");
-        MTD_WCU(cudaMalloc((void **)&W->d_xall, all), "walker ranks");
-        MTD_WCU(cudaHostAlloc((void **)&W->h_xloc, loc, cudaHostAllocDefault), "walker ranks");
-        MTD_WCU(cudaHostAlloc((void **)&W->h_xall, all, cudaHostAllocDefault), "walker ranks");
-        std::memset(W->h_xall, 0, all);
-    }
-    if (!W->hills_path.empty() && W->rank == 0) {   // sharded: rank 0 alone writes the group's HILLS
-        W->f_hills = std::fopen(W->hills_path.c_str(), "w");
-        if (!W->f_hills) return wfail(W, MTD_ERR_IO, "Cannot open HILLS file for writing/appending.");
-        if (c0->cfg.cv_dim == 2) std::fprintf(W->f_hills, "# step cv1 cv2 height sigma\n");
-        if (c0->cfg.cv_dim == 1) std::fprintf(W->f_hills, "# step cv_values height sigma\n");
-        std::fflush(W->f_hills);
-    }
-    return MTD_OK;
-}
-
-static mtd_status walkers_set_ranks(mtd_walkers *W, int rank, int nranks, mtd_allgather_fn fn,
-                             mtd_allgather_device_fn fn_dev, void *user) {
-    if (!W) return MTD_ERR_INVALID_ARG;
-    if (W->initialized) return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks must be set before the first step");
-    if (nranks < 1 || rank < 0 || rank >= nranks || (!fn && !fn_dev))
-        return wfail(W, MTD_ERR_INVALID_ARG, "walker ranks need 0 <= rank < nranks and an allgather callback");
-    W->rank = rank;
-    W->nranks = nranks;
-    W->ag = fn;
-    W->ag_dev = fn_dev;
-    W->ag_user = user;
-    W->use_graph = false;   // the exchange sits between the captured phases
-    return MTD_OK;
-}
-
-mtd_status mtd_walkers_set_ranks(mtd_walkers *W, int rank, int nranks, mtd_allgather_fn fn, void *user) {
-    return walkers_set_ranks(W, rank, nranks, fn, nullptr, user);
-}
-
-mtd_status mtd_walkers_set_ranks_device(mtd_walkers *W, int rank, int nranks, mtd_allgather_device_fn fn,
-                                        void *user) {
-    return walkers_set_ranks(W, rank, nranks, nullptr, fn, user);
-}
-
-mtd_status mtd_walkers_enable_graph(mtd_walkers *W, int enable) {
-    if (!W) return MTD_ERR_INVALID_ARG;
-    if (W->st) cudaStreamSynchronize(W->st);
-    walkers_drop_graph(W);
-    W->use_graph = enable != 0 && W->nranks == 0;
-    return MTD_OK;
-}
-
-mtd_status mtd_walkers_sync(mtd_walkers *W);
-
-mtd_status mtd_walkers_step_device(mtd_walkers *W, int64_t step, const int *n, const double *const *d_x,
-                                   double *const *d_f) {
-    if (!W || !n || !d_x || !d_f) return MTD_ERR_INVALID_ARG;
-    if (!W->initialized) {
-        const mtd_status s = mtd_walkers_init(W);
-        if (s != MTD_OK) return s;
-    }
-    const int nw = (int)W->w.size();
-    for (int k = 0; k < nw; ++k)
-        if (n[k] < 1 || !d_x[k] || !d_f[k]) return wfail(W, MTD_ERR_INVALID_ARG, "every walker needs atoms");
-    if (W->pending) {
-        const mtd_status s = mtd_walkers_sync(W);
-        if (s != MTD_OK) return s;
-    }
-    *W->h_step = step;
-    bool same = (int)W->g_n.size() == nw;
-    for (int k = 0; same && k < nw; ++k) same = W->g_n[k] == n[k] && W->g_x[k] == d_x[k] && W->g_f[k] == d_f[k];
-    if (W->use_graph && same && W->gexec) {
-        MTD_WCU(cudaGraphLaunch(W->gexec, W->st), "graph launch");
-    } else if (W->use_graph && same) {
-        // the same arguments ran once eagerly (allocations done): capture, then launch
-        MTD_WCU(cudaStreamBeginCapture(W->st, cudaStreamCaptureModeThreadLocal), "capture");
-        const mtd_status s = walkers_enqueue(W, step, n, d_x, d_f);
-        cudaGraph_t g = nullptr;
-        const cudaError_t ce = cudaStreamEndCapture(W->st, &g);
-        if (s != MTD_OK) {
-            if (g) cudaGraphDestroy(g);
-            return s;
-        }
-        MTD_WCU(ce, "capture");
-        W->graph = g;
-        MTD_WCU(cudaGraphInstantiate(&W->gexec, W->graph, 0), "graph instantiate");
-        MTD_WCU(cudaGraphLaunch(W->gexec, W->st), "graph launch");
-    } else {
-        walkers_drop_graph(W);
-        W->g_n.assign(n, n + nw);
-        W->g_x.assign(d_x, d_x + nw);
-        W->g_f.assign(d_f, d_f + nw);
-        const mtd_status s = walkers_enqueue(W, step, n, d_x, d_f);
-        if (s != MTD_OK) return s;
-    }
-    for (mtd_ctx *c : W->w) {
-        c->pending = true;
-        c->pending_step = step;
-        c->want_virial = false;
-    }
-    W->pending = true;
-    W->pending_step = step;
-    return MTD_OK;
-}
-
-mtd_status mtd_walkers_autotune(mtd_walkers *W, const int *n, const double *const *d_x, int reps, int *choices) {
-    if (!W || !n || !d_x || reps < 1) return MTD_ERR_INVALID_ARG;
-    if (!W->initialized) {
-        const mtd_status s = mtd_walkers_init(W);
-        if (s != MTD_OK) return s;
-    }
-    if (W->pending) {
-        const mtd_status s = mtd_walkers_sync(W);
-        if (s != MTD_OK) return s;
-    }
-    for (size_t k = 0; k < W->w.size(); ++k) {
-        if (n[k] < 1 || !d_x[k]) return wfail(W, MTD_ERR_INVALID_ARG, "every walker needs atoms");
-        const mtd_status s = autotune_idle(W->w[k], n[k], d_x[k], nullptr, reps, choices ? choices + 3 * k : nullptr);
-        if (s != MTD_OK) return wfail(W, s, W->w[k]->err);
-    }
-    walkers_drop_graph(W);   // the next steps run (and capture) the chosen shapes
-    W->g_n.clear();
-    return MTD_OK;
-}
-
-mtd_status mtd_walkers_sync(mtd_walkers *W) {
-    if (!W) return MTD_ERR_INVALID_ARG;
-    MTD_WCU(cudaStreamSynchronize(W->st), "sync");
-    if (!W->pending) return MTD_OK;
-    W->pending = false;
-    bool overflow = false;
-    for (mtd_ctx *c : W->w) {
-        if (c->h_status->overflow) {
-            const int need = (int)c->h_status->overflow;
-            for (Env &e : c->envs)
-                if (e.M < need) {
-                    e.M = ((need + 8) + 3) & ~3;
-                    alloc_env(c, e, c->cap_n);
-                }
-            cudaMemset(c->d_status, 0, sizeof(DevStatus));
-            c->h_status->overflow = 0;
-            overflow = true;
-        }
-    }
-    if (W->nranks > 0)   // sharded: a walker of any rank overflowed, so every rank repeats the step
-        for (int r = 0; r < W->nranks * (int)W->w.size(); ++r)
-            if (W->h_xall[(size_t)r * kWalkRec + kMaxDim + 2] != 0.0) overflow = true;
-    if (overflow) {
-        walkers_drop_graph(W);
-        W->g_n.clear();
-        for (mtd_ctx *c : W->w) c->pending = false;
-        return wfail(W, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded; capacity grown, repeat the step");
-    }
-    // the group's hills (walker 0's ring) go to the group HILLS file
-    mtd_ctx *c0 = W->w[0];
-    const unsigned long long nh = *c0->h_nhills;
-    if (nh > W->hills_written) {
-        unsigned long long from = W->hills_written;
-        if (nh - from > (unsigned long long)kHillCap) from = nh - kHillCap;
-        for (unsigned long long h = from; h < nh; ++h) {
-            HillRec r;
-            MTD_WCU(cudaMemcpy(&r, c0->d_hills + (h % kHillCap), sizeof(HillRec), cudaMemcpyDeviceToHost), "hill");
-            if (W->f_hills) {
-                std::fprintf(W->f_hills, "%lld", r.step);
-                for (int d = 0; d < c0->cfg.cv_dim; ++d) std::fprintf(W->f_hills, " %.16g", r.s[d]);
-                std::fprintf(W->f_hills, " %.16g %.16g\n", r.w, r.sigma);
-            }
-        }
-        if (W->f_hills) std::fflush(W->f_hills);
-        W->hills_written = nh;
-    }
-    for (mtd_ctx *c : W->w) {
-        c->hills_written = nh;
-        const mtd_status s = collect(c);
-        if (s != MTD_OK) return wfail(W, s, c->err);
-    }
-    return MTD_OK;
-}
-
-double mtd_walkers_cv(const mtd_walkers *W, int k, int d) {
-    if (!W || k < 0 || k >= (int)W->w.size()) return 0.0;
-    return mtd_compute_vector(W->w[k], d);
-}
-
-double mtd_walkers_bias(const mtd_walkers *W, int k) {
-    if (!W || k < 0 || k >= (int)W->w.size()) return 0.0;
-    return mtd_compute_scalar(W->w[k]);
-}
-
-mtd_status mtd_walkers_get_grid(mtd_walkers *W, double *out, int64_t count) {
-    if (!W || !out) return MTD_ERR_INVALID_ARG;
-    MTD_WCU(cudaStreamSynchronize(W->st), "grid");
-    const mtd_status s = mtd_get_grid(W->w[0], out, count);
-    return s == MTD_OK ? s : wfail(W, s, W->w[0]->err);
-}
-
-int mtd_walkers_last_launch_count(const mtd_walkers *W) { return W ? W->launches : 0; }
 
 }  // extern "C"

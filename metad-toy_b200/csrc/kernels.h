@@ -299,7 +299,7 @@ void launch_bias_step(const BiasPlan *d_plan, long long step, cudaStream_t st);
 // Domain decomposition: this rank's totals of every unit ([nunit][8], the
 // block partials reduced in the order the bias kernel uses), the rho(k) (2K)
 // and atom count of each S(k) unit in unit order, and last this step's
-// neighbour-overflow count (0: none).
+// neighbour-overflow count (0: none) and non-finite-position flag (0: none).
 void launch_unit_sums(const BiasPlan *d_plan, double *out, cudaStream_t st);
 int unit_sums_count(const BiasPlan &P);
 void launch_domain_flag(const double *gflag, DevStatus *status, cudaStream_t st);

@@ -45,7 +45,7 @@ constexpr int ob3 = ow3 + kH;
 constexpr int kNP = ob3 + 1;            // 17,281 parameters
 constexpr int kNPpad = (kNP + 3) / 4 * 4;
 constexpr int kTileSmem = 6 * 32768 + (4 * kH + 3 * kH) * 4 + 64;   // operand tiles + small weights
-constexpr int kWaitTries = 1 << 20;     // bounded mbarrier waits
+constexpr int kWaitTries = 1 << 20;     // bounded mbarrier waits (default limit)
 
 enum { MODE_FWD = 0, MODE_GRAD_S = 1, MODE_TRAIN = 2 };
 
@@ -75,10 +75,16 @@ __device__ __forceinline__ void rows_sum(float *scratch, const float *vals, int 
     __syncthreads();
 }
 
+// A bounded wait that runs out (in any thread: the block votes) ends the
+// tile: it issues no further MMA, reads no TMEM and overlays no operand the
+// tensor core may still be reading; it waits once more (same limit) for the
+// batch in flight, releases its TMEM, sets *err and returns.  stall != 0 is
+// the check of that path: after the first batch has completed, every thread
+// waits on the barrier's next phase, which no commit will complete.
 template <int MODE>
 __global__ void __launch_bounds__(128, 1)
     k_mlp_tile(MlpDev p, int npts, const float *__restrict__ x, const float *__restrict__ t, float *y_out,
-               float *ds_out, float *part, float *loss_part, float grad_scale, int *err) {
+               float *ds_out, float *part, float *loss_part, float grad_scale, int *err, int tries, int stall) {
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char *sA = sm;                   // h1        rows m, K k
     unsigned char *sBf = sm + 32768;          // W2        rows n, K k
@@ -145,7 +151,16 @@ __global__ void __launch_bounds__(128, 1)
         }
         umma_commit(&mbar);
     }
-    bool ok = mbar_wait(&mbar, 0, kWaitTries);
+    bool ok = mbar_wait(&mbar, 0, tries);
+    if (stall) ok = mbar_wait(&mbar, 1, tries) && ok;
+    if (!__syncthreads_and(ok)) {
+        mbar_wait(&mbar, 0, tries);
+        tc_fence_before();
+        __syncthreads();
+        if (warp == 0) tmem_dealloc(taddr, 512);
+        if (m == 0) atomicExch(err, 1);
+        return;
+    }
     tc_fence_after();
     const uint32_t lane_addr = taddr + (static_cast<uint32_t>(warp * 32) << 16);
     // forward epilogue: z2 = D + b2, y = w3 . silu(z2) + b3
@@ -164,7 +179,6 @@ __global__ void __launch_bounds__(128, 1)
         tc_fence_before();
         __syncthreads();
         if (warp == 0) tmem_dealloc(taddr, 512);
-        if (!ok && m == 0) atomicExch(err, 1);
         return;
     }
     float dy = 0.0f;
@@ -227,7 +241,14 @@ __global__ void __launch_bounds__(128, 1)
         }
         umma_commit(&mbar);
     }
-    ok = mbar_wait(&mbar, 1, kWaitTries) && ok;
+    if (!__syncthreads_and(mbar_wait(&mbar, 1, tries))) {
+        mbar_wait(&mbar, 1, tries);
+        tc_fence_before();
+        __syncthreads();
+        if (warp == 0) tmem_dealloc(taddr, 512);
+        if (m == 0) atomicExch(err, 1);
+        return;
+    }
     tc_fence_after();
     // layer 1 backward: dL/dz1 = dL/dh1 silu'(z1); input gradient and W1, b1 gradients
     float dsu[kIn] = {0.f, 0.f, 0.f, 0.f};
@@ -274,7 +295,6 @@ __global__ void __launch_bounds__(128, 1)
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(taddr, 512);
-    if (!ok && m == 0) atomicExch(err, 1);
 }
 
 __device__ __forceinline__ float bf16_round(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
@@ -526,6 +546,8 @@ struct mtd_nnbias {
     bool validated = false;
     double tol = 1e-3, last_max_err = -1.0;
     unsigned long long seed = 1;
+    int wait_tries = kWaitTries;   // limit of the tile kernel's mbarrier waits
+    int wait_stall = 0;            // 1: tiles take their timeout path (mtd_nnbias_set_wait)
 };
 
 namespace {
@@ -653,19 +675,25 @@ mtd_status nb_forward_batch(mtd_nnbias *b, int npts, const float *d_x, float *d_
     const int ntiles = (npts + kH - 1) / kH;
     if (d_ds)
         k_mlp_tile<MODE_GRAD_S><<<ntiles, 128, kTileSmem, b->st>>>(nb_dev(b), npts, d_x, nullptr, d_y, d_ds,
-                                                                   nullptr, nullptr, 0.f, b->d_err);
+                                                                   nullptr, nullptr, 0.f, b->d_err, b->wait_tries,
+                                                                   b->wait_stall);
     else
         k_mlp_tile<MODE_FWD><<<ntiles, 128, kTileSmem, b->st>>>(nb_dev(b), npts, d_x, nullptr, d_y, nullptr, nullptr,
-                                                                nullptr, 0.f, b->d_err);
+                                                                nullptr, 0.f, b->d_err, b->wait_tries,
+                                                                b->wait_stall);
     NB_CU(cudaGetLastError(), "MLP forward");
     return MTD_OK;
 }
 
+// Reads and clears the tile kernels' timeout flag.
 mtd_status nb_check_err(mtd_nnbias *b) {
     int h = 0;
     NB_CU(cudaMemcpyAsync(&h, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->st), "status");
     NB_CU(cudaStreamSynchronize(b->st), "sync");
-    if (h) return nb_fail(b, MTD_ERR_TIMEOUT, "tensor-core wait ran out of tries");
+    if (h) {
+        NB_CU(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->st), "status");
+        return nb_fail(b, MTD_ERR_TIMEOUT, "tensor-core wait ran out of tries");
+    }
     return MTD_OK;
 }
 
@@ -826,7 +854,8 @@ mtd_status mtd_nnbias_loss_grad(mtd_nnbias *b, int npts, const double *pts, cons
     cudaMemcpyAsync(d_x, x.data(), sizeof(float) * x.size(), cudaMemcpyHostToDevice, b->st);
     cudaMemcpyAsync(d_t, t.data(), sizeof(float) * npts, cudaMemcpyHostToDevice, b->st);
     k_mlp_tile<MODE_TRAIN><<<ntiles, 128, kTileSmem, b->st>>>(nb_dev(b), npts, d_x, d_t, nullptr, nullptr, b->d_part,
-                                                              b->d_loss, 2.0f / npts, b->d_err);
+                                                              b->d_loss, 2.0f / npts, b->d_err, b->wait_tries,
+                                                              b->wait_stall);
     k_mlp_gradsum<<<(kNP + 255) / 256, 256, 0, b->st>>>(ntiles, b->d_part, d_g);
     std::vector<float> lp(ntiles);
     cudaMemcpyAsync(grad, d_g, sizeof(float) * kNP, cudaMemcpyDeviceToHost, b->st);
@@ -919,7 +948,7 @@ mtd_status mtd_nnbias_fit(mtd_nnbias *b, int ntrain, int iters, int batch, doubl
                                                                                    std::max(1, iters - iters / 2)))));
         k_mlp_tile<MODE_TRAIN><<<ntiles, 128, kTileSmem, b->st>>>(
             nb_dev(b), nb, b->d_xt + (size_t)bi * batch * kIn, b->d_tt + (size_t)bi * batch, nullptr, nullptr,
-            b->d_part, b->d_loss, 2.0f / nb, b->d_err);
+            b->d_part, b->d_loss, 2.0f / nb, b->d_err, b->wait_tries, b->wait_stall);
         k_mlp_adam<<<(kNP + 255) / 256, 256, 0, b->st>>>(ntiles, b->d_part, b->d_master, b->d_mom, b->d_vel,
                                                          std::max(lr_t, (float)(lr * 0.02)), b1c, b2c, b->d_W1,
                                                          b->d_b1, b->d_W2, b->d_W2t, b->d_b2, b->d_w3, b->d_b3, 1);
@@ -1006,12 +1035,26 @@ mtd_status mtd_nnbias_eval_device(mtd_nnbias *b, int npts, const double *d_pts, 
     const int ntiles = (npts + kH - 1) / kH;
     if (d_dV)
         k_mlp_tile<MODE_GRAD_S><<<ntiles, 128, kTileSmem, st>>>(nb_dev(b), npts, b->d_bx, nullptr, b->d_by, b->d_bds,
-                                                                nullptr, nullptr, 0.f, b->d_err);
+                                                                nullptr, nullptr, 0.f, b->d_err, b->wait_tries,
+                                                                b->wait_stall);
     else
         k_mlp_tile<MODE_FWD><<<ntiles, 128, kTileSmem, st>>>(nb_dev(b), npts, b->d_bx, nullptr, b->d_by, nullptr,
-                                                             nullptr, nullptr, 0.f, b->d_err);
+                                                             nullptr, nullptr, 0.f, b->d_err, b->wait_tries,
+                                                             b->wait_stall);
     k_nb_outputs<<<nb, 256, 0, st>>>(b->D, npts, b->d_by, b->d_bds, b->vscale, sc[0], sc[1], sc[2], sc[3], d_V, d_dV);
     NB_CU(cudaGetLastError(), "network");
+    return MTD_OK;
+}
+
+mtd_status mtd_nnbias_sync(mtd_nnbias *b) {
+    if (!b) return MTD_ERR_INVALID_ARG;
+    return nb_check_err(b);
+}
+
+mtd_status mtd_nnbias_set_wait(mtd_nnbias *b, int tries, int stall) {
+    if (!b || tries < 0) return MTD_ERR_INVALID_ARG;
+    b->wait_tries = tries > 0 ? tries : kWaitTries;
+    b->wait_stall = stall ? 1 : 0;
     return MTD_OK;
 }
 

@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(256) k_na_partial(int n, const double *__restr
         double acc[kNaChunk];
 #pragma unroll
         for (int t = 0; t < kNaChunk; ++t) acc[t] = 0.0;
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t stride = (size_t)gridDim.x * blockDim.x;
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
             if (mask && !(mask[i] & groupbit)) continue;
             if (k0 == 0) cnt += 1.0;
             const double px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
@@ -168,13 +169,23 @@ extern "C" mtd_status mtd_sk_noalloc(int n, const double *d_x, const int *d_mask
     }
     int nb = kNaScratchDoubles / (2 * nk + 1);
     if (nb > kNaMaxBlocks) nb = kNaMaxBlocks;
-    const int need = (n + 255) / 256;
-    if (nb > need) nb = need > 0 ? need : 1;
+    const long long need = ((long long)n + 255) / 256;
+    if (nb > need) nb = need > 0 ? (int)need : 1;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (precision == MTD_PREC_FP64) k_na_partial<true><<<nb, 256, 0, st>>>(n, d_x, d_mask, groupbit, nk, d_k, scratch);
-    else k_na_partial<false><<<nb, 256, 0, st>>>(n, d_x, d_mask, groupbit, nk, d_k, scratch);
-    k_na_finish<<<1, 256, 0, st>>>(nk, nb, scratch, d_rho, d_s);
-    if (cudaGetLastError() != cudaSuccess) {
+    // each launch's own status (cudaGetLastError could report an earlier,
+    // unrelated launch of the caller's as this call's failure)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nb);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaError_t e = precision == MTD_PREC_FP64
+                        ? cudaLaunchKernelEx(&cfg, k_na_partial<true>, n, d_x, d_mask, groupbit, nk, d_k, scratch)
+                        : cudaLaunchKernelEx(&cfg, k_na_partial<false>, n, d_x, d_mask, groupbit, nk, d_k, scratch);
+    if (e == cudaSuccess) {
+        cfg.gridDim = dim3(1);
+        e = cudaLaunchKernelEx(&cfg, k_na_finish, nk, nb, (const double *)scratch, d_rho, d_s);
+    }
+    if (e != cudaSuccess) {
         na_msg(err, errlen, "mtd_sk_noalloc: kernel launch failed");
         return MTD_ERR_CUDA;
     }

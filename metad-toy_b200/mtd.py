@@ -35,7 +35,7 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
            "mtd_nnbias_num_hills", "mtd_nnbias_exact", "mtd_nnbias_eval", "mtd_nnbias_fit", "mtd_nnbias_validate",
            "mtd_nnbias_usable", "mtd_nnbias_point_device", "mtd_nnbias_eval_device", "mtd_nnbias_get_params", "mtd_nnbias_set_params",
-           "mtd_nnbias_vscale", "mtd_nnbias_loss_grad",
+           "mtd_nnbias_vscale", "mtd_nnbias_loss_grad", "mtd_nnbias_set_wait", "mtd_nnbias_sync",
            "mtd_walkers_create", "mtd_walkers_destroy", "mtd_walkers_last_error", "mtd_walkers_count",
            "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
            "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
@@ -165,6 +165,8 @@ def lib():
         L.mtd_nnbias_vscale.argtypes = [vp]
         L.mtd_nnbias_vscale.restype = C.c_double
         L.mtd_nnbias_loss_grad.argtypes = [vp, C.c_int, dp, dp, C.c_double, C.POINTER(C.c_float), dp]
+        L.mtd_nnbias_set_wait.argtypes = [vp, C.c_int, C.c_int]
+        L.mtd_nnbias_sync.argtypes = [vp]
         L.mtd_sk_noalloc.argtypes = [C.c_int, vp, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, C.c_char_p,
                                      C.c_int]
         _lib = L
@@ -468,6 +470,15 @@ class NNBias:
         if self._h:
             lib().mtd_nnbias_destroy(self._h)
             self._h = None
+
+    def sync_device(self):
+        """Waits for the object's stream; raises TIMEOUT if a network tile gave up a wait."""
+        self._check(lib().mtd_nnbias_sync(self._h))
+
+    def set_wait(self, tries=0, stall=False):
+        """Limit of the tile kernel's tensor-core waits (0: default); stall=True
+        makes the next batched call take the timeout path (MTD_ERR_TIMEOUT)."""
+        self._check(lib().mtd_nnbias_set_wait(self._h, int(tries), 1 if stall else 0))
 
     def __del__(self):
         try:

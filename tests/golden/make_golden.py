@@ -1,9 +1,9 @@
 """Generates the golden fixtures in this directory from the reference checkout.
 
-Run in a container that has the reference (default /root/reference) after
-`make -C oracle ref`:
+Run in a container that has the reference checkout, after
+`make -C oracle ref REF_DIR=<checkout>`:
 
-    python tests/golden/make_golden.py [REF_DIR]
+    python tests/golden/make_golden.py <checkout>      (or REF_DIR=<checkout> in the environment)
 
 Outputs (committed):
   ylm_reference.npz          Y_lm (l = 3, 4, 6) and dY_lm/dd (l = 4, 6) at 256
@@ -32,7 +32,10 @@ import oracle as O  # noqa: E402
 import systems  # noqa: E402
 
 
-def main(ref_dir="/root/reference"):
+def main(ref_dir=None):
+    ref_dir = ref_dir or os.environ.get("REF_DIR")
+    if not ref_dir:
+        raise SystemExit("usage: make_golden.py <reference checkout>  (or set REF_DIR)")
     R = O.ref_lib()
     if R is None:
         raise SystemExit("build oracle/_ref first: make -C oracle ref")

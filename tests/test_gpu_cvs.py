@@ -195,7 +195,7 @@ def test_hills_file_and_restart(tmp_path):
     assert len(lines2) == len(lines) + 1 and lines2[-1].startswith("25 ")
 
 
-@pytest.mark.parametrize("bad", ["10 0.25 0.005\n", "10 0.25 abc 0.01\n"])
+@pytest.mark.parametrize("bad", ["10 0.25 0.005\n", "10 0.25 abc 0.01\n", "ten 0.25 0.005 0.01\n"])
 def test_corrupt_hills_line_is_an_error(tmp_path, bad):
     """A truncated or non-numeric HILLS row stops the restart with
     MTD_ERR_IO and the offending line, before any step (comment and blank
@@ -207,6 +207,24 @@ def test_corrupt_hills_line_is_an_error(tmp_path, bad):
     with pytest.raises(mtd.MetadError, match="malformed HILLS line"):
         m.init()
     m.close()
+
+
+def test_empty_hills_file_restarts_fresh_with_a_header(tmp_path):
+    """METAD_RESTART 1 with an existing but empty HILLS file: nothing to
+    replay, the file is rewritten with its header (not appended to without
+    one), and the first deposit lands below the header."""
+    x0, L = systems.config1()
+    hills = tmp_path / "HILLS"
+    hills.write_text("")
+    m = mtd.Metad(H.fix_args_q(wt=1, pace=5) + ["METAD_RESTART", 1], precision="fp64", hills_path=str(hills))
+    m.set_box([0, 0, 0], L)
+    m.init()
+    assert np.all(m.grid(1000) == 0.0)
+    x = systems.jitter(x0, 0.15, 3, 0)
+    m.post_force(0, x, np.zeros_like(x))
+    m.close()
+    lines = hills.read_text().splitlines()
+    assert lines[0] == "# step cv_values height sigma" and len(lines) == 2 and lines[1].startswith("0 ")
 
 
 def test_reference_hills_fixture_replays():

@@ -271,3 +271,66 @@ def test_domain_api_errors():
     with pytest.raises(mtd.MetadError, match="before the first step"):
         m.set_domain(5, 0, red.for_rank(0))
     m.close()
+
+
+def test_non_finite_position_on_one_rank_stops_every_rank(tmp_path):
+    """A NaN coordinate among rank 0's owned atoms: the non-finite flag travels
+    with the totals, so neither rank deposits or applies a bias force, both
+    report MTD_ERR_NAN for that step (a LAMMPS error->all() is then reached by
+    every rank), the replicated grids stay equal, and the next good step runs
+    on both ranks."""
+    args = CASES["steinh_l_step"]()
+    x, L = _fcc(nc=7)
+    probe = mtd.Metad(args, precision="mixed")
+    cut = probe.ghost_cutoff
+    probe.close()
+    red = domain.LocalAllreduce(2, timeout=120)
+    ctx = []
+    for r in range(2):
+        m = mtd.Metad(args, precision="mixed", hills_path="HILLS", work_dir=str(tmp_path))
+        m.set_domain(0, r, red.for_rank(r))
+        ctx.append(m)
+    status = [[None] * 3 for _ in range(2)]
+    forces = [[None] * 3 for _ in range(2)]
+    grids = [[None] * 3 for _ in range(2)]
+    errs = []
+
+    def run(r):
+        try:
+            m = ctx[r]
+            for step in range(3):
+                rk = domain.decompose(x, [0, 0, 0], L, (2, 1, 1), cut)[r]
+                xr = rk["x"].copy()
+                if step == 1 and r == 0:
+                    xr[0, 1] = np.nan
+                m.set_box(rk["lo"], rk["hi"], (0, 0, 0))
+                m.set_nlocal(rk["owned"].size)
+                f0 = np.full_like(xr, 0.25)
+                f = f0.copy()
+                try:
+                    m.post_force(step, xr, f)
+                    status[r][step] = "ok"
+                except mtd.MetadError as e:
+                    status[r][step] = "nan" if "non-finite" in str(e) else str(e)
+                forces[r][step] = np.array_equal(f, f0)
+                grids[r][step] = m.grid(200 * 200)
+        except BaseException as e:
+            errs.append(e)
+            red.abort()
+
+    ts = [threading.Thread(target=run, args=(r,)) for r in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    for m in ctx:
+        m.close()
+    if errs:
+        raise errs[0]
+    assert status[0] == ["ok", "nan", "ok"] and status[1] == ["ok", "nan", "ok"]
+    assert forces[0][1] and forces[1][1]              # no bias force on either rank at the bad step
+    assert not forces[0][2] and not forces[1][2]      # the next step applies it again
+    for s in range(3):
+        assert np.array_equal(grids[0][s], grids[1][s])
+    assert np.array_equal(grids[0][1], grids[0][0])   # nothing deposited at the bad step
+    assert not np.array_equal(grids[0][2], grids[0][1])

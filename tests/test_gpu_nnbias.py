@@ -157,3 +157,43 @@ def test_device_batch_equals_host_batch():
             assert np.abs(V - ref[0]).max() <= 1e-5 * np.abs(ref[0]).max()
             assert np.abs(dV - ref[1]).max() <= 1e-4 * np.abs(ref[1]).max()
     nb.close()
+
+
+def test_tensor_core_wait_timeout_path():
+    """The tile kernel's bounded-wait failure path, taken safely: with stall
+    on, every tile waits (64 polls) on a barrier phase that no commit
+    completes, after its real tensor-core batch has finished.  Each of the
+    three tile modes (values only, values and input gradient, training) then
+    returns MTD_ERR_TIMEOUT with no work left in flight (the tile issued no
+    further MMA and released its tensor memory); with stall off the next
+    calls equal the evaluations made before."""
+    import torch
+
+    w = _random_params(14)
+    nb = mtd.NNBias(systems.CV4_LO, systems.CV4_HI)
+    nb.set_params(w, 0.5)
+    p = _box_points(700, 10)
+    t = np.sin(p[:, 0])
+    d_p = torch.from_numpy(np.ascontiguousarray(p)).cuda()
+    d_v = torch.zeros(len(p), dtype=torch.float64, device="cuda")
+
+    def values_only():
+        nb.eval_device(len(p), d_p.data_ptr(), d_v.data_ptr(), 0, use_nn=1)
+        nb.sync_device()
+        return d_v.cpu().numpy().copy()
+
+    ref_v, ref_g, ref_t = values_only(), nb.eval(p), nb.loss_grad(p, t, 1.0)
+    nb.set_wait(64, stall=True)
+    with pytest.raises(mtd.MetadError, match="TIMEOUT"):
+        values_only()
+    with pytest.raises(mtd.MetadError, match="TIMEOUT"):
+        nb.eval(p)
+    with pytest.raises(mtd.MetadError, match="TIMEOUT"):
+        nb.loss_grad(p, t, 1.0)
+    nb.set_wait(0, stall=False)
+    assert np.array_equal(values_only(), ref_v)
+    V, dV = nb.eval(p)
+    assert np.array_equal(V, ref_g[0]) and np.array_equal(dV, ref_g[1])
+    g, loss = nb.loss_grad(p, t, 1.0)
+    assert np.array_equal(g, ref_t[0]) and loss == ref_t[1]
+    nb.close()

@@ -91,3 +91,58 @@ def test_group_mask_matches_context():
     torch.cuda.synchronize()
     ref = _context_s(x, L, nk, kmag, seed, "fp64", groups={"all": 1, "half": 2}, mask=mask)
     assert H.rel(float(d_s.item()), ref) < 1e-10
+
+
+@pytest.mark.gpu
+def test_largest_k_set_and_empty_input():
+    """nk = 1024, the stated maximum (63 partial blocks fill the fixed
+    scratch), against a NumPy FP64 sum; then n = 0, which gives S = 0 and
+    rho = 0 without reading any atom."""
+    import torch
+
+    nk = 1024
+    x, L = _system(21)
+    kv = systems.kvectors(nk, systems.KMAG_111, 17)
+    d_x = torch.tensor(x, dtype=torch.float64, device="cuda")
+    d_k = torch.tensor(kv, dtype=torch.float64, device="cuda")
+    d_s = torch.zeros(1, dtype=torch.float64, device="cuda")
+    d_rho = torch.zeros(2 * nk, dtype=torch.float64, device="cuda")
+    mtd.sk_noalloc(x.shape[0], d_x.data_ptr(), d_k.data_ptr(), nk, d_s.data_ptr(), rho_ptr=d_rho.data_ptr(),
+                   precision="fp64")
+    torch.cuda.synchronize()
+    ph = x @ kv.T
+    re, im = np.cos(ph).sum(0), np.sin(ph).sum(0)
+    assert H.rel(d_rho.cpu().numpy(), np.stack([re, im], axis=1).reshape(-1)) < 1e-10
+    assert H.rel(float(d_s.item()), float(np.sum(re * re + im * im)) / x.shape[0] / nk) < 1e-10
+    d_s.fill_(7.0)
+    d_rho.fill_(7.0)
+    mtd.sk_noalloc(0, 0, d_k.data_ptr(), nk, d_s.data_ptr(), rho_ptr=d_rho.data_ptr(), precision="fp64")
+    torch.cuda.synchronize()
+    assert float(d_s.item()) == 0.0 and np.all(d_rho.cpu().numpy() == 0.0)
+
+
+@pytest.mark.gpu
+def test_a_call_allocates_no_device_memory():
+    """After the set-up call, further calls leave the device's free memory
+    unchanged (cudaMemGetInfo before and after): the scratch is the static
+    array, not memory from an allocator."""
+    import torch
+
+    nk = 96
+    x, L = _system(22)
+    kv = systems.kvectors(nk, systems.KMAG_111, 23)
+    d_x = torch.tensor(x, dtype=torch.float64, device="cuda")
+    d_k = torch.tensor(kv, dtype=torch.float64, device="cuda")
+    d_s = torch.zeros(1, dtype=torch.float64, device="cuda")
+    d_rho = torch.zeros(2 * nk, dtype=torch.float64, device="cuda")
+    for precision in ("mixed", "fp64"):
+        mtd.sk_noalloc(x.shape[0], d_x.data_ptr(), d_k.data_ptr(), nk, d_s.data_ptr(), rho_ptr=d_rho.data_ptr(),
+                       precision=precision)   # set-up and first launch of each kernel
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for precision in ("mixed", "fp64", "mixed"):
+        mtd.sk_noalloc(x.shape[0], d_x.data_ptr(), d_k.data_ptr(), nk, d_s.data_ptr(), rho_ptr=d_rho.data_ptr(),
+                       precision=precision)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
