@@ -155,45 +155,131 @@ def ncu_traffic(kernel):
         return None
 
 
-def cpu_baseline(xs, L, budget_s=15.0, threads=None):
-    """The FP64 oracle (C, OpenMP) running the same step on the host cores."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    if threads:
-        O.set_threads(threads)
+    return O
+
+
+def cpu_model():
+    """The host CPU's model name (lscpu, else /proc/cpuinfo)."""
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def oracle_steps(O, xs, L, steps, first=0):
+    """`steps` full FP64 oracle steps of the headline workload (both orders
+    with forces, the WT grid, a deposit every 10 steps); returns seconds."""
     sw = O.make_sw("STEP", r0=3.9)
     g = O.Grid([[0, 1], [0, 1]], [200, 200], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
-    n = xs[0].shape[0]
-    steps, t0 = 0, time.perf_counter()
-    while True:
-        x = xs[steps % len(xs)]
+    t0 = time.perf_counter()
+    for k in range(first, first + steps):
+        x = xs[k % len(xs)]
         o4 = O.steinh_l(4, x, L, 3.9, sw)
         o6 = O.steinh_l(6, x, L, 3.9, sw)
         s = [o4["cv"], o6["cv"]]
-        if (steps * 1) % 10 == 0:
+        if k % 10 == 0:
             g.add_hill(s)
         V, dV = g.value(s)
         _ = -(dV[0] * o4["grad"] + dV[1] * o6["grad"])
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(xs, L, budget_s=15.0, threads=None):
+    """The FP64 oracle (C, OpenMP) running the same step on the host cores: as
+    many full steps as fit the budget (at most 50) on `threads` threads, and
+    one full step on one thread."""
+    O = _oracle()
+    n = xs[0].shape[0]
+    if threads:
+        O.set_threads(threads)
+    cores = O.get_threads()
+    oracle_steps(O, xs, L, 1)   # warm-up (page-in, thread pool)
+    steps, el = 0, 0.0
+    while el < budget_s and steps < 50:
+        el += oracle_steps(O, xs, L, 1, first=steps)
         steps += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or steps >= 50:
-            break
-    return {"value": n * steps / el, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
-            "sample": "%d full steps of the 256,000-atom workload (FP64 oracle, both orders with forces, grid)" % steps}
+    O.set_threads(1)
+    el1 = oracle_steps(O, xs, L, 1)
+    O.set_threads(cores)
+    return {"value": n * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d full steps of the 256,000-atom workload (FP64 oracle, both orders with forces, grid)" % steps,
+            "cpu_model": cpu_model(), "cores_available": os.cpu_count(),
+            "one_thread": {"value": n / el1, "unit": UNIT, "sample": "1 full step on 1 thread"}}
+
+
+def error_vs_fp64(xs, L, precision, device):
+    """Errors of one step of the timed workload against the FP64 oracle: a
+    fresh context (deposit step 0) on the first positions; CVs and bias
+    relative, forces relative to the largest force component, per-atom
+    neighbour counts compared exactly.  Outside every timed region."""
+    import mtd
+    O = _oracle()
+    x = xs[0]
+    n = x.shape[0]
+    m = mtd.Metad(fix_args(), precision=precision, device=device)
+    m.set_box([0, 0, 0], L)
+    f = np.zeros_like(x)
+    m.post_force(0, x, f)
+    st = O.make_sw("STEP", r0=3.9)
+    o4, o6 = O.steinh_l(4, x, L, 3.9, st), O.steinh_l(6, x, L, 3.9, st)
+    g = O.Grid([[0, 1], [0, 1]], [200, 200], 0.01, 0.005, 9.0, 300.0, 8.617343e-5, True)
+    s = [o4["cv"], o6["cv"]]
+    g.add_hill(s)
+    V, dV = g.value(s)
+    fo = -(dV[0] * o4["grad"] + dV[1] * o6["grad"])
+    fmax = float(np.abs(fo).max())
+    nnb = m.extract("Q4.nnb", n).astype(np.int32)
+    out = {"precision": precision, "step": "0 (deposit)",
+           "cv_rel": [abs(m.cv[d] - s[d]) / abs(s[d]) for d in range(2)],
+           "bias_rel": abs(m.compute_scalar() - V) / abs(V),
+           "force_rel_max": float(np.abs(f - fo).max()) / fmax,
+           "force_rel_rms": float(np.sqrt(np.mean((f - fo) ** 2))) / fmax,
+           "lq_rel_max": [float(np.abs(m.extract("Q%d.stein_q" % l, n) - o["LQ"]).max() / np.abs(o["LQ"]).max())
+                          for l, o in ((4, o4), (6, o6))],
+           "neighbor_counts_equal": bool(np.array_equal(nnb, o4["nnb"])),
+           "cv_target_1e-6_met": bool(max(abs(m.cv[d] - s[d]) / abs(s[d]) for d in range(2)) <= 1e-6)}
+    m.close()
+    return out
 
 
 def run_reference(args, rank):
+    """The reference arm: the FP64 oracle port of the reference algorithm on
+    all host cores, `warmup` untimed and exactly `steps` timed full steps of
+    the headline workload; rank 0 alone (other ranks exit without work)."""
     if rank != 0:
         return 0
     xs, L = load_system()
+    O = _oracle()
     cores = os.cpu_count() or 1
-    base = cpu_baseline(xs, L, budget_s=max(10.0, 2.0 * args.steps), threads=cores)
-    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+    O.set_threads(cores)
+    n = xs[0].shape[0]
+    oracle_steps(O, xs, L, args.warmup)
+    el = oracle_steps(O, xs, L, args.steps, first=args.warmup)
+    value = n * args.steps / el
+    base = {"value": value, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+            "sample": "%d full steps of the 256,000-atom workload after %d untimed (FP64 oracle, both orders "
+                      "with forces, grid)" % (args.steps, args.warmup),
+            "cpu_model": cpu_model()}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded slab geometry)",
-            "config": {"workload": WORKLOAD, "atoms": int(xs[0].shape[0])},
+            "config": {"workload": WORKLOAD, "atoms": int(n)},
             "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
@@ -705,6 +791,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(xs, L, budget_s=15.0, threads=os.cpu_count())
+    err = None
+    if rank == 0 and not args.no_cpu:
+        err = error_vs_fp64(xs, L, args.precision, local)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "mixed" else "f64",
@@ -719,7 +808,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": launches * args.steps,
-            "roofline": roof, "clocks": clocks, "cpu_baseline": cpu}
+            "roofline": roof, "clocks": clocks, "cpu_baseline": cpu, "error_vs_fp64": err}
     if rank == 0:
         print(json.dumps(line))
     m.close()

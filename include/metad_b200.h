@@ -156,7 +156,9 @@ int mtd_cv_dim(const mtd_ctx *ctx);
 
 /* Per-atom export for `compute metad/atom` / Fix::extract
  * ("colvar_peratom:<CAL>.<prop>", props stein_q, dcvdx_x/y/z, stru_f,
- * chem_pair_r for WEIGHT_CHEM).
+ * chem_pair_r for WEIGHT_CHEM; nnb = neighbours the CV used, for STEINH Q
+ * min(neighbours within cutoff_r, cutoff_Natoms); nrc = neighbours within
+ * the list criterion before any cap).
  * Copies n values (caller order) into out.  dcvdx_* is the exact gradient of
  * the CV that the first SYMBOL on <CAL> selects, at the last step's positions
  * (STEINH Q and L, STRU_FACTOR, STRU_FACTOR_K); it re-runs that CAL's force
@@ -167,6 +169,19 @@ int mtd_cv_dim(const mtd_ctx *ctx);
  * STEIN_QL::get_peratom_ptr (src/cvs/CVs_Steinhardt.cu:1278-1322),
  * Stru_factor::get_peratom_ptr (src/cvs/CVs_Strufactor.cu:974-979). */
 mtd_status mtd_extract_peratom(mtd_ctx *ctx, const char *key, double *out, int n);
+
+/* The last step's neighbour lists of CAL `cal` (STEINH Q / L, STRU_FACTOR),
+ * caller order: counts[i] (n values) = neighbours atom i's CV terms use (for
+ * STEINH Q the cutoff_Natoms nearest within cutoff_r, ties by caller index;
+ * for STEINH L those with sigma(r) >= cutoff_eps; for STRU_FACTOR those within
+ * cutoff_r).  idx may be NULL; otherwise idx[i * max_per_atom + t] receives
+ * their caller indices in ascending order, -1 padded, and a count above
+ * max_per_atom returns MTD_ERR_INVALID_ARG.  Replaces the reference's
+ * per-atom list and counts d_calculated_numneigh, d_neigh_both_in_r_N and
+ * d_neigh_in_cutoff_r of get_environment_Steinhardt_Q
+ * (src/cvs/CVs_Steinhardt.cu:1324-1406) and the lists of
+ * get_environment_Steinhardt_LocalQ (src/cvs/CVs_Steinhardt_Local.cu:1210-1285). */
+mtd_status mtd_get_neighbors(mtd_ctx *ctx, const char *cal, int n, int *counts, int *idx, int max_per_atom);
 
 /* Replays a HILLS file into the grid (rows `step cv[D] height sigma`).
  * Replaces GH_t0_uniformGrid::init_hills (src/grids/GH_t0_uniformGrid.cu:101-192). */

@@ -3,6 +3,8 @@
 // structure factor, and neighbour-list reporting.
 #include "context.h"
 
+#include <algorithm>
+
 extern "C" {
 
 mtd_status mtd_get_peratom(mtd_ctx *c, const char *key, double *out) {
@@ -48,6 +50,67 @@ static mtd_status dcvdx(mtd_ctx *c, const std::string &cal) {
     return MTD_OK;
 }
 
+// The last step's neighbour lists of CAL `cal`, in caller order: kept[i] the
+// neighbours the CV uses (for STEINH Q those inside the cutoff_Natoms cap),
+// inrc[i] the neighbours inside the list criterion before the cap, and, when
+// `lists` is given, the caller indices of the kept neighbours in ascending order.
+static mtd_status host_lists(mtd_ctx *c, const std::string &cal, std::vector<int> &kept, std::vector<int> &inrc,
+                             std::vector<std::vector<int>> *lists) {
+    const Env *env = nullptr;
+    for (const Unit &u : c->units)
+        for (const std::string &cn : u.calnames)
+            if (cn == cal && u.env >= 0) env = &c->envs[u.env];
+    if (!env) return fail(c, MTD_ERR_INVALID_ARG, "no neighbour list for CAL " + cal);
+    if (c->step_gen == 0) return fail(c, MTD_ERR_INVALID_ARG, "no step has run");
+    const int n = c->n, M = env->M;
+    const size_t stride = (size_t)c->cap_n;
+    MTD_CU(cudaStreamSynchronize(c->st), "neighbour lists");
+    std::vector<int> perm(n), cnt(n), raw;
+    if (n > 0) {
+        MTD_CU(cudaMemcpy(perm.data(), c->perm, sizeof(int) * n, cudaMemcpyDeviceToHost), "perm");
+        MTD_CU(cudaMemcpy(cnt.data(), env->count, sizeof(int) * n, cudaMemcpyDeviceToHost), "neighbour counts");
+        raw.resize((size_t)M * stride);
+        MTD_CU(cudaMemcpy(raw.data(), env->list, sizeof(int) * raw.size(), cudaMemcpyDeviceToHost), "neighbour lists");
+    }
+    kept.assign(n, 0);
+    inrc.assign(n, 0);
+    if (lists) lists->assign(n, std::vector<int>());
+    const int low = (1 << kFlagBit) - 1;
+    for (int k = 0; k < n; ++k) {
+        const int i = perm[k];
+        const int m = std::min(cnt[k], M);
+        inrc[i] = cnt[k];
+        int nk = 0;
+        for (int t = 0; t < m; ++t) {
+            const int e = raw[(size_t)t * stride + k];
+            if (env->kind == ENV_Q && !(e & (1 << kFlagBit))) continue;
+            ++nk;
+            if (lists) (*lists)[i].push_back(perm[e & low]);
+        }
+        kept[i] = nk;
+        if (lists) std::sort((*lists)[i].begin(), (*lists)[i].end());
+    }
+    return MTD_OK;
+}
+
+mtd_status mtd_get_neighbors(mtd_ctx *c, const char *cal, int n, int *counts, int *idx, int max_per_atom) {
+    if (!c || !cal || !counts || n < 0 || (idx && max_per_atom < 0)) return MTD_ERR_INVALID_ARG;
+    if (n != c->n) return fail(c, MTD_ERR_INVALID_ARG, "atom count differs from the last step");
+    std::vector<int> kept, inrc;
+    std::vector<std::vector<int>> lists;
+    const mtd_status s = host_lists(c, cal, kept, inrc, idx ? &lists : nullptr);
+    if (s != MTD_OK) return s;
+    for (int i = 0; i < n; ++i) {
+        counts[i] = kept[i];
+        if (!idx) continue;
+        if (kept[i] > max_per_atom)
+            return fail(c, MTD_ERR_INVALID_ARG, "atom " + std::to_string(i) + " has " + std::to_string(kept[i]) +
+                                                    " neighbours, more than max_per_atom");
+        for (int t = 0; t < max_per_atom; ++t) idx[(size_t)i * max_per_atom + t] = t < kept[i] ? lists[i][t] : -1;
+    }
+    return MTD_OK;
+}
+
 mtd_status mtd_extract_peratom(mtd_ctx *c, const char *key, double *out, int n) {
     if (!c || !key || !out) return MTD_ERR_INVALID_ARG;
     std::string k(key);
@@ -62,6 +125,13 @@ mtd_status mtd_extract_peratom(mtd_ctx *c, const char *key, double *out, int n) 
         if (s != MTD_OK) return s;
         const int a = prop.back() - 'x';
         for (int t = 0; t < n; ++t) out[t] = c->h_dcv[3 * (size_t)t + a];
+        return MTD_OK;
+    }
+    if (prop == "nnb" || prop == "nrc") {   // neighbour counts (src/cvs/CVs_Steinhardt.cu:1324-1406)
+        std::vector<int> kept, inrc;
+        const mtd_status s = host_lists(c, cal, kept, inrc, nullptr);
+        if (s != MTD_OK) return s;
+        for (int t = 0; t < n; ++t) out[t] = prop == "nnb" ? kept[t] : inrc[t];
         return MTD_OK;
     }
     for (Unit &u : c->units) {

@@ -29,7 +29,7 @@ PREC = {"mixed": 0, "fp64": 1}
 # Every entry point declared in include/metad_b200.h.
 EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args", "mtd_eval_expression", "mtd_set_box", "mtd_init", "mtd_post_force",
            "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
-           "mtd_extract_peratom", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
+           "mtd_extract_peratom", "mtd_get_neighbors", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
            "mtd_set_stream", "mtd_profile_enable", "mtd_profile_report",
            "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc", "mtd_nn_state",
            "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
@@ -105,6 +105,7 @@ def lib():
         L.mtd_get_grid.argtypes = [vp, dp, C.c_int64]
         L.mtd_last_launch_count.argtypes = [vp]
         L.mtd_max_neighbors.argtypes = [vp, C.c_char_p]
+        L.mtd_get_neighbors.argtypes = [vp, C.c_char_p, C.c_int, ip, ip, C.c_int]
         L.mtd_set_types.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.mtd_needs_types.argtypes = [vp]
         L.mtd_set_domain.argtypes = [vp, C.c_int, C.c_int, ALLREDUCE_FN, vp]
@@ -324,6 +325,20 @@ class Metad:
 
     def max_neighbors(self, cal):
         return lib().mtd_max_neighbors(self._h, cal.encode())
+
+    def neighbors(self, cal, n, max_per_atom=None):
+        """Last step's neighbour lists of CAL `cal`: (counts[n], lists) with
+        lists an (n, max_per_atom) array of ascending caller indices, -1
+        padded (None when max_per_atom is None)."""
+        counts = np.zeros(n, dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        if max_per_atom is None:
+            self._check(lib().mtd_get_neighbors(self._h, cal.encode(), int(n), counts.ctypes.data_as(ip), None, 0))
+            return counts, None
+        idx = np.zeros((n, max_per_atom), dtype=np.int32)
+        self._check(lib().mtd_get_neighbors(self._h, cal.encode(), int(n), counts.ctypes.data_as(ip),
+                                            idx.ctypes.data_as(ip), int(max_per_atom)))
+        return counts, idx
 
     def autotune(self, n, x_ptr, mask_ptr=0, reps=5):
         """Device pointers (ints); returns (neighbour shape, q block, lambda block)."""

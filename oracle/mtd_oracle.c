@@ -477,6 +477,32 @@ int orc_steinh_q(int l, int n, const double *x, const orc_box *box, const int *i
 /* STEINH L: src/cvs/CVs_Steinhardt_Local.cu:1210-1580 (values),              */
 /* :695-745 (CV), :1622-2130 (gradient; restated from its exact derivation)   */
 /* ------------------------------------------------------------------------- */
+/* The neighbour lists orc_steinh_l uses: j != i with r <= rlist and
+ * sigma(r) >= eps (Local.cu:1257-1262), CSR with j ascending.  Caller frees
+ * *off and *nbr with orc_free. */
+int orc_local_lists(int n, const double *x, const orc_box *box, double rlist, const orc_sw *swr, double eps,
+                    int64_t **off_out, int **nbr_out) {
+    int64_t *off; int *nbr;
+    orc_pairs(n, x, box, rlist, &off, &nbr);
+    int64_t *o2 = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n + 1));
+    int *n2 = (int *)malloc(sizeof(int) * (size_t)(off[n] > 0 ? off[n] : 1));
+    o2[0] = 0;
+    for (int i = 0; i < n; i++) {
+        int64_t c = o2[i];
+        for (int64_t p = off[i]; p < off[i + 1]; p++) {
+            double d[3];
+            orc_minimg(box, x + 3 * i, x + 3 * nbr[p], d);
+            if (orc_sw_f(swr, sqrt(orc_r2(d))) >= eps) n2[c++] = nbr[p];
+        }
+        o2[i + 1] = c;
+    }
+    free(off);
+    free(nbr);
+    *off_out = o2;
+    *nbr_out = n2;
+    return 0;
+}
+
 int orc_steinh_l(int l, int n, const double *x, const orc_box *box, const int *ingroup,
                  double rlist, const orc_sw *swr, double eps, const orc_sw *swcv, int mode,
                  double *LQ, double *LQlm, double *qlm, double *NF, int *nnb,

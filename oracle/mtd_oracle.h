@@ -70,6 +70,10 @@ int orc_steinh_l(int l, int n, const double *x, const orc_box *box, const int *i
                  double *LQ, double *LQlm, double *qlm, double *NF, int *nnb,
                  double *cv, double *sums, double *grad);
 
+/* The lists of orc_steinh_l: j != i, r <= rlist, sigma(r) >= eps; CSR, j ascending. */
+int orc_local_lists(int n, const double *x, const orc_box *box, double rlist, const orc_sw *swr, double eps,
+                    int64_t **off, int **nbr);
+
 /* STRU_FACTOR (Debye form): S_i = 1 + sum_j sin(q r)/(q r) s(r), r2 in [1e-12, rc^2].
  * mode 0 AVE, 1 COUNT (src/cvs/CVs_Strufactor.cu:642-674, :1082-1271). */
 int orc_debye(int n, const double *x, const orc_box *box, const int *ingroup,

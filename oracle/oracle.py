@@ -92,6 +92,10 @@ def lib():
         L.orc_grid_value.restype = C.c_double
         L.orc_grid_value.argtypes = [C.c_int, ip, dp, dp, dp, dp]
         L.orc_hill_sum.argtypes = [C.c_int, C.c_int, dp, dp, dp, C.c_int, dp, dp, dp]
+        i64pp, ipp = C.POINTER(C.POINTER(C.c_int64)), C.POINTER(C.POINTER(C.c_int))
+        L.orc_pairs.argtypes = [C.c_int, dp, C.POINTER(Box), C.c_double, i64pp, ipp]
+        L.orc_local_lists.argtypes = [C.c_int, dp, C.POINTER(Box), C.c_double, C.POINTER(Sw), C.c_double, i64pp, ipp]
+        L.orc_free.argtypes = [C.c_void_p]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
         _LIB = L
@@ -181,6 +185,32 @@ def steinh_q(l, x, L, rc, cap, mode="AVE", swcv=None, ingroup=None, periodic=(1,
     if grad:
         out["grad"] = gr.reshape(n, 3)
     return out
+
+
+def _csr(fn, n, *args):
+    off, nbr = C.POINTER(C.c_int64)(), C.POINTER(C.c_int)()
+    fn(*args, C.byref(off), C.byref(nbr))
+    o = np.ctypeslib.as_array(off, shape=(n + 1,)).copy()
+    m = int(o[-1])
+    v = np.ctypeslib.as_array(nbr, shape=(max(m, 1),))[:m].copy()
+    lib().orc_free(C.cast(off, C.c_void_p))
+    lib().orc_free(C.cast(nbr, C.c_void_p))
+    return o, v
+
+
+def pairs(x, L, rcut, periodic=(1, 1, 1)):
+    """All ordered pairs (i, j != i) with r2 <= rcut^2: CSR (off[n+1], nbr), j ascending."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    box = make_box(L, periodic)
+    return _csr(lib().orc_pairs, x.shape[0], x.shape[0], _dp(x), C.byref(box), float(rcut))
+
+
+def local_lists(x, L, rlist, swr, eps=1e-6, periodic=(1, 1, 1)):
+    """The neighbour lists of steinh_l (r <= rlist, sigma(r) >= eps): CSR, j ascending."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    box = make_box(L, periodic)
+    return _csr(lib().orc_local_lists, x.shape[0], x.shape[0], _dp(x), C.byref(box), float(rlist), C.byref(swr),
+                float(eps))
 
 
 LOCAL_MODES = {"MEAN_SOLID": 0, "AVE": 0, "NSOLID": 1, "SW_FUNC": 1, "FRAC": 2}
