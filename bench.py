@@ -39,15 +39,22 @@ sys.path[:0] = [os.path.join(ROOT, "metad-toy_b200")]
 METRIC = "CV+bias+force atom-steps/s at 256k atoms; NN vs exact hill bias, same error"
 UNIT = "atom-steps/s"
 WORKLOAD = "256k-atom FCC/BCC/liquid slabs, STEINH L Q4+Q6 MEAN_SOLID with forces, 2D 200x200 WT grid, PACE 10"
+# neighbour lists: candidates within cutoff + 1.0 A kept across steps, filtered
+# to the exact lists every step, rebuilt when an atom moves more than 0.5 A and
+# at least every 10 steps (the timed steps include those rebuilds)
+SKIN, EVERY = 1.0, 10
 
 
-def fix_args():
-    return ["GAUSSIAN", 0.01, 0.005, 9.0, "PACE", 10, "TEMP", 300.0,
-            "CAL", "NAME", "ST", "SW_FUNC", "STEP", "r_0", 3.9,
-            "CAL", "NAME", "Q4", "STEINH", "L", 4, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18, "SW_FUNC_r", "ST",
-            "CAL", "NAME", "Q6", "STEINH", "L", 6, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18, "SW_FUNC_r", "ST",
-            "SYMBOL", "v1", "Q4.MEAN_SOLID", "SYMBOL", "v2", "Q6.MEAN_SOLID",
-            "CV_dim", 2, "DIM", 1, 0, 1, 200, "v1", "DIM", 2, 0, 1, 200, "v2", "WT", 1]
+def fix_args(skin=SKIN, every=EVERY):
+    a = ["GAUSSIAN", 0.01, 0.005, 9.0, "PACE", 10, "TEMP", 300.0,
+         "CAL", "NAME", "ST", "SW_FUNC", "STEP", "r_0", 3.9,
+         "CAL", "NAME", "Q4", "STEINH", "L", 4, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18, "SW_FUNC_r", "ST",
+         "CAL", "NAME", "Q6", "STEINH", "L", 6, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18, "SW_FUNC_r", "ST",
+         "SYMBOL", "v1", "Q4.MEAN_SOLID", "SYMBOL", "v2", "Q6.MEAN_SOLID",
+         "CV_dim", 2, "DIM", 1, 0, 1, 200, "v1", "DIM", 2, 0, 1, 200, "v2", "WT", 1]
+    if skin > 0:
+        a += ["NEIGH_SKIN", skin, "NEIGH_EVERY", every]
+    return a
 
 
 def load_system(seed=2024, copies=4):
@@ -741,6 +748,7 @@ def main():
         # timed, device-resident
         if dist:
             dist.barrier()
+        builds0 = m.neighbor_stats()[0]
         torch.cuda.synchronize()
         for k in range(args.steps):
             flush.zero_()
@@ -750,6 +758,8 @@ def main():
         m.sync()
         torch.cuda.synchronize()
         dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+        builds_timed, skin_active = m.neighbor_stats()
+        builds_timed -= builds0
 
         # e2e through the C ABI on pinned host buffers
         m.set_stream(0)
@@ -804,6 +814,12 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "autotuned_shapes": {"neighbors": ["fast/256", "fast/128", "flat/128"][tuned[0]],
                                             "q_block": tuned[1], "lambda_block": tuned[2]},
+                       "neighbor_lists": {"skin_A": SKIN, "rebuild_every_steps": EVERY,
+                                          "rebuild_when_moved_A": SKIN / 2, "skin_active": skin_active,
+                                          "rebuilds_in_timed_steps": builds_timed,
+                                          "rule": "exact lists every step, filtered from candidates within "
+                                                  "cutoff + skin; cell list and candidates rebuilt when an atom "
+                                                  "moves more than skin/2 and at least every 10 steps"},
                        "cv": [float(v) for v in m.cv]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps},

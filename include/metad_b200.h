@@ -183,6 +183,20 @@ mtd_status mtd_extract_peratom(mtd_ctx *ctx, const char *key, double *out, int n
  * get_environment_Steinhardt_LocalQ (src/cvs/CVs_Steinhardt_Local.cu:1210-1285). */
 mtd_status mtd_get_neighbors(mtd_ctx *ctx, const char *cal, int n, int *counts, int *idx, int max_per_atom);
 
+/* Skin lists (the `fix metad` extension keywords NEIGH_SKIN s and NEIGH_EVERY
+ * k): neighbour candidates within cutoff + s are kept across steps and
+ * filtered to the exact lists every step; the cell list and the candidates
+ * are rebuilt when an atom has moved more than s / 2 since the last rebuild,
+ * when a position is not finite, when the atom count or the box changes, and
+ * at least every k steps (k = 0: only then).  The neighbour sets equal the
+ * per-step ones exactly (the sums may differ in their last bits: the
+ * neighbours come in another order).  rebuilds receives the rebuilds so far,
+ * skin_active whether the last step used skin lists (they apply where every
+ * periodic side is at least 2 (cutoff + s) and holds 3 cells of cutoff + s).
+ * The reference reads LAMMPS's skin lists and filters them by r < cutoff_r
+ * every step (src/cvs/CVs_Steinhardt.cu:135-147, src/core/neigh_hub.cu:191-222). */
+mtd_status mtd_neighbor_stats(mtd_ctx *ctx, int64_t *rebuilds, int *skin_active);
+
 /* Replays a HILLS file into the grid (rows `step cv[D] height sigma`).
  * Replaces GH_t0_uniformGrid::init_hills (src/grids/GH_t0_uniformGrid.cu:101-192). */
 mtd_status mtd_hills_replay(mtd_ctx *ctx, const char *path);

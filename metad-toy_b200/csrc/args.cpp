@@ -454,6 +454,14 @@ std::string parse_fix_args(int narg, const char *const *arg, const GroupTable &g
             if (!need_int(c, i + 1, v, "WT")) return c.err;
             cfg.wt = v != 0;
             i += 2;
+        } else if (!std::strcmp(kw, "NEIGH_SKIN")) {   // extension: neighbour lists kept across steps
+            if (!need_double(c, i + 1, cfg.neigh_skin, "NEIGH_SKIN")) return c.err;
+            if (!(cfg.neigh_skin >= 0.0)) return "Error: NEIGH_SKIN must be >= 0.";
+            i += 2;
+        } else if (!std::strcmp(kw, "NEIGH_EVERY")) {
+            if (!need_int(c, i + 1, cfg.neigh_every, "NEIGH_EVERY")) return c.err;
+            if (cfg.neigh_every < 0) return "Error: NEIGH_EVERY must be >= 0.";
+            i += 2;
         } else {
             return std::string("Error: Unknown keyword in fix metadynamics command: ") + kw;
         }

@@ -79,6 +79,10 @@ struct Config {
     int nn_refit = 1000;          // NN_REFIT: new hills between fits
     int nn_iters = 2000;          // NN_ITERS: Adam steps per fit
     bool hill_list() const { return nn || cv_dim > 3; }
+    // neighbour lists kept across steps (extensions, no reference keyword: the
+    // reference reads LAMMPS's skin lists, src/cvs/CVs_Steinhardt.cu:135-147)
+    double neigh_skin = 0.0;      // NEIGH_SKIN: candidates within cutoff + skin; 0 = exact lists rebuilt every step
+    int neigh_every = 0;          // NEIGH_EVERY: rebuild at least every k steps (0: only when an atom moved > skin/2)
     std::map<std::string, SwParams> sws;
     std::map<std::string, CalDef> cals;     // std::map: alphabetical order, as cal_registry
     std::vector<SymbolDef> symbols;

@@ -7,15 +7,6 @@
 namespace mtd {
 namespace ctx {
 
-// Grows every list that a step reported too small (as mtd_sync does).
-void grow_lists(mtd_ctx *c, unsigned need) {
-    for (Env &e : c->envs)
-        if (e.M < (int)need) {
-            e.M = (((int)need + 8) + 3) & ~3;
-            alloc_env(c, e, c->cap_n);
-        }
-}
-
 // The tuning passes of one idle context: a values pass on the given
 // positions (lists grown until they fit), then each interchangeable kernel
 // shape timed over `reps` launches with CUDA events on the context stream,
@@ -32,12 +23,13 @@ mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask
         DevStatus hs{};
         MTD_CU(cudaMemcpyAsync(&hs, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->st), "status");
         MTD_CU(cudaStreamSynchronize(c->st), "autotune");
-        if (hs.overflow == 0) break;
+        if (hs.overflow == 0 && hs.cand_overflow == 0) break;
         if (attempt == 3) {
             s = fail(c, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded");
             break;
         }
-        grow_lists(c, hs.overflow);
+        s = grow_lists(c, hs.overflow, hs.cand_overflow);
+        if (s != MTD_OK) break;
     }
     if (s != MTD_OK) {
         c->prof.on = prof;
@@ -57,7 +49,8 @@ mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask
         return ms;
     };
     const CellGrid g = c->last_grid;
-    const SysDev sd = c->last_sys;
+    SysDev sd = c->last_sys;
+    sd.skin = nullptr;   // the timed neighbour searches run in full (no skin gate)
     float best = 1e30f;
     for (int v = 0; v < 3; ++v) {
         const float t = timed([&] {

@@ -321,7 +321,8 @@ __device__ void phase_deposit(const BiasPlan &P, const double *s, double w, cons
 // A step whose neighbour lists overflowed is repeated by the host: it must
 // leave no hill and no bias force behind.
 __device__ __forceinline__ bool status_failed(const DevStatus *st) {
-    return st && (*(volatile const unsigned *)&st->overflow != 0u || *(volatile const unsigned *)&st->bad_pos != 0u);
+    return st && (*(volatile const unsigned *)&st->overflow != 0u || *(volatile const unsigned *)&st->bad_pos != 0u ||
+                  *(volatile const unsigned *)&st->cand_overflow != 0u);
 }
 __device__ __forceinline__ bool step_failed(const BiasPlan &P) { return status_failed(P.status); }
 
@@ -735,7 +736,7 @@ __global__ void __launch_bounds__(256) k_unit_sums(const BiasPlan *__restrict__ 
         off += 2 * U.K + 1;
     }
     if (threadIdx.x == 0) {
-        out[off] = P.status ? (double)P.status->overflow : 0.0;
+        out[off] = P.status ? (double)max(P.status->overflow, P.status->cand_overflow) : 0.0;
         out[off + 1] = P.status ? (double)P.status->bad_pos : 0.0;
     }
 }

@@ -119,6 +119,8 @@ struct DevStatus {
     unsigned int nan_force;       // a force component was not finite
     unsigned int timeout;         // a bounded wait gave up
     unsigned int bad_pos;         // an atom position was not finite (NaN or Inf)
+    unsigned int cand_overflow;   // max skin-list candidate count seen when above capacity
+    unsigned int pad[3];
 };
 
 // First statement of every step kernel: wait until the previous kernel of the

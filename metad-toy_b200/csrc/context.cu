@@ -61,10 +61,10 @@ void use_slot(mtd_ctx *c, int k) {
     c->h_nhills = &o.nhills;
 }
 
-CellGrid make_grid(const mtd_ctx *c) {
+CellGrid make_grid(const mtd_ctx *c, double extra) {
     CellGrid g{};
     double rmax = 0.0;
-    for (const Env &e : c->envs) rmax = std::fmax(rmax, env_cutoff(e));
+    for (const Env &e : c->envs) rmax = std::fmax(rmax, env_cutoff(e) + extra);
     double Lmax = 0.0;
     for (int d = 0; d < 3; ++d) Lmax = std::fmax(Lmax, c->hi[d] - c->lo[d]);
     const double guard = 1e-6 * Lmax + 1e-6;
@@ -89,6 +89,28 @@ CellGrid make_grid(const mtd_ctx *c) {
     }
     g.ncell = (int)ncell;
     return g;
+}
+
+static bool same_grid(const CellGrid &a, const CellGrid &b) {
+    for (int d = 0; d < 3; ++d)
+        if (a.nc[d] != b.nc[d] || a.periodic[d] != b.periodic[d] || a.L[d] != b.L[d] || a.lo[d] != b.lo[d])
+            return false;
+    return true;
+}
+
+bool skin_grid(const mtd_ctx *c, CellGrid &g) {
+    const double skin = c->cfg.neigh_skin;
+    if (skin > 0.0 && !c->envs.empty()) {
+        double rmax = 0.0;
+        for (const Env &e : c->envs) rmax = std::fmax(rmax, env_cutoff(e) + skin);
+        g = make_grid(c, skin);
+        bool ok = true;
+        for (int d = 0; d < 3; ++d)
+            if (g.periodic[d] && (g.nc[d] < 3 || g.L[d] < 2.0 * rmax)) ok = false;
+        if (ok) return true;
+    }
+    g = make_grid(c);
+    return false;
 }
 
 // Neighbour criterion of an environment; the FP32 band [lo2, hi2] around the
@@ -123,6 +145,15 @@ int estimate_M(const mtd_ctx *c, double rc, int n) {
     int M = (int)std::ceil(1.6 * expect + 8.0);
     M = (M + 3) & ~3;
     return M < 8 ? 8 : M;
+}
+
+mtd_status alloc_cand(mtd_ctx *c, Env &e, int npad) {
+    dfree(e.cand);
+    dfree(e.ccount);
+    MTD_CU(dalloc(&e.cand, sizeof(int) * (size_t)e.Mc * npad), "skin candidates");
+    MTD_CU(dalloc(&e.ccount, sizeof(int) * (size_t)npad), "skin candidates");
+    c->skin_valid = false;
+    return MTD_OK;
 }
 
 mtd_status alloc_env(mtd_ctx *c, Env &e, int npad) {
@@ -208,11 +239,26 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
         c->cap_vpart = 8 * ((cap + 255) / 256) * (int)(c->units.size() + 1);
         MTD_CU(dalloc(&c->d_vpart, sizeof(double) * 8 * (size_t)c->cap_vpart), "virial partials");
         c->cap_n = cap;
+        const bool skin = c->cfg.neigh_skin > 0.0 && !c->envs.empty();
+        if (skin) {
+            dfree(c->xref);
+            MTD_CU(dalloc(&c->xref, sizeof(double) * 3 * (size_t)cap), "skin positions");
+            if (!c->d_skin) {
+                MTD_CU(dalloc(&c->d_skin, sizeof(SkinState)), "skin state");
+                MTD_CU(cudaMemset(c->d_skin, 0, sizeof(SkinState)), "skin state");
+            }
+        }
+        c->skin_valid = false;
         for (Env &e : c->envs) {
             if (e.M == 0) e.M = estimate_M(c, e.rc, n);
             if (e.kind == ENV_Q && e.M > 64) e.M = 64;
             mtd_status s = alloc_env(c, e, cap);
             if (s != MTD_OK) return s;
+            if (skin) {
+                if (e.Mc == 0) e.Mc = estimate_M(c, e.rc + c->cfg.neigh_skin, n);
+                s = alloc_cand(c, e, cap);
+                if (s != MTD_OK) return s;
+            }
         }
         for (Unit &u : c->units) {
             mtd_status s = alloc_unit(c, u, cap);
@@ -229,9 +275,30 @@ mtd_status ensure_cells(mtd_ctx *c, int ncell) {
         dfree(c->start);
         const int cap = ncell + 1 + ncell / 4;
         MTD_CU(dalloc(&c->count, sizeof(int) * (size_t)cap), "cell counts");
+        // zero once here; every build's scatter pass zeroes the counts it used
+        MTD_CU(cudaMemset(c->count, 0, sizeof(int) * (size_t)cap), "cell counts");
+        c->skin_valid = false;
         // ncell + 1 starts followed by the scan's per-1024-cell block totals
         MTD_CU(dalloc(&c->start, sizeof(int) * (size_t)(cap + 1 + cap / 1024 + 2)), "cell starts");
         c->cap_cell = cap;
+    }
+    return MTD_OK;
+}
+
+mtd_status grow_lists(mtd_ctx *c, unsigned need, unsigned cand_need) {
+    for (Env &e : c->envs) {
+        if (need > 0 && e.M < (int)need) {
+            if (e.kind == ENV_Q && need > 64)
+                return fail(c, MTD_ERR_UNSUPPORTED, "STEINH Q: more than 64 atoms within cutoff_r");
+            e.M = (((int)need + 8) + 3) & ~3;
+            const mtd_status s = alloc_env(c, e, c->cap_n);
+            if (s != MTD_OK) return s;
+        }
+        if (cand_need > 0 && e.Mc < (int)cand_need) {
+            e.Mc = (((int)cand_need + 8) + 3) & ~3;
+            const mtd_status s = alloc_cand(c, e, c->cap_n);   // the next step rebuilds
+            if (s != MTD_OK) return s;
+        }
     }
     return MTD_OK;
 }
@@ -527,7 +594,23 @@ template <typename T> void run_values(mtd_ctx *c, const CellGrid &g, const doubl
     cudaStream_t st = c->st;
     for (Unit &u : c->units) {
         if (u.kind == CAL_STEINH_L) {
-            launch_local_values<T>(local_dev<T>(c, u, g), st);
+            LocalDev<T> d = local_dev<T>(c, u, g);
+            if (c->skin_last && u.env >= 0 && u.env < (int)c->env_fused.size() && c->env_fused[u.env]) {
+                // skin lists: this unit's q pass filters its candidates first
+                const Env &e = c->envs[u.env];
+                d.filter = 1;
+                d.fgf = geo_f(g, c->pf);
+                d.fgd = geo_d(g, c->xs);
+                d.fspec = neigh_spec(e);
+                d.cand = env_dev(e);
+                d.cand.list = e.cand;
+                d.cand.count = e.ccount;
+                d.cand.M = e.Mc;
+                d.status = c->d_status;
+                d.reset = c->skin_reset_pending ? c->d_skin : nullptr;
+                c->skin_reset_pending = false;
+            }
+            launch_local_values<T>(d, st);
             c->launches += 2;
         } else if (u.kind == CAL_STEINH_Q) {
             launch_global_values<T>(global_dev<T>(c, u, g), st);
@@ -614,7 +697,8 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
                "domain totals");
         c->plan_dirty = true;
     }
-    CellGrid g = make_grid(c);
+    CellGrid g;
+    const bool skin = skin_grid(c, g);
     c->last_grid = g;
     if (c->plan_dirty) {
         build_plan(c);
@@ -628,13 +712,69 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
         if (sc != MTD_OK) return sc;
         s.count = c->count;
         s.start = c->start;
-        c->launches += launch_build_cells(g, s, c->st);
-        for (Env &e : c->envs) {
-            NeighSpec ns = neigh_spec(e);
-            ns.variant = c->tune_nbr;
-            launch_neighbors(g, s, ns, env_dev(e), c->d_status, c->st);
-            c->launches += ns.cap > 0 ? 2 : 1;
+        if (skin) {
+            // kept sorted order and candidate lists: repack and test every
+            // step, rebuild (the gated kernels) only when due, then filter
+            // the candidates to the exact lists at the current positions
+            const bool same = c->skin_valid && c->skin_n == n && same_grid(c->skin_grid, g);
+            s.skin = c->d_skin;
+            s.xref = c->xref;
+            launch_refresh(g, s, c->cfg.neigh_every, 0.5 * c->cfg.neigh_skin, same ? 0 : 1, c->st);
+            c->launches += 1 + launch_build_cells(g, s, c->st);
+            for (Env &e : c->envs) {
+                NeighSpec ns = neigh_spec(e);
+                ns.variant = c->tune_nbr;
+                ns.kind = NK_CAND;
+                ns.cap = 0;
+                const double rb = e.rc + c->cfg.neigh_skin;
+                ns.hi2 = (float)(rb * rb * (1.0 + 2e-5) + 1e-4);
+                NeighDev cd = env_dev(e);
+                cd.list = e.cand;
+                cd.count = e.ccount;
+                cd.M = e.Mc;
+                launch_neighbors(g, s, ns, cd, c->d_status, c->st);
+                c->launches += 1;
+            }
+            // an environment that only one STEINH L unit reads is filtered
+            // inside that unit's q pass; the others by their own kernel
+            c->env_fused.assign(c->envs.size(), 0);
+            std::vector<int> users(c->envs.size(), 0);
+            for (const Unit &u : c->units)
+                if (u.env >= 0) users[u.env] += 1;
+            for (const Unit &u : c->units)
+                if (u.env >= 0 && u.kind == CAL_STEINH_L && users[u.env] == 1) c->env_fused[u.env] = 1;
+            bool first = true;
+            for (size_t ei = 0; ei < c->envs.size(); ++ei) {
+                if (c->env_fused[ei]) continue;
+                Env &e = c->envs[ei];
+                const NeighSpec ns = neigh_spec(e);
+                NeighDev cd = env_dev(e);
+                cd.list = e.cand;
+                cd.count = e.ccount;
+                cd.M = e.Mc;
+                launch_filter(g, s, ns, env_dev(e), cd, c->d_status, first ? c->d_skin : nullptr, c->st);
+                first = false;
+                c->launches += 1;
+                if (ns.cap > 0) {
+                    launch_select_cap(g, s, ns, env_dev(e), c->st);
+                    c->launches += 1;
+                }
+            }
+            c->skin_reset_pending = first;
+            c->skin_valid = true;
+            c->skin_n = n;
+            c->skin_grid = g;
+        } else {
+            c->launches += launch_build_cells(g, s, c->st);
+            for (Env &e : c->envs) {
+                NeighSpec ns = neigh_spec(e);
+                ns.variant = c->tune_nbr;
+                launch_neighbors(g, s, ns, env_dev(e), c->d_status, c->st);
+                c->launches += ns.cap > 0 ? 2 : 1;
+            }
+            c->skin_valid = false;
         }
+        c->skin_last = skin;
     }
     for (const Unit &u : c->units)
         if (u.chem && c->types_n != n)
@@ -765,8 +905,9 @@ mtd_status drain(mtd_ctx *c, bool block) {
         }
         c->fifo.pop_front();
         use_slot(c, p.slot);
-        if (c->h_status->overflow) {
+        if (c->h_status->overflow || c->h_status->cand_overflow) {
             c->overflow_seen = std::max(c->overflow_seen, c->h_status->overflow);
+            c->overflow_cand_seen = std::max(c->overflow_cand_seen, c->h_status->cand_overflow);
             continue;
         }
         c->pending = true;
@@ -912,7 +1053,10 @@ void mtd_destroy(mtd_ctx *c) {
     if (c->h_slots) drain(c, true);   // hills of steps not yet collected still reach the HILLS file
     for (Env &e : c->envs) {
         dfree(e.list); dfree(e.count); dfree(e.key_r2); dfree(e.key_id); dfree(e.nkept);
+        dfree(e.cand); dfree(e.ccount);
     }
+    dfree(c->xref);
+    dfree(c->d_skin);
     for (Unit &u : c->units) {
         void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S, &u.w};
         for (void **a : arrs) dfree(*a);
@@ -957,6 +1101,7 @@ mtd_status mtd_set_box(mtd_ctx *c, const double lo[3], const double hi[3], const
         if (c->periodic[d] && hi[d] - lo[d] < 2.0 * rmax)
             return fail(c, MTD_ERR_INVALID_ARG, "Warning: box < cutoff_r, please check your system ! (periodic box must be >= 2 cutoff_r)");
     c->box_set = true;
+    c->skin_valid = false;
     return MTD_OK;
 }
 
@@ -1059,18 +1204,11 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
         // the forces go back in the same stream pass (a failed attempt's are overwritten by the retry)
         MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
         MTD_CU(cudaStreamSynchronize(c->st), "step");
-        if (c->h_status->overflow == 0) break;
+        if (c->h_status->overflow == 0 && c->h_status->cand_overflow == 0) break;
         c->fifo.pop_back();   // the failed attempt is not collected
         // neighbour capacity too small: grow and run the step again
-        const int need = (int)c->h_status->overflow;
-        for (Env &e : c->envs) {
-            if (e.M >= need) continue;
-            if (e.kind == ENV_Q && need > 64)
-                return fail(c, MTD_ERR_UNSUPPORTED, "STEINH Q: more than 64 atoms within cutoff_r");
-            e.M = ((need + 8) + 3) & ~3;
-            s = alloc_env(c, e, c->cap_n);
-            if (s != MTD_OK) return s;
-        }
+        s = grow_lists(c, c->h_status->overflow, c->h_status->cand_overflow);
+        if (s != MTD_OK) return s;
         if (attempt == 3) return fail(c, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded");
     }
     s = drain(c, true);
@@ -1166,16 +1304,15 @@ mtd_status mtd_sync(mtd_ctx *c) {
     MTD_CU(cudaStreamSynchronize(c->st), "sync");
     const mtd_status sd = drain(c, true);
     if (sd != MTD_OK) return sd;
-    if (c->overflow_seen) {
-        const int need = (int)c->overflow_seen;
+    if (c->overflow_seen || c->overflow_cand_seen) {
+        const unsigned need = c->overflow_seen, cneed = c->overflow_cand_seen;
         c->overflow_seen = 0;
-        for (Env &e : c->envs)
-            if (e.M < need) {
-                e.M = ((need + 8) + 3) & ~3;
-                alloc_env(c, e, c->cap_n);
-            }
+        c->overflow_cand_seen = 0;
+        const mtd_status sg = grow_lists(c, need, cneed);
+        if (sg != MTD_OK) return sg;
         cudaMemset(c->d_status, 0, sizeof(DevStatus));
         c->h_status->overflow = 0;
+        c->h_status->cand_overflow = 0;
         c->pending = false;
         return fail(c, MTD_ERR_NEIGH_OVERFLOW, "neighbour list capacity exceeded; capacity grown, repeat the step");
     }

@@ -42,6 +42,10 @@ struct Env {
     int *key_id = nullptr;
     int *nkept = nullptr;
     std::vector<int> cals;
+    // skin lists (NEIGH_SKIN): candidates within cutoff + skin, slot-major [Mc][npad]
+    int Mc = 0;
+    int *cand = nullptr;
+    int *ccount = nullptr;
 };
 
 struct Unit {
@@ -210,6 +214,16 @@ struct mtd_ctx {
     int staged_n = -1;                   // atoms uploaded and not yet stepped (-1: none)
     bool staged_mask = false;
     int fix_groupbit = 1;
+    // skin lists (NEIGH_SKIN > 0): candidate lists and the sorted order kept across steps
+    SkinState *d_skin = nullptr;
+    double *xref = nullptr;              // sorted raw coordinates at the last rebuild
+    bool skin_valid = false;             // the kept sorted order and candidates match n and the grid
+    int skin_n = -1;
+    CellGrid skin_grid{};
+    bool skin_last = false;              // the last step used the skin lists
+    std::vector<char> env_fused;         // skin lists: environment filtered inside its STEINH L unit's q pass
+    bool skin_reset_pending = false;     // the step's first fused q pass closes the skin gate
+    unsigned overflow_cand_seen = 0;     // largest candidate count of an overflowed step drained since mtd_sync
 };
 
 namespace mtd {
@@ -228,10 +242,17 @@ mtd_status cuda_check(mtd_ctx *c, cudaError_t e, const char *what);
 size_t real_size(const mtd_ctx *c);
 int record_stride(const mtd_ctx *c, const Unit &u);
 void use_slot(mtd_ctx *c, int k);
-CellGrid make_grid(const mtd_ctx *c);
+CellGrid make_grid(const mtd_ctx *c, double extra = 0.0);
+// Skin lists apply (NEIGH_SKIN > 0, every periodic side >= 2 (cutoff + skin)
+// and >= 3 cells of cutoff + skin): the step's cell grid into g either way.
+bool skin_grid(const mtd_ctx *c, CellGrid &g);
+// Grows the lists a step reported too small: exact lists to hold `need`
+// neighbours, skin candidate lists `cand_need` (which forces a rebuild).
+mtd_status grow_lists(mtd_ctx *c, unsigned need, unsigned cand_need);
 NeighSpec neigh_spec(const Env &e);
 int estimate_M(const mtd_ctx *c, double rc, int n);
 mtd_status alloc_env(mtd_ctx *c, Env &e, int npad);
+mtd_status alloc_cand(mtd_ctx *c, Env &e, int npad);
 mtd_status alloc_unit(mtd_ctx *c, Unit &u, int npad);
 mtd_status ensure_capacity(mtd_ctx *c, int n);
 mtd_status ensure_cells(mtd_ctx *c, int ncell);
@@ -282,7 +303,6 @@ mtd_status replay_records(mtd_ctx *c, const std::vector<HillRec> &recs);
 mtd_status read_hills(mtd_ctx *c, const std::string &path, std::vector<HillRec> &recs, bool *exists);
 
 // autotune.cu
-void grow_lists(mtd_ctx *c, unsigned need);
 mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask, int reps, int *choice);
 
 }  // namespace ctx

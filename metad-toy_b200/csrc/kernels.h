@@ -64,6 +64,20 @@ template <> inline Geo<double> make_geo<double>(const CellGrid &g, const float4 
     return r;
 }
 
+// Skin lists (NEIGH_SKIN): candidate lists built at cutoff + skin are kept
+// across steps.  Every step k_refresh repacks the positions in the kept
+// sorted order and sets `gate` when a rebuild is due (an atom moved more than
+// skin / 2 since the build, a non-finite position, `age` reached NEIGH_EVERY,
+// or the host forced it); the rebuild kernels return at once while the gate
+// is closed.  The first kernel after them updates age / builds and clears the
+// gate for the next step.
+struct SkinState {
+    unsigned int gate;            // 1: this step rebuilds the cell list and candidate lists
+    unsigned int age;             // steps the current candidate lists have served
+    unsigned int builds;          // rebuilds so far
+    unsigned int pad;
+};
+
 struct SysDev {
     int n, npad;
     const double *x;      // caller order, AoS n*3
@@ -76,13 +90,16 @@ struct SysDev {
     double *xs;           // sorted raw coordinates AoS npad*3
     float4 *pf;           // sorted cell-relative coordinates + packed cell
     DevStatus *status;    // k_bin flags non-finite positions (bad_pos)
+    SkinState *skin;      // skin lists: the rebuild kernels are gated on skin->gate (null: every step)
+    double *xref;         // skin lists: sorted raw coordinates at the last rebuild (AoS npad*3)
 };
 
 // Neighbour criteria (the reference's per-CV filters).
 enum NeighKind {
     NK_RANGE = 0,    // 1e-12 <= r2 <= rc2           (STEINH Q :1358, STRU_FACTOR :1048)
     NK_STEP = 1,     // r2 <= rc2 and r < r0         (STEINH L with a STEP switch)
-    NK_SWITCH = 2    // r2 <= rc2 and sw(r) >= eps   (STEINH L, Local.cu:1257-1262)
+    NK_SWITCH = 2,   // r2 <= rc2 and sw(r) >= eps   (STEINH L, Local.cu:1257-1262)
+    NK_CAND = 3      // skin-list candidates: FP32 r2 <= hi2 (a superset of cutoff + skin)
 };
 
 // The FP32 distance decides a candidate when it is outside [lo2, hi2]; inside
@@ -151,10 +168,22 @@ void launch_k(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t sm
 }
 
 // ------------------------------------------------------------------ neighbours
+// Cell list (counting sort by cell).  The cell counts must be zero on entry:
+// they are zeroed when allocated and again by the scatter pass after use.
 // Returns the number of kernels launched.
 int launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st);
+// Neighbour lists from the cell list (ns.kind NK_CAND: skin-list candidates;
+// for a cap, the cap selection follows unless ns.kind is NK_CAND).
 void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, DevStatus *status,
                       cudaStream_t st);
+void launch_select_cap(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, cudaStream_t st);
+// Skin lists: the per-step repack and rebuild decision (force: the kept
+// sorted order is not valid, rebuild without reading it), and the exact
+// lists of one environment filtered from its candidates (reset: the first
+// kernel after the gated rebuild, which clears the gate).
+void launch_refresh(const CellGrid &g, const SysDev &s, int every, double half_skin, int force, cudaStream_t st);
+void launch_filter(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, NeighDev cand,
+                   DevStatus *status, SkinState *reset, cudaStream_t st);
 
 // ------------------------------------------------------------------ STEINH L
 template <typename T> struct LocalDev {
@@ -170,6 +199,14 @@ template <typename T> struct LocalDev {
     double *partials;           // [nblocks][8]: S1A S0A S1B S0B N
     const double *coef;         // c1A c2A c1B c2B (written by the bias kernel)
     int qblock, lblock;         // threads per block of the q and lambda passes (0: kBlock); same results
+    // skin lists: the q pass first filters this unit's candidates into nb (filter != 0)
+    int filter;
+    GeoF fgf;                   // FP32 cell-relative positions (the exact decision's first test)
+    GeoD fgd;                   // FP64 raw positions (the guard band)
+    NeighSpec fspec;
+    NeighDev cand;
+    DevStatus *status;
+    SkinState *reset;           // the first kernel after the gated rebuild: closes the gate
 };
 template <typename T> void launch_local_values(const LocalDev<T> &d, cudaStream_t st);
 // Reals per STEINH L record (both orders): a multiple of 32 bytes.

@@ -20,7 +20,7 @@
 // (Q4 and Q6 of one neighbour environment) are fused in one pass.  With a STEP
 // switch sigma = 1 and sigma' = 0 on every listed pair, so the LQ and lambda
 // passes need neighbour indices only.
-#include "kernels.h"
+#include "filter.cuh"
 #include "ylm.cuh"
 
 namespace mtd {
@@ -129,22 +129,43 @@ __device__ __forceinline__ int nb_index(const NeighDev &nb, int npad, int t, int
     return __ldg(nb.list + (size_t)t * npad + k) & ((1 << kFlagBit) - 1);
 }
 
-// Pass 1: q_lm and NF for every atom.
-template <int LA, int LB, typename T, bool STEP>
+// Pass 1: q_lm and NF for every atom.  With skin lists (FILTER) the pass
+// first filters the atom's candidates into its exact list (the same
+// decisions as k_filter), then sums over that list.
+template <int LA, int LB, typename T, bool STEP, bool FILTER>
 __global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
     pdl_entry();
     using S = LSet<LA, LB, T>;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (FILTER && d.reset && k == 0) {
+        SkinState *r = d.reset;
+        if (r->gate) {
+            r->age = 1;
+            r->builds += 1;
+        } else {
+            r->age += 1;
+        }
+        r->gate = 0;
+    }
     if (k >= d.n) return;
+    int c;
+    if constexpr (FILTER)
+        c = min(filter_atom<STEP ? NK_STEP : NK_SWITCH>(d.fgf, d.fgd, d.fgd.xs, d.fspec, d.cand, d.nb, d.npad, k,
+                                                        d.status),
+                d.nb.M);
+    else
+        c = min(d.nb.count[k], d.nb.M);
     const auto a = d.geo.load(k);
-    const int c = min(d.nb.count[k], d.nb.M);
     T acc[S::SQ];
 #pragma unroll
     for (int t = 0; t < S::SQ; ++t) acc[t] = T(0);
     T nf = T(0);
     for (int t = 0; t < c; ++t) {
         T ux, uy, uz, rinv, sg, dsg;
-        pair_geom<T, STEP>(d, a, nb_index(d.nb, d.npad, t, k), ux, uy, uz, rinv, sg, dsg);
+        // a list this kernel wrote is read back through the coherent path
+        const int j = FILTER ? (d.nb.list[(size_t)t * d.npad + k] & ((1 << kFlagBit) - 1))
+                             : nb_index(d.nb, d.npad, t, k);
+        pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
         nf += sg;
         ylm_accum<LA, T>(ux, uy, uz, sg, acc);
         if constexpr (LB > 0) ylm_accum<LB, T>(ux, uy, uz, sg, acc + S::SA);
@@ -408,12 +429,14 @@ template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cuda
     const int nb = (d.n + kBlock - 1) / kBlock;
     const int qb = d.qblock > 0 ? d.qblock : kBlock, qg = (d.n + qb - 1) / qb;   // no block reduction in q
     if (d.sw_r.type == SW_STEP) {
-        launch_k(k_local_q<LA, LB, T, true>, qg, qb, 0, st, d);
+        if (d.filter) launch_k(k_local_q<LA, LB, T, true, true>, qg, qb, 0, st, d);
+        else launch_k(k_local_q<LA, LB, T, true, false>, qg, qb, 0, st, d);
         prof_mark("local_q", st);
         launch_k(k_local_lq<LA, LB, T, true>, nb, kBlock, 0, st, d);
         prof_mark("local_lq", st);
     } else {
-        launch_k(k_local_q<LA, LB, T, false>, qg, qb, 0, st, d);
+        if (d.filter) launch_k(k_local_q<LA, LB, T, false, true>, qg, qb, 0, st, d);
+        else launch_k(k_local_q<LA, LB, T, false, false>, qg, qb, 0, st, d);
         prof_mark("local_q", st);
         launch_k(k_local_lq<LA, LB, T, false>, nb, kBlock, 0, st, d);
         prof_mark("local_lq", st);

@@ -13,7 +13,16 @@
 // FP32 cell-relative distance unless it lies within ~1e-5 of the bound, where
 // the FP64 test on the caller's raw coordinates (the FP64 oracle's operation
 // order) decides -- the neighbour sets are exact.
-#include "kernels.h"
+//
+// With skin lists (NEIGH_SKIN) the cell list and candidate lists (cutoff +
+// skin) are rebuilt only when k_refresh finds an atom that moved more than
+// skin / 2 since the last rebuild (or NEIGH_EVERY steps have passed); every
+// step the candidates are filtered to the exact lists at the current
+// positions, so the neighbour sets are exact either way.  This is the model
+// of the reference, which reads LAMMPS's skin lists and filters them by
+// r < cutoff_r every step (src/cvs/CVs_Steinhardt.cu:135-147,
+// src/core/neigh_hub.cu:191-222).
+#include "filter.cuh"
 
 #include <math_constants.h>
 
@@ -34,8 +43,15 @@ __device__ __forceinline__ int cell_coord(double v, const CellGrid &g, int c, do
     return k;
 }
 
+// The rebuild kernels return at once while the skin gate is closed (the
+// gate is written by k_refresh, complete before pdl_entry returns).
+__device__ __forceinline__ bool gate_closed(const SkinState *sk) {
+    return sk && *(volatile const unsigned *)&sk->gate == 0u;
+}
+
 __global__ void k_bin(CellGrid g, SysDev s) {
     pdl_entry();
+    if (gate_closed(s.skin)) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
     double w;
@@ -84,8 +100,9 @@ __device__ __forceinline__ int block_excl_scan(int v, int &total) {
 // Three-pass exclusive scan of the cell histogram: per-block scan, scan of the
 // block totals, add-back.  The totals live in start[ncell + 1 ...].
 __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int *__restrict__ count, int *__restrict__ start,
-                                                            int *__restrict__ bsum, int ncell) {
+                                                            int *__restrict__ bsum, int ncell, const SkinState *skin) {
     pdl_entry();
+    if (gate_closed(skin)) return;
     const int i = blockIdx.x * kScanBlock + threadIdx.x;
     int total;
     const int e = block_excl_scan(i < ncell ? count[i] : 0, total);
@@ -94,8 +111,9 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const int *__restric
 }
 
 __global__ void __launch_bounds__(kScanBlock) k_scan_top(int *__restrict__ bsum, int nb, int *__restrict__ start,
-                                                         int ncell) {
+                                                         int ncell, const SkinState *skin) {
     pdl_entry();
+    if (gate_closed(skin)) return;
     int carry = 0;
     for (int base = 0; base < nb; base += kScanBlock) {
         const int i = base + threadIdx.x;
@@ -108,8 +126,9 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_top(int *__restrict__ bsum,
 }
 
 __global__ void __launch_bounds__(kScanBlock) k_scan_add(int *__restrict__ start, const int *__restrict__ bsum,
-                                                         int ncell) {
+                                                         int ncell, const SkinState *skin) {
     pdl_entry();
+    if (gate_closed(skin)) return;
     const int i = blockIdx.x * kScanBlock + threadIdx.x;
     if (i < ncell) start[i] += bsum[blockIdx.x];
 }
@@ -117,8 +136,9 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add(int *__restrict__ start
 // Single-kernel add-back when the block totals fit one block: each block sums
 // the totals of the blocks before it (the last block also writes the total).
 __global__ void __launch_bounds__(kScanBlock) k_scan_add_fused(int *__restrict__ start, const int *__restrict__ bsum,
-                                                               int ncell, int nb) {
+                                                               int ncell, int nb, const SkinState *skin) {
     pdl_entry();
+    if (gate_closed(skin)) return;
     __shared__ int red[32];
     const int b = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int v = threadIdx.x < b ? bsum[threadIdx.x] : 0;
@@ -134,9 +154,12 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add_fused(int *__restrict__
     if (b == nb - 1 && threadIdx.x == 0) start[ncell] = off + bsum[b];
 }
 
-__global__ void k_scatter(SysDev s) {
+// Also zeroes the cell counts for the next build (the scan has consumed them).
+__global__ void k_scatter(SysDev s, int ncell) {
     pdl_entry();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gate_closed(s.skin)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int c = i; c < ncell; c += gridDim.x * blockDim.x) s.count[c] = 0;
     if (i >= s.n) return;
     s.arrival[s.start[s.cellof[i]] + s.slot[i]] = i;
 }
@@ -146,6 +169,7 @@ __global__ void k_scatter(SysDev s) {
 // arrival order), and its sorted per-atom arrays are written there.
 __global__ void k_place(CellGrid g, SysDev s) {
     pdl_entry();
+    if (gate_closed(s.skin)) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
     const int i = s.arrival[k];
@@ -159,6 +183,11 @@ __global__ void k_place(CellGrid g, SysDev s) {
     s.xs[3 * d] = x0;
     s.xs[3 * d + 1] = x1;
     s.xs[3 * d + 2] = x2;
+    if (s.xref) {   // skin lists: positions of this build, for the displacement test
+        s.xref[3 * d] = x0;
+        s.xref[3 * d + 1] = x1;
+        s.xref[3 * d + 2] = x2;
+    }
     const int cz = c % g.nc[2], cy = (c / g.nc[2]) % g.nc[1], cx = c / (g.nc[2] * g.nc[1]);
     double w0, w1, w2;
     cell_coord(x0, g, 0, w0);
@@ -173,20 +202,11 @@ __global__ void k_place(CellGrid g, SysDev s) {
     s.smask[d] = i < s.nown ? (s.mask ? s.mask[i] : -1) : 0;
 }
 
-// FP64 decision on raw coordinates (the oracle's criterion, operation by operation).
-template <int KIND>
-__device__ __noinline__ bool exact_decide(const GeoD &gd, const NeighSpec &ns, const double *xk, const double *xj) {
-    double d[3];
-    const double r2 = exact_disp(gd, xk, xj, d);
-    if (KIND == NK_RANGE) return (r2 <= ns.rc2) && (r2 >= 1e-12);
-    if (KIND == NK_STEP) return (r2 <= ns.rc2) && (__dsqrt_rn(r2) < ns.r0);
-    return (r2 <= ns.rc2) && (sw_f<double>(ns.sw, __dsqrt_rn(r2)) >= ns.eps);
-}
-
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
                                                       DevStatus *status) {
     pdl_entry();
+    if (gate_closed(s.skin)) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
     const GeoF gf = geo_f(g, s.pf);
@@ -262,6 +282,7 @@ template <int KIND>
 __global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
                                                            DevStatus *status) {
     pdl_entry();
+    if (gate_closed(s.skin)) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= s.n) return;
     const GeoD gd = geo_d(g, s.xs);
@@ -304,7 +325,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s,
                     const float r2f = dx * dx + dy * dy + dz * dz;
                     if (r2f > ns.hi2 || j == k) continue;
                     bool in;
-                    if (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f) {
+                    if (KIND == NK_CAND || (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f)) {
                         in = true;
                     } else {
                         const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
@@ -319,7 +340,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s,
         }
     }
     nd.count[k] = cnt;
-    if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
+    if (cnt > nd.M) atomicMax(KIND == NK_CAND ? &status->cand_overflow : &status->overflow, (unsigned)cnt);
 }
 
 // Same lists as k_neighbors_fast (same cells in the same order, same tests),
@@ -336,6 +357,7 @@ __global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDe
     pdl_entry();
     // [cell][thread]: a lane's entry sits in the same bank whatever cell it reads
     __shared__ int2 rng[27][kFlatBlock];
+    if (gate_closed(s.skin)) return;
     const int tid = threadIdx.x;
     const int k = blockIdx.x * blockDim.x + tid;
     if (k >= s.n) return;   // no block-wide synchronisation below
@@ -409,7 +431,7 @@ __global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDe
         const float r2f = dx * dx + dy * dy + dz * dz;
         if (r2f > ns.hi2 || jj == k) continue;
         bool in;
-        if (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f) {
+        if (KIND == NK_CAND || (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f)) {
             in = true;
         } else {
             const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
@@ -421,7 +443,7 @@ __global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDe
         ++cnt;
     }
     nd.count[k] = cnt;
-    if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
+    if (cnt > nd.M) atomicMax(KIND == NK_CAND ? &status->cand_overflow : &status->overflow, (unsigned)cnt);
 }
 
 constexpr int kMaxCapList = 64;
@@ -461,27 +483,91 @@ __global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, Nei
     nd.nkept[k] = c < ns.cap ? c : ns.cap;
 }
 
+// Skin lists, every step: one thread per sorted slot of the last rebuild.
+// Repacks the caller's positions into that order (xs, and pf as FP32 offsets
+// from the slot's build cell, which stays within half a cell of it while the
+// lists are valid), refreshes the group mask, and opens the gate when a
+// rebuild is due: an atom moved more than skin / 2 (minimum image) since the
+// build, a non-finite position, NEIGH_EVERY reached, or force (the sorted
+// order is not valid yet: nothing else is read).
+__global__ void k_refresh(CellGrid g, SysDev s, int every, double half2, int force) {
+    pdl_entry();
+    SkinState *sk = s.skin;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0 && (force || (every > 0 && sk->age >= (unsigned)every))) atomicOr(&sk->gate, 1u);
+    if (force || k >= s.n) return;
+    const int i = s.perm[k];
+    const double x[3] = {s.x[3 * (size_t)i], s.x[3 * (size_t)i + 1], s.x[3 * (size_t)i + 2]};
+    const bool finite = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]);
+    if (!finite && s.status) atomicOr(&s.status->bad_pos, 1u);
+    double d2 = 0.0;
+    const float4 p = s.pf[k];
+    const int w = __float_as_int(p.w);
+    const int cc[3] = {w & 1023, (w >> 10) & 1023, w >> 20};
+    float off[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double t = x[c] - s.xref[3 * (size_t)k + c];
+        double o = (x[c] - g.lo[c]) - cc[c] * g.h[c];
+        if (g.periodic[c]) {
+            t -= g.L[c] * rint(t * g.invL[c]);
+            o -= g.L[c] * rint((o - 0.5 * g.h[c]) * g.invL[c]);
+        }
+        d2 += t * t;
+        off[c] = (float)o;
+    }
+    const unsigned moved = !(finite && d2 <= half2);
+    const unsigned ballot = __ballot_sync(__activemask(), moved);   // one atomic per warp
+    if (ballot && (threadIdx.x & 31) == __ffs(ballot) - 1) atomicOr(&sk->gate, 1u);
+    s.xs[3 * (size_t)k] = x[0];
+    s.xs[3 * (size_t)k + 1] = x[1];
+    s.xs[3 * (size_t)k + 2] = x[2];
+    s.pf[k] = make_float4(off[0], off[1], off[2], p.w);
+    s.smask[k] = i < s.nown ? (s.mask ? s.mask[i] : -1) : 0;
+}
+
+// Skin lists, every step: the exact lists of one environment from its
+// candidates.  reset (the first kernel after the gated rebuild kernels)
+// records the step in the skin state and closes the gate.
+template <int KIND>
+__global__ void __launch_bounds__(kBlock) k_filter(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd, NeighDev cand,
+                                                   DevStatus *status, SkinState *reset) {
+    pdl_entry();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (reset && k == 0) {
+        if (reset->gate) {
+            reset->age = 1;
+            reset->builds += 1;
+        } else {
+            reset->age += 1;
+        }
+        reset->gate = 0;
+    }
+    if (k >= s.n) return;
+    filter_atom<KIND>(geo_f(g, s.pf), geo_d(g, s.xs), s.xs, ns, cand, nd, s.npad, k, status);
+}
+
 }  // namespace
 
 int launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
-    cudaMemsetAsync(s.count, 0, sizeof(int) * (size_t)g.ncell, st);
     const int nb = (s.n + kBlock - 1) / kBlock;
+    const SkinState *sk = s.skin;
     if (s.n > 0) launch_k(k_bin, nb, kBlock, 0, st, g, s);
     prof_mark("cell_bin", st);
     {
         const int sb = (g.ncell + kScanBlock - 1) / kScanBlock;
         int *bsum = s.start + g.ncell + 1;   // scratch after the ncell + 1 starts
-        launch_k(k_scan_blocks, sb, kScanBlock, 0, st, s.count, s.start, bsum, g.ncell);
+        launch_k(k_scan_blocks, sb, kScanBlock, 0, st, s.count, s.start, bsum, g.ncell, sk);
         if (sb <= kScanBlock) {
-            launch_k(k_scan_add_fused, sb, kScanBlock, 0, st, s.start, bsum, g.ncell, sb);
+            launch_k(k_scan_add_fused, sb, kScanBlock, 0, st, s.start, bsum, g.ncell, sb, sk);
         } else {
-            launch_k(k_scan_top, 1, kScanBlock, 0, st, bsum, sb, s.start, g.ncell);
-            launch_k(k_scan_add, sb, kScanBlock, 0, st, s.start, bsum, g.ncell);
+            launch_k(k_scan_top, 1, kScanBlock, 0, st, bsum, sb, s.start, g.ncell, sk);
+            launch_k(k_scan_add, sb, kScanBlock, 0, st, s.start, bsum, g.ncell, sk);
         }
     }
     prof_mark("cell_scan", st);
     if (s.n > 0) {
-        launch_k(k_scatter, nb, kBlock, 0, st, s);
+        launch_k(k_scatter, nb, kBlock, 0, st, s, g.ncell);
         prof_mark("cell_scatter", st);
         launch_k(k_place, nb, kBlock, 0, st, g, s);
         prof_mark("cell_sort", st);
@@ -499,25 +585,47 @@ void launch_neighbors(const CellGrid &g, const SysDev &s, const NeighSpec &ns, N
         if (g.periodic[c] && g.nc[c] < 3) fast = false;
     // the fast path has three interchangeable shapes (identical lists): 256- or
     // 128-thread blocks of k_neighbors_fast, or k_neighbors_flat (autotuned)
+    // skin-list candidates need the fast path (the context builds them only where it applies)
     if (fast && ns.variant == 2 && s.n < (1 << 26)) {
         const int fb = (s.n + kFlatBlock - 1) / kFlatBlock;
         if (ns.kind == NK_RANGE) launch_k(k_neighbors_flat<NK_RANGE>, fb, kFlatBlock, 0, st, g, s, ns, nd, status);
         else if (ns.kind == NK_STEP) launch_k(k_neighbors_flat<NK_STEP>, fb, kFlatBlock, 0, st, g, s, ns, nd, status);
+        else if (ns.kind == NK_CAND) launch_k(k_neighbors_flat<NK_CAND>, fb, kFlatBlock, 0, st, g, s, ns, nd, status);
         else launch_k(k_neighbors_flat<NK_SWITCH>, fb, kFlatBlock, 0, st, g, s, ns, nd, status);
     } else if (fast) {
         const int tb = ns.variant == 1 ? 128 : kBlock;
         const int gb = (s.n + tb - 1) / tb;
         if (ns.kind == NK_RANGE) launch_k(k_neighbors_fast<NK_RANGE>, gb, tb, 0, st, g, s, ns, nd, status);
         else if (ns.kind == NK_STEP) launch_k(k_neighbors_fast<NK_STEP>, gb, tb, 0, st, g, s, ns, nd, status);
+        else if (ns.kind == NK_CAND) launch_k(k_neighbors_fast<NK_CAND>, gb, tb, 0, st, g, s, ns, nd, status);
         else launch_k(k_neighbors_fast<NK_SWITCH>, gb, tb, 0, st, g, s, ns, nd, status);
     } else if (ns.kind == NK_RANGE) launch_k(k_neighbors<NK_RANGE>, nb, kBlock, 0, st, g, s, ns, nd, status);
     else if (ns.kind == NK_STEP) launch_k(k_neighbors<NK_STEP>, nb, kBlock, 0, st, g, s, ns, nd, status);
     else launch_k(k_neighbors<NK_SWITCH>, nb, kBlock, 0, st, g, s, ns, nd, status);
-    prof_mark("neighbors", st);
-    if (ns.cap > 0) {
-        launch_k(k_select_cap, nb, kBlock, 0, st, g, s, ns, nd);
-        prof_mark("select_cap", st);
-    }
+    prof_mark(ns.kind == NK_CAND ? "neighbor_candidates" : "neighbors", st);
+    if (ns.cap > 0 && ns.kind != NK_CAND) launch_select_cap(g, s, ns, nd, st);
+}
+
+void launch_select_cap(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, cudaStream_t st) {
+    if (s.n == 0) return;
+    const int nb = (s.n + kBlock - 1) / kBlock;
+    launch_k(k_select_cap, nb, kBlock, 0, st, g, s, ns, nd);
+    prof_mark("select_cap", st);
+}
+
+void launch_refresh(const CellGrid &g, const SysDev &s, int every, double half_skin, int force, cudaStream_t st) {
+    const int nb = s.n > 0 ? (s.n + kBlock - 1) / kBlock : 1;
+    launch_k(k_refresh, nb, kBlock, 0, st, g, s, every, half_skin * half_skin, force);
+    prof_mark("skin_refresh", st);
+}
+
+void launch_filter(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, NeighDev cand,
+                   DevStatus *status, SkinState *reset, cudaStream_t st) {
+    const int nb = s.n > 0 ? (s.n + kBlock - 1) / kBlock : 1;
+    if (ns.kind == NK_RANGE) launch_k(k_filter<NK_RANGE>, nb, kBlock, 0, st, g, s, ns, nd, cand, status, reset);
+    else if (ns.kind == NK_STEP) launch_k(k_filter<NK_STEP>, nb, kBlock, 0, st, g, s, ns, nd, cand, status, reset);
+    else launch_k(k_filter<NK_SWITCH>, nb, kBlock, 0, st, g, s, ns, nd, cand, status, reset);
+    prof_mark("skin_filter", st);
 }
 
 }  // namespace mtd

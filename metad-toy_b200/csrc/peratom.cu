@@ -93,6 +93,18 @@ static mtd_status host_lists(mtd_ctx *c, const std::string &cal, std::vector<int
     return MTD_OK;
 }
 
+mtd_status mtd_neighbor_stats(mtd_ctx *c, int64_t *rebuilds, int *skin_active) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    SkinState sk{};
+    if (c->d_skin) {
+        MTD_CU(cudaStreamSynchronize(c->st), "neighbour statistics");
+        MTD_CU(cudaMemcpy(&sk, c->d_skin, sizeof(SkinState), cudaMemcpyDeviceToHost), "neighbour statistics");
+    }
+    if (rebuilds) *rebuilds = sk.builds;
+    if (skin_active) *skin_active = c->skin_last ? 1 : 0;
+    return MTD_OK;
+}
+
 mtd_status mtd_get_neighbors(mtd_ctx *c, const char *cal, int n, int *counts, int *idx, int max_per_atom) {
     if (!c || !cal || !counts || n < 0 || (idx && max_per_atom < 0)) return MTD_ERR_INVALID_ARG;
     if (n != c->n) return fail(c, MTD_ERR_INVALID_ARG, "atom count differs from the last step");

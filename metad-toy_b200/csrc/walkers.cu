@@ -348,15 +348,12 @@ mtd_status mtd_walkers_sync(mtd_walkers *W) {
     W->pending = false;
     bool overflow = false;
     for (mtd_ctx *c : W->w) {
-        if (c->h_status->overflow) {
-            const int need = (int)c->h_status->overflow;
-            for (Env &e : c->envs)
-                if (e.M < need) {
-                    e.M = ((need + 8) + 3) & ~3;
-                    alloc_env(c, e, c->cap_n);
-                }
+        if (c->h_status->overflow || c->h_status->cand_overflow) {
+            const mtd_status s = grow_lists(c, c->h_status->overflow, c->h_status->cand_overflow);
+            if (s != MTD_OK) return wfail(W, s, c->err);
             cudaMemset(c->d_status, 0, sizeof(DevStatus));
             c->h_status->overflow = 0;
+            c->h_status->cand_overflow = 0;
             overflow = true;
         }
     }
