@@ -57,15 +57,21 @@ def fix_args(skin=SKIN, every=EVERY):
     return a
 
 
-def load_system(seed=2024, copies=4):
+def load_base(seed=2024):
+    """The slab geometry before jitter (cached: its hard-core liquid takes seconds)."""
     import systems
     cache = os.path.join(tempfile.gettempdir(), "mtd_config2_%d.npz" % seed)
     if os.path.exists(cache):
         z = np.load(cache)
-        x, L = z["x"], z["L"]
-    else:
-        x, L = systems.config2(seed=seed)
-        np.savez(cache, x=x, L=L)
+        return z["x"], z["L"]
+    x, L = systems.config2(seed=seed)
+    np.savez(cache, x=x, L=L)
+    return x, L
+
+
+def load_system(seed=2024, copies=4):
+    import systems
+    x, L = load_base(seed)
     xs = [np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.05, seed + 1, c), L)) for c in range(copies)]
     return xs, L
 
@@ -515,6 +521,47 @@ def run_nnbias(args, local):
     return 0
 
 
+def tile_rank_positions(x0, L, world, rank, cut, seed, copies):
+    """Rank `rank`'s atoms of the decomposed multi-GPU workload: `world`
+    copies of the slab geometry tiled along x (tile t jittered with its own
+    seed), rank r owning tile r and receiving as ghosts the atoms of the
+    neighbouring tiles within `cut` of its faces (what LAMMPS's Comm
+    supplies).  Returns the per-step position arrays (owned rows first, then
+    ghosts, in tile-local coordinates), the number of owned atoms, and the
+    box (lo, hi, periodic): x non-periodic and grown by `cut`, y and z
+    periodic over the tile."""
+    import systems
+    Lx = L[0]
+
+    def tile(t, c):
+        # jittered, wrapped in y and z only: an atom of tile t stays tile t's
+        # (ownership by tile, as between two reneighborings of an MD code)
+        x = systems.jitter(x0, 0.05, seed + 1 + 1000 * (t % world), c)
+        if world == 1:
+            return systems.wrap(x, L)
+        x[:, 1:] -= np.floor(x[:, 1:] / L[1:]) * L[1:]
+        return x
+
+    # the ghost atoms are chosen once (on the unjittered geometry, with a
+    # margin above the jitter), as an MD code keeps its ghosts between
+    # reneighborings; their positions follow every step
+    margin = 0.5
+    gi_r = np.nonzero(x0[:, 0] < cut + margin)[0]
+    gi_l = np.nonzero(x0[:, 0] >= Lx - cut - margin)[0]
+    out = []
+    for c in range(copies):
+        own = tile(rank, c)
+        if world == 1:
+            out.append(np.ascontiguousarray(own))
+            continue
+        gr = tile(rank + 1, c)[gi_r] + np.array([Lx, 0.0, 0.0])
+        gl = tile(rank - 1, c)[gi_l] - np.array([Lx, 0.0, 0.0])
+        out.append(np.ascontiguousarray(np.concatenate([own, gr, gl])))
+    if world == 1:
+        return out, out[0].shape[0], ([0.0, 0.0, 0.0], list(L), (1, 1, 1))
+    return out, x0.shape[0], ([-cut, 0.0, 0.0], [Lx + cut, L[1], L[2]], (0, 1, 1))
+
+
 def max_over_ranks(vals, dist, device):
     """Timings (ms) reduced to their maximum over the ranks (the slowest replica
     sets the job's time); identity without a process group."""
@@ -673,6 +720,9 @@ def main():
                          "q: 4,000-atom STEINH Q (FP64); nn: learned 4D bias vs exact hill sum; "
                          "walkers: 32 walkers sharing one grid; domain: cost of the decomposition exchange")
     ap.add_argument("--nn-iters", type=int, default=20000, help="Adam steps of the learned-bias fit (--workload nn)")
+    ap.add_argument("--split", default="domain", choices=["domain", "replicas"],
+                    help="with several GPUs: domain decomposition of tiled slabs (per-step NCCL allreduce) or "
+                         "independent replicas")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -699,9 +749,22 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     xs, L = load_system()
-    n = xs[0].shape[0]
+    split = args.split if world > 1 else "none"
+    nown = xs[0].shape[0]
     m = mtd.Metad(fix_args(), precision=args.precision, device=local)
-    m.set_box([0, 0, 0], L)
+    if split == "domain":
+        # the reference's multi-rank model: tiles of the slab over the ranks,
+        # ghosts from the neighbouring tiles, the per-step unit totals summed
+        # over the ranks by NCCL on the library's stream
+        import domain
+        x0, _ = load_base(2024)
+        cut = m.ghost_cutoff
+        xs, nown, (blo, bhi, bper) = tile_rank_positions(x0, L, world, rank, cut, 2024, 4)
+        m.set_domain_device(nown, rank, domain.TorchDeviceAllreduce())
+        m.set_box(blo, bhi, bper)
+    else:
+        m.set_box([0, 0, 0], L)
+    n = xs[0].shape[0]
     m.init()
     stream = timing_stream()
     m.set_stream(stream.cuda_stream)
@@ -779,8 +842,9 @@ def main():
     clocks = clk.summary()
 
     dev_ms, e2e_ms = max_over_ranks([dev_ms, e2e_s * 1e3], dist, "cuda")
-    value, e2e_value = replica_throughput(n, args.steps, world, dev_ms), replica_throughput(n, args.steps, world,
-                                                                                           e2e_ms)
+    # whole-job throughput counts owned atoms (ghosts are copies)
+    value, e2e_value = replica_throughput(nown, args.steps, world, dev_ms), replica_throughput(nown, args.steps,
+                                                                                              world, e2e_ms)
 
     # roofline of the dominant kernel
     peak, peak_kind = peaks()
@@ -802,7 +866,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(xs, L, budget_s=15.0, threads=os.cpu_count())
     err = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:
         err = error_vs_fp64(xs, L, args.precision, local)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
@@ -811,7 +875,13 @@ def main():
             "config": {"workload": WORKLOAD, "atoms": n, "mean_neighbors": nbar,
                        "max_neighbors": m.max_neighbors("Q4"), "cap_cutoff_Natoms": 18,
                        "precision": args.precision, "l2": "flushed (256 MB write) before each timed step",
-                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "parallelism": {"none": "single GPU",
+                                       "replicas": "%d independent replicas (no data-path collective)" % world,
+                                       "domain": "domain decomposition over %d ranks: x tiles of the slab, ghost "
+                                                 "shell %.1f A, per-step NCCL allreduce of the unit totals on the "
+                                                 "library stream; ghost-force reverse communication is the MD "
+                                                 "code's and is not timed" % (world, m.ghost_cutoff)}[split],
+                       "atoms_per_rank": {"owned": int(nown), "with_ghosts": int(n)},
                        "autotuned_shapes": {"neighbors": ["fast/256", "fast/128", "flat/128"][tuned[0]],
                                             "q_block": tuned[1], "lambda_block": tuned[2]},
                        "neighbor_lists": {"skin_A": SKIN, "rebuild_every_steps": EVERY,

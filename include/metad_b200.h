@@ -291,7 +291,10 @@ mtd_status mtd_set_domain_device(mtd_ctx *ctx, int nlocal, int rank, mtd_allredu
 mtd_status mtd_set_nlocal(mtd_ctx *ctx, int nlocal);
 /* Ghost shell the caller must supply under domain decomposition: cutoff_r of
  * STEINH Q and STRU_FACTOR, 2 x the cutoff of STEINH L (its centres read q_lm
- * of neighbours, which need their own neighbours), 0 for S(k) alone. */
+ * of neighbours, which need their own neighbours), 0 for S(k) alone; with
+ * skin lists (NEIGH_SKIN s) the shell grows by s, and the ghost atoms chosen
+ * with it should stay the same between rebuilds (as LAMMPS keeps its ghosts
+ * between reneighborings): a change of the atom count forces a rebuild. */
 double mtd_ghost_cutoff(const mtd_ctx *ctx);
 
 /* Largest neighbour count seen by the last step for CAL `name` (cap reporting). */

@@ -587,7 +587,54 @@ SkDev sk_dev(mtd_ctx *c, Unit &u, const double *x, const int *mask) {
     d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
     d.fp64 = c->fp64;
     d.nown = owned(c);
+    d.tab = u.sk_tab;
+    d.tstride = u.sk_tstride;
+    for (int a = 0; a < 3; ++a) {
+        d.nct[a] = u.sk_nct[a];
+        d.to[a] = u.sk_to[a];
+        d.th[a] = u.sk_th[a];
+        d.tih[a] = 1.0 / u.sk_th[a];
+    }
     return d;
+}
+
+// Mixed-precision S(k): the per-dimension phase tables of each unit for the
+// current box, T_d[k][c] = k_d (o_d + (c + 1/2) h_d) reduced to [-pi, pi] in
+// FP64, cells of about 2 A over the box and a 4 A margin on each side
+// (coordinates beyond take the FP64 phase).  Rebuilt when the box changes.
+mtd_status ensure_sk_tables(mtd_ctx *c) {
+    if (c->fp64) return MTD_OK;
+    for (Unit &u : c->units) {
+        if (u.kind != CAL_STRU_FACTOR_K) continue;
+        const double box[6] = {c->lo[0], c->lo[1], c->lo[2], c->hi[0], c->hi[1], c->hi[2]};
+        if (u.sk_tab && std::memcmp(box, u.sk_box, sizeof box) == 0) continue;
+        const double margin = 4.0;
+        int ts = 1;
+        for (int a = 0; a < 3; ++a) {
+            const double span = (c->hi[a] - c->lo[a]) + 2.0 * margin;
+            const int nc = std::max(1, std::min(kSkTabCells, (int)std::ceil(span / 2.0)));
+            u.sk_nct[a] = nc;
+            u.sk_to[a] = c->lo[a] - margin;
+            u.sk_th[a] = span / nc;
+            ts = std::max(ts, nc);
+        }
+        u.sk_tstride = ts;
+        const CalDef &cd = c->cfg.cals[u.calnames[0]];
+        std::vector<float> tab((size_t)3 * u.K * ts, 0.0f);
+        for (int a = 0; a < 3; ++a)
+            for (int k = 0; k < u.K; ++k)
+                for (int cc = 0; cc < u.sk_nct[a]; ++cc) {
+                    const double ph = cd.kvecs[3 * k + a] * (u.sk_to[a] + (cc + 0.5) * u.sk_th[a]);
+                    tab[((size_t)a * u.K + k) * ts + cc] = (float)(ph - 2.0 * kPi * std::rint(ph / (2.0 * kPi)));
+                }
+        dfree(u.sk_tab);
+        MTD_CU(dalloc(&u.sk_tab, sizeof(float) * tab.size()), "S(k) phase tables");
+        MTD_CU(cudaMemcpyAsync(u.sk_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, c->st),
+               "S(k) phase tables");
+        MTD_CU(cudaStreamSynchronize(c->st), "S(k) phase tables");
+        std::memcpy(u.sk_box, box, sizeof box);
+    }
+    return MTD_OK;
 }
 
 template <typename T> void run_values(mtd_ctx *c, const CellGrid &g, const double *x, const int *mask) {
@@ -776,6 +823,8 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
         }
         c->skin_last = skin;
     }
+    const mtd_status stab = ensure_sk_tables(c);
+    if (stab != MTD_OK) return stab;
     for (const Unit &u : c->units)
         if (u.chem && c->types_n != n)
             return fail(c, MTD_ERR_INVALID_ARG,
@@ -1061,6 +1110,7 @@ void mtd_destroy(mtd_ctx *c) {
         void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S, &u.w};
         for (void **a : arrs) dfree(*a);
         dfree(u.partials); dfree(u.coef); dfree(u.kvec); dfree(u.rho); dfree(u.skn); dfree(u.d_wtab);
+        dfree(u.sk_tab);
     }
     dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
     dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask); dfree(c->arrival);

@@ -69,6 +69,11 @@ struct Unit {
     double *coef = nullptr;
     int K = 0;
     double *kvec = nullptr, *rho = nullptr, *skn = nullptr;
+    // S(k), mixed precision: per-dimension phase tables for the box they were built for
+    float *sk_tab = nullptr;
+    int sk_tstride = 0, sk_nct[3] = {0, 0, 0};
+    double sk_to[3] = {0, 0, 0}, sk_th[3] = {1, 1, 1};
+    double sk_box[6] = {0, 0, 0, 0, 0, 0};
     // STRU_FACTOR Chemical: type-weight parameters, the table built from the
     // types of mtd_set_types, and the per-atom weights (sorted order)
     bool chem = false, wchem = false;

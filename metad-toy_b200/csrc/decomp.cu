@@ -96,6 +96,9 @@ double mtd_ghost_cutoff(const mtd_ctx *c) {
     if (!c) return 0.0;
     double g = 0.0;
     for (const Env &e : c->envs) g = std::fmax(g, e.kind == ENV_L ? 2.0 * e.rc : e.rc);
+    // skin lists: atoms move up to skin / 2 between rebuilds, so the shell
+    // taken at a rebuild must reach that much further for each of the two
+    if (g > 0.0 && c->cfg.neigh_skin > 0.0) g += c->cfg.neigh_skin;
     return g;
 }
 

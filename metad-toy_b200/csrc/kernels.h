@@ -267,7 +267,14 @@ struct SkDev {
     double *ngroup;             // group count
     const double *coef;         // alpha
     int fp64;
+    // mixed precision: per-dimension phase tables, tab[(d * K + k) * tstride + c] =
+    // k_d (o_d + (c + 1/2) h_d) reduced to [-pi, pi] (FP64 on the host, stored FP32)
+    const float *tab;
+    int tstride;
+    int nct[3];
+    double to[3], th[3], tih[3];
 };
+constexpr int kSkTabCells = 320;    // phase-table cells per dimension at most (bounds the shared-memory chunks)
 void launch_sk_values(const SkDev &d, cudaStream_t st);
 void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                       double *vpart, cudaStream_t st);
