@@ -390,6 +390,25 @@ mtd_status mtd_walkers_sync(mtd_walkers *W);
  * picks into choices[3k..3k+2], may be NULL); the next step re-captures the
  * CUDA graph with the chosen shapes. */
 mtd_status mtd_walkers_autotune(mtd_walkers *W, const int *n, const double *const *d_x, int reps, int *choices);
+/* One launch per MD step: when every walker holds one STEINH L unit (one or
+ * two orders) on one neighbour environment, without skin lists and not
+ * sharded over ranks, a step runs as ONE persistent cooperative kernel over
+ * all walkers (cell lists, neighbour lists, CVs, the deposit in walker
+ * order, V, dV/ds and forces, phases separated by a grid barrier whose every
+ * wait is bounded), with the same arithmetic as the per-walker kernels and
+ * the same results bit for bit; with the CUDA graph enabled that launch is
+ * replayed.  enable 0 selects the per-walker kernels (the path for every
+ * other deck).  mtd_walkers_persistent_active tells whether the last step
+ * ran as one launch.  No counterpart in the reference. */
+mtd_status mtd_walkers_enable_persistent(mtd_walkers *W, int enable);
+int mtd_walkers_persistent_active(const mtd_walkers *W);
+/* Diagnostics of the persistent step's grid barrier: every wait polls at
+ * most `limit` times (0: the default, 2^22) before the step gives up, and
+ * mtd_walkers_sync then returns MTD_ERR_TIMEOUT (the step is incomplete and
+ * should be repeated); stall = 1 makes one block skip the first barrier so
+ * that the others' waits run out (a check of that path), 0 restores normal
+ * operation. */
+mtd_status mtd_walkers_set_wait(mtd_walkers *W, int limit, int stall);
 double mtd_walkers_cv(const mtd_walkers *W, int k, int d);
 double mtd_walkers_bias(const mtd_walkers *W, int k);
 mtd_status mtd_walkers_get_grid(mtd_walkers *W, double *out, int64_t count);

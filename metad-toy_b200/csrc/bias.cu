@@ -44,7 +44,7 @@ __device__ __forceinline__ void stencil_load(const BiasPlan &P, const int *ix, d
         size_t g = (size_t)(ix[0] - 1 + q);
         if (P.D >= 2) g = g * P.nbin[1] + (ix[1] - 1 + t);
         if (P.D >= 3) g = g * P.nbin[2] + (ix[2] - 1 + u);
-        S[e] = P.grid[g];
+        S[e] = __ldcg(P.grid + g);   // through L2: other blocks may have deposited since this SM last read it
     }
 }
 
@@ -528,17 +528,18 @@ __global__ void __launch_bounds__(256) k_list_finish(const BiasPlan *__restrict_
 // receives its increments in walker order).  C: per walker V, dV/ds on the
 // updated grid and the force coefficients.  The step is read from device
 // memory so the three launches can sit in a CUDA graph.
-__global__ void __launch_bounds__(256) k_walk_cvs(const BiasPlan *const *__restrict__ plans,
-                                                  const long long *__restrict__ d_step, WalkState *ws) {
-    pdl_entry();
+// Walker w's CVs (one block): totals, symbols, DIM values, and on a deposit
+// step the WT height from the grid as it stood at the start of the step.
+__device__ void walk_cvs_block(const BiasPlan *const *__restrict__ plans, int w, const long long *__restrict__ d_step,
+                               WalkState *ws) {
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
-    stage_plan(plans[blockIdx.x], plan_raw);
+    stage_plan(plans[w], plan_raw);
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
-    const long long step = *d_step;
+    const long long step = *(volatile const long long *)d_step;
     phase_cvs(P, S.smem, S.usum, S.s_sym, S.s_jac, S.sv);
     const int dep = (P.pace != 0) && (step % P.pace == 0) && !step_failed(P);
-    WalkState &W = ws[blockIdx.x];
+    WalkState &W = ws[w];
     if (dep) {
         int ix[3] = {1, 1, 1};
         double fx[3] = {0, 0, 0};
@@ -553,6 +554,13 @@ __global__ void __launch_bounds__(256) k_walk_cvs(const BiasPlan *const *__restr
         W.jac[e / kMaxSymbols][e % kMaxSymbols] = S.s_jac[e / kMaxSymbols][e % kMaxSymbols];
     if (threadIdx.x < kMaxDim) W.s[threadIdx.x] = threadIdx.x < P.D ? S.sv[threadIdx.x] : 0.0;
     if (threadIdx.x == 0) W.dep = dep;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_walk_cvs(const BiasPlan *const *__restrict__ plans,
+                                                  const long long *__restrict__ d_step, WalkState *ws) {
+    pdl_entry();
+    walk_cvs_block(plans, blockIdx.x, d_step, ws);
 }
 
 // True (in every thread) when any walker's neighbour lists overflowed this
@@ -570,35 +578,43 @@ __device__ bool group_failed(const BiasPlan *const *__restrict__ plans, int nwal
     return failed != 0;
 }
 
-__global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__restrict__ plans, int nwalk,
-                                                      const long long *__restrict__ d_step, const WalkState *ws) {
-    pdl_entry();
+// The group's hills in walker order (one block).
+__device__ void walk_deposit_block(const BiasPlan *const *__restrict__ plans, int nwalk,
+                                   const long long *__restrict__ d_step, const WalkState *ws) {
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     stage_plan(plans[0], plan_raw);
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
-    if (group_failed(plans, nwalk)) return;
-    const long long step = *d_step;
-    if (!(P.pace != 0 && step % P.pace == 0)) return;   // every walker shares PACE
-    int ix[3] = {1, 1, 1};
-    for (int w = 0; w < nwalk; ++w) {
-        phase_deposit(P, ws[w].s, ws[w].hill_w, ix, nullptr);
-        if (threadIdx.x == 0) record_hill(P, step, ws[w].s, ws[w].hill_w);
-        __syncthreads();
+    const bool failed = group_failed(plans, nwalk);
+    const long long step = *(volatile const long long *)d_step;
+    if (!failed && P.pace != 0 && step % P.pace == 0) {   // every walker shares PACE
+        int ix[3] = {1, 1, 1};
+        for (int w = 0; w < nwalk; ++w) {
+            phase_deposit(P, ws[w].s, ws[w].hill_w, ix, nullptr);
+            if (threadIdx.x == 0) record_hill(P, step, ws[w].s, ws[w].hill_w);
+            __syncthreads();
+        }
     }
+    __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__restrict__ plans, int nwalk,
-                                                   const WalkState *ws) {
+__global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__restrict__ plans, int nwalk,
+                                                      const long long *__restrict__ d_step, const WalkState *ws) {
     pdl_entry();
+    walk_deposit_block(plans, nwalk, d_step, ws);
+}
+
+// Walker w's V, dV/ds on the updated grid and force coefficients (one block).
+__device__ void walk_coef_block(const BiasPlan *const *__restrict__ plans, int nwalk, int w, const WalkState *ws) {
     __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
     __shared__ BiasShared S;
-    stage_plan(plans[blockIdx.x], plan_raw);
+    stage_plan(plans[w], plan_raw);
     const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
     if (group_failed(plans, nwalk)) {
         for (int e = threadIdx.x; e < P.nunit * 8; e += blockDim.x) P.unit[e / 8].coef[e % 8] = 0.0;
+        __syncthreads();
         return;
     }
-    const WalkState &W = ws[blockIdx.x];
+    const WalkState &W = ws[w];
     for (int e = threadIdx.x; e < kMaxUnits * 8; e += blockDim.x) S.usum[e / 8][e % 8] = W.usum[e / 8][e % 8];
     for (int e = threadIdx.x; e < kMaxDim * kMaxSymbols; e += blockDim.x)
         S.s_jac[e / kMaxSymbols][e % kMaxSymbols] = W.jac[e / kMaxSymbols][e % kMaxSymbols];
@@ -610,6 +626,13 @@ __global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__rest
     stencil_load(P, ix, S.sten);
     __syncthreads();
     phase_coef(P, S.sten, fx, S.sv, S.s_jac, S.usum, W.dep, S.row, &S.s_V, S.s_dV, S.s_alpha);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_walk_coef(const BiasPlan *const *__restrict__ plans, int nwalk,
+                                                   const WalkState *ws) {
+    pdl_entry();
+    walk_coef_block(plans, nwalk, blockIdx.x, ws);
 }
 
 // ---- walkers sharded over ranks: each rank steps its own walkers; their
@@ -719,6 +742,20 @@ __global__ void k_virial_finalize(const double *__restrict__ vpart, int nparts, 
 }
 
 }  // namespace
+
+// The three bias phases of the multi-walker step as block-level functions
+// for the persistent step kernel (walk_step.cu), compiled here with this
+// file's arithmetic.
+__device__ void walk_phase_cvs(const BiasPlan *const *plans, int w, const long long *d_step, WalkState *ws) {
+    walk_cvs_block(plans, w, d_step, ws);
+}
+__device__ void walk_phase_deposit(const BiasPlan *const *plans, int nwalk, const long long *d_step,
+                                   const WalkState *ws) {
+    walk_deposit_block(plans, nwalk, d_step, ws);
+}
+__device__ void walk_phase_coef(const BiasPlan *const *plans, int nwalk, int w, const WalkState *ws) {
+    walk_coef_block(plans, nwalk, w, ws);
+}
 
 __global__ void __launch_bounds__(256) k_unit_sums(const BiasPlan *__restrict__ Pp, double *out) {
     pdl_entry();

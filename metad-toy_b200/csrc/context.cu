@@ -278,8 +278,9 @@ mtd_status ensure_cells(mtd_ctx *c, int ncell) {
         // zero once here; every build's scatter pass zeroes the counts it used
         MTD_CU(cudaMemset(c->count, 0, sizeof(int) * (size_t)cap), "cell counts");
         c->skin_valid = false;
-        // ncell + 1 starts followed by the scan's per-1024-cell block totals
-        MTD_CU(dalloc(&c->start, sizeof(int) * (size_t)(cap + 1 + cap / 1024 + 2)), "cell starts");
+        // ncell + 1 starts followed by the scan's per-block totals (1024-cell
+        // blocks; 256-cell chunks in the persistent multi-walker step)
+        MTD_CU(dalloc(&c->start, sizeof(int) * (size_t)(cap + 1 + cap / 256 + 2)), "cell starts");
         c->cap_cell = cap;
     }
     return MTD_OK;
@@ -515,7 +516,7 @@ mtd_status plan_units(mtd_ctx *c) {
 int owned(const mtd_ctx *c) { return c->nown >= 0 ? std::min(c->nown, c->n) : c->n; }
 
 NeighDev env_dev(const Env &e) {
-    NeighDev nd;
+    NeighDev nd{};
     nd.list = e.list;
     nd.count = e.count;
     nd.key_r2 = e.key_r2;
@@ -526,7 +527,7 @@ NeighDev env_dev(const Env &e) {
 }
 
 SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
-    SysDev s;
+    SysDev s{};   // every field set (skin, xref: null unless the skin path sets them)
     s.n = c->n;
     s.npad = c->cap_n;
     s.x = x;
@@ -967,6 +968,63 @@ mtd_status drain(mtd_ctx *c, bool block) {
     }
     return MTD_OK;
 }
+
+// One walker's arguments for the persistent multi-walker step: the host part
+// of enqueue_values and enqueue_forces (capacity, plan, cell arrays, the
+// per-step lists' layout) with no launch.  The caller checked that the
+// context has one STEINH L unit on one environment and no skin lists;
+// *ok = false when this step's cell grid cannot use the fast neighbour
+// search (a periodic side with fewer than three cells).
+template <typename T>
+mtd_status walk_desc(mtd_ctx *c, int n, const double *x, double *f, WalkDesc<T> &d, bool *ok) {
+    if (!c->box_set) return fail(c, MTD_ERR_INVALID_ARG, "mtd_set_box must be called before the first step");
+    mtd_status st = ensure_capacity(c, n);
+    if (st != MTD_OK) return st;
+    const CellGrid g = make_grid(c);
+    *ok = true;
+    for (int a = 0; a < 3; ++a)
+        if (g.periodic[a] && g.nc[a] < 3) *ok = false;
+    if (!*ok) return MTD_OK;
+    c->last_grid = g;
+    if (c->plan_dirty) {
+        build_plan(c);
+        MTD_CU(cudaMemcpyAsync(c->d_plan, &c->plan, sizeof(BiasPlan), cudaMemcpyHostToDevice, c->st), "plan");
+        MTD_CU(cudaStreamSynchronize(c->st), "plan");
+        c->plan_dirty = false;
+    }
+    st = ensure_cells(c, g.ncell);
+    if (st != MTD_OK) return st;
+    SysDev s = sys_dev(c, x, nullptr, nullptr);
+    s.count = c->count;
+    s.start = c->start;
+    Unit &u = c->units[0];
+    Env &e = c->envs[u.env];
+    std::memset(&d, 0, sizeof d);
+    d.g = g;
+    d.s = s;
+    d.ns = neigh_spec(e);
+    d.nd = env_dev(e);
+    d.ld = local_dev<T>(c, u, g);
+    d.f_src = f;
+    d.f_dst = f;
+    d.nb = (n + kBlock - 1) / kBlock;
+    d.nchunk = (g.ncell + 255) / 256;
+    d.d_out = c->d_out;
+    d.d_status = c->d_status;
+    d.d_nhills = c->d_nhills;
+    use_slot(c, 0);
+    d.h_out = c->h_out;
+    d.h_status = c->h_status;
+    d.h_nhills = c->h_nhills;
+    c->last_sys = s;
+    c->last_x = x;
+    c->last_mask = nullptr;
+    c->step_gen += 1;
+    c->skin_last = false;
+    return MTD_OK;
+}
+template mtd_status walk_desc<float>(mtd_ctx *, int, const double *, double *, WalkDesc<float> &, bool *);
+template mtd_status walk_desc<double>(mtd_ctx *, int, const double *, double *, WalkDesc<double> &, bool *);
 
 template void run_values<float>(mtd_ctx *, const CellGrid &, const double *, const int *);
 template void run_values<double>(mtd_ctx *, const CellGrid &, const double *, const int *);

@@ -295,6 +295,8 @@ mtd_status enqueue_forces(mtd_ctx *c, long long step, const double *x, const int
 mtd_status enqueue_step(mtd_ctx *c, long long step, int n, const double *x, const int *mask, const int *image,
                         const double *fin, double *fout, bool virial, cudaEvent_t f_ready = nullptr);
 mtd_status collect(mtd_ctx *c);
+template <typename T>
+mtd_status walk_desc(mtd_ctx *c, int n, const double *x, double *f, WalkDesc<T> &d, bool *ok);
 mtd_status drain(mtd_ctx *c, bool block);
 
 // decomp.cu

@@ -369,6 +369,48 @@ void launch_walk_finish(const BiasPlan *const *d_plans, int nwalk, const long lo
                         const double *recs, int nrec, cudaStream_t st);
 void launch_hills_replay(const BiasPlan *d_plan, const HillRec *h, int nh, int ncell, cudaStream_t st);
 
+// ------------------------------------------------------------------ persistent multi-walker step
+// One walker's arguments for the single-launch step (walk_step.cu); device
+// memory, written by the host before the launch and read-only during it.
+template <typename T> struct WalkDesc {
+    CellGrid g;
+    SysDev s;                   // per-step lists (no skin gate)
+    NeighSpec ns;
+    NeighDev nd;
+    LocalDev<T> ld;
+    const double *f_src;
+    double *f_dst;
+    int nb;                     // 256-atom blocks
+    int nchunk;                 // 256-cell chunks of the count scan
+    const double *d_out;        // the walker's bias outputs (device) ...
+    const DevStatus *d_status;
+    const unsigned long long *d_nhills;
+    double *h_out;              // ... and their pinned host copies, written at the end of the step
+    DevStatus *h_status;
+    unsigned long long *h_nhills;
+};
+// The grid barrier's words (device memory, zero when no launch is in flight).
+struct GridBar {
+    unsigned int count, gen, err, pad;
+};
+constexpr int kWalkPersistMax = 1024;   // walkers of one persistent step at most
+struct WalkStepArgs {
+    int nwalk;
+    const int *pa, *pc;         // prefix sums of WalkDesc::nb and ::nchunk over the walkers (nwalk + 1)
+    const BiasPlan *const *plans;
+    const long long *step;      // the step number (pinned host memory)
+    WalkState *ws;
+    GridBar *bar;
+    int limit;                  // barrier polls before a wait gives up
+    int stall;                  // diagnostics: block 0 skips the first barrier (the others' waits run out)
+};
+// Co-resident blocks of the step kernel for STEINH L orders (LA, LB) in
+// precision T (0: no such kernel), and its cooperative launch.
+template <typename T> int walk_step_blocks(int LA, int LB, bool step_switch);
+template <typename T>
+cudaError_t launch_walk_step(int LA, int LB, bool step_switch, const WalkDesc<T> *d_desc, const WalkStepArgs &a,
+                             int blocks, cudaStream_t st);
+
 // Hill-list bias (no grid; CV_dim up to 4): the CV values and chain factors
 // into ws[0]; then, with V and dV/ds at s from the hill sum or the learned
 // bias in vdv (V, dV[0..D)), the deposit record, V += the new hill's height

@@ -22,7 +22,7 @@
 // of the reference, which reads LAMMPS's skin lists and filters them by
 // r < cutoff_r every step (src/cvs/CVs_Steinhardt.cu:135-147,
 // src/core/neigh_hub.cu:191-222).
-#include "filter.cuh"
+#include "neigh_body.cuh"
 
 #include <math_constants.h>
 
@@ -30,18 +30,6 @@ namespace mtd {
 
 namespace {
 
-__device__ __forceinline__ int cell_coord(double v, const CellGrid &g, int c, double &w) {
-    w = v - g.lo[c];
-    if (g.periodic[c]) {
-        w = w - g.L[c] * floor(w * g.invL[c]);
-        if (w >= g.L[c]) w -= g.L[c];
-        if (w < 0.0) w = 0.0;
-    }
-    int k = (int)(w * g.inv_h[c]);
-    if (k < 0) k = 0;
-    if (k >= g.nc[c]) k = g.nc[c] - 1;
-    return k;
-}
 
 // The rebuild kernels return at once while the skin gate is closed (the
 // gate is written by k_refresh, complete before pdl_entry returns).
@@ -49,23 +37,11 @@ __device__ __forceinline__ bool gate_closed(const SkinState *sk) {
     return sk && *(volatile const unsigned *)&sk->gate == 0u;
 }
 
+
 __global__ void k_bin(CellGrid g, SysDev s) {
     pdl_entry();
     if (gate_closed(s.skin)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.n) return;
-    double w;
-    const double x0 = s.x[3 * i + 0], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
-    // a non-finite coordinate is binned into a valid cell (cell_coord clamps),
-    // matches no neighbour test (every comparison with NaN is false), and
-    // fails the step: no deposit, no bias force, an error on the host
-    if (!(isfinite(x0) && isfinite(x1) && isfinite(x2)) && s.status) atomicOr(&s.status->bad_pos, 1u);
-    const int cx = cell_coord(x0, g, 0, w);
-    const int cy = cell_coord(x1, g, 1, w);
-    const int cz = cell_coord(x2, g, 2, w);
-    const int cell = (cx * g.nc[1] + cy) * g.nc[2] + cz;
-    s.cellof[i] = cell;
-    s.slot[i] = atomicAdd(&s.count[cell], 1);
+    bin_body(g, s, blockIdx.x);
 }
 
 // Exclusive block scan of one value per thread (blockDim.x == kScanBlock).
@@ -154,14 +130,13 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_add_fused(int *__restrict__
     if (b == nb - 1 && threadIdx.x == 0) start[ncell] = off + bsum[b];
 }
 
+
+
 // Also zeroes the cell counts for the next build (the scan has consumed them).
 __global__ void k_scatter(SysDev s, int ncell) {
     pdl_entry();
     if (gate_closed(s.skin)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int c = i; c < ncell; c += gridDim.x * blockDim.x) s.count[c] = 0;
-    if (i >= s.n) return;
-    s.arrival[s.start[s.cellof[i]] + s.slot[i]] = i;
+    scatter_body(s, ncell, blockIdx.x, gridDim.x);
 }
 
 // One thread per sorted slot: the atom that arrived there takes the place of
@@ -170,36 +145,7 @@ __global__ void k_scatter(SysDev s, int ncell) {
 __global__ void k_place(CellGrid g, SysDev s) {
     pdl_entry();
     if (gate_closed(s.skin)) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= s.n) return;
-    const int i = s.arrival[k];
-    const int c = s.cellof[i];
-    const int b = s.start[c], e = s.start[c + 1];
-    int rank = 0;
-    for (int t = b; t < e; ++t) rank += s.arrival[t] < i;
-    const int d = b + rank;
-    s.perm[d] = i;
-    const double x0 = s.x[3 * i], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
-    s.xs[3 * d] = x0;
-    s.xs[3 * d + 1] = x1;
-    s.xs[3 * d + 2] = x2;
-    if (s.xref) {   // skin lists: positions of this build, for the displacement test
-        s.xref[3 * d] = x0;
-        s.xref[3 * d + 1] = x1;
-        s.xref[3 * d + 2] = x2;
-    }
-    const int cz = c % g.nc[2], cy = (c / g.nc[2]) % g.nc[1], cx = c / (g.nc[2] * g.nc[1]);
-    double w0, w1, w2;
-    cell_coord(x0, g, 0, w0);
-    cell_coord(x1, g, 1, w1);
-    cell_coord(x2, g, 2, w2);
-    float4 p;
-    p.x = (float)(w0 - cx * g.h[0]);
-    p.y = (float)(w1 - cy * g.h[1]);
-    p.z = (float)(w2 - cz * g.h[2]);
-    p.w = __int_as_float(pack_cell(cx, cy, cz));
-    s.pf[d] = p;
-    s.smask[d] = i < s.nown ? (s.mask ? s.mask[i] : -1) : 0;
+    place_body(g, s, blockIdx.x);
 }
 
 template <int KIND>
@@ -274,73 +220,15 @@ __global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, Neig
     if (cnt > nd.M) atomicMax(&status->overflow, (unsigned)cnt);
 }
 
-// Fast path, valid when every periodic dimension has at least three cells:
-// the 27 stencil cells are then distinct and the displacement to an atom of
-// the cell at offset o is exactly o h + (off_j - off_k), so each cell's shift
-// o h - off_k is formed once and a candidate costs one load and three adds.
+
+// Fast path, valid when every periodic dimension has at least three cells
+// (neighbors_fast_body).
 template <int KIND>
 __global__ void __launch_bounds__(kBlock) k_neighbors_fast(CellGrid g, SysDev s, NeighSpec ns, NeighDev nd,
                                                            DevStatus *status) {
     pdl_entry();
     if (gate_closed(s.skin)) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= s.n) return;
-    const GeoD gd = geo_d(g, s.xs);
-    const float4 a = s.pf[k];
-    const int w = __float_as_int(a.w);
-    const int cx = w & 1023, cy = (w >> 10) & 1023, cz = w >> 20;
-    const int nx = g.nc[0], ny = g.nc[1], nz = g.nc[2];
-    int cnt = 0;
-#pragma unroll 1
-    for (int ox = -1; ox <= 1; ++ox) {
-        int x = cx + ox;
-        if (x < 0 || x >= nx) {
-            if (!g.periodic[0]) continue;
-            x += x < 0 ? nx : -nx;
-        }
-        const float sx = (float)ox * g.hf[0] - a.x;
-#pragma unroll 1
-        for (int oy = -1; oy <= 1; ++oy) {
-            int y = cy + oy;
-            if (y < 0 || y >= ny) {
-                if (!g.periodic[1]) continue;
-                y += y < 0 ? ny : -ny;
-            }
-            const float sy = (float)oy * g.hf[1] - a.y;
-            const int col = (x * ny + y) * nz;
-#pragma unroll
-            for (int oz = -1; oz <= 1; ++oz) {
-                int z = cz + oz;
-                if (z < 0 || z >= nz) {
-                    if (!g.periodic[2]) continue;
-                    z += z < 0 ? nz : -nz;
-                }
-                const float sz = (float)oz * g.hf[2] - a.z;
-                const int jb = __ldg(s.start + col + z), je = __ldg(s.start + col + z + 1);
-                float4 nxt = jb < je ? __ldg(s.pf + jb) : make_float4(0.f, 0.f, 0.f, 0.f);
-                for (int j = jb; j < je; ++j) {
-                    const float4 b = nxt;
-                    if (j + 1 < je) nxt = __ldg(s.pf + j + 1);
-                    const float dx = b.x + sx, dy = b.y + sy, dz = b.z + sz;
-                    const float r2f = dx * dx + dy * dy + dz * dz;
-                    if (r2f > ns.hi2 || j == k) continue;
-                    bool in;
-                    if (KIND == NK_CAND || (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f)) {
-                        in = true;
-                    } else {
-                        const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
-                        const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
-                        in = exact_decide<KIND>(gd, ns, xk, xj);
-                    }
-                    if (!in) continue;
-                    if (cnt < nd.M) nd.list[(size_t)cnt * s.npad + k] = j;
-                    ++cnt;
-                }
-            }
-        }
-    }
-    nd.count[k] = cnt;
-    if (cnt > nd.M) atomicMax(KIND == NK_CAND ? &status->cand_overflow : &status->overflow, (unsigned)cnt);
+    neighbors_fast_body<KIND>(g, s, ns, nd, status, blockIdx.x);
 }
 
 // Same lists as k_neighbors_fast (same cells in the same order, same tests),

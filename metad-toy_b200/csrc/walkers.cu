@@ -10,6 +10,11 @@
 // for the forces.  With the CUDA graph enabled the whole step is captured
 // once per (atom counts, array pointers) and replayed; the step number
 // travels through device memory.
+//
+// Decks whose walkers hold one STEINH L unit (one or two orders) on one
+// neighbour environment, without skin lists and not sharded over ranks, run
+// the step instead as ONE persistent kernel launch (walk_step.cu): the same
+// bodies, the same block partials, the same results bit for bit.
 struct mtd_walkers {
     std::vector<mtd_ctx *> w;
     std::string err;
@@ -40,6 +45,17 @@ struct mtd_walkers {
     void *ag_user = nullptr;
     double *d_xloc = nullptr, *d_xall = nullptr;   // [nwalk][kWalkRec], [nranks * nwalk][kWalkRec]
     double *h_xloc = nullptr, *h_xall = nullptr;   // pinned staging of the same
+    // persistent single-launch step
+    bool persist_enabled = true;              // mtd_walkers_enable_persistent
+    bool persist_last = false;                // the last step ran as one launch
+    void *d_desc = nullptr;                   // WalkDesc<T>[nwalk]
+    std::vector<unsigned char> h_desc;        // the descriptors last uploaded
+    int *d_pre = nullptr;                     // prefix sums: atom blocks, then cell chunks (2 (nwalk + 1))
+    std::vector<int> h_pre;
+    GridBar *d_bar = nullptr;
+    int persist_blocks = 0;
+    int wait_limit = 1 << 22;                 // barrier polls (mtd_walkers_set_wait)
+    int wait_stall = 0;
 };
 
 namespace {
@@ -116,6 +132,98 @@ mtd_status walkers_enqueue(mtd_walkers *W, long long step, const int *n, const d
     return MTD_OK;
 }
 
+// The persistent path applies: every walker one STEINH L unit on one
+// environment, no skin lists, not sharded, a step kernel for the orders.
+bool persist_eligible(const mtd_walkers *W) {
+    if (!W->persist_enabled || W->nranks > 0 || (int)W->w.size() > kWalkPersistMax) return false;
+    for (const mtd_ctx *c : W->w)
+        if (c->units.size() != 1 || c->units[0].kind != CAL_STEINH_L || c->envs.size() != 1 ||
+            c->units[0].env != 0 || c->cfg.neigh_skin > 0.0)
+            return false;
+    return true;
+}
+
+template <typename T>
+mtd_status walkers_persist_step(mtd_walkers *W, const int *n, const double *const *d_x, double *const *d_f,
+                                bool *done) {
+    const int nw = (int)W->w.size();
+    *done = false;
+    std::vector<unsigned char> desc(sizeof(WalkDesc<T>) * nw);
+    std::vector<int> pre(2 * (nw + 1), 0);
+    for (int k = 0; k < nw; ++k) {
+        mtd_ctx *c = W->w[k];
+        WalkDesc<T> d;
+        bool ok = true;
+        const mtd_status s = walk_desc<T>(c, n[k], d_x[k], d_f[k], d, &ok);
+        if (s != MTD_OK) return wfail(W, s, "walker " + std::to_string(k) + ": " + c->err);
+        if (!ok) return MTD_OK;   // a thin periodic box: the per-walker kernels handle it
+        std::memcpy(desc.data() + sizeof(WalkDesc<T>) * k, &d, sizeof d);
+        pre[k + 1] = pre[k] + d.nb;
+        pre[nw + 1 + k + 1] = pre[nw + 1 + k] + d.nchunk;
+    }
+    const Unit &u = W->w[0]->units[0];
+    const bool step_switch = u.sw_r.type == SW_STEP;
+    if (!W->d_desc) {
+        W->persist_blocks = walk_step_blocks<T>(u.LA, u.LB, step_switch);
+        if (W->persist_blocks < 1) return MTD_OK;
+        MTD_WCU(cudaMalloc(&W->d_desc, sizeof(WalkDesc<T>) * nw), "walker descriptors");
+        MTD_WCU(cudaMalloc(&W->d_pre, sizeof(int) * 2 * (nw + 1)), "walker descriptors");
+        MTD_WCU(cudaMalloc(&W->d_bar, sizeof(GridBar)), "grid barrier");
+        MTD_WCU(cudaMemset(W->d_bar, 0, sizeof(GridBar)), "grid barrier");
+    }
+    const bool changed = desc != W->h_desc || pre != W->h_pre;
+    if (changed) {   // new arguments: no graph holds the old ones
+        walkers_drop_graph(W);
+        MTD_WCU(cudaMemcpyAsync(W->d_desc, desc.data(), desc.size(), cudaMemcpyHostToDevice, W->st), "descriptors");
+        MTD_WCU(cudaMemcpyAsync(W->d_pre, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, W->st),
+                "descriptors");
+        MTD_WCU(cudaStreamSynchronize(W->st), "descriptors");
+        W->h_desc.swap(desc);
+        W->h_pre.swap(pre);
+    }
+    WalkStepArgs a{};
+    a.nwalk = nw;
+    a.pa = W->d_pre;
+    a.pc = W->d_pre + nw + 1;
+    a.plans = W->d_plans;
+    a.step = W->h_step;   // pinned: the launch reads the step the host set
+    a.ws = W->d_ws;
+    a.bar = W->d_bar;
+    a.limit = W->wait_limit;
+    a.stall = W->wait_stall;
+    const WalkDesc<T> *dd = static_cast<const WalkDesc<T> *>(W->d_desc);
+    auto launch = [&]() {
+        return launch_walk_step<T>(u.LA, u.LB, step_switch, dd, a, W->persist_blocks, W->st);
+    };
+    if (W->use_graph && !changed && W->gexec) {
+        MTD_WCU(cudaGraphLaunch(W->gexec, W->st), "graph launch");
+    } else if (W->use_graph && !changed) {
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamBeginCapture(W->st, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) {
+            const cudaError_t le = launch();
+            ce = cudaStreamEndCapture(W->st, &g);
+            if (le != cudaSuccess) ce = le;
+        }
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&W->gexec, g, 0);
+        if (ce == cudaSuccess) {
+            W->graph = g;
+            MTD_WCU(cudaGraphLaunch(W->gexec, W->st), "graph launch");
+        } else {   // the launch cannot be captured here: plain launches
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            W->gexec = nullptr;
+            W->use_graph = false;
+            MTD_WCU(launch(), "walker step launch");
+        }
+    } else {
+        MTD_WCU(launch(), "walker step launch");
+    }
+    W->launches = 1;
+    *done = true;
+    return MTD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -178,6 +286,9 @@ void mtd_walkers_destroy(mtd_walkers *W) {
     if (W->d_xall) cudaFree(W->d_xall);
     if (W->h_xloc) cudaFreeHost(W->h_xloc);
     if (W->h_xall) cudaFreeHost(W->h_xall);
+    if (W->d_desc) cudaFree(W->d_desc);
+    if (W->d_pre) cudaFree(W->d_pre);
+    if (W->d_bar) cudaFree(W->d_bar);
     if (W->st) cudaStreamDestroy(W->st);
     if (W->f_hills) std::fclose(W->f_hills);
     delete W;
@@ -285,6 +396,25 @@ mtd_status mtd_walkers_step_device(mtd_walkers *W, int64_t step, const int *n, c
         if (s != MTD_OK) return s;
     }
     *W->h_step = step;
+    if (persist_eligible(W)) {
+        bool done = false;
+        const mtd_status s = W->w[0]->fp64 ? walkers_persist_step<double>(W, n, d_x, d_f, &done)
+                                           : walkers_persist_step<float>(W, n, d_x, d_f, &done);
+        if (s != MTD_OK) return s;
+        if (done) {
+            W->persist_last = true;
+            W->g_n.clear();   // the per-walker graph (if any) no longer matches
+            for (mtd_ctx *c : W->w) {
+                c->pending = true;
+                c->pending_step = step;
+                c->want_virial = false;
+            }
+            W->pending = true;
+            W->pending_step = step;
+            return MTD_OK;
+        }
+    }
+    W->persist_last = false;
     bool same = (int)W->g_n.size() == nw;
     for (int k = 0; same && k < nw; ++k) same = W->g_n[k] == n[k] && W->g_x[k] == d_x[k] && W->g_f[k] == d_f[k];
     if (W->use_graph && same && W->gexec) {
@@ -346,6 +476,17 @@ mtd_status mtd_walkers_sync(mtd_walkers *W) {
     MTD_WCU(cudaStreamSynchronize(W->st), "sync");
     if (!W->pending) return MTD_OK;
     W->pending = false;
+    if (W->persist_last && W->d_bar) {   // a grid-barrier wait of the persistent step ran out
+        GridBar hb{};
+        MTD_WCU(cudaMemcpy(&hb, W->d_bar, sizeof hb, cudaMemcpyDeviceToHost), "grid barrier");
+        if (hb.err) {
+            MTD_WCU(cudaMemset(W->d_bar, 0, sizeof(GridBar)), "grid barrier");
+            walkers_drop_graph(W);
+            for (mtd_ctx *c : W->w) c->pending = false;
+            return wfail(W, MTD_ERR_TIMEOUT,
+                         "walker step: a grid-barrier wait ran out; the step is incomplete, repeat it");
+        }
+    }
     bool overflow = false;
     for (mtd_ctx *c : W->w) {
         if (c->h_status->overflow || c->h_status->cand_overflow) {
@@ -410,5 +551,27 @@ mtd_status mtd_walkers_get_grid(mtd_walkers *W, double *out, int64_t count) {
 }
 
 int mtd_walkers_last_launch_count(const mtd_walkers *W) { return W ? W->launches : 0; }
+
+mtd_status mtd_walkers_enable_persistent(mtd_walkers *W, int enable) {
+    if (!W) return MTD_ERR_INVALID_ARG;
+    if (W->st) cudaStreamSynchronize(W->st);
+    walkers_drop_graph(W);
+    W->g_n.clear();
+    W->h_desc.clear();
+    W->persist_enabled = enable != 0;
+    return MTD_OK;
+}
+
+int mtd_walkers_persistent_active(const mtd_walkers *W) { return W && W->persist_last ? 1 : 0; }
+
+mtd_status mtd_walkers_set_wait(mtd_walkers *W, int limit, int stall) {
+    if (!W || limit < 0) return MTD_ERR_INVALID_ARG;
+    if (W->st) cudaStreamSynchronize(W->st);
+    walkers_drop_graph(W);
+    W->h_desc.clear();
+    W->wait_limit = limit > 0 ? limit : (1 << 22);
+    W->wait_stall = stall ? 1 : 0;
+    return MTD_OK;
+}
 
 }  // extern "C"

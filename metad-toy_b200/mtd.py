@@ -39,7 +39,8 @@ EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args",
            "mtd_walkers_create", "mtd_walkers_destroy", "mtd_walkers_last_error", "mtd_walkers_count",
            "mtd_walkers_set_box", "mtd_walkers_init", "mtd_walkers_enable_graph", "mtd_walkers_step_device",
            "mtd_walkers_sync", "mtd_walkers_cv", "mtd_walkers_bias", "mtd_walkers_get_grid",
-           "mtd_walkers_last_launch_count", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types",
+           "mtd_walkers_last_launch_count", "mtd_walkers_enable_persistent", "mtd_walkers_persistent_active",
+           "mtd_walkers_set_wait", "mtd_autotune", "mtd_set_tuning", "mtd_walkers_autotune", "mtd_set_types", "mtd_needs_types",
            "mtd_set_domain", "mtd_set_nlocal", "mtd_ghost_cutoff",
            "mtd_set_positions_f64", "mtd_step", "mtd_get_peratom", "mtd_create_from_config",
            "mtd_set_domain_device", "mtd_walkers_set_ranks", "mtd_walkers_set_ranks_device"]
@@ -149,6 +150,9 @@ def lib():
         L.mtd_walkers_bias.restype = C.c_double
         L.mtd_walkers_get_grid.argtypes = [vp, dp, C.c_int64]
         L.mtd_walkers_last_launch_count.argtypes = [vp]
+        L.mtd_walkers_enable_persistent.argtypes = [vp, C.c_int]
+        L.mtd_walkers_persistent_active.argtypes = [vp]
+        L.mtd_walkers_set_wait.argtypes = [vp, C.c_int, C.c_int]
         L.mtd_nnbias_create.argtypes = [C.c_int, dp, dp, C.c_uint64, C.POINTER(vp)]
         L.mtd_nnbias_destroy.argtypes = [vp]
         L.mtd_nnbias_last_error.argtypes = [vp]
@@ -675,6 +679,19 @@ class Walkers:
 
     def launch_count(self):
         return lib().mtd_walkers_last_launch_count(self._h)
+
+    def enable_persistent(self, on=True):
+        """One persistent kernel launch per step where the deck allows it (default on)."""
+        self._check(lib().mtd_walkers_enable_persistent(self._h, 1 if on else 0))
+
+    @property
+    def persistent_active(self):
+        return bool(lib().mtd_walkers_persistent_active(self._h))
+
+    def set_wait(self, limit=0, stall=False):
+        """Grid-barrier wait limit of the persistent step (0: default); stall=True
+        makes the next step's waits run out (MTD_ERR_TIMEOUT from sync)."""
+        self._check(lib().mtd_walkers_set_wait(self._h, int(limit), 1 if stall else 0))
 
     def autotune(self, ns, x_ptrs, reps=5):
         """Per walker (neighbour shape, q block, lambda block), tuned on its own device positions."""
