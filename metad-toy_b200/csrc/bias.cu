@@ -144,48 +144,19 @@ __device__ double eval_code(const ExprInstr *code, int n, const double *sym, int
             ++sp;
             continue;
         }
-        if (c.op == EOP_ADD || c.op == EOP_SUB || c.op == EOP_MUL || c.op == EOP_DIV || c.op == EOP_POW ||
-            c.op == EOP_MIN || c.op == EOP_MAX || c.op == EOP_ATAN2) {
-            Dual &a = st[sp - 2];
-            const Dual &b = st[sp - 1];
-            double v, da, db;
-            switch (c.op) {
-            case EOP_ADD: v = a.v + b.v; da = 1; db = 1; break;
-            case EOP_SUB: v = a.v - b.v; da = 1; db = -1; break;
-            case EOP_MUL: v = a.v * b.v; da = b.v; db = a.v; break;
-            case EOP_DIV: v = a.v / b.v; da = 1.0 / b.v; db = -a.v / (b.v * b.v); break;
-            case EOP_POW: v = pow(a.v, b.v); da = b.v * pow(a.v, b.v - 1.0); db = (a.v > 0) ? v * log(a.v) : 0.0; break;
-            case EOP_MIN: v = a.v <= b.v ? a.v : b.v; da = a.v <= b.v; db = !(a.v <= b.v); break;
-            case EOP_MAX: v = a.v >= b.v ? a.v : b.v; da = a.v >= b.v; db = !(a.v >= b.v); break;
-            default: { double r2 = a.v * a.v + b.v * b.v; v = atan2(a.v, b.v); da = b.v / r2; db = -a.v / r2; }
-            }
-            for (int k = 0; k < nsym; ++k) a.g[k] = da * a.g[k] + db * b.g[k];
-            a.v = v;
-            --sp;
-            continue;
+        const int na = expr_arity(c.op);
+        double a[3] = {0.0, 0.0, 0.0}, d[3];
+        for (int i = 0; i < na; ++i) a[i] = st[sp - na + i].v;
+        const double v = expr_apply(c.op, a, d);
+        Dual &r = st[sp - na];
+        for (int k = 0; k < nsym; ++k) {
+            double g = 0.0;   // an operand with a zero partial (an unselected branch) contributes nothing
+            for (int i = 0; i < na; ++i)
+                if (d[i] != 0.0) g += d[i] * st[sp - na + i].g[k];
+            r.g[k] = g;
         }
-        Dual &a = st[sp - 1];
-        const double x = a.v;
-        double v = 0, dv = 0;
-        switch (c.op) {
-        case EOP_NEG: v = -x; dv = -1; break;
-        case EOP_SIN: v = sin(x); dv = cos(x); break;
-        case EOP_COS: v = cos(x); dv = -sin(x); break;
-        case EOP_TAN: v = tan(x); dv = 1.0 + v * v; break;
-        case EOP_ASIN: v = asin(x); dv = 1.0 / sqrt(1.0 - x * x); break;
-        case EOP_ACOS: v = acos(x); dv = -1.0 / sqrt(1.0 - x * x); break;
-        case EOP_ATAN: v = atan(x); dv = 1.0 / (1.0 + x * x); break;
-        case EOP_EXP: v = exp(x); dv = v; break;
-        case EOP_LOG: v = log(x); dv = 1.0 / x; break;
-        case EOP_LOG10: v = log10(x); dv = 1.0 / (x * 2.30258509299404568402); break;
-        case EOP_SQRT: v = sqrt(x); dv = 0.5 / v; break;
-        case EOP_ABS: v = fabs(x); dv = (x > 0) - (x < 0); break;
-        case EOP_TANH: v = tanh(x); dv = 1.0 - v * v; break;
-        case EOP_SINH: v = sinh(x); dv = cosh(x); break;
-        case EOP_COSH: v = cosh(x); dv = sinh(x); break;
-        }
-        for (int k = 0; k < nsym; ++k) a.g[k] *= dv;
-        a.v = v;
+        r.v = v;
+        sp -= na - 1;
     }
     for (int k = 0; k < nsym; ++k) grad[k] = st[0].g[k];
     return st[0].v;

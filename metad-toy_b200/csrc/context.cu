@@ -211,6 +211,18 @@ mtd_status alloc_unit(mtd_ctx *c, Unit &u, int npad) {
     return MTD_OK;
 }
 
+cudaError_t h2d_pieces(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+    constexpr size_t kPiece = size_t(3) << 20;
+    const size_t pieces = (bytes + kPiece - 1) / kPiece;
+    for (size_t p = 0; p < pieces; ++p) {
+        const size_t a = bytes * p / pieces, b = bytes * (p + 1) / pieces;
+        const cudaError_t e = cudaMemcpyAsync(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, b - a,
+                                              cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 mtd_status ensure_capacity(mtd_ctx *c, int n) {
     const int npad = ((n + kBlock - 1) / kBlock) * kBlock + kBlock;
     c->n = n;
@@ -1301,7 +1313,7 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
     mtd_status s = MTD_OK;
     MTD_CU(cudaEventRecord(c->f_ready, c->st), "force upload");   // the side copies start after the previous step
     MTD_CU(cudaStreamWaitEvent(c->side_st, c->f_ready, 0), "force upload");
-    MTD_CU(cudaMemcpyAsync(c->d_fin, f, b3, cudaMemcpyHostToDevice, c->side_st), "f upload");
+    MTD_CU(h2d_pieces(c->d_fin, f, b3, c->side_st), "f upload");
     if (image && virial) MTD_CU(cudaMemcpyAsync(c->d_image, image, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->side_st), "image upload");
     MTD_CU(cudaEventRecord(c->f_ready, c->side_st), "force upload");
     for (int attempt = 0; attempt < 4; ++attempt) {
@@ -1339,7 +1351,7 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
     const size_t b3 = sizeof(double) * 3 * (size_t)n;
     // x (and mask) first on the step's stream; f (and image, read by the force
     // kernels only) on the side stream, overlapping the CV passes
-    MTD_CU(cudaMemcpyAsync(c->d_x, x, b3, cudaMemcpyHostToDevice, c->st), "x upload");
+    MTD_CU(h2d_pieces(c->d_x, x, b3, c->st), "x upload");
     if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
     return step_uploaded(c, step, n, mask != nullptr, image, f, virial);
 }
@@ -1357,7 +1369,7 @@ mtd_status mtd_set_positions_f64(mtd_ctx *c, const double *x, const int *type, c
         s = mtd_set_types(c, n, type);
         if (s != MTD_OK) return s;
     }
-    MTD_CU(cudaMemcpyAsync(c->d_x, x, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, c->st), "x upload");
+    MTD_CU(h2d_pieces(c->d_x, x, sizeof(double) * 3 * (size_t)n, c->st), "x upload");
     if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
     MTD_CU(cudaStreamSynchronize(c->st), "x upload");   // the caller's arrays are borrowed for this call only
     c->staged_n = n;

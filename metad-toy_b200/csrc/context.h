@@ -260,6 +260,10 @@ mtd_status alloc_env(mtd_ctx *c, Env &e, int npad);
 mtd_status alloc_cand(mtd_ctx *c, Env &e, int npad);
 mtd_status alloc_unit(mtd_ctx *c, Unit &u, int npad);
 mtd_status ensure_capacity(mtd_ctx *c, int n);
+// Host -> device copy from pinned memory in pieces of at most 3 MB: one
+// multi-megabyte cudaMemcpyAsync moves ~25 GB/s over the host link, pieces of
+// a few MB back to back reach ~50 GB/s.
+cudaError_t h2d_pieces(void *dst, const void *src, size_t bytes, cudaStream_t st);
 mtd_status ensure_cells(mtd_ctx *c, int ncell);
 void build_plan(mtd_ctx *c);
 mtd_status plan_units(mtd_ctx *c);

@@ -3,20 +3,18 @@
 //
 // It replaces the exprtk expressions and exprtk::derivative of
 // src/grids/DimSet.cu:54-97: the value is the same expression, and the chain
-// factor dS/dv is exact instead of exprtk's central difference (h = 1e-8,
-// which adds ~1e-8 relative noise to the reference's forces).
+// factor dS/dv is exact instead of exprtk's five-point difference (h = 1e-8,
+// which adds ~1e-8 relative noise to the reference's forces).  The grammar is
+// exprtk's expression subset (no statements, assignments, strings, vectors or
+// loops); the operations and their semantics are listed in expr_ops.h.
 #pragma once
 
 #include <string>
 #include <vector>
 
-namespace mtd {
+#include "expr_ops.h"
 
-enum ExprOp {
-    EOP_CONST = 0, EOP_SYM, EOP_ADD, EOP_SUB, EOP_MUL, EOP_DIV, EOP_POW, EOP_NEG,
-    EOP_SIN, EOP_COS, EOP_TAN, EOP_ASIN, EOP_ACOS, EOP_ATAN, EOP_EXP, EOP_LOG, EOP_LOG10,
-    EOP_SQRT, EOP_ABS, EOP_TANH, EOP_SINH, EOP_COSH, EOP_MIN, EOP_MAX, EOP_ATAN2
-};
+namespace mtd {
 
 struct ExprInstr {
     int op;

@@ -481,6 +481,11 @@ mtd_status mtd_walkers_sync(mtd_walkers *W) {
         MTD_WCU(cudaMemcpy(&hb, W->d_bar, sizeof hb, cudaMemcpyDeviceToHost), "grid barrier");
         if (hb.err) {
             MTD_WCU(cudaMemset(W->d_bar, 0, sizeof(GridBar)), "grid barrier");
+            // the launch may have binned atoms without reaching the scatter
+            // pass that zeroes the cell counts: zero them for the next build
+            for (mtd_ctx *c : W->w)
+                if (c->count) MTD_WCU(cudaMemset(c->count, 0, sizeof(int) * (size_t)c->cap_cell), "cell counts");
+            MTD_WCU(cudaDeviceSynchronize(), "grid barrier");
             walkers_drop_graph(W);
             for (mtd_ctx *c : W->w) c->pending = false;
             return wfail(W, MTD_ERR_TIMEOUT,

@@ -336,149 +336,349 @@ class _Dual:
     __slots__ = ("v", "d")
 
     def __init__(self, v, d):
-        self.v, self.d = v, d
+        self.v, self.d = float(v), d
 
 
+def _np(f):
+    def g(*a):
+        with np.errstate(all="ignore"):
+            return float(f(*[np.float64(x) for x in a]))
+    return g
+
+
+_sin, _cos, _tan, _exp, _log, _sqrt = (_np(np.sin), _np(np.cos), _np(np.tan), _np(np.exp), _np(np.log),
+                                       _np(np.sqrt))
+_pow, _floor, _ceil, _trunc, _fmod = _np(np.power), _np(np.floor), _np(np.ceil), _np(np.trunc), _np(np.fmod)
+
+
+def _erf(x):
+    return math.erf(x) if math.isfinite(x) else (math.copysign(1.0, x) if not math.isnan(x) else math.nan)
+
+
+def _erfc(x):
+    return 1.0 - _erf(x) if not math.isfinite(x) else math.erfc(x)
+
+
+def _round(v):   # exprtk round_impl: half away from zero through floor / ceil
+    return _ceil(v - 0.5) if v < 0 else _floor(v + 0.5)
+
+
+def _sinc(x):
+    return (_sin(x) / x, (_cos(x) - _sin(x) / x) / x) if abs(x) >= 2.220446049250313e-16 else (1.0, 0.0)
+
+
+def _root(x, n):
+    if x < 0:
+        odd = n == _trunc(n) and _fmod(n, 2.0) != 0.0
+        v = -_pow(-x, 1.0 / n) if odd else math.nan
+    else:
+        v = _pow(x, 1.0 / n)
+    with np.errstate(all="ignore"):
+        dx = float(np.float64(v) / (np.float64(n) * np.float64(x)))
+    dn = -v * _log(abs(x)) / (n * n) if x != 0 else 0.0
+    return v, dx, dn
+
+
+def _near(a, b):   # exprtk equal(): within 1e-10 of max(1, |a|, |b|)
+    return abs(a - b) <= max(1.0, abs(a), abs(b)) * 1e-10
+
+
+_PI = math.pi
+# name -> (value(x), d value / dx)
 _FUNCS1 = {
-    "sin": (math.sin, math.cos), "cos": (math.cos, lambda x: -math.sin(x)),
-    "exp": (math.exp, math.exp), "log": (math.log, lambda x: 1.0 / x),
-    "sqrt": (math.sqrt, lambda x: 0.5 / math.sqrt(x)), "tanh": (math.tanh, lambda x: 1.0 - math.tanh(x) ** 2),
+    "sin": (_sin, _cos), "cos": (_cos, lambda x: -_sin(x)), "tan": (_tan, lambda x: 1.0 + _tan(x) ** 2),
+    "asin": (_np(np.arcsin), lambda x: 1.0 / _sqrt(1.0 - x * x)),
+    "acos": (_np(np.arccos), lambda x: -1.0 / _sqrt(1.0 - x * x)),
+    "atan": (_np(np.arctan), lambda x: 1.0 / (1.0 + x * x)),
+    "exp": (_exp, _exp), "log": (_log, lambda x: 1.0 / x),
+    "log10": (_np(np.log10), lambda x: 1.0 / (x * math.log(10.0))),
+    "log2": (_np(np.log2), lambda x: 1.0 / (x * math.log(2.0))),
+    "log1p": (_np(np.log1p), lambda x: 1.0 / (1.0 + x)), "expm1": (_np(np.expm1), _exp),
+    "sqrt": (_sqrt, lambda x: 0.5 / _sqrt(x)),
     "abs": (abs, lambda x: (1.0 if x > 0 else (-1.0 if x < 0 else 0.0))),
+    "tanh": (_np(np.tanh), lambda x: 1.0 - _np(np.tanh)(x) ** 2),
+    "sinh": (_np(np.sinh), _np(np.cosh)), "cosh": (_np(np.cosh), _np(np.sinh)),
+    "asinh": (_np(np.arcsinh), lambda x: 1.0 / _sqrt(x * x + 1.0)),
+    "acosh": (_np(np.arccosh), lambda x: 1.0 / _sqrt(x * x - 1.0)),
+    "atanh": (_np(np.arctanh), lambda x: 1.0 / (1.0 - x * x)),
+    "sec": (lambda x: 1.0 / _cos(x), lambda x: _tan(x) / _cos(x)),
+    "csc": (lambda x: 1.0 / _sin(x), lambda x: -1.0 / (_sin(x) * _tan(x))),
+    "cot": (lambda x: 1.0 / _tan(x), lambda x: -(1.0 + 1.0 / _tan(x) ** 2)),
+    "erf": (_erf, lambda x: 2.0 / math.sqrt(_PI) * _exp(-x * x)),
+    "erfc": (_erfc, lambda x: -2.0 / math.sqrt(_PI) * _exp(-x * x)),
+    "ncdf": (lambda x: 0.5 * _erfc(-x / math.sqrt(2.0)), lambda x: _exp(-0.5 * x * x) / math.sqrt(2.0 * _PI)),
+    "sinc": (lambda x: _sinc(x)[0], lambda x: _sinc(x)[1]),
+    "not": (lambda x: 0.0 if x != 0 else 1.0, lambda x: 0.0),
+    "sgn": (lambda x: 1.0 if x > 0 else (-1.0 if x < 0 else 0.0), lambda x: 0.0),
+    "floor": (_floor, lambda x: 0.0), "ceil": (_ceil, lambda x: 0.0), "round": (_round, lambda x: 0.0),
+    "trunc": (_trunc, lambda x: 0.0), "frac": (lambda x: x - _trunc(x), lambda x: 1.0),
+    "deg2rad": (lambda x: x * (_PI / 180.0), lambda x: _PI / 180.0),
+    "rad2deg": (lambda x: x * (180.0 / _PI), lambda x: 180.0 / _PI),
+    "deg2grad": (lambda x: x * (10.0 / 9.0), lambda x: 10.0 / 9.0),
+    "grad2deg": (lambda x: x * (9.0 / 10.0), lambda x: 9.0 / 10.0),
 }
 
+_FUNC_NAMES = set(_FUNCS1) | {"min", "max", "sum", "avg", "mul", "mand", "mor", "pow", "atan2", "mod", "hypot",
+                               "logn", "root", "roundn", "equal", "not_equal", "shl", "shr", "if", "clamp",
+                               "iclamp", "inrange"}
+_RESERVED = {"assert", "break", "case", "continue", "const", "default", "false", "for", "if", "else", "ilike",
+             "in", "like", "and", "nand", "nor", "not", "null", "or", "repeat", "return", "shl", "shr", "swap",
+             "switch", "true", "until", "var", "while", "xnor", "xor"}
+# binary operators: token -> (left precedence, right precedence, name)
+_BIN = {"+": (7, 8, "add"), "-": (7, 8, "sub"), "*": (10, 11, "mul"), "/": (10, 11, "div"),
+        "%": (10, 11, "mod"), "^": (12, 12, "pow"), "<": (5, 6, "lt"), "<=": (5, 6, "le"), ">": (5, 6, "gt"),
+        ">=": (5, 6, "ge"), "==": (5, 6, "eq"), "=": (5, 6, "eq"), "!=": (5, 6, "ne"), "<>": (5, 6, "ne"),
+        "and": (3, 4, "and"), "nand": (3, 4, "nand"), "or": (1, 2, "or"), "nor": (1, 2, "nor"),
+        "xor": (1, 2, "xor"), "xnor": (1, 2, "xnor")}
 
-def eval_expr(expr, values):
-    """Evaluate expression `expr` over symbol values dict -> (value, {sym: d/dsym})."""
-    syms = list(values.keys())
-    idx = {s: i for i, s in enumerate(syms)}
-    toks = []
-    i = 0
+
+def _binary(name, a, b):
+    """Value and partials (da, db) of a binary operation."""
+    x, y = a.v, b.v
+    t = lambda c: 1.0 if c else 0.0
+    if name == "add":
+        return x + y, 1.0, 1.0
+    if name == "sub":
+        return x - y, 1.0, -1.0
+    if name == "mul":
+        return x * y, y, x
+    if name == "div":
+        with np.errstate(all="ignore"):
+            return float(np.float64(x) / y), float(1.0 / np.float64(y)), float(-np.float64(x) / (np.float64(y) * y))
+    if name == "pow":
+        v = _pow(x, y)
+        return v, y * _pow(x, y - 1.0), (v * _log(x) if x > 0 else 0.0)
+    if name == "mod":
+        return _fmod(x, y), 1.0, -_trunc(x / y)
+    if name in ("lt", "le", "gt", "ge", "eq", "ne"):
+        r = {"lt": x < y, "le": x <= y, "gt": x > y, "ge": x >= y, "eq": x == y, "ne": x != y}[name]
+        return t(r), 0.0, 0.0
+    p, q = x != 0, y != 0
+    r = {"and": p and q, "nand": not (p and q), "or": p or q, "nor": not (p or q), "xor": p != q,
+         "xnor": p == q}[name]
+    return t(r), 0.0, 0.0
+
+
+def _lex(expr):
+    toks, i = [], 0
     while i < len(expr):
         ch = expr[i]
         if ch.isspace():
             i += 1
-        elif ch.isdigit() or ch == ".":
+        elif ch.isdigit() or (ch == "." and i + 1 < len(expr) and expr[i + 1].isdigit()):
             j = i
-            while j < len(expr) and (expr[j].isdigit() or expr[j] in ".eE" or
-                                     (expr[j] in "+-" and expr[j - 1] in "eE")):
+            while j < len(expr) and expr[j].isdigit():
                 j += 1
+            if j < len(expr) and expr[j] == ".":
+                j += 1
+                while j < len(expr) and expr[j].isdigit():
+                    j += 1
+            if j < len(expr) and expr[j] in "eE":
+                k = j + 1
+                if k < len(expr) and expr[k] in "+-":
+                    k += 1
+                if k < len(expr) and expr[k].isdigit():
+                    while k < len(expr) and expr[k].isdigit():
+                        k += 1
+                    j = k
             toks.append(("num", float(expr[i:j])))
             i = j
         elif ch.isalpha() or ch == "_":
-            j = i
-            while j < len(expr) and (expr[j].isalnum() or expr[j] == "_"):
+            j = i + 1
+            while j < len(expr) and (expr[j].isalnum() or expr[j] in "_."):
                 j += 1
             toks.append(("id", expr[i:j]))
             i = j
-        else:
+        elif ch in "&|":
+            toks.append(("id", "and" if ch == "&" else "or"))
+            i += 1
+        elif expr[i:i + 2] in ("<=", ">=", "==", "!=", "<>"):
+            toks.append(("op", expr[i:i + 2]))
+            i += 2
+        elif ch in "+-*/%^<>=()[]{},?:":
             toks.append(("op", ch))
             i += 1
-    pos = [0]
+        else:
+            raise ValueError("unexpected character %r" % ch)
+    plain = lambda t: t[0] == "id" and t[1].lower() not in _RESERVED
+    out = []
+    for k, t in enumerate(toks):   # implicit multiplication, as exprtk inserts it
+        if k:
+            a = toks[k - 1]
+            if ((a[0] == "num" and (plain(t) or t in (("op", "("), ("op", "["), ("op", "{")))) or
+                    (plain(a) and (t[0] == "num" or plain(t))) or
+                    (plain(a) and a[1].lower() not in _FUNC_NAMES and t in (("op", "("), ("op", "["), ("op", "{"))) or
+                    (a in (("op", ")"), ("op", "]"), ("op", "}")) and (t[0] == "num" or plain(t)))):
+                out.append(("op", "*"))
+        out.append(t)
+    return out
+
+
+def eval_expr(expr, values):
+    """Evaluate a DIM expression over symbol values -> (value, {sym: d/dsym}).
+
+    An independent restatement of the expression language exprtk::parser<double>
+    accepts with default settings (src/grids/DimSet.cu:54-66): precedence
+    (low -> high) ternary ?:, or/nor/xor/xnor, and/nand, comparisons, + -,
+    * / %, unary minus, ^ (right-associative); functions, if(c,a,b) and the
+    variadic min/max/sum/avg/mul/mand/mor; implicit multiplication; names
+    case-insensitive.  Derivatives are exact (forward mode) where exprtk takes
+    a five-point difference."""
+    syms = list(values.keys())
+    low = {s.lower(): s for s in reversed(syms)}
     nd = len(syms)
+    toks = _lex(expr) + [("end", None)]
+    pos = [0]
 
     def peek():
-        return toks[pos[0]] if pos[0] < len(toks) else ("end", None)
+        return toks[pos[0]]
 
     def take():
-        t = peek()
+        t = toks[pos[0]]
         pos[0] += 1
         return t
 
     def const(v):
         return _Dual(v, [0.0] * nd)
 
-    def add(a, b, s=1.0):
-        return _Dual(a.v + s * b.v, [x + s * y for x, y in zip(a.d, b.d)])
-
-    def mul(a, b):
-        return _Dual(a.v * b.v, [a.v * y + b.v * x for x, y in zip(a.d, b.d)])
-
-    def div(a, b):
-        return _Dual(a.v / b.v, [(x * b.v - a.v * y) / (b.v * b.v) for x, y in zip(a.d, b.d)])
-
-    def pw(a, b):
-        v = a.v ** b.v
-        d = []
-        for x, y in zip(a.d, b.d):
-            t = b.v * a.v ** (b.v - 1) * x if x != 0.0 else 0.0
-            if y != 0.0:
-                t += v * math.log(a.v) * y
-            d.append(t)
+    def comb(v, parts):   # value v with partials (coefficient, operand) pairs; zero partials ignored
+        d = [0.0] * nd
+        for c, a in parts:
+            if c != 0.0:
+                d = [x + c * y for x, y in zip(d, a.d)]
         return _Dual(v, d)
 
-    def primary():
+    def close(open_):
+        want = {"(": ")", "[": "]", "{": "}"}[open_]
+        if take() != ("op", want):
+            raise ValueError("expected %r" % want)
+
+    def call(name, args):
+        n = len(args)
+        if name in _FUNCS1:
+            assert n == 1, name
+            f, df = _FUNCS1[name]
+            a = args[0]
+            return comb(f(a.v), [(df(a.v), a)])
+        if name in ("min", "max", "sum", "avg", "mul", "mand", "mor"):
+            acc = args[0]
+            if n == 1 and name in ("mand", "mor"):
+                return const(1.0 if acc.v != 0 else 0.0)
+            for b in args[1:]:
+                if name == "min":
+                    acc = b if b.v < acc.v else acc
+                elif name == "max":
+                    acc = b if acc.v < b.v else acc
+                elif name in ("sum", "avg"):
+                    acc = comb(acc.v + b.v, [(1.0, acc), (1.0, b)])
+                elif name == "mul":
+                    acc = comb(acc.v * b.v, [(b.v, acc), (acc.v, b)])
+                else:
+                    acc = const(_binary("and" if name == "mand" else "or", acc, b)[0])
+            if name == "avg":
+                acc = comb(acc.v / n, [(1.0 / n, acc)])
+            return acc
+        if name in ("pow", "atan2", "mod", "hypot", "logn", "root", "roundn", "equal", "not_equal", "shl", "shr"):
+            assert n == 2, name
+            a, b = args
+            x, y = a.v, b.v
+            if name == "pow":
+                v, da, db = _binary("pow", a, b)
+            elif name == "mod":
+                v, da, db = _binary("mod", a, b)
+            elif name == "atan2":
+                r2 = x * x + y * y
+                v, da, db = math.atan2(x, y), y / r2, -x / r2
+            elif name == "hypot":
+                v = _sqrt(x * x + y * y)
+                v, da, db = v, x / v, y / v
+            elif name == "logn":
+                v = _log(x) / _log(y)
+                v, da, db = v, 1.0 / (x * _log(y)), -v / (y * _log(y))
+            elif name == "root":
+                v, da, db = _root(x, y)
+            elif name == "roundn":
+                p = 10.0 ** max(0, min(16, int(math.floor(y))))
+                v, da, db = (_ceil(x * p - 0.5) if x < 0 else _floor(x * p + 0.5)) / p, 0.0, 0.0
+            elif name in ("equal", "not_equal"):
+                e = _near(x, y)
+                v, da, db = (1.0 if e == (name == "equal") else 0.0), 0.0, 0.0
+            else:
+                s = 2.0 ** int(y)
+                s = s if name == "shl" else 1.0 / s
+                v, da, db = x * s, s, 0.0
+            return comb(v, [(da, a), (db, b)])
+        if name in ("if", "clamp", "iclamp", "inrange"):
+            assert n == 3, name
+            a, b, c = args
+            if name == "if":
+                return b if a.v != 0 else c
+            if name == "clamp":
+                return a if b.v < a.v else (c if b.v > c.v else b)
+            if name == "iclamp":
+                if b.v <= a.v or b.v >= c.v:
+                    return b
+                return a if 2.0 * b.v <= c.v + a.v else c
+            return const(0.0 if (b.v < a.v or b.v > c.v) else 1.0)
+        raise ValueError("unknown function " + name)
+
+    def branch():
         t = take()
+        if t == ("op", "-"):
+            v = expression(11)
+            return _Dual(-v.v, [-x for x in v.d])
+        if t == ("op", "+"):
+            return expression(13)
         if t[0] == "num":
             return const(t[1])
+        if t in (("op", "("), ("op", "["), ("op", "{")):
+            v = expression(0)
+            close(t[1])
+            return v
         if t[0] == "id":
-            name = t[1]
-            if peek() == ("op", "("):
+            name, lname = t[1], t[1].lower()
+            nxt = peek()
+            if nxt in (("op", "("), ("op", "["), ("op", "{")) and lname in _FUNC_NAMES:
                 take()
-                args = [expr_()]
+                args = [expression(0)]
                 while peek() == ("op", ","):
                     take()
-                    args.append(expr_())
-                assert take() == ("op", ")")
-                if name in _FUNCS1:
-                    f, df = _FUNCS1[name]
-                    a = args[0]
-                    g = df(a.v)
-                    return _Dual(f(a.v), [g * x for x in a.d])
-                if name == "pow":
-                    return pw(args[0], args[1])
-                if name in ("min", "max"):
-                    a, b = args
-                    pick = (a.v <= b.v) if name == "min" else (a.v >= b.v)
-                    return a if pick else b
-                raise ValueError("unknown function " + name)
-            if name == "pi":
-                return const(math.pi)
-            if name == "e" and name not in idx:
-                return const(math.e)
-            d = [0.0] * nd
-            d[idx[name]] = 1.0
-            return _Dual(values[name], d)
-        if t == ("op", "("):
-            v = expr_()
-            assert take() == ("op", ")")
-            return v
+                    args.append(expression(0))
+                close(nxt[1])
+                return call(lname, args)
+            sym = name if name in values else low.get(lname)
+            if sym is not None:
+                d = [0.0] * nd
+                d[syms.index(sym)] = 1.0
+                return _Dual(values[sym], d)
+            consts = {"true": 1.0, "false": 0.0, "pi": math.pi, "e": math.e}
+            if lname in consts:
+                return const(consts[lname])
+            raise ValueError("unknown symbol " + name)
         raise ValueError("bad token %r" % (t,))
 
-    def unary():
-        # unary minus binds looser than '^':  -a^b = -(a^b),  a^-b = a^(-b)
-        if peek() == ("op", "-"):
+    def expression(prec):
+        v = branch()
+        while True:
+            t = peek()
+            key = t[1] if t[0] == "op" else (t[1].lower() if t[0] == "id" else None)
+            op = _BIN.get(key) if t[0] in ("op", "id") else None
+            if op is None or op[0] < prec:
+                break
             take()
-            v = unary()
-            return _Dual(-v.v, [-x for x in v.d])
-        if peek() == ("op", "+"):
+            r = expression(op[1])
+            val, da, db = _binary(op[2], v, r)
+            v = comb(val, [(da, v), (db, r)])
+        if prec == 0 and peek() == ("op", "?"):
             take()
-            return unary()
-        return power()
-
-    def power():
-        b = primary()
-        if peek() == ("op", "^"):
-            take()
-            e = unary()
-            return pw(b, e)
-        return b
-
-    def term():
-        v = unary()
-        while peek() in (("op", "*"), ("op", "/")):
-            op = take()[1]
-            r = unary()
-            v = mul(v, r) if op == "*" else div(v, r)
+            a = expression(0)
+            if take() != ("op", ":"):
+                raise ValueError("expected ':'")
+            b = expression(0)
+            v = a if v.v != 0 else b
         return v
 
-    def expr_():
-        v = term()
-        while peek() in (("op", "+"), ("op", "-")):
-            op = take()[1]
-            r = term()
-            v = add(v, r, 1.0 if op == "+" else -1.0)
-        return v
-
-    res = expr_()
-    assert peek()[0] == "end", "trailing tokens in expression"
+    res = expression(0)
+    if peek()[0] != "end":
+        raise ValueError("trailing tokens in expression")
     return res.v, dict(zip(syms, res.d))
