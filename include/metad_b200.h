@@ -197,6 +197,15 @@ mtd_status mtd_get_neighbors(mtd_ctx *ctx, const char *cal, int n, int *counts, 
  * every step (src/cvs/CVs_Steinhardt.cu:135-147, src/core/neigh_hub.cu:191-222). */
 mtd_status mtd_neighbor_stats(mtd_ctx *ctx, int64_t *rebuilds, int *skin_active);
 
+/* Skin lists: the rebuild (cell list and candidate lists) runs as one
+ * cooperative launch whose phases are separated by grid barriers.  Every
+ * barrier wait polls at most `limit` times (0: the default, 4,194,304) before
+ * it gives up; a rebuild that gave up makes that step return MTD_ERR_TIMEOUT
+ * (no hill deposited, no bias force applied) and the next step rebuild from
+ * scratch.  stall = 1 (diagnostics) makes the next rebuild's waits run out.
+ * Extension (the reference has no device-side rebuild). */
+mtd_status mtd_neighbor_set_wait(mtd_ctx *ctx, int limit, int stall);
+
 /* Replays a HILLS file into the grid (rows `step cv[D] height sigma`).
  * Replaces GH_t0_uniformGrid::init_hills (src/grids/GH_t0_uniformGrid.cu:101-192). */
 mtd_status mtd_hills_replay(mtd_ctx *ctx, const char *path);

@@ -293,7 +293,8 @@ __device__ void phase_deposit(const BiasPlan &P, const double *s, double w, cons
 // leave no hill and no bias force behind.
 __device__ __forceinline__ bool status_failed(const DevStatus *st) {
     return st && (*(volatile const unsigned *)&st->overflow != 0u || *(volatile const unsigned *)&st->bad_pos != 0u ||
-                  *(volatile const unsigned *)&st->cand_overflow != 0u);
+                  *(volatile const unsigned *)&st->cand_overflow != 0u ||
+                  *(volatile const unsigned *)&st->timeout != 0u);
 }
 __device__ __forceinline__ bool step_failed(const BiasPlan &P) { return status_failed(P.status); }
 

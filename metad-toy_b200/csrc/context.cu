@@ -258,6 +258,8 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
             if (!c->d_skin) {
                 MTD_CU(dalloc(&c->d_skin, sizeof(SkinState)), "skin state");
                 MTD_CU(cudaMemset(c->d_skin, 0, sizeof(SkinState)), "skin state");
+                MTD_CU(dalloc(&c->d_rbar, sizeof(GridBar)), "rebuild barrier");
+                MTD_CU(cudaMemset(c->d_rbar, 0, sizeof(GridBar)), "rebuild barrier");
             }
         }
         c->skin_valid = false;
@@ -780,8 +782,14 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
             s.skin = c->d_skin;
             s.xref = c->xref;
             launch_refresh(g, s, c->cfg.neigh_every, 0.5 * c->cfg.neigh_skin, same ? 0 : 1, c->st);
-            c->launches += 1 + launch_build_cells(g, s, c->st);
-            for (Env &e : c->envs) {
+            c->launches += 1;
+            // the gated rebuild: cell list and the first environment's
+            // candidates as one cooperative launch where it can run, else
+            // the separate gated kernels
+            const bool one = c->d_rbar && rebuild_blocks() > 0;
+            if (!one) c->launches += launch_build_cells(g, s, c->st);
+            for (size_t ei = 0; ei < c->envs.size(); ++ei) {
+                Env &e = c->envs[ei];
                 NeighSpec ns = neigh_spec(e);
                 ns.variant = c->tune_nbr;
                 ns.kind = NK_CAND;
@@ -792,7 +800,14 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
                 cd.list = e.cand;
                 cd.count = e.ccount;
                 cd.M = e.Mc;
-                launch_neighbors(g, s, ns, cd, c->d_status, c->st);
+                if (one && ei == 0) {
+                    MTD_CU(launch_rebuild(g, s, ns, cd, c->d_status, c->d_rbar, c->rebuild_limit, c->rebuild_stall,
+                                          c->st),
+                           "skin-list rebuild");
+                    c->rebuild_stall = 0;
+                } else {
+                    launch_neighbors(g, s, ns, cd, c->d_status, c->st);
+                }
                 c->launches += 1;
             }
             // an environment that only one STEINH L unit reads is filtered
@@ -947,6 +962,15 @@ mtd_status collect(mtd_ctx *c) {
     }
     if (c->h_status->bad_pos)
         return fail(c, MTD_ERR_NAN, "non-finite atom position (NaN or Inf): the step deposited nothing and applied no bias force");
+    if (c->h_status->timeout) {
+        // a grid-barrier wait of the one-launch skin-list rebuild ran out: the
+        // device marked the skin state invalid (the next step rebuilds from
+        // scratch); the barrier words are reset for the next rebuild
+        if (c->d_rbar) MTD_CU(cudaMemsetAsync(c->d_rbar, 0, sizeof(GridBar), c->st), "rebuild barrier");
+        return fail(c, MTD_ERR_TIMEOUT,
+                    "neighbour-list rebuild: a grid-barrier wait ran out; the step deposited nothing and applied no "
+                    "bias force, the next step rebuilds the lists");
+    }
     if (c->h_status->nan_force) return fail(c, MTD_ERR_NAN, "STEIN_QL CV error: force is infinity, check your system or cv_value.");
     return MTD_OK;
 }
@@ -1176,6 +1200,7 @@ void mtd_destroy(mtd_ctx *c) {
     }
     dfree(c->xref);
     dfree(c->d_skin);
+    dfree(c->d_rbar);
     for (Unit &u : c->units) {
         void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S, &u.w};
         for (void **a : arrs) dfree(*a);

@@ -221,6 +221,9 @@ struct mtd_ctx {
     int fix_groupbit = 1;
     // skin lists (NEIGH_SKIN > 0): candidate lists and the sorted order kept across steps
     SkinState *d_skin = nullptr;
+    GridBar *d_rbar = nullptr;            // grid barrier of the one-launch skin-list rebuild
+    int rebuild_limit = 1 << 22;          // its polls per wait (mtd_neighbor_set_wait)
+    int rebuild_stall = 0;                // diagnostics: the next rebuild's waits run out
     double *xref = nullptr;              // sorted raw coordinates at the last rebuild
     bool skin_valid = false;             // the kept sorted order and candidates match n and the grid
     int skin_n = -1;

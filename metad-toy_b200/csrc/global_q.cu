@@ -137,11 +137,14 @@ __global__ void __launch_bounds__(kBlock) k_global_force(GlobalDev<T> d, const d
         }
         const int i = myid;
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;
-        f_dst[3 * i] = f_src[3 * i] + fx;
-        f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
-        f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        const bool own = (unsigned)i < (unsigned)d.n;   // a sorted order left by a rebuild that gave up is not trusted
+        if (own) {
+            f_dst[3 * i] = f_src[3 * i] + fx;
+            f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
+            f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        }
         if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&status->nan_force, 1u);
-        if (vpart) {
+        if (vpart && own) {
             double ux = xk[0], uy = xk[1], uz = xk[2];
             if (s.image) {
                 int ix, iy, iz;

@@ -75,7 +75,7 @@ struct SkinState {
     unsigned int gate;            // 1: this step rebuilds the cell list and candidate lists
     unsigned int age;             // steps the current candidate lists have served
     unsigned int builds;          // rebuilds so far
-    unsigned int pad;
+    unsigned int invalid;         // a rebuild gave up (grid-barrier wait): the next step rebuilds from scratch
 };
 
 struct SysDev {
@@ -184,6 +184,14 @@ void launch_select_cap(const CellGrid &g, const SysDev &s, const NeighSpec &ns, 
 void launch_refresh(const CellGrid &g, const SysDev &s, int every, double half_skin, int force, cudaStream_t st);
 void launch_filter(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev nd, NeighDev cand,
                    DevStatus *status, SkinState *reset, cudaStream_t st);
+struct GridBar;
+// Skin lists: the gated rebuild (cell list and candidates of one environment,
+// fast path) as one cooperative launch with grid barriers (limit: polls per
+// wait; stall: diagnostics, one block skips the first barrier).  Co-resident
+// blocks of that launch (0: not available, use the separate gated kernels).
+int rebuild_blocks();
+cudaError_t launch_rebuild(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev cd, DevStatus *status,
+                           GridBar *bar, int limit, int stall, cudaStream_t st);
 
 // ------------------------------------------------------------------ STEINH L
 template <typename T> struct LocalDev {

@@ -130,27 +130,64 @@ __device__ __forceinline__ void local_q_body(const LocalDev<T> &d, int bid) {
         r->gate = 0;
     }
     if (k >= d.n) return;
-    int c;
-    if constexpr (FILTER)
-        c = min(filter_atom<STEP ? NK_STEP : NK_SWITCH>(d.fgf, d.fgd, d.fgd.xs, d.fspec, d.cand, d.nb, d.npad, k,
-                                                        d.status),
-                d.nb.M);
-    else
-        c = min(d.nb.count[k], d.nb.M);
     const auto a = d.geo.load(k);
     T acc[S::SQ];
 #pragma unroll
     for (int t = 0; t < S::SQ; ++t) acc[t] = T(0);
     T nf = T(0);
-    for (int t = 0; t < c; ++t) {
-        T ux, uy, uz, rinv, sg, dsg;
-        // a list this kernel wrote is read back through the coherent path
-        const int j = FILTER ? (d.nb.list[(size_t)t * d.npad + k] & ((1 << kFlagBit) - 1))
-                             : nb_index(d.nb, d.npad, t, k);
-        pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
-        nf += sg;
-        ylm_accum<LA, T>(ux, uy, uz, sg, acc);
-        if constexpr (LB > 0) ylm_accum<LB, T>(ux, uy, uz, sg, acc + S::SA);
+    int c = 0;
+    if constexpr (FILTER) {
+        // one loop: each candidate is tested (the decisions of filter_atom)
+        // and, when kept, written to the exact list and summed at once, so
+        // the list is not read back; the sum runs in list order
+        constexpr int KIND = STEP ? NK_STEP : NK_SWITCH;
+        const float4 af = __ldg(d.fgf.pf + k);
+        const int nc = min(__ldg(d.cand.count + k), d.cand.M);
+        int jn = nc > 0 ? __ldg(d.cand.list + k) : 0;
+        float4 bn = nc > 0 ? __ldg(d.fgf.pf + jn) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int t = 0; t < nc; ++t) {
+            const int j = jn;
+            const float4 b = bn;
+            if (t + 1 < nc) {   // the next candidate's index and position in flight
+                jn = __ldg(d.cand.list + (size_t)(t + 1) * d.npad + k);
+                bn = __ldg(d.fgf.pf + jn);
+            }
+            float fx, fy, fz;
+            disp_f(d.fgf, af, b, fx, fy, fz);
+            if (!decide<KIND>(d.fgd, d.fspec, d.fgd.xs, k, j, fx * fx + fy * fy + fz * fz)) continue;
+            if (c < d.nb.M) {
+                d.nb.list[(size_t)c * d.npad + k] = j;
+                T dx, dy, dz;
+                if constexpr (sizeof(T) == sizeof(float)) {   // the same FP32 displacement pair_geom forms
+                    dx = fx;
+                    dy = fy;
+                    dz = fz;
+                } else {
+                    d.geo.disp(a, d.geo.load(j), dx, dy, dz);
+                }
+                const T r2 = dx * dx + dy * dy + dz * dz;
+                const T rinv = t_rsqrt<T>(r2);
+                T sg = T(1);
+                if (!STEP) sg = sw_f<T>(d.sw_r, r2 * rinv);
+                nf += sg;
+                ylm_accum<LA, T>(dx * rinv, dy * rinv, dz * rinv, sg, acc);
+                if constexpr (LB > 0) ylm_accum<LB, T>(dx * rinv, dy * rinv, dz * rinv, sg, acc + S::SA);
+            }
+            ++c;
+        }
+        d.nb.count[k] = c;
+        if (c > d.nb.M) atomicMax(&d.status->overflow, (unsigned)c);
+        c = min(c, d.nb.M);
+    } else {
+        c = min(d.nb.count[k], d.nb.M);
+        for (int t = 0; t < c; ++t) {
+            T ux, uy, uz, rinv, sg, dsg;
+            const int j = nb_index(d.nb, d.npad, t, k);
+            pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
+            nf += sg;
+            ylm_accum<LA, T>(ux, uy, uz, sg, acc);
+            if constexpr (LB > 0) ylm_accum<LB, T>(ux, uy, uz, sg, acc + S::SA);
+        }
     }
     const bool active = c > 0 && nf >= T(1e-12);
     const T inv = active ? T(1) / nf : T(0);
@@ -380,11 +417,13 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
         }
         const int i = d.perm[k];
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;   // delta f = -dV/dx
-        f_dst[3 * i] = f_src[3 * i] + fx;
-        f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
-        f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        if ((unsigned)i < (unsigned)d.n) {   // a sorted order left by a rebuild that gave up is not trusted
+            f_dst[3 * i] = f_src[3 * i] + fx;
+            f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
+            f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        }
         if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&status->nan_force, 1u);
-        if (vpart) {
+        if (vpart && (unsigned)i < (unsigned)d.n) {
             double ux_ = s.xs[3 * k], uy_ = s.xs[3 * k + 1], uz_ = s.xs[3 * k + 2];
             if (s.image) {
                 int ix, iy, iz;

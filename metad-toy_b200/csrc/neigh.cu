@@ -22,7 +22,7 @@
 // of the reference, which reads LAMMPS's skin lists and filters them by
 // r < cutoff_r every step (src/cvs/CVs_Steinhardt.cu:135-147,
 // src/core/neigh_hub.cu:191-222).
-#include "neigh_body.cuh"
+#include "persist.cuh"
 
 #include <math_constants.h>
 
@@ -377,11 +377,13 @@ __global__ void __launch_bounds__(kBlock) k_select_cap(CellGrid g, SysDev s, Nei
 // lists are valid), refreshes the group mask, and opens the gate when a
 // rebuild is due: an atom moved more than skin / 2 (minimum image) since the
 // build, a non-finite position, NEIGH_EVERY reached, or force (the sorted
-// order is not valid yet: nothing else is read).
+// order is not valid yet, or the last rebuild gave up: nothing else is read).
 __global__ void k_refresh(CellGrid g, SysDev s, int every, double half2, int force) {
     pdl_entry();
     SkinState *sk = s.skin;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    // a rebuild that gave up leaves the sorted order and lists unusable: rebuild as if forced
+    if (*(volatile const unsigned *)&sk->invalid) force = 1;
     if (k == 0 && (force || (every > 0 && sk->age >= (unsigned)every))) atomicOr(&sk->gate, 1u);
     if (force || k >= s.n) return;
     const int i = s.perm[k];
@@ -435,7 +437,78 @@ __global__ void __launch_bounds__(kBlock) k_filter(CellGrid g, SysDev s, NeighSp
     filter_atom<KIND>(geo_f(g, s.pf), geo_d(g, s.xs), s.xs, ns, cand, nd, s.npad, k, status);
 }
 
+// Skin lists, the whole rebuild as one cooperative launch: while the gate is
+// closed every block returns at once (one launch instead of six that each
+// return at once); when it is open the phases run with grid barriers between
+// them: cell counts zeroed, bin, chunk scan, chunk offsets, scatter, place,
+// candidates.  The same per-thread bodies and 256-atom blocks as the separate
+// kernels, so the sorted order and the candidate lists are the same.  A
+// barrier wait that runs out marks the step (status->timeout, no deposit, no
+// bias force) and the skin state invalid (the next step rebuilds from scratch).
+__global__ void __launch_bounds__(kPersistBlock) k_rebuild(CellGrid g, SysDev s, NeighSpec ns, NeighDev cd,
+                                                           DevStatus *status, GridBar *bar, int limit, int stall) {
+    pdl_entry();
+    if (gate_closed(s.skin)) return;
+    const int G = gridDim.x;
+    const int nb = (s.n + kPersistBlock - 1) / kPersistBlock;
+    const int nchunk = (g.ncell + kPersistBlock - 1) / kPersistBlock;
+    int *bsum = s.start + g.ncell + 1;
+    auto fail = [&]() {
+        if (threadIdx.x == 0) {
+            atomicOr(&status->timeout, 1u);
+            atomicExch(&s.skin->invalid, 1u);
+        }
+    };
+    // counts are zero after every complete build; a build that gave up may
+    // have left some, so the rebuild starts from zero
+    for (int c = blockIdx.x * kPersistBlock + threadIdx.x; c < g.ncell; c += G * kPersistBlock) s.count[c] = 0;
+    if (!grid_barrier(bar, limit, stall && blockIdx.x == 0)) return fail();
+    for (int v = blockIdx.x; v < nb; v += G) bin_body(g, s, v);
+    if (!grid_barrier(bar, limit, false)) return fail();
+    for (int v = blockIdx.x; v < nchunk; v += G) scan_chunk(s, g.ncell, v, bsum);
+    if (!grid_barrier(bar, limit, false)) return fail();
+    for (int v = blockIdx.x; v < nchunk; v += G) scan_offset(s, g.ncell, v, nchunk, bsum);
+    if (!grid_barrier(bar, limit, false)) return fail();
+    for (int v = blockIdx.x; v < nb; v += G) scatter_body(s, g.ncell, v, nb);
+    if (!grid_barrier(bar, limit, false)) return fail();
+    for (int v = blockIdx.x; v < nb; v += G) place_body(g, s, v);
+    if (!grid_barrier(bar, limit, false)) return fail();
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.skin->invalid = 0u;
+    for (int v = blockIdx.x; v < nb; v += G) neighbors_fast_body<NK_CAND>(g, s, ns, cd, status, v);
+}
+
 }  // namespace
+
+int rebuild_blocks() {
+    static int blocks[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (blocks[dev] == 0) {
+        int sms = 0, per = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rebuild, kPersistBlock, 0) != cudaSuccess) return 0;
+        blocks[dev] = per * sms > 0 ? per * sms : -1;
+    }
+    return blocks[dev] > 0 ? blocks[dev] : 0;
+}
+
+cudaError_t launch_rebuild(const CellGrid &g, const SysDev &s, const NeighSpec &ns, NeighDev cd, DevStatus *status,
+                           GridBar *bar, int limit, int stall, cudaStream_t st) {
+    const int blocks = rebuild_blocks();
+    if (blocks < 1) return cudaErrorInvalidConfiguration;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kPersistBlock);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_rebuild, g, s, ns, cd, status, bar, limit, stall);
+    prof_mark("skin_rebuild", st);
+    return e;
+}
 
 int launch_build_cells(const CellGrid &g, SysDev &s, cudaStream_t st) {
     const int nb = (s.n + kBlock - 1) / kBlock;

@@ -105,6 +105,13 @@ mtd_status mtd_neighbor_stats(mtd_ctx *c, int64_t *rebuilds, int *skin_active) {
     return MTD_OK;
 }
 
+mtd_status mtd_neighbor_set_wait(mtd_ctx *c, int limit, int stall) {
+    if (!c || limit < 0) return MTD_ERR_INVALID_ARG;
+    c->rebuild_limit = limit > 0 ? limit : (1 << 22);
+    c->rebuild_stall = stall ? 1 : 0;
+    return MTD_OK;
+}
+
 mtd_status mtd_get_neighbors(mtd_ctx *c, const char *cal, int n, int *counts, int *idx, int max_per_atom) {
     if (!c || !cal || !counts || n < 0 || (idx && max_per_atom < 0)) return MTD_ERR_INVALID_ARG;
     if (n != c->n) return fail(c, MTD_ERR_INVALID_ARG, "atom count differs from the last step");

@@ -46,7 +46,8 @@ template <typename T> __global__ void k_chem_weights(DebyeDev<T> d) {
     pdl_entry();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
-    const int t = d.types[d.perm[k]];
+    const int i = d.perm[k];
+    const int t = (unsigned)i < (unsigned)d.n ? d.types[i] : 0;
     d.w[k] = (T)(t >= 0 && t < d.ntab ? d.wtab[t] : 0.0);
 }
 
@@ -123,11 +124,13 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
         }
         const int i = d.perm[k];
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;
-        f_dst[3 * i] = f_src[3 * i] + fx;
-        f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
-        f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        if ((unsigned)i < (unsigned)d.n) {   // a sorted order left by a rebuild that gave up is not trusted
+            f_dst[3 * i] = f_src[3 * i] + fx;
+            f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
+            f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;
+        }
         if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&status->nan_force, 1u);
-        if (vpart) {
+        if (vpart && (unsigned)i < (unsigned)d.n) {
             double ux = s.xs[3 * k], uy = s.xs[3 * k + 1], uz = s.xs[3 * k + 2];
             if (s.image) {
                 int ix, iy, iz;

@@ -13,17 +13,17 @@
 // per-walker kernels' bit for bit.  The step number and the outputs go
 // through pinned host memory, so the step is this one launch.
 //
-// Grid barrier: a counter and a generation word; every wait polls at most
-// `limit` times, after which the block records the failure and leaves the
-// kernel, and every other block leaves at its next barrier (the host reports
-// MTD_ERR_TIMEOUT and resets the barrier).  The cooperative launch makes all
-// blocks co-resident, so the waits end in normal operation.
+// Grid barrier (persist.cuh): every wait polls at most `limit` times, after
+// which the block records the failure and leaves the kernel, and every other
+// block leaves at its next barrier (the host reports MTD_ERR_TIMEOUT and
+// resets the barrier).  The cooperative launch makes all blocks co-resident,
+// so the waits end in normal operation.
 //
 // The deposit rule is GH_t0_uniformGrid::add_hill
 // (src/grids/GH_t0_uniformGrid.cu:195-208) applied to each walker's hill in
 // turn, with heights from the grid as it stood at the start of the step.
 #include "local_body.cuh"
-#include "neigh_body.cuh"
+#include "persist.cuh"
 
 namespace mtd {
 
@@ -35,94 +35,7 @@ __device__ void walk_phase_coef(const BiasPlan *const *plans, int nwalk, int w, 
 
 namespace {
 
-constexpr int kWalkBlock = 256;
-
-// Exclusive scan of one value per thread over a block of kWalkBlock threads.
-__device__ __forceinline__ int scan256(int v, int &total) {
-    __shared__ int warp_tot[kWalkBlock / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_tot[warp] = x;
-    __syncthreads();
-    int before = 0;
-    total = 0;
-#pragma unroll
-    for (int w = 0; w < kWalkBlock / 32; ++w) {
-        const int t = warp_tot[w];
-        if (w < warp) before += t;
-        total += t;
-    }
-    __syncthreads();
-    return before + x - v;
-}
-
-// Chunk c of one walker's cells: exclusive scan of the counts into start,
-// the chunk total into bsum[c].
-__device__ __forceinline__ void scan_chunk(const SysDev &s, int ncell, int c, int *bsum) {
-    const int i = c * kWalkBlock + threadIdx.x;
-    int total;
-    const int e = scan256(i < ncell ? s.count[i] : 0, total);
-    if (i < ncell) s.start[i] = e;
-    if (threadIdx.x == 0) bsum[c] = total;
-}
-
-// The totals of the chunks before c added to chunk c; the last chunk writes
-// start[ncell].
-__device__ __forceinline__ void scan_offset(const SysDev &s, int ncell, int c, int nchunk, const int *bsum) {
-    __shared__ int red[kWalkBlock / 32];
-    int v = 0;
-    for (int t = threadIdx.x; t < c; t += kWalkBlock) v += bsum[t];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    int off = 0;
-#pragma unroll
-    for (int w = 0; w < kWalkBlock / 32; ++w) off += red[w];
-    __syncthreads();
-    const int i = c * kWalkBlock + threadIdx.x;
-    if (i < ncell) s.start[i] += off;
-    if (c == nchunk - 1 && threadIdx.x == 0) s.start[ncell] = off + bsum[c];
-}
-
-// Bounded grid barrier; false when this block or another gave up a wait.
-// stall (diagnostics): this block does not arrive, so the others' waits run out.
-__device__ bool grid_barrier(GridBar *b, int limit, bool stall) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int good = 1;
-        volatile unsigned *gen = &b->gen;
-        const unsigned g = *gen;
-        __threadfence();
-        if (stall) {
-            good = 0;
-        } else if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
-        } else {
-            int it = 0;
-            while (*gen == g) {
-                if (++it > limit) {
-                    atomicExch(&b->err, 1u);
-                    good = 0;
-                    break;
-                }
-                __nanosleep(100);
-            }
-        }
-        __threadfence();
-        ok = good && *(volatile unsigned *)&b->err == 0u;
-    }
-    __syncthreads();
-    return ok != 0;
-}
+constexpr int kWalkBlock = kPersistBlock;
 
 // Virtual block v of a phase -> (walker, block within the walker) from the
 // prefix sums pre[0..nwalk].

@@ -188,3 +188,42 @@ def test_thin_box_falls_back_to_per_step_lists():
     o4 = H.oracle_local(x, L, 4)
     assert H.rel(out[0][0][0], o4["cv"]) < 1e-9
     m.close()
+
+
+def test_rebuild_barrier_timeout_reports_and_recovers():
+    """The skin-list rebuild is one cooperative launch with bounded grid
+    barriers.  A block that never arrives (mtd_neighbor_set_wait's stall
+    switch) makes the others give up after the wait limit: the step returns
+    MTD_ERR_TIMEOUT, deposits no hill, applies no bias force, and the next
+    step rebuilds from scratch and equals a run without the stall bit for bit
+    (NEIGH_EVERY 1: both runs rebuild every step)."""
+    xs, L = _trajectory(4)
+    args = H.fix_args_local(pace=2) + ["NEIGH_SKIN", 0.6, "NEIGH_EVERY", 1]
+    ref = mtd.Metad(args, precision="fp64")
+    ref.set_box([0, 0, 0], L)
+    f_ref = []
+    for s in range(4):
+        f = np.zeros_like(xs[s])
+        ref.post_force(s, xs[s], f)
+        f_ref.append((ref.cv.copy(), ref.compute_scalar(), f))
+    grid_ref = ref.grid(200 * 200)
+    ref.close()
+    m = mtd.Metad(args, precision="fp64")
+    m.set_box([0, 0, 0], L)
+    for s in range(2):
+        m.post_force(s, xs[s], np.zeros_like(xs[s]))
+    grid1 = m.grid(200 * 200)
+    m.neighbor_set_wait(limit=2000, stall=True)
+    f = np.zeros_like(xs[2])
+    with pytest.raises(mtd.MetadError, match="TIMEOUT"):
+        m.post_force(2, xs[2], f)
+    assert float(np.abs(f).max()) == 0.0
+    assert np.array_equal(m.grid(200 * 200), grid1)
+    m.neighbor_set_wait(limit=0, stall=False)
+    for s in (2, 3):
+        f = np.zeros_like(xs[s])
+        m.post_force(s, xs[s], f)
+        cv, b, fr = f_ref[s]
+        assert np.array_equal(m.cv, cv) and m.compute_scalar() == b and np.array_equal(f, fr)
+    assert np.array_equal(m.grid(200 * 200), grid_ref)
+    m.close()

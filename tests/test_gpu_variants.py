@@ -130,17 +130,19 @@ def test_steinh_l_switching_functions(case, precision):
     (rk, rkw), (ck, ckw), mode = L_CASES[case]
     swr, swc = _sw_oracle(rk, **rkw), _sw_oracle(ck, **ckw)
     rl = O.sw_invert_for_eps(swr, 1e-6)
-    scale = float(n) if mode == "NSOLID" else 1.0
+    o4 = O.steinh_l(4, x, L, rl, swr, 1e-6, swc, mode)
+    o6 = O.steinh_l(6, x, L, rl, swr, 1e-6, swc, mode)
+    # the DIMs scale both CVs into the middle of the grid, where V and dV/ds
+    # are of the hill's size (outside it they are a hill's far tail)
+    scale = 2.5 * max(abs(o4["cv"]), abs(o6["cv"]))
     args = (["GAUSSIAN", 0.01, 0.005, 9.0, "PACE", 10, "TEMP", 300.0] + _sw_args("SWR", rk, **rkw) +
             _sw_args("SWC", ck, **ckw))
     for l in (4, 6):
         args += ["CAL", "NAME", "Q%d" % l, "STEINH", "L", l, "all", "SW_FUNC_r", "SWR"]
     args += ["SYMBOL", "v1", "Q4.%s.SWC" % mode, "SYMBOL", "v2", "Q6.%s.SWC" % mode, "CV_dim", 2,
-             "DIM", 1, 0.0, 1.0, 100, "v1/%r" % (2 * scale), "DIM", 2, 0.0, 1.0, 100, "v2/%r" % (2 * scale),
+             "DIM", 1, 0.0, 1.0, 100, "v1/%r" % scale, "DIM", 2, 0.0, 1.0, 100, "v2/%r" % scale,
              "WT", 1]
-    o4 = O.steinh_l(4, x, L, rl, swr, 1e-6, swc, mode)
-    o6 = O.steinh_l(6, x, L, rl, swr, 1e-6, swc, mode)
-    c = 1.0 / (2 * scale)
+    c = 1.0 / scale
     m = _step_and_compare(args, x, L, precision, [o4["cv"], o6["cv"]], [o4["grad"], o6["grad"]],
                           [[0.0, 1.0, 100], [0.0, 1.0, 100]], True, biasf=9.0,
                           expr_chain=lambda v: (v * c, np.diag([c, c])))

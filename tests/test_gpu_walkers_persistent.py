@@ -31,7 +31,7 @@ def _walker_systems(count=3, seed=20):
     return out
 
 
-def _run(args, syss, steps, persistent, precision="fp64", graph=False, hills_path="", moving=False):
+def _run(args, syss, steps, persistent, precision="fp64", graph=False, hills_path="", moving=False, bins=200 * 200):
     """Steps every walker through `steps`; returns per step the CVs, bias and
     forces of each walker, the grid at the end, whether the last step ran as
     one launch and the launch count of the last step."""
@@ -55,7 +55,7 @@ def _run(args, syss, steps, persistent, precision="fp64", graph=False, hills_pat
         W.step_device(step, [x.shape[0] for x, _ in syss], [v.data_ptr() for v in dx], [v.data_ptr() for v in df])
         W.sync()
         out.append([(W.cv(k, 2), W.bias(k), df[k].cpu().numpy()) for k in range(len(syss))])
-    grid = W.grid(200 * 200)
+    grid = W.grid(bins)
     info = (W.persistent_active, W.launch_count())
     W.close()
     return out, grid, info
@@ -92,9 +92,10 @@ def test_persistent_step_single_orders_and_many_walkers():
             "CAL", "NAME", "Q6", "STEINH", "L", 6, "all", "cutoff_r", 3.9, "cutoff_Natoms", 18, "SW_FUNC_r", "SWR",
             "SYMBOL", "v1", "Q6.MEAN_SOLID", "CV_dim", 1, "DIM", 1, 0, 1, 200, "v1", "WT", 1]
     steps = list(range(4))
-    ref = _run(args, syss, steps, persistent=False, moving=True)
-    got = _run(args, syss, steps, persistent=True, moving=True)
+    ref = _run(args, syss, steps, persistent=False, moving=True, bins=200)
+    got = _run(args, syss, steps, persistent=True, moving=True, bins=200)
     assert got[2] == (True, 1)
+    assert np.array_equal(ref[1], got[1])
     for sa, sb in zip(ref[0], got[0]):
         for (cv1, b1, f1), (cv2, b2, f2) in zip(sa, sb):
             assert np.array_equal(cv1[:1], cv2[:1]) and b1 == b2 and np.array_equal(f1, f2)
