@@ -94,6 +94,40 @@ mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask
         }
     }
     c->tune_l = bl;
+    // S(k) k-tiles of the mixed-precision passes (value pass: register tile;
+    // force pass: shared-memory table chunk), those whose chunk fits
+    int dev = 0, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    for (Unit &u : c->units) {
+        if (u.kind != CAL_STRU_FACTOR_K || c->fp64 || !u.sk_tab) continue;
+        const SkDev d = sk_dev(c, u, d_x, d_mask);
+        best = 1e30f;
+        int bv = c->tune_skq;
+        for (int qv : {4, 8, 16}) {
+            if (sk_smem_values(d, qv) > (size_t)smem_max) continue;
+            c->tune_skq = qv;
+            const float t = timed([&] { run_values<float>(c, g, d_x, d_mask); });
+            if (t < best) {
+                best = t;
+                bv = qv;
+            }
+        }
+        c->tune_skq = bv;
+        best = 1e30f;
+        int bf = c->tune_skqf;
+        for (int qf : {8, 16, 32}) {
+            if (sk_smem_force(d, qf) > (size_t)smem_max) continue;
+            c->tune_skqf = qf;
+            const float t = timed([&] { run_forces<float>(c, sd, g, d_x, d_mask, c->d_fin, c->d_fout, false); });
+            if (t < best) {
+                best = t;
+                bf = qf;
+            }
+        }
+        c->tune_skqf = bf;
+        break;   // one set of tiles per context
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
@@ -122,6 +156,21 @@ mtd_status mtd_autotune(mtd_ctx *c, int n, const double *d_x, const int *d_mask,
     const mtd_status s = mtd_sync(c);
     if (s != MTD_OK) return s;
     return autotune_idle(c, n, d_x, d_mask, reps, choice);
+}
+
+mtd_status mtd_sk_tiles(mtd_ctx *c, int *q_values, int *q_force) {
+    if (!c) return MTD_ERR_INVALID_ARG;
+    if (q_values) *q_values = c->tune_skq;
+    if (q_force) *q_force = c->tune_skqf;
+    return MTD_OK;
+}
+
+mtd_status mtd_set_sk_tiles(mtd_ctx *c, int q_values, int q_force) {
+    if (!c || (q_values != 4 && q_values != 8 && q_values != 16) || (q_force != 8 && q_force != 16 && q_force != 32))
+        return MTD_ERR_INVALID_ARG;
+    c->tune_skq = q_values;
+    c->tune_skqf = q_force;
+    return MTD_OK;
 }
 
 mtd_status mtd_set_tuning(mtd_ctx *c, int neighbor_shape, int q_block, int lambda_block) {

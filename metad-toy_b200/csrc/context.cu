@@ -604,6 +604,8 @@ SkDev sk_dev(mtd_ctx *c, Unit &u, const double *x, const int *mask) {
     d.nown = owned(c);
     d.tab = u.sk_tab;
     d.tstride = u.sk_tstride;
+    d.qv = c->tune_skq;
+    d.qf = c->tune_skqf;
     for (int a = 0; a < 3; ++a) {
         d.nct[a] = u.sk_nct[a];
         d.to[a] = u.sk_to[a];

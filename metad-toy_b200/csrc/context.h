@@ -194,6 +194,7 @@ struct mtd_ctx {
     // kernel shapes chosen by mtd_autotune (every choice gives bitwise-identical results)
     int tune_nbr = 0;                    // neighbour search: 0 fast/256, 1 fast/128, 2 flat/128
     int tune_q = 0, tune_l = 0;          // threads per block of the q and lambda passes (0: 256)
+    int tune_skq = 8, tune_skqf = 32;    // S(k) k-tiles of the mixed-precision value and force passes
     // per-atom dCV/dx export (compute metad/atom): last step's inputs, cached result
     const double *last_x = nullptr;
     const int *last_mask = nullptr;
@@ -258,6 +259,7 @@ bool skin_grid(const mtd_ctx *c, CellGrid &g);
 // neighbours, skin candidate lists `cand_need` (which forces a rebuild).
 mtd_status grow_lists(mtd_ctx *c, unsigned need, unsigned cand_need);
 NeighSpec neigh_spec(const Env &e);
+SkDev sk_dev(mtd_ctx *c, Unit &u, const double *x, const int *mask);
 int estimate_M(const mtd_ctx *c, double rc, int n);
 mtd_status alloc_env(mtd_ctx *c, Env &e, int npad);
 mtd_status alloc_cand(mtd_ctx *c, Env &e, int npad);

@@ -281,12 +281,16 @@ struct SkDev {
     int tstride;
     int nct[3];
     double to[3], th[3], tih[3];
+    int qv, qf;                 // k-tiles of the mixed-precision value and force passes (4 / 8 / 16, 8 / 16 / 32)
 };
 constexpr int kSkTabCells = 320;    // phase-table cells per dimension at most (bounds the shared-memory chunks)
 void launch_sk_values(const SkDev &d, cudaStream_t st);
 void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                       double *vpart, cudaStream_t st);
 int sk_blocks(int n);
+// Dynamic shared memory of the mixed-precision passes with k-tile qv / qf.
+size_t sk_smem_values(const SkDev &d, int qv);
+size_t sk_smem_force(const SkDev &d, int qf);
 
 // ------------------------------------------------------------------ bias grid
 enum SymKind {

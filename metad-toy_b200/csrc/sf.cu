@@ -151,11 +151,13 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
 }
 
 // ------------------------------------------------------------------ S(k)
-constexpr int kSkChunk = 16;       // reals per register tile (8 k-vectors per pass over the atoms)
 constexpr int kSkBlocks = 148 * 4;  // grid for the partial sums (4 blocks per SM: more atoms per thread, fewer block sums)
-constexpr int kSkQ = kSkChunk / 2;  // k-vectors per chunk of the partial-sum pass
-constexpr int kSkQF = 32;          // k-vectors per table chunk of the mixed-precision force pass
 constexpr int kSkAtoms = 8;        // atoms per thread of the mixed-precision force pass
+// k-tiles (k-vectors per pass over the atoms): Q of the partial-sum pass (a
+// register tile of 2Q sums per thread), QF of the mixed-precision force pass
+// (a shared-memory table chunk).  Every k is summed in the same order
+// whatever the tile, so every tile gives bitwise-identical results; the
+// autotuner picks them (SkDev::qv, ::qf).
 
 // Mixed precision, phase tables: the phase of k at x is split as
 //   k.x = sum_d T_d[k][c_d] + k.delta,   T_d[k][c] = k_d (o_d + (c + 1/2) h_d) mod 2 pi,
@@ -202,7 +204,9 @@ __device__ __forceinline__ float tab_phase(const float *tc, int tstride, int q, 
 
 // k-vectors (and, in the force pass, rho) staged in dynamic shared memory
 // sized to K, so a small K leaves room for more resident blocks.
-template <bool FP64> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
+template <bool FP64, int QV> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
+    constexpr int kSkChunk = 2 * QV;   // reals per register tile
+    constexpr int kSkQ = QV;
     pdl_entry();
     __shared__ double smem[kSkChunk * 32];
     extern __shared__ double kk[];   // 3K doubles; mixed: then 3K floats and a table chunk
@@ -372,6 +376,7 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
 // in chunks whose tables are staged in shared memory; the block's virial
 // partial goes to vpart[blockIdx.x] and block 0 zeroes the partials of the
 // one-atom-per-thread layout beyond the grid.
+template <int kSkQF>
 __global__ void __launch_bounds__(256) k_sk_force_tab(SkDev d, const double *__restrict__ f_src,
                                                       double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                       double *vpart, int nparts) {
@@ -486,15 +491,39 @@ template <typename K> static void allow_smem(K kernel, size_t bytes) {
 
 size_t sk_table_smem(const SkDev &d, int q) { return sizeof(float) * 3 * q * (size_t)d.tstride; }
 
+template <int QV> static void launch_sk_partial_mixed(const SkDev &d, cudaStream_t st) {
+    const size_t sm = (sizeof(double) + sizeof(float)) * 3 * (size_t)d.K + sk_table_smem(d, QV);
+    allow_smem(k_sk_partial<false, QV>, sm);
+    launch_k(k_sk_partial<false, QV>, d.nblocks, 256, sm, st, d);
+}
+
+template <int QF>
+static void launch_sk_force_mixed(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s,
+                                  const CellGrid &g, double *vpart, int nb, cudaStream_t st) {
+    const int tb = (d.n + 256 * kSkAtoms - 1) / (256 * kSkAtoms);   // kSkAtoms atoms per thread
+    const size_t sm = sizeof(double) * 3 * (size_t)d.K + sizeof(float) * 5 * (size_t)d.K + sk_table_smem(d, QF);
+    allow_smem(k_sk_force_tab<QF>, sm);
+    launch_k(k_sk_force_tab<QF>, tb, 256, sm, st, d, f_src, f_dst, s, g, vpart, nb);
+}
+
+size_t sk_smem_values(const SkDev &d, int qv) {
+    return (sizeof(double) + sizeof(float)) * 3 * (size_t)d.K + sk_table_smem(d, qv);
+}
+size_t sk_smem_force(const SkDev &d, int qf) {
+    return sizeof(double) * 3 * (size_t)d.K + sizeof(float) * 5 * (size_t)d.K + sk_table_smem(d, qf);
+}
+
 void launch_sk_values(const SkDev &d, cudaStream_t st) {
     if (d.fp64) {
         const size_t sm = sizeof(double) * 3 * (size_t)d.K;
-        allow_smem(k_sk_partial<true>, sm);
-        launch_k(k_sk_partial<true>, d.nblocks, 256, sm, st, d);
+        allow_smem(k_sk_partial<true, 8>, sm);
+        launch_k(k_sk_partial<true, 8>, d.nblocks, 256, sm, st, d);
+    } else if (d.qv == 4) {
+        launch_sk_partial_mixed<4>(d, st);
+    } else if (d.qv == 16) {
+        launch_sk_partial_mixed<16>(d, st);
     } else {
-        const size_t sm = (sizeof(double) + sizeof(float)) * 3 * (size_t)d.K + sk_table_smem(d, kSkQ);
-        allow_smem(k_sk_partial<false>, sm);
-        launch_k(k_sk_partial<false>, d.nblocks, 256, sm, st, d);
+        launch_sk_partial_mixed<8>(d, st);
     }
     prof_mark("sk_partial", st);
     launch_k(k_sk_reduce, 2 * d.K + 1, 256, 0, st, d);
@@ -509,11 +538,12 @@ void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const 
         const size_t sm = sizeof(double) * 5 * (size_t)d.K;
         allow_smem(k_sk_force<true>, sm);
         launch_k(k_sk_force<true>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
+    } else if (d.qf == 8) {
+        launch_sk_force_mixed<8>(d, f_src, f_dst, s, g, vpart, nb, st);
+    } else if (d.qf == 16) {
+        launch_sk_force_mixed<16>(d, f_src, f_dst, s, g, vpart, nb, st);
     } else {
-        const int tb = (d.n + 256 * kSkAtoms - 1) / (256 * kSkAtoms);   // kSkAtoms atoms per thread
-        const size_t sm = sizeof(double) * 3 * (size_t)d.K + sizeof(float) * 5 * (size_t)d.K + sk_table_smem(d, kSkQF);
-        allow_smem(k_sk_force_tab, sm);
-        launch_k(k_sk_force_tab, tb, 256, sm, st, d, f_src, f_dst, s, g, vpart, nb);
+        launch_sk_force_mixed<32>(d, f_src, f_dst, s, g, vpart, nb, st);
     }
     prof_mark("sk_force", st);
 }

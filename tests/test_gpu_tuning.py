@@ -103,3 +103,43 @@ def test_walkers_autotune_keeps_the_steps():
     for (cv1, f1), (cv2, f2) in zip(*results):
         assert cv1 == cv2
         assert all(np.array_equal(a, b) for a, b in zip(f1, f2))
+
+
+def test_sk_tiles_give_identical_steps_and_autotune_picks_one():
+    """STRU_FACTOR_K in mixed precision (phase tables): every k-tile of the
+    value pass (4, 8, 16) and of the force pass (8, 16, 32) gives bitwise-
+    identical CVs, bias, forces and virial; mtd_autotune picks one of them."""
+    import torch
+
+    x = systems.jitter(systems.fcc(10, 5.26), 0.2, 61)
+    L = np.array([10 * 5.26] * 3)
+    x = np.ascontiguousarray(systems.wrap(x, L))
+    args = ["GAUSSIAN", 0.5, 0.005, 10.0, "PACE", 1,
+            "CAL", "NAME", "SK", "STRU_FACTOR_K", "all", "nk", 40, "kmag", systems.KMAG_111, "seed", 5,
+            "SYMBOL", "v1", "SK.AVE", "CV_dim", 1, "DIM", 1, 0.0, 100.0, 500, "v1", "WT", 0]
+
+    def run(tiles):
+        m = mtd.Metad(args, precision="mixed")
+        m.set_box([0, 0, 0], L)
+        if tiles is not None:
+            m.set_sk_tiles(*tiles)
+        out = []
+        for step in range(2):
+            f = np.zeros_like(x)
+            vir = m.post_force(step, x, f, virial=True)
+            out.append((m.cv.copy(), m.compute_scalar(), f, np.array(vir)))
+        m.close()
+        return out
+
+    ref = run(None)
+    for tiles in [(4, 8), (16, 16), (8, 32), (4, 32), (16, 8)]:
+        got = run(tiles)
+        for a, b in zip(ref, got):
+            assert all(np.array_equal(u, v) for u, v in zip(a, b)), tiles
+    m = mtd.Metad(args, precision="mixed")
+    m.set_box([0, 0, 0], L)
+    dx = torch.from_numpy(x).cuda()
+    m.autotune(x.shape[0], dx.data_ptr(), reps=2)
+    qv, qf = m.sk_tiles()
+    assert qv in (4, 8, 16) and qf in (8, 16, 32)
+    m.close()

@@ -134,7 +134,7 @@ def test_steinh_l_switching_functions(case, precision):
     o6 = O.steinh_l(6, x, L, rl, swr, 1e-6, swc, mode)
     # the DIMs scale both CVs into the middle of the grid, where V and dV/ds
     # are of the hill's size (outside it they are a hill's far tail)
-    scale = 2.5 * max(abs(o4["cv"]), abs(o6["cv"]))
+    scale = float(2.5 * max(abs(o4["cv"]), abs(o6["cv"])))
     args = (["GAUSSIAN", 0.01, 0.005, 9.0, "PACE", 10, "TEMP", 300.0] + _sw_args("SWR", rk, **rkw) +
             _sw_args("SWC", ck, **ckw))
     for l in (4, 6):
