@@ -371,6 +371,7 @@ def run_secondary(args, local):
     f = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     step = 0
+    tuned = m.autotune(n, dx[0].data_ptr(), reps=3)   # shapes only: results do not depend on them
     for _ in range(args.warmup):
         m.post_force_device(step, n, dx[step % len(dx)].data_ptr(), f.data_ptr(), f.data_ptr())
         step += 1
@@ -421,7 +422,8 @@ def run_secondary(args, local):
                        "l2": "flushed (256 MB write) before each timed step", "cv": [float(v) for v in m.cv]},
             "e2e": {"value": n * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_s * 1e3 / args.steps},
-            "gpu_launches": launches * args.steps, "kernels_ms_per_step": kernels, "clocks": clk.summary()}
+            "gpu_launches": launches * args.steps, "kernels_ms_per_step": kernels, "clocks": clk.summary(),
+            "autotuned_shapes": {"neighbors_q_lambda": list(tuned), "sk_tiles": list(m.sk_tiles())}}
     if args.workload == "sk":
         pairs = n * 96
         ms = {k: v for k, v in kernels.items()}
@@ -436,30 +438,35 @@ def run_secondary(args, local):
     return 0
 
 
-# FP32 operations per (atom, k) pair of the S(k) passes, counted in the
-# kernels' source (an FMA counts 2): the phase from the per-dimension tables
-# and the residual k . dl (8), the Cody-Waite reduction and the sin / cos
-# polynomials (29), then the value pass accumulates cos and sin (2) and the
-# force pass projects on rho(k) and k (9).
-SK_FLOP_PER_PAIR = {"sk_partial": 39, "sk_force": 46}
+# Operations per (atom, k) pair of the S(k) passes, counted in the kernels'
+# source (an FMA counts 2): FP64 -- the phase k.x (6) and its reduction to a
+# quarter turn (5); FP32 -- the sin / cos polynomials (22), then the value
+# pass accumulates cos and sin (2) and the force pass projects on rho(k) and
+# k (9).
+SK_FLOP_PER_PAIR = {"sk_partial": {"fp64": 11, "fp32": 24}, "sk_force": {"fp64": 11, "fp32": 31}}
 
 
 def sk_roofline(kernels, n, nk, clocks):
-    """The S(k) passes are bound by FP32 issue, not DRAM: achieved FP32 rate
-    of the dominant pass against the FP32 (non-tensor) peak of the part at
-    the sampled SM clock: 148 SMs x 128 FP32 lanes x 2 (FMA) x clock."""
+    """The S(k) passes are bound by arithmetic, not DRAM: achieved FP32 and
+    FP64 rates of the dominant pass against the (non-tensor) peaks of the
+    part at the sampled SM clock: 148 SMs x 128 FP32 lanes x 2 (FMA) x clock,
+    and half that for FP64."""
     sk = {k: v for k, v in kernels.items() if k in SK_FLOP_PER_PAIR and v > 0}
     if not sk:
         return None
     name, ms = max(sk.items(), key=lambda kv: kv[1])
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    achieved = SK_FLOP_PER_PAIR[name] * n * nk / (ms / 1e3) / 1e12
+    per = SK_FLOP_PER_PAIR[name]
+    a32 = per["fp32"] * n * nk / (ms / 1e3) / 1e12
+    a64 = per["fp64"] * n * nk / (ms / 1e3) / 1e12
     peak_hbm, kind = peaks()
     bytes_ = n * 24 + 2 * 8 * nk * 1024   # positions once, per-block FP64 partials of rho(k)
-    return {"bound": "fp32", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "flop_per_pair": SK_FLOP_PER_PAIR[name], "avg_launch_ms": ms,
-            "peak_source": "148 SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled)" % mhz,
+    return {"bound": "fp32", "kernel": name, "achieved": a32, "peak": peak, "unit": "TFLOP/s",
+            "frac": a32 / peak, "flop_per_pair": per, "avg_launch_ms": ms,
+            "fp64": {"achieved": a64, "peak": peak / 2, "frac": a64 / (peak / 2)},
+            "issue_frac": (a32 / peak) + (a64 / (peak / 2)),
+            "peak_source": "148 SMs x 128 FP32 lanes x 2 x %.0f MHz (sampled); FP64 half of it" % mhz,
             "hbm": {"achieved": bytes_ / (ms / 1e3) / 1e9, "peak": peak_hbm, "unit": "GB/s",
                     "frac": bytes_ / (ms / 1e3) / 1e9 / peak_hbm, "peak_source": kind}}
 
@@ -919,6 +926,17 @@ def main():
             e2e_s += time.perf_counter() - t0
             step += 1
     clocks = clk.summary()
+    # where the end-to-end step goes: the library's event marks around the
+    # host copies and kernels of a few more calls (a separate, untimed pass)
+    m.profile(True)
+    for k in range(5):
+        flush.zero_()
+        torch.cuda.synchronize()
+        hf.zero_()
+        m.post_force(step, hx[step % len(hx)].numpy(), hf.numpy())
+        step += 1
+    split = {k: v[1] / max(v[0], 1) for k, v in sorted(m.profile_report().items(), key=lambda kv: -kv[1][1])}
+    m.profile(False)
 
     dev_ms, e2e_ms = max_over_ranks([dev_ms, e2e_s * 1e3], dist, "cuda")
     # whole-job throughput counts owned atoms (ghosts are copies)
@@ -971,7 +989,8 @@ def main():
                                                   "moves more than skin/2 and at least every 10 steps"},
                        "cv": [float(v) for v in m.cv]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
-                    "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps},
+                    "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps,
+                    "split_ms": split},
             "gpu_launches": launches * args.steps,
             "roofline": roof, "clocks": clocks, "cpu_baseline": cpu, "error_vs_fp64": err}
     if rank == 0:

@@ -242,12 +242,11 @@ int mtd_profile_report(mtd_ctx *ctx, char *buf, int len);
 mtd_status mtd_autotune(mtd_ctx *ctx, int n, const double *d_x, const int *d_mask, int reps, int choice[3]);
 mtd_status mtd_set_tuning(mtd_ctx *ctx, int neighbor_shape, int q_block, int lambda_block);
 
-/* S(k) k-tiles of the mixed-precision STRU_FACTOR_K passes, chosen by
- * mtd_autotune when the deck has that CAL: k-vectors per pass over the atoms
- * of the value pass (4, 8 or 16: a register tile) and of the force pass (8,
- * 16 or 32: a shared-memory phase-table chunk).  Every k is summed in the
- * same order whatever the tile, so the results are bitwise identical.
- * Defaults 8 and 32. */
+/* Shapes of the STRU_FACTOR_K passes, chosen by mtd_autotune when the deck
+ * has that CAL: k-vectors per pass over the atoms of the value pass (4, 8 or
+ * 16: a register tile of partial sums) and the unroll depth of the force
+ * pass's loop over k (1, 2 or 4).  Every k is summed in the same order
+ * whatever the shape, so the results are bitwise identical.  Defaults 8, 2. */
 mtd_status mtd_sk_tiles(mtd_ctx *ctx, int *q_values, int *q_force);
 mtd_status mtd_set_sk_tiles(mtd_ctx *ctx, int q_values, int q_force);
 

@@ -94,20 +94,17 @@ mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask
         }
     }
     c->tune_l = bl;
-    // S(k) k-tiles of the mixed-precision passes (value pass: register tile;
-    // force pass: shared-memory table chunk), those whose chunk fits
-    int dev = 0, smem_max = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    // S(k) shapes: k-vectors per pass of the value pass, unroll depth of the force pass
     for (Unit &u : c->units) {
-        if (u.kind != CAL_STRU_FACTOR_K || c->fp64 || !u.sk_tab) continue;
-        const SkDev d = sk_dev(c, u, d_x, d_mask);
+        if (u.kind != CAL_STRU_FACTOR_K) continue;
         best = 1e30f;
         int bv = c->tune_skq;
         for (int qv : {4, 8, 16}) {
-            if (sk_smem_values(d, qv) > (size_t)smem_max) continue;
             c->tune_skq = qv;
-            const float t = timed([&] { run_values<float>(c, g, d_x, d_mask); });
+            const float t = timed([&] {
+                if (c->fp64) run_values<double>(c, g, d_x, d_mask);
+                else run_values<float>(c, g, d_x, d_mask);
+            });
             if (t < best) {
                 best = t;
                 bv = qv;
@@ -116,17 +113,19 @@ mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask
         c->tune_skq = bv;
         best = 1e30f;
         int bf = c->tune_skqf;
-        for (int qf : {8, 16, 32}) {
-            if (sk_smem_force(d, qf) > (size_t)smem_max) continue;
+        for (int qf : {1, 2, 4}) {
             c->tune_skqf = qf;
-            const float t = timed([&] { run_forces<float>(c, sd, g, d_x, d_mask, c->d_fin, c->d_fout, false); });
+            const float t = timed([&] {
+                if (c->fp64) run_forces<double>(c, sd, g, d_x, d_mask, c->d_fin, c->d_fout, false);
+                else run_forces<float>(c, sd, g, d_x, d_mask, c->d_fin, c->d_fout, false);
+            });
             if (t < best) {
                 best = t;
                 bf = qf;
             }
         }
         c->tune_skqf = bf;
-        break;   // one set of tiles per context
+        break;   // one set of shapes per context
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -166,7 +165,7 @@ mtd_status mtd_sk_tiles(mtd_ctx *c, int *q_values, int *q_force) {
 }
 
 mtd_status mtd_set_sk_tiles(mtd_ctx *c, int q_values, int q_force) {
-    if (!c || (q_values != 4 && q_values != 8 && q_values != 16) || (q_force != 8 && q_force != 16 && q_force != 32))
+    if (!c || (q_values != 4 && q_values != 8 && q_values != 16) || (q_force != 1 && q_force != 2 && q_force != 4))
         return MTD_ERR_INVALID_ARG;
     c->tune_skq = q_values;
     c->tune_skqf = q_force;

@@ -192,20 +192,6 @@ __device__ __forceinline__ void phase_sincos_f32(double ph, float &s, float &c) 
     quadrant_sincos_f32(r, q, s, c);
 }
 
-// FP32 sin and cos of an FP32 phase, |ph| < 2^21: the nearest multiple n of
-// pi / 2 (adding 1.5 * 2^23 rounds ph * 2 / pi to an integer held in the low
-// mantissa bits), then r = ph - n pi / 2 with pi / 2 split into two FP32
-// constants (Cody and Waite's reduction; each FMA forms n * C exactly), and
-// the polynomials below on |r| <= pi / 4.
-__device__ __forceinline__ void sincos_f32_reduced(float ph, float &s, float &c) {
-    constexpr float kRound = 12582912.0f;                                // 1.5 * 2^23
-    const float t = fmaf(ph, 0.636619772367581343f, kRound);             // 2 / pi
-    const float n = t - kRound;
-    float r = fmaf(-n, 1.57079637050628662109f, ph);                     // pi / 2, leading FP32 part
-    r = fmaf(-n, -4.37113900018624283e-8f, r);                           // pi / 2 minus that part
-    quadrant_sincos_f32(r, __float_as_int(t) & 3, s, c);
-}
-
 // sin and cos of r + q pi / 2 for |r| <= pi / 4: Taylor series of sin and cos
 // to degree 9 and 10, then the quadrant rotation.
 __device__ __forceinline__ void quadrant_sincos_f32(float r, int q, float &s, float &c) {

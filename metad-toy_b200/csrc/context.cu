@@ -20,6 +20,7 @@ namespace mtd {
 void pdl_set(bool on) { g_pdl = on; }
 bool pdl_on() { return g_pdl; }
 void prof_set(Prof *p) { g_prof = p; }
+Prof *prof_get() { return g_prof; }
 void prof_mark(const char *name, cudaStream_t st) {
     Prof *p = g_prof;
     if (!p || !p->on || p->n >= kProfMax) return;
@@ -234,7 +235,7 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
     if (npad > c->cap_n) {
         const int cap = npad + npad / 4;
         dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
-        dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask); dfree(c->arrival);
+        dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->iperm); dfree(c->smask); dfree(c->arrival);
         dfree(c->xs); dfree(c->pf); dfree(c->d_vpart);
         MTD_CU(dalloc(&c->d_x, sizeof(double) * 3 * (size_t)cap), "x");
         MTD_CU(dalloc(&c->d_fin, sizeof(double) * 3 * (size_t)cap), "f");
@@ -244,6 +245,7 @@ mtd_status ensure_capacity(mtd_ctx *c, int n) {
         MTD_CU(dalloc(&c->cellof, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->slot, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->perm, sizeof(int) * (size_t)cap), "perm");
+        MTD_CU(dalloc(&c->iperm, sizeof(int) * (size_t)cap), "perm");
         MTD_CU(dalloc(&c->arrival, sizeof(int) * (size_t)cap), "cells");
         MTD_CU(dalloc(&c->smask, sizeof(int) * (size_t)cap), "mask");
         MTD_CU(dalloc(&c->xs, sizeof(double) * 3 * (size_t)cap), "x sorted");
@@ -552,6 +554,7 @@ SysDev sys_dev(mtd_ctx *c, const double *x, const int *mask, const int *image) {
     s.count = c->count;
     s.start = c->start;
     s.perm = c->perm;
+    s.iperm = c->iperm;
     s.arrival = c->arrival;
     s.smask = c->smask;
     s.xs = c->xs;
@@ -602,56 +605,9 @@ SkDev sk_dev(mtd_ctx *c, Unit &u, const double *x, const int *mask) {
     d.partials = u.partials; d.nblocks = u.nblocks; d.rho = u.rho; d.ngroup = u.skn; d.coef = u.coef;
     d.fp64 = c->fp64;
     d.nown = owned(c);
-    d.tab = u.sk_tab;
-    d.tstride = u.sk_tstride;
     d.qv = c->tune_skq;
     d.qf = c->tune_skqf;
-    for (int a = 0; a < 3; ++a) {
-        d.nct[a] = u.sk_nct[a];
-        d.to[a] = u.sk_to[a];
-        d.th[a] = u.sk_th[a];
-        d.tih[a] = 1.0 / u.sk_th[a];
-    }
     return d;
-}
-
-// Mixed-precision S(k): the per-dimension phase tables of each unit for the
-// current box, T_d[k][c] = k_d (o_d + (c + 1/2) h_d) reduced to [-pi, pi] in
-// FP64, cells of about 2 A over the box and a 4 A margin on each side
-// (coordinates beyond take the FP64 phase).  Rebuilt when the box changes.
-mtd_status ensure_sk_tables(mtd_ctx *c) {
-    if (c->fp64) return MTD_OK;
-    for (Unit &u : c->units) {
-        if (u.kind != CAL_STRU_FACTOR_K) continue;
-        const double box[6] = {c->lo[0], c->lo[1], c->lo[2], c->hi[0], c->hi[1], c->hi[2]};
-        if (u.sk_tab && std::memcmp(box, u.sk_box, sizeof box) == 0) continue;
-        const double margin = 4.0;
-        int ts = 1;
-        for (int a = 0; a < 3; ++a) {
-            const double span = (c->hi[a] - c->lo[a]) + 2.0 * margin;
-            const int nc = std::max(1, std::min(kSkTabCells, (int)std::ceil(span / 2.0)));
-            u.sk_nct[a] = nc;
-            u.sk_to[a] = c->lo[a] - margin;
-            u.sk_th[a] = span / nc;
-            ts = std::max(ts, nc);
-        }
-        u.sk_tstride = ts;
-        const CalDef &cd = c->cfg.cals[u.calnames[0]];
-        std::vector<float> tab((size_t)3 * u.K * ts, 0.0f);
-        for (int a = 0; a < 3; ++a)
-            for (int k = 0; k < u.K; ++k)
-                for (int cc = 0; cc < u.sk_nct[a]; ++cc) {
-                    const double ph = cd.kvecs[3 * k + a] * (u.sk_to[a] + (cc + 0.5) * u.sk_th[a]);
-                    tab[((size_t)a * u.K + k) * ts + cc] = (float)(ph - 2.0 * kPi * std::rint(ph / (2.0 * kPi)));
-                }
-        dfree(u.sk_tab);
-        MTD_CU(dalloc(&u.sk_tab, sizeof(float) * tab.size()), "S(k) phase tables");
-        MTD_CU(cudaMemcpyAsync(u.sk_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, c->st),
-               "S(k) phase tables");
-        MTD_CU(cudaStreamSynchronize(c->st), "S(k) phase tables");
-        std::memcpy(u.sk_box, box, sizeof box);
-    }
-    return MTD_OK;
 }
 
 template <typename T> void run_values(mtd_ctx *c, const CellGrid &g, const double *x, const int *mask) {
@@ -694,6 +650,36 @@ template <typename T>
 void run_forces(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, const int *mask, const double *fin,
                 double *fout, bool virial) {
     cudaStream_t st = c->st;
+    c->chunk_done = false;
+    // mtd_post_force with one STEINH L unit and no virial: the force pass runs
+    // in caller-order chunks and each chunk of f goes to the host while the
+    // next chunk is computed (the same per-atom arithmetic)
+    int used = 0;
+    Unit *only = nullptr;
+    for (Unit &u : c->units)
+        if (u.used) {
+            ++used;
+            only = &u;
+        }
+    if (c->chunk_host && !virial && used == 1 && only->kind == CAL_STEINH_L && c->n >= 4096 && c->copy_st) {
+        LocalDev<T> d = local_dev<T>(c, *only, g);
+        launch_local_lambda<T>(d, st);
+        d.iperm = c->iperm;
+        for (int k = 0; k < kForceChunks; ++k) {
+            d.i0 = (int)((long long)c->n * k / kForceChunks);
+            d.i1 = (int)((long long)c->n * (k + 1) / kForceChunks);
+            launch_local_force_pass<T>(d, fin, fout, s, g, nullptr, c->d_status, st);
+            cudaEventRecord(c->chunk_ev[k], st);
+            cudaStreamWaitEvent(c->copy_st, c->chunk_ev[k], 0);
+            cudaMemcpyAsync(c->chunk_host + 3 * (size_t)d.i0, fout + 3 * (size_t)d.i0,
+                            sizeof(double) * 3 * (size_t)(d.i1 - d.i0), cudaMemcpyDeviceToHost, c->copy_st);
+        }
+        cudaEventRecord(c->copies_done, c->copy_st);
+        cudaStreamWaitEvent(st, c->copies_done, 0);
+        c->launches += 1 + kForceChunks;
+        c->chunk_done = true;
+        return;
+    }
     bool first = true;
     int voff = 0;
     for (Unit &u : c->units) {
@@ -853,8 +839,6 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
         }
         c->skin_last = skin;
     }
-    const mtd_status stab = ensure_sk_tables(c);
-    if (stab != MTD_OK) return stab;
     for (const Unit &u : c->units)
         if (u.chem && c->types_n != n)
             return fail(c, MTD_ERR_INVALID_ARG,
@@ -1166,6 +1150,9 @@ mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, 
     c->own_st = c->st;
     cudaStreamCreateWithFlags(&c->side_st, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&c->f_ready, cudaEventDisableTiming);
+    cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking);
+    for (int k = 0; k < kForceChunks; ++k) cudaEventCreateWithFlags(&c->chunk_ev[k], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->copies_done, cudaEventDisableTiming);
     c->cv.assign(c->cfg.cv_dim, 0.0);
     mtd_status s = plan_units(c);
     if (s == MTD_OK) {
@@ -1207,10 +1194,9 @@ void mtd_destroy(mtd_ctx *c) {
         void **arrs[] = {&u.q, &u.nf, &u.lq, &u.lqs, &u.e12, &u.lam, &u.g, &u.tu, &u.Q, &u.S, &u.w};
         for (void **a : arrs) dfree(*a);
         dfree(u.partials); dfree(u.coef); dfree(u.kvec); dfree(u.rho); dfree(u.skn); dfree(u.d_wtab);
-        dfree(u.sk_tab);
     }
     dfree(c->d_x); dfree(c->d_fin); dfree(c->d_fout); dfree(c->d_mask); dfree(c->d_image);
-    dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->smask); dfree(c->arrival);
+    dfree(c->cellof); dfree(c->slot); dfree(c->perm); dfree(c->iperm); dfree(c->smask); dfree(c->arrival);
     dfree(c->xs); dfree(c->pf); dfree(c->count); dfree(c->start); dfree(c->d_vpart);
     dfree(c->d_plan); dfree(c->d_grid); dfree(c->d_hills); dfree(c->d_nhills); dfree(c->d_out);
     dfree(c->d_status); dfree(c->d_vir);
@@ -1219,6 +1205,10 @@ void mtd_destroy(mtd_ctx *c) {
         if (c->slot_ev[k]) cudaEventDestroy(c->slot_ev[k]);
     if (c->own_st) cudaStreamDestroy(c->own_st);
     if (c->side_st) cudaStreamDestroy(c->side_st);
+    if (c->copy_st) cudaStreamDestroy(c->copy_st);
+    for (int k = 0; k < kForceChunks; ++k)
+        if (c->chunk_ev[k]) cudaEventDestroy(c->chunk_ev[k]);
+    if (c->copies_done) cudaEventDestroy(c->copies_done);
     if (c->nb) mtd_nnbias_destroy(c->nb);
     dfree(c->d_vdv);
     dfree(c->d_ws1);
@@ -1345,11 +1335,14 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
     MTD_CU(cudaEventRecord(c->f_ready, c->side_st), "force upload");
     for (int attempt = 0; attempt < 4; ++attempt) {
         MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
+        c->chunk_host = f;   // the force pass may copy f back in chunks as it goes
         s = enqueue_step(c, step, n, c->d_x, mask, (image && virial) ? c->d_image : nullptr,
                          c->d_fin, c->d_fout, virial != nullptr, c->f_ready);
+        c->chunk_host = nullptr;
         if (s != MTD_OK) return s;
         // the forces go back in the same stream pass (a failed attempt's are overwritten by the retry)
-        MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
+        if (!c->chunk_done) MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
+        prof_mark("f_download", c->st);
         MTD_CU(cudaStreamSynchronize(c->st), "step");
         if (c->h_status->overflow == 0 && c->h_status->cand_overflow == 0) break;
         c->fifo.pop_back();   // the failed attempt is not collected
@@ -1378,7 +1371,9 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
     const size_t b3 = sizeof(double) * 3 * (size_t)n;
     // x (and mask) first on the step's stream; f (and image, read by the force
     // kernels only) on the side stream, overlapping the CV passes
+    ProfScope prof_scope(c);
     MTD_CU(h2d_pieces(c->d_x, x, b3, c->st), "x upload");
+    prof_mark("x_upload", c->st);
     if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
     return step_uploaded(c, step, n, mask != nullptr, image, f, virial);
 }

@@ -70,10 +70,6 @@ struct Unit {
     int K = 0;
     double *kvec = nullptr, *rho = nullptr, *skn = nullptr;
     // S(k), mixed precision: per-dimension phase tables for the box they were built for
-    float *sk_tab = nullptr;
-    int sk_tstride = 0, sk_nct[3] = {0, 0, 0};
-    double sk_to[3] = {0, 0, 0}, sk_th[3] = {1, 1, 1};
-    double sk_box[6] = {0, 0, 0, 0, 0, 0};
     // STRU_FACTOR Chemical: type-weight parameters, the table built from the
     // types of mtd_set_types, and the per-atom weights (sorted order)
     bool chem = false, wchem = false;
@@ -114,6 +110,8 @@ struct PendingOut {
     bool virial;
 };
 
+constexpr int kForceChunks = 4;     // caller-order chunks of the host-buffer force pass
+
 struct mtd_ctx {
     int fp64 = 0;
     int device = 0;
@@ -133,6 +131,7 @@ struct mtd_ctx {
     double *d_x = nullptr, *d_fin = nullptr, *d_fout = nullptr;
     int *d_mask = nullptr, *d_image = nullptr;
     int *cellof = nullptr, *slot = nullptr, *perm = nullptr, *smask = nullptr, *arrival = nullptr;
+    int *iperm = nullptr;                // caller index -> sorted slot
     double *xs = nullptr;
     float4 *pf = nullptr;
     int *count = nullptr, *start = nullptr;
@@ -181,6 +180,13 @@ struct mtd_ctx {
     SysDev last_sys{};
     cudaStream_t own_st = nullptr;
     cudaStream_t side_st = nullptr;      // host -> device force upload beside the CV passes
+    // mtd_post_force: the force pass in caller-order chunks, each chunk's
+    // forces copied to the host while the next chunk runs
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t chunk_ev[kForceChunks] = {};
+    cudaEvent_t copies_done = nullptr;
+    double *chunk_host = nullptr;        // the host f of the call in progress (null: no chunked copies)
+    bool chunk_done = false;             // the last force pass copied its chunks
     // hill-list bias (CV_dim 4 or NN_BIAS 1): hills, exact sum, learned bias
     mtd_nnbias *nb = nullptr;
     double *d_vdv = nullptr;             // V, dV/ds at this step's s
@@ -194,7 +200,7 @@ struct mtd_ctx {
     // kernel shapes chosen by mtd_autotune (every choice gives bitwise-identical results)
     int tune_nbr = 0;                    // neighbour search: 0 fast/256, 1 fast/128, 2 flat/128
     int tune_q = 0, tune_l = 0;          // threads per block of the q and lambda passes (0: 256)
-    int tune_skq = 8, tune_skqf = 32;    // S(k) k-tiles of the mixed-precision value and force passes
+    int tune_skq = 8, tune_skqf = 2;     // S(k): k-vectors per pass of the value pass, unroll of the force pass
     // per-atom dCV/dx export (compute metad/atom): last step's inputs, cached result
     const double *last_x = nullptr;
     const int *last_mask = nullptr;
@@ -288,14 +294,15 @@ struct PdlScope {
 };
 
 struct ProfScope {
-    explicit ProfScope(mtd_ctx *c) {
+    Prof *prev;
+    explicit ProfScope(mtd_ctx *c) : prev(prof_get()) {
         if (c->prof.on) {
             if (c->prof.n > kProfMax - 64) prof_collect(c);
             prof_set(&c->prof);
             prof_mark("start", c->st);
         }
     }
-    ~ProfScope() { prof_set(nullptr); }
+    ~ProfScope() { prof_set(prev); }
 };
 
 mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, const int *image);

@@ -84,6 +84,7 @@ struct SysDev {
     const int *mask;      // caller order, may be null (all groups)
     const int *image;     // caller order, may be null
     int *cellof, *slot, *count, *start, *perm, *smask;
+    int *iperm;           // caller index -> sorted slot (null: not kept)
     int *arrival;         // [n] atoms by cell in atomic arrival order (cell-list scratch)
     int nown;             // caller indices >= nown are ghosts (domain decomposition): their
                           // sorted group mask is 0, so they are neighbours and never centres
@@ -136,6 +137,7 @@ struct Prof {
     const char *name[kProfMax];
 };
 void prof_set(Prof *p);                          // active profiler of this host thread (null: off)
+Prof *prof_get();
 void prof_mark(const char *name, cudaStream_t st);
 
 // ------------------------------------------------------------------ programmatic dependent launch
@@ -215,6 +217,10 @@ template <typename T> struct LocalDev {
     NeighDev cand;
     DevStatus *status;
     SkinState *reset;           // the first kernel after the gated rebuild: closes the gate
+    // force pass over caller indices i0 .. i1 - 1 (iperm: caller -> sorted
+    // slot) instead of sorted slots; the same per-atom arithmetic
+    const int *iperm;
+    int i0, i1;
 };
 template <typename T> void launch_local_values(const LocalDev<T> &d, cudaStream_t st);
 // Reals per STEINH L record (both orders): a multiple of 32 bytes.
@@ -222,6 +228,12 @@ int local_record_stride(int LA, int LB, int fp64);
 template <typename T>
 void launch_local_forces(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                          double *vpart, DevStatus *status, cudaStream_t st);
+// The two force-stage passes separately: lambda, then the force pass (over
+// caller indices d.i0 .. d.i1 - 1 when d.iperm is set; no virial then).
+template <typename T> void launch_local_lambda(const LocalDev<T> &d, cudaStream_t st);
+template <typename T>
+void launch_local_force_pass(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s,
+                             const CellGrid &g, double *vpart, DevStatus *status, cudaStream_t st);
 
 // ------------------------------------------------------------------ STEINH Q
 template <typename T> struct GlobalDev {
@@ -275,22 +287,13 @@ struct SkDev {
     double *ngroup;             // group count
     const double *coef;         // alpha
     int fp64;
-    // mixed precision: per-dimension phase tables, tab[(d * K + k) * tstride + c] =
-    // k_d (o_d + (c + 1/2) h_d) reduced to [-pi, pi] (FP64 on the host, stored FP32)
-    const float *tab;
-    int tstride;
-    int nct[3];
-    double to[3], th[3], tih[3];
-    int qv, qf;                 // k-tiles of the mixed-precision value and force passes (4 / 8 / 16, 8 / 16 / 32)
+    int qv, qf;                 // k-vectors per pass of the value pass (4 / 8 / 16), unroll of the force pass (1 / 2 / 4)
 };
-constexpr int kSkTabCells = 320;    // phase-table cells per dimension at most (bounds the shared-memory chunks)
 void launch_sk_values(const SkDev &d, cudaStream_t st);
 void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                       double *vpart, cudaStream_t st);
 int sk_blocks(int n);
-// Dynamic shared memory of the mixed-precision passes with k-tile qv / qf.
-size_t sk_smem_values(const SkDev &d, int qv);
-size_t sk_smem_force(const SkDev &d, int qf);
+
 
 // ------------------------------------------------------------------ bias grid
 enum SymKind {

@@ -350,6 +350,8 @@ __device__ __forceinline__ void local_lambda_body(const LocalDev<T> &d, int bid)
 }
 
 // Pass 4: gather forces, f_dst = f_src - dV/dx, plus the virial block partials.
+// One thread per sorted slot, or (d.iperm set) per caller index of d.i0 ..
+// d.i1 - 1, so a caller-order range of f is complete when its launch is.
 template <int LA, int LB, typename T, bool STEP>
 __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const double *__restrict__ f_src,
                                                  double *__restrict__ f_dst, const SysDev &s, const CellGrid &g,
@@ -357,8 +359,17 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
     using S = LSet<LA, LB, T>;
     constexpr bool DSIG = !STEP;
     __shared__ double smem[6 * 32];
-    const int k = bid * blockDim.x + threadIdx.x;
-    const bool valid = k < d.n;
+    int k, ic = 0;
+    bool valid;
+    if (d.iperm) {
+        ic = d.i0 + bid * blockDim.x + threadIdx.x;
+        valid = ic < d.i1;
+        k = valid ? d.iperm[ic] : 0;
+        valid = valid && (unsigned)k < (unsigned)d.n;
+    } else {
+        k = bid * blockDim.x + threadIdx.x;
+        valid = k < d.n;
+    }
     double vir[6] = {0, 0, 0, 0, 0, 0};
     if (valid) {
         T la[S::SQ];
@@ -415,7 +426,7 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
                 }
             }
         }
-        const int i = d.perm[k];
+        const int i = d.iperm ? ic : d.perm[k];
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;   // delta f = -dV/dx
         if ((unsigned)i < (unsigned)d.n) {   // a sorted order left by a rebuild that gave up is not trusted
             f_dst[3 * i] = f_src[3 * i] + fx;

@@ -28,7 +28,7 @@ namespace {
 
 // The passes as kernels (local_body.cuh).
 template <int LA, int LB, typename T, bool STEP, bool FILTER>
-__global__ void __launch_bounds__(kBlock) k_local_q(LocalDev<T> d) {
+__global__ void __launch_bounds__(kBlock, 4) k_local_q(LocalDev<T> d) {
     pdl_entry();
     local_q_body<LA, LB, T, STEP, FILTER>(d, blockIdx.x);
 }
@@ -69,6 +69,26 @@ template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cuda
         launch_k(k_local_lq<LA, LB, T, false>, nb, kBlock, 0, st, d);
         prof_mark("local_lq", st);
     }
+}
+
+template <int LA, int LB, typename T> void run_lambda(const LocalDev<T> &d, cudaStream_t st) {
+    const int lb = d.lblock > 0 ? d.lblock : kBlock, lg = (d.n + lb - 1) / lb;
+    if (d.sw_r.type == SW_STEP) launch_k(k_local_lambda<LA, LB, T, true>, lg, lb, 0, st, d);
+    else launch_k(k_local_lambda<LA, LB, T, false>, lg, lb, 0, st, d);
+    prof_mark("local_lambda", st);
+}
+
+template <int LA, int LB, typename T>
+void run_force_pass(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                    double *vpart, DevStatus *status, cudaStream_t st) {
+    const int cnt = d.iperm ? d.i1 - d.i0 : d.n;
+    if (cnt <= 0) return;
+    const int nb = (cnt + kBlock - 1) / kBlock;
+    if (d.sw_r.type == SW_STEP)
+        launch_k(k_local_force<LA, LB, T, true>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
+    else
+        launch_k(k_local_force<LA, LB, T, false>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
+    prof_mark("local_force", st);
 }
 
 template <int LA, int LB, typename T>
@@ -124,6 +144,24 @@ void launch_local_forces(const LocalDev<T> &d, const double *f_src, double *f_ds
     MTD_LOCAL_DISPATCH(run_forces, d, f_src, f_dst, s, g, vpart, status, st);
 }
 
+template <typename T> void launch_local_lambda(const LocalDev<T> &d, cudaStream_t st) {
+    if (d.n == 0) return;
+    MTD_LOCAL_DISPATCH(run_lambda, d, st);
+}
+
+template <typename T>
+void launch_local_force_pass(const LocalDev<T> &d, const double *f_src, double *f_dst, const SysDev &s,
+                             const CellGrid &g, double *vpart, DevStatus *status, cudaStream_t st) {
+    if (d.n == 0) return;
+    MTD_LOCAL_DISPATCH(run_force_pass, d, f_src, f_dst, s, g, vpart, status, st);
+}
+
+template void launch_local_lambda<float>(const LocalDev<float> &, cudaStream_t);
+template void launch_local_lambda<double>(const LocalDev<double> &, cudaStream_t);
+template void launch_local_force_pass<float>(const LocalDev<float> &, const double *, double *, const SysDev &,
+                                             const CellGrid &, double *, DevStatus *, cudaStream_t);
+template void launch_local_force_pass<double>(const LocalDev<double> &, const double *, double *, const SysDev &,
+                                              const CellGrid &, double *, DevStatus *, cudaStream_t);
 template void launch_local_values<float>(const LocalDev<float> &, cudaStream_t);
 template void launch_local_values<double>(const LocalDev<double> &, cudaStream_t);
 template void launch_local_forces<float>(const LocalDev<float> &, const double *, double *, const SysDev &,

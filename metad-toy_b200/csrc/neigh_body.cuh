@@ -58,6 +58,7 @@ __device__ __forceinline__ void place_body(const CellGrid &g, const SysDev &s, i
     for (int t = b; t < e; ++t) rank += s.arrival[t] < i;
     const int d = b + rank;
     s.perm[d] = i;
+    if (s.iperm) s.iperm[i] = d;
     const double x0 = s.x[3 * i], x1 = s.x[3 * i + 1], x2 = s.x[3 * i + 2];
     s.xs[3 * d] = x0;
     s.xs[3 * d + 1] = x1;

@@ -152,79 +152,26 @@ __global__ void __launch_bounds__(kBlock) k_debye_force(DebyeDev<T> d, const dou
 
 // ------------------------------------------------------------------ S(k)
 constexpr int kSkBlocks = 148 * 4;  // grid for the partial sums (4 blocks per SM: more atoms per thread, fewer block sums)
-constexpr int kSkAtoms = 8;        // atoms per thread of the mixed-precision force pass
-// k-tiles (k-vectors per pass over the atoms): Q of the partial-sum pass (a
-// register tile of 2Q sums per thread), QF of the mixed-precision force pass
-// (a shared-memory table chunk).  Every k is summed in the same order
-// whatever the tile, so every tile gives bitwise-identical results; the
-// autotuner picks them (SkDev::qv, ::qf).
+// Shapes the autotuner picks (SkDev::qv, ::qf): QV k-vectors per pass over
+// the atoms in the partial-sum pass (a register tile of 2 QV sums per thread),
+// and the unroll depth U of the force pass's loop over k.  Every k is summed
+// in the same order whatever the shape, so all give bitwise-identical
+// results.  The phase k.x is formed in FP64 (B200 runs FP64 at half the FP32
+// rate) and reduced to [-pi/4, pi/4] before the FP32 polynomials; a
+// per-dimension FP32 phase-table variant (three shared-memory loads and an
+// FP32 reduction per pair) measured 2.2x slower and was removed.
 
-// Mixed precision, phase tables: the phase of k at x is split as
-//   k.x = sum_d T_d[k][c_d] + k.delta,   T_d[k][c] = k_d (o_d + (c + 1/2) h_d) mod 2 pi,
-// with c_d the table cell of x_d and |delta_d| <= h_d / 2 the FP32 offset from
-// its centre.  The tables are formed and reduced in FP64 once per box; a pair
-// then costs three shared-memory loads and FP32 arithmetic only.  A
-// coordinate outside the tables' range takes the FP64 phase instead.
-struct TabCell {
-    int c[3];
-    float dl[3];
-    bool in;
-};
-__device__ __forceinline__ TabCell tab_cell(const SkDev &d, double x, double y, double z) {
-    TabCell t;
-    const double v[3] = {x, y, z};
-    t.in = true;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double u = (v[a] - d.to[a]) * d.tih[a];
-        const int c = (int)floor(u);
-        t.in = t.in && u >= 0.0 && c < d.nct[a];
-        t.c[a] = c;
-        t.dl[a] = (float)(v[a] - (d.to[a] + (c + 0.5) * d.th[a]));
-    }
-    return t;
-}
-
-// Copies the tables of k-vectors k0 .. k0 + Q - 1 into shared memory:
-// tc[(a * Q + q) * tstride + c].
-template <int Q> __device__ __forceinline__ void load_tab_chunk(const SkDev &d, int k0, float *tc) {
-    const int per = Q * d.tstride;
-    for (int e = threadIdx.x; e < 3 * per; e += blockDim.x) {
-        const int a = e / per, r = e - a * per, q = r / d.tstride, c = r - q * d.tstride;
-        tc[e] = k0 + q < d.K ? __ldg(d.tab + ((size_t)a * d.K + k0 + q) * d.tstride + c) : 0.f;
-    }
-}
-
-template <int Q>
-__device__ __forceinline__ float tab_phase(const float *tc, int tstride, int q, const TabCell &t, const float *kf) {
-    const float base = tc[q * tstride + t.c[0]] + tc[(Q + q) * tstride + t.c[1]] + tc[(2 * Q + q) * tstride + t.c[2]];
-    return base + fmaf(kf[0], t.dl[0], fmaf(kf[1], t.dl[1], kf[2] * t.dl[2]));
-}
-
-
-// k-vectors (and, in the force pass, rho) staged in dynamic shared memory
-// sized to K, so a small K leaves room for more resident blocks.
 template <bool FP64, int QV> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
     constexpr int kSkChunk = 2 * QV;   // reals per register tile
-    constexpr int kSkQ = QV;
     pdl_entry();
     __shared__ double smem[kSkChunk * 32];
-    extern __shared__ double kk[];   // 3K doubles; mixed: then 3K floats and a table chunk
-    float *kf = reinterpret_cast<float *>(kk + 3 * d.K);
-    float *tc = kf + 3 * d.K;
-    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) {
-        kk[t] = d.k[t];
-        if (!FP64) kf[t] = (float)d.k[t];
-    }
+    extern __shared__ double kk[];   // 3K
+    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
     __syncthreads();
     double cnt = 0.0;
-    for (int k0 = 0; k0 < d.K; k0 += kSkChunk / 2) {
-        if (!FP64) {
-            load_tab_chunk<kSkQ>(d, k0, tc);
-            __syncthreads();
-        }
+    for (int k0 = 0; k0 < d.K; k0 += QV) {
         double acc[kSkChunk];
-        // mixed precision: a thread's few atoms (grid-stride, about n / (1184 * 256))
+        // mixed precision: a thread's few atoms (grid-stride, about n / (592 * 256))
         // are summed in FP32, every sum across threads and blocks in FP64
         float facc[kSkChunk];
 #pragma unroll
@@ -236,26 +183,19 @@ template <bool FP64, int QV> __global__ void __launch_bounds__(256) k_sk_partial
             if (d.mask && !(d.mask[i] & d.groupbit)) continue;
             if (k0 == 0) cnt += 1.0;
             const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
-            TabCell tcell{};
-            if (!FP64) tcell = tab_cell(d, x, y, z);
 #pragma unroll
-            for (int q = 0; q < kSkChunk / 2; ++q) {
+            for (int q = 0; q < QV; ++q) {
                 const int kq = k0 + q;
                 if (kq < d.K) {
+                    const double ph = kk[3 * kq] * x + kk[3 * kq + 1] * y + kk[3 * kq + 2] * z;
                     if (FP64) {
-                        const double ph = kk[3 * kq] * x + kk[3 * kq + 1] * y + kk[3 * kq + 2] * z;
                         double s, c;
                         sincos(ph, &s, &c);
                         acc[2 * q] += c;
                         acc[2 * q + 1] += s;
                     } else {
                         float s, c;
-                        if (tcell.in) {
-                            sincos_f32_reduced(tab_phase<kSkQ>(tc, d.tstride, q, tcell, kf + 3 * kq), s, c);
-                        } else {
-                            const double ph = kk[3 * kq] * x + kk[3 * kq + 1] * y + kk[3 * kq + 2] * z;
-                            phase_sincos_f32(ph, s, c);
-                        }
+                        phase_sincos_f32(ph, s, c);
                         facc[2 * q] += c;
                         facc[2 * q + 1] += s;
                     }
@@ -268,7 +208,7 @@ template <bool FP64, int QV> __global__ void __launch_bounds__(256) k_sk_partial
         }
         block_sum<kSkChunk>(acc, smem);
         if (threadIdx.x == 0)
-            for (int q = 0; q < kSkChunk / 2; ++q)
+            for (int q = 0; q < QV; ++q)
                 if (k0 + q < d.K) {
                     d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * (k0 + q)] = acc[2 * q];
                     d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * (k0 + q) + 1] = acc[2 * q + 1];
@@ -294,7 +234,7 @@ __global__ void __launch_bounds__(256) k_sk_reduce(SkDev d) {
     }
 }
 
-template <bool FP64>
+template <bool FP64, int U>
 __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restrict__ f_src, double *__restrict__ f_dst,
                                                   SysDev s, CellGrid g, double *vpart) {
     pdl_entry();
@@ -322,6 +262,7 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
         if (i < d.nown && (!d.mask || (d.mask[i] & d.groupbit))) {
             const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
             if (FP64) {
+#pragma unroll U
                 for (int q = 0; q < d.K; ++q) {
                     const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
                     double sn, cs;
@@ -333,6 +274,7 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
                 }
             } else {
                 float fx = 0.f, fy = 0.f, fz = 0.f;
+#pragma unroll U
                 for (int q = 0; q < d.K; ++q) {
                     const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
                     float sn, cs;
@@ -371,90 +313,6 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
     }
 }
 
-// Mixed precision force pass with the phase tables: each thread keeps the
-// gradient of up to kSkAtoms atoms (grid stride) while the k-vectors pass by
-// in chunks whose tables are staged in shared memory; the block's virial
-// partial goes to vpart[blockIdx.x] and block 0 zeroes the partials of the
-// one-atom-per-thread layout beyond the grid.
-template <int kSkQF>
-__global__ void __launch_bounds__(256) k_sk_force_tab(SkDev d, const double *__restrict__ f_src,
-                                                      double *__restrict__ f_dst, SysDev s, CellGrid g,
-                                                      double *vpart, int nparts) {
-    pdl_entry();
-    __shared__ double smem[6 * 32];
-    extern __shared__ double kk[];   // 3K doubles, 3K floats (k), 2K floats (rho), the table chunk
-    float *kf = reinterpret_cast<float *>(kk + 3 * d.K);
-    float *rrf = kf + 3 * d.K;
-    float *tc = rrf + 2 * d.K;
-    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) {
-        kk[t] = d.k[t];
-        kf[t] = (float)d.k[t];
-    }
-    for (int t = threadIdx.x; t < 2 * d.K; t += blockDim.x) rrf[t] = (float)d.rho[t];
-    const int stride = gridDim.x * blockDim.x;
-    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
-    float fx[kSkAtoms], fy[kSkAtoms], fz[kSkAtoms];
-#pragma unroll
-    for (int j = 0; j < kSkAtoms; ++j) fx[j] = fy[j] = fz[j] = 0.f;
-    for (int k0 = 0; k0 < d.K; k0 += kSkQF) {
-        __syncthreads();
-        load_tab_chunk<kSkQF>(d, k0, tc);
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < kSkAtoms; ++j) {
-            const int i = i0 + j * stride;
-            if (i >= d.nown || (d.mask && !(d.mask[i] & d.groupbit))) continue;
-            const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
-            const TabCell tcell = tab_cell(d, x, y, z);
-            for (int q = 0; q < kSkQF && k0 + q < d.K; ++q) {
-                const int kq = k0 + q;
-                float sn, cs;
-                if (tcell.in) {
-                    sincos_f32_reduced(tab_phase<kSkQF>(tc, d.tstride, q, tcell, kf + 3 * kq), sn, cs);
-                } else {
-                    const double ph = kk[3 * kq] * x + kk[3 * kq + 1] * y + kk[3 * kq + 2] * z;
-                    phase_sincos_f32(ph, sn, cs);
-                }
-                const float w = fmaf(rrf[2 * kq + 1], cs, -rrf[2 * kq] * sn);
-                fx[j] = fmaf(w, kf[3 * kq], fx[j]);
-                fy[j] = fmaf(w, kf[3 * kq + 1], fy[j]);
-                fz[j] = fmaf(w, kf[3 * kq + 2], fz[j]);
-            }
-        }
-    }
-    const double a = d.coef[0];
-    double vir[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int j = 0; j < kSkAtoms; ++j) {
-        const int i = i0 + j * stride;
-        if (i >= d.n) continue;
-        const double gx = -a * (double)fx[j], gy = -a * (double)fy[j], gz = -a * (double)fz[j];
-        f_dst[3 * i] = f_src[3 * i] + gx;
-        f_dst[3 * i + 1] = f_src[3 * i + 1] + gy;
-        f_dst[3 * i + 2] = f_src[3 * i + 2] + gz;
-        if (vpart) {
-            double ux = d.x[3 * i], uy = d.x[3 * i + 1], uz = d.x[3 * i + 2];
-            if (s.image) {
-                int ix, iy, iz;
-                unpack_image(s.image[i], ix, iy, iz);
-                ux += ix * g.L[0];
-                uy += iy * g.L[1];
-                uz += iz * g.L[2];
-            }
-            vir[0] += gx * ux; vir[1] += gy * uy; vir[2] += gz * uz;
-            vir[3] += gx * uy; vir[4] += gx * uz; vir[5] += gy * uz;
-        }
-    }
-    if (vpart) {
-        block_sum<6>(vir, smem);
-        if (threadIdx.x == 0)
-            for (int t = 0; t < 6; ++t) vpart[blockIdx.x * 8 + t] = vir[t];
-        if (blockIdx.x == 0)
-            for (int b = gridDim.x + threadIdx.x; b < nparts; b += blockDim.x)
-                for (int t = 0; t < 6; ++t) vpart[(size_t)b * 8 + t] = 0.0;
-    }
-}
-
 }  // namespace
 
 template <typename T> void launch_debye_values(const DebyeDev<T> &d, cudaStream_t st) {
@@ -482,49 +340,23 @@ int sk_blocks(int n) {
     return b < kSkBlocks ? (b < 1 ? 1 : b) : kSkBlocks;
 }
 
-// Dynamic shared memory above the 48 KB default (the phase-table chunks of a
-// large K or a long box), granted once per kernel.
-template <typename K> static void allow_smem(K kernel, size_t bytes) {
-    if (bytes > 48 * 1024)
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+template <int QV> static void launch_sk_partial_q(const SkDev &d, size_t sm, cudaStream_t st) {
+    if (d.fp64) launch_k(k_sk_partial<true, QV>, d.nblocks, 256, sm, st, d);
+    else launch_k(k_sk_partial<false, QV>, d.nblocks, 256, sm, st, d);
 }
 
-size_t sk_table_smem(const SkDev &d, int q) { return sizeof(float) * 3 * q * (size_t)d.tstride; }
-
-template <int QV> static void launch_sk_partial_mixed(const SkDev &d, cudaStream_t st) {
-    const size_t sm = (sizeof(double) + sizeof(float)) * 3 * (size_t)d.K + sk_table_smem(d, QV);
-    allow_smem(k_sk_partial<false, QV>, sm);
-    launch_k(k_sk_partial<false, QV>, d.nblocks, 256, sm, st, d);
-}
-
-template <int QF>
-static void launch_sk_force_mixed(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s,
-                                  const CellGrid &g, double *vpart, int nb, cudaStream_t st) {
-    const int tb = (d.n + 256 * kSkAtoms - 1) / (256 * kSkAtoms);   // kSkAtoms atoms per thread
-    const size_t sm = sizeof(double) * 3 * (size_t)d.K + sizeof(float) * 5 * (size_t)d.K + sk_table_smem(d, QF);
-    allow_smem(k_sk_force_tab<QF>, sm);
-    launch_k(k_sk_force_tab<QF>, tb, 256, sm, st, d, f_src, f_dst, s, g, vpart, nb);
-}
-
-size_t sk_smem_values(const SkDev &d, int qv) {
-    return (sizeof(double) + sizeof(float)) * 3 * (size_t)d.K + sk_table_smem(d, qv);
-}
-size_t sk_smem_force(const SkDev &d, int qf) {
-    return sizeof(double) * 3 * (size_t)d.K + sizeof(float) * 5 * (size_t)d.K + sk_table_smem(d, qf);
+template <int U>
+static void launch_sk_force_u(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
+                              double *vpart, size_t sm, int nb, cudaStream_t st) {
+    if (d.fp64) launch_k(k_sk_force<true, U>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
+    else launch_k(k_sk_force<false, U>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
 }
 
 void launch_sk_values(const SkDev &d, cudaStream_t st) {
-    if (d.fp64) {
-        const size_t sm = sizeof(double) * 3 * (size_t)d.K;
-        allow_smem(k_sk_partial<true, 8>, sm);
-        launch_k(k_sk_partial<true, 8>, d.nblocks, 256, sm, st, d);
-    } else if (d.qv == 4) {
-        launch_sk_partial_mixed<4>(d, st);
-    } else if (d.qv == 16) {
-        launch_sk_partial_mixed<16>(d, st);
-    } else {
-        launch_sk_partial_mixed<8>(d, st);
-    }
+    const size_t sm = sizeof(double) * 3 * (size_t)d.K;
+    if (d.qv == 4) launch_sk_partial_q<4>(d, sm, st);
+    else if (d.qv == 16) launch_sk_partial_q<16>(d, sm, st);
+    else launch_sk_partial_q<8>(d, sm, st);
     prof_mark("sk_partial", st);
     launch_k(k_sk_reduce, 2 * d.K + 1, 256, 0, st, d);
     prof_mark("sk_reduce", st);
@@ -534,17 +366,10 @@ void launch_sk_forces(const SkDev &d, const double *f_src, double *f_dst, const 
                       double *vpart, cudaStream_t st) {
     if (d.n == 0) return;
     const int nb = (d.n + 255) / 256;
-    if (d.fp64) {
-        const size_t sm = sizeof(double) * 5 * (size_t)d.K;
-        allow_smem(k_sk_force<true>, sm);
-        launch_k(k_sk_force<true>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
-    } else if (d.qf == 8) {
-        launch_sk_force_mixed<8>(d, f_src, f_dst, s, g, vpart, nb, st);
-    } else if (d.qf == 16) {
-        launch_sk_force_mixed<16>(d, f_src, f_dst, s, g, vpart, nb, st);
-    } else {
-        launch_sk_force_mixed<32>(d, f_src, f_dst, s, g, vpart, nb, st);
-    }
+    const size_t sm = sizeof(double) * 3 * (size_t)d.K + (d.fp64 ? sizeof(double) * 2 : sizeof(float) * 5) * (size_t)d.K;
+    if (d.qf == 1) launch_sk_force_u<1>(d, f_src, f_dst, s, g, vpart, sm, nb, st);
+    else if (d.qf == 4) launch_sk_force_u<4>(d, f_src, f_dst, s, g, vpart, sm, nb, st);
+    else launch_sk_force_u<2>(d, f_src, f_dst, s, g, vpart, sm, nb, st);
     prof_mark("sk_force", st);
 }
 

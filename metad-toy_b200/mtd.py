@@ -341,7 +341,7 @@ class Metad:
         return r.value, bool(a.value)
 
     def sk_tiles(self):
-        """(value-pass, force-pass) k-tiles of the mixed-precision S(k) passes."""
+        """S(k) shapes: (k-vectors per value pass, unroll depth of the force pass)."""
         a, b = C.c_int(), C.c_int()
         self._check(lib().mtd_sk_tiles(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
