@@ -935,7 +935,7 @@ def main():
         hf.zero_()
         m.post_force(step, hx[step % len(hx)].numpy(), hf.numpy())
         step += 1
-    split = {k: v[1] / max(v[0], 1) for k, v in sorted(m.profile_report().items(), key=lambda kv: -kv[1][1])}
+    e2e_split = {k: v[1] / max(v[0], 1) for k, v in sorted(m.profile_report().items(), key=lambda kv: -kv[1][1])}
     m.profile(False)
 
     dev_ms, e2e_ms = max_over_ranks([dev_ms, e2e_s * 1e3], dist, "cuda")
@@ -990,7 +990,7 @@ def main():
                        "cv": [float(v) for v in m.cv]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps,
-                    "split_ms": split},
+                    "split_ms": e2e_split},
             "gpu_launches": launches * args.steps,
             "roofline": roof, "clocks": clocks, "cpu_baseline": cpu, "error_vs_fp64": err}
     if rank == 0:

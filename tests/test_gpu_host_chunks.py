@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _system():
-    x, L = systems.small_slab(seed=5, nxy=8, nz_fcc=4, nz_bcc=5, n_liq=900)
+    x, L = systems.small_slab(seed=5, nxy=12, nz_fcc=4, nz_bcc=6, n_liq=3000)
     return np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.05, 51), L)), L
 
 
