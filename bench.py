@@ -990,7 +990,9 @@ def main():
                        "cv": [float(v) for v in m.cv]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps,
-                    "split_ms": e2e_split},
+                    "split_ms": e2e_split,
+                    "copies": "x uploaded in 3 MB pieces; f (pinned) read and written in place by the force pass "
+                              "over the host link (zero copy), so its bytes cross PCIe inside that kernel"},
             "gpu_launches": launches * args.steps,
             "roofline": roof, "clocks": clocks, "cpu_baseline": cpu, "error_vs_fp64": err}
     if rank == 0:

@@ -645,39 +645,35 @@ template <typename T> void run_values(mtd_ctx *c, const CellGrid &g, const doubl
     }
 }
 
-// Forces: the first unit reads f_in, the later ones accumulate into f_out.
-template <typename T>
-void run_forces(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, const int *mask, const double *fin,
-                double *fout, bool virial) {
-    cudaStream_t st = c->st;
-    c->chunk_done = false;
-    // mtd_post_force with one STEINH L unit and no virial: the force pass runs
-    // in caller-order chunks and each chunk of f goes to the host while the
-    // next chunk is computed (the same per-atom arithmetic)
-    int used = 0;
+// The deck's one force-producing unit when it is a STEINH L unit, else null.
+Unit *single_local_unit(mtd_ctx *c) {
     Unit *only = nullptr;
+    int used = 0;
     for (Unit &u : c->units)
         if (u.used) {
             ++used;
             only = &u;
         }
-    if (c->chunk_host && !virial && used == 1 && only->kind == CAL_STEINH_L && c->n >= 4096 && c->copy_st) {
+    return used == 1 && only->kind == CAL_STEINH_L ? only : nullptr;
+}
+
+// Forces: the first unit reads f_in, the later ones accumulate into f_out.
+template <typename T>
+void run_forces(mtd_ctx *c, const SysDev &s, const CellGrid &g, const double *x, const int *mask, const double *fin,
+                double *fout, bool virial) {
+    cudaStream_t st = c->st;
+    // mtd_post_force on pinned host f (zero copy): the force pass runs over
+    // caller indices, so each warp reads and writes one contiguous stretch
+    // of the host array; the same per-atom arithmetic as the sorted order
+    if (c->zc_on && !virial) {
+        Unit *only = single_local_unit(c);
         LocalDev<T> d = local_dev<T>(c, *only, g);
         launch_local_lambda<T>(d, st);
         d.iperm = c->iperm;
-        for (int k = 0; k < kForceChunks; ++k) {
-            d.i0 = (int)((long long)c->n * k / kForceChunks);
-            d.i1 = (int)((long long)c->n * (k + 1) / kForceChunks);
-            launch_local_force_pass<T>(d, fin, fout, s, g, nullptr, c->d_status, st);
-            cudaEventRecord(c->chunk_ev[k], st);
-            cudaStreamWaitEvent(c->copy_st, c->chunk_ev[k], 0);
-            cudaMemcpyAsync(c->chunk_host + 3 * (size_t)d.i0, fout + 3 * (size_t)d.i0,
-                            sizeof(double) * 3 * (size_t)(d.i1 - d.i0), cudaMemcpyDeviceToHost, c->copy_st);
-        }
-        cudaEventRecord(c->copies_done, c->copy_st);
-        cudaStreamWaitEvent(st, c->copies_done, 0);
-        c->launches += 1 + kForceChunks;
-        c->chunk_done = true;
+        d.i0 = 0;
+        d.i1 = c->n;
+        launch_local_force_pass<T>(d, fin, fout, s, g, nullptr, c->d_status, st);
+        c->launches += 2;
         return;
     }
     bool first = true;
@@ -1150,9 +1146,6 @@ mtd_status mtd_create(int narg, const char *const *arg, const mtd_options *opt, 
     c->own_st = c->st;
     cudaStreamCreateWithFlags(&c->side_st, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&c->f_ready, cudaEventDisableTiming);
-    cudaStreamCreateWithFlags(&c->copy_st, cudaStreamNonBlocking);
-    for (int k = 0; k < kForceChunks; ++k) cudaEventCreateWithFlags(&c->chunk_ev[k], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&c->copies_done, cudaEventDisableTiming);
     c->cv.assign(c->cfg.cv_dim, 0.0);
     mtd_status s = plan_units(c);
     if (s == MTD_OK) {
@@ -1205,10 +1198,6 @@ void mtd_destroy(mtd_ctx *c) {
         if (c->slot_ev[k]) cudaEventDestroy(c->slot_ev[k]);
     if (c->own_st) cudaStreamDestroy(c->own_st);
     if (c->side_st) cudaStreamDestroy(c->side_st);
-    if (c->copy_st) cudaStreamDestroy(c->copy_st);
-    for (int k = 0; k < kForceChunks; ++k)
-        if (c->chunk_ev[k]) cudaEventDestroy(c->chunk_ev[k]);
-    if (c->copies_done) cudaEventDestroy(c->copies_done);
     if (c->nb) mtd_nnbias_destroy(c->nb);
     dfree(c->d_vdv);
     dfree(c->d_ws1);
@@ -1328,20 +1317,36 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
     const size_t b3 = sizeof(double) * 3 * (size_t)n;
     const int *mask = has_mask ? c->d_mask : nullptr;
     mtd_status s = MTD_OK;
-    MTD_CU(cudaEventRecord(c->f_ready, c->st), "force upload");   // the side copies start after the previous step
-    MTD_CU(cudaStreamWaitEvent(c->side_st, c->f_ready, 0), "force upload");
-    MTD_CU(h2d_pieces(c->d_fin, f, b3, c->side_st), "f upload");
-    if (image && virial) MTD_CU(cudaMemcpyAsync(c->d_image, image, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->side_st), "image upload");
-    MTD_CU(cudaEventRecord(c->f_ready, c->side_st), "force upload");
+    // f in pinned host memory, one STEINH L unit, no virial: the force pass
+    // reads and writes f in place over the host link (zero copy), so no f
+    // upload or download runs beside the step
+    double *zf = nullptr;
+    if (!virial && n >= 4096 && single_local_unit(c)) {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, f) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer)
+            zf = static_cast<double *>(pa.devicePointer);
+        else
+            cudaGetLastError();
+    }
+    if (!zf) {
+        MTD_CU(cudaEventRecord(c->f_ready, c->st), "force upload");   // the side copies start after the previous step
+        MTD_CU(cudaStreamWaitEvent(c->side_st, c->f_ready, 0), "force upload");
+        MTD_CU(h2d_pieces(c->d_fin, f, b3, c->side_st), "f upload");
+        if (image && virial)
+            MTD_CU(cudaMemcpyAsync(c->d_image, image, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->side_st),
+                   "image upload");
+        MTD_CU(cudaEventRecord(c->f_ready, c->side_st), "force upload");
+    }
     for (int attempt = 0; attempt < 4; ++attempt) {
         MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
-        c->chunk_host = f;   // the force pass may copy f back in chunks as it goes
-        s = enqueue_step(c, step, n, c->d_x, mask, (image && virial) ? c->d_image : nullptr,
-                         c->d_fin, c->d_fout, virial != nullptr, c->f_ready);
-        c->chunk_host = nullptr;
+        c->zc_on = zf != nullptr;
+        s = enqueue_step(c, step, n, c->d_x, mask, (image && virial) ? c->d_image : nullptr, zf ? zf : c->d_fin,
+                         zf ? zf : c->d_fout, virial != nullptr, zf ? nullptr : c->f_ready);
+        c->zc_on = false;
         if (s != MTD_OK) return s;
-        // the forces go back in the same stream pass (a failed attempt's are overwritten by the retry)
-        if (!c->chunk_done) MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
+        // the forces go back in the same stream pass (a failed attempt's are
+        // overwritten by the retry; with zero copy a failed attempt writes f back unchanged)
+        if (!zf) MTD_CU(cudaMemcpyAsync(f, c->d_fout, b3, cudaMemcpyDeviceToHost, c->st), "f download");
         prof_mark("f_download", c->st);
         MTD_CU(cudaStreamSynchronize(c->st), "step");
         if (c->h_status->overflow == 0 && c->h_status->cand_overflow == 0) break;

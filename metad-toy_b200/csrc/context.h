@@ -110,8 +110,6 @@ struct PendingOut {
     bool virial;
 };
 
-constexpr int kForceChunks = 4;     // caller-order chunks of the host-buffer force pass
-
 struct mtd_ctx {
     int fp64 = 0;
     int device = 0;
@@ -180,13 +178,7 @@ struct mtd_ctx {
     SysDev last_sys{};
     cudaStream_t own_st = nullptr;
     cudaStream_t side_st = nullptr;      // host -> device force upload beside the CV passes
-    // mtd_post_force: the force pass in caller-order chunks, each chunk's
-    // forces copied to the host while the next chunk runs
-    cudaStream_t copy_st = nullptr;
-    cudaEvent_t chunk_ev[kForceChunks] = {};
-    cudaEvent_t copies_done = nullptr;
-    double *chunk_host = nullptr;        // the host f of the call in progress (null: no chunked copies)
-    bool chunk_done = false;             // the last force pass copied its chunks
+    bool zc_on = false;                  // this step's force pass reads and writes pinned host f in place
     // hill-list bias (CV_dim 4 or NN_BIAS 1): hills, exact sum, learned bias
     mtd_nnbias *nb = nullptr;
     double *d_vdv = nullptr;             // V, dV/ds at this step's s

@@ -143,15 +143,19 @@ __device__ __forceinline__ void local_q_body(const LocalDev<T> &d, int bid) {
         constexpr int KIND = STEP ? NK_STEP : NK_SWITCH;
         const float4 af = __ldg(d.fgf.pf + k);
         const int nc = min(__ldg(d.cand.count + k), d.cand.M);
+        // the next candidate's position and the one after's index in flight,
+        // so no load waits on another issued in the same iteration
         int jn = nc > 0 ? __ldg(d.cand.list + k) : 0;
         float4 bn = nc > 0 ? __ldg(d.fgf.pf + jn) : make_float4(0.f, 0.f, 0.f, 0.f);
+        int jn2 = nc > 1 ? __ldg(d.cand.list + (size_t)d.npad + k) : 0;
         for (int t = 0; t < nc; ++t) {
             const int j = jn;
             const float4 b = bn;
-            if (t + 1 < nc) {   // the next candidate's index and position in flight
-                jn = __ldg(d.cand.list + (size_t)(t + 1) * d.npad + k);
+            if (t + 1 < nc) {
+                jn = jn2;
                 bn = __ldg(d.fgf.pf + jn);
             }
+            if (t + 2 < nc) jn2 = __ldg(d.cand.list + (size_t)(t + 2) * d.npad + k);
             float fx, fy, fz;
             disp_f(d.fgf, af, b, fx, fy, fz);
             if (!decide<KIND>(d.fgd, d.fspec, d.fgd.xs, k, j, fx * fx + fy * fy + fz * fz)) continue;
@@ -180,9 +184,13 @@ __device__ __forceinline__ void local_q_body(const LocalDev<T> &d, int bid) {
         c = min(c, d.nb.M);
     } else {
         c = min(d.nb.count[k], d.nb.M);
+        // each neighbour's index is loaded an iteration ahead, so its record
+        // load waits on one memory latency instead of two
+        int jn = c > 0 ? nb_index(d.nb, d.npad, 0, k) : 0;
         for (int t = 0; t < c; ++t) {
             T ux, uy, uz, rinv, sg, dsg;
-            const int j = nb_index(d.nb, d.npad, t, k);
+            const int j = jn;
+            if (t + 1 < c) jn = nb_index(d.nb, d.npad, t + 1, k);
             pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
             nf += sg;
             ylm_accum<LA, T>(ux, uy, uz, sg, acc);
@@ -214,8 +222,12 @@ __device__ __forceinline__ void local_lq_body(const LocalDev<T> &d, int bid) {
             load_rec32(d.q + (size_t)k * S::SQ, A);
             const auto a = d.geo.load(k);
             const int c = min(d.nb.count[k], d.nb.M);
+            // each neighbour's index is loaded an iteration ahead, so its record
+            // load waits on one memory latency instead of two
+            int jn = c > 0 ? nb_index(d.nb, d.npad, 0, k) : 0;
             for (int t = 0; t < c; ++t) {
-                const int j = nb_index(d.nb, d.npad, t, k);
+                const int j = jn;
+                if (t + 1 < c) jn = nb_index(d.nb, d.npad, t + 1, k);
                 const T sg = pair_sigma<T, STEP>(d, a, j);
                 T qj[S::SQ];
                 load_rec32(d.q + (size_t)j * S::SQ, qj);
@@ -316,8 +328,12 @@ __device__ __forceinline__ void local_lambda_body(const LocalDev<T> &d, int bid)
     }
     const auto a = d.geo.load(k);
     const int c = min(d.nb.count[k], d.nb.M);
+    // each neighbour's index is loaded an iteration ahead, so its record
+    // load waits on one memory latency instead of two
+    int jn = c > 0 ? nb_index(d.nb, d.npad, 0, k) : 0;
     for (int t = 0; t < c; ++t) {
-        const int j = nb_index(d.nb, d.npad, t, k);
+        const int j = jn;
+        if (t + 1 < c) jn = nb_index(d.nb, d.npad, t + 1, k);
         T ej[4];
         load_rec(d.e12 + 4 * (size_t)j, ej);
         const T wjA = c1A * ej[0] + c2A * ej[1];
@@ -352,7 +368,7 @@ __device__ __forceinline__ void local_lambda_body(const LocalDev<T> &d, int bid)
 // Pass 4: gather forces, f_dst = f_src - dV/dx, plus the virial block partials.
 // One thread per sorted slot, or (d.iperm set) per caller index of d.i0 ..
 // d.i1 - 1, so a caller-order range of f is complete when its launch is.
-template <int LA, int LB, typename T, bool STEP>
+template <int LA, int LB, typename T, bool STEP, bool CALLER = false>
 __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const double *__restrict__ f_src,
                                                  double *__restrict__ f_dst, const SysDev &s, const CellGrid &g,
                                                  double *vpart, DevStatus *status, int bid) {
@@ -361,7 +377,7 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
     __shared__ double smem[6 * 32];
     int k, ic = 0;
     bool valid;
-    if (d.iperm) {
+    if constexpr (CALLER) {
         ic = d.i0 + bid * blockDim.x + threadIdx.x;
         valid = ic < d.i1;
         k = valid ? d.iperm[ic] : 0;
@@ -387,8 +403,12 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
         const int c = min(d.nb.count[k], d.nb.M);
         constexpr T sgnA = (LA & 1) ? T(-1) : T(1);
         constexpr T sgnB = (LB & 1) ? T(-1) : T(1);
+        // each neighbour's index is loaded an iteration ahead, so its record
+        // load waits on one memory latency instead of two
+        int jn = c > 0 ? nb_index(d.nb, d.npad, 0, k) : 0;
         for (int t = 0; t < c; ++t) {
-            const int j = nb_index(d.nb, d.npad, t, k);
+            const int j = jn;
+            if (t + 1 < c) jn = nb_index(d.nb, d.npad, t + 1, k);
             T ux, uy, uz, rinv, sg, dsg;
             pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
             T lj[S::SQ];
@@ -426,7 +446,7 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
                 }
             }
         }
-        const int i = d.iperm ? ic : d.perm[k];
+        const int i = CALLER ? ic : d.perm[k];
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;   // delta f = -dV/dx
         if ((unsigned)i < (unsigned)d.n) {   // a sorted order left by a rebuild that gave up is not trusted
             f_dst[3 * i] = f_src[3 * i] + fx;

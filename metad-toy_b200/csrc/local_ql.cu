@@ -45,12 +45,12 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
     local_lambda_body<LA, LB, T, STEP>(d, blockIdx.x);
 }
 
-template <int LA, int LB, typename T, bool STEP>
+template <int LA, int LB, typename T, bool STEP, bool CALLER = false>
 __global__ void __launch_bounds__(kBlock, 4) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
                                                         double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                         double *vpart, DevStatus *status) {
     pdl_entry();
-    local_force_body<LA, LB, T, STEP>(d, f_src, f_dst, s, g, vpart, status, blockIdx.x);
+    local_force_body<LA, LB, T, STEP, CALLER>(d, f_src, f_dst, s, g, vpart, status, blockIdx.x);
 }
 
 template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cudaStream_t st) {
@@ -84,10 +84,16 @@ void run_force_pass(const LocalDev<T> &d, const double *f_src, double *f_dst, co
     const int cnt = d.iperm ? d.i1 - d.i0 : d.n;
     if (cnt <= 0) return;
     const int nb = (cnt + kBlock - 1) / kBlock;
-    if (d.sw_r.type == SW_STEP)
+    if (d.iperm) {
+        if (d.sw_r.type == SW_STEP)
+            launch_k(k_local_force<LA, LB, T, true, true>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
+        else
+            launch_k(k_local_force<LA, LB, T, false, true>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
+    } else if (d.sw_r.type == SW_STEP) {
         launch_k(k_local_force<LA, LB, T, true>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
-    else
+    } else {
         launch_k(k_local_force<LA, LB, T, false>, nb, kBlock, 0, st, d, f_src, f_dst, s, g, vpart, status);
+    }
     prof_mark("local_force", st);
 }
 

@@ -1,0 +1,61 @@
+"""mtd_post_force on pinned host f with one STEINH L unit and no virial: the
+force pass reads and writes f in place over the host link (zero copy), one
+thread per caller index so each warp touches one contiguous stretch of f.
+The per-atom arithmetic is the sorted-order pass's, so forces, CVs and bias
+equal the device-buffer path (mtd_post_force_device) bit for bit.  Pageable
+host f, or the virial asked for, take the upload / download path with the
+same forces."""
+import numpy as np
+import pytest
+
+import helpers as H
+import mtd
+import systems
+
+pytestmark = pytest.mark.gpu
+
+
+def _system():
+    x, L = systems.small_slab(seed=5, nxy=12, nz_fcc=4, nz_bcc=6, n_liq=3000)
+    return np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.05, 51), L)), L
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("skin", [False, True])
+def test_zero_copy_host_forces_equal_device_path(precision, skin):
+    import torch
+
+    x0, L = _system()
+    assert x0.shape[0] >= 4096
+    args = H.fix_args_local(pace=2) + (["NEIGH_SKIN", 0.6] if skin else [])
+    xs = [np.ascontiguousarray(systems.wrap(systems.jitter(x0, 0.02, 90 + s), L)) for s in range(4)]
+    host = mtd.Metad(args, precision=precision)
+    dev = mtd.Metad(args, precision=precision)
+    for m in (host, dev):
+        m.set_box([0, 0, 0], L)
+    for s, x in enumerate(xs):
+        f_in = np.random.default_rng(s).normal(size=x.shape)
+        fh = torch.from_numpy(f_in.copy()).pin_memory()   # pinned: the zero-copy path
+        host.post_force(s, x, fh.numpy())
+        dx = torch.from_numpy(x).cuda()
+        df_in = torch.from_numpy(f_in).cuda()
+        df = torch.empty_like(df_in)
+        dev.post_force_device(s, x.shape[0], dx.data_ptr(), df_in.data_ptr(), df.data_ptr())
+        dev.sync()
+        assert np.array_equal(fh.numpy(), df.cpu().numpy())
+        assert np.array_equal(host.cv, dev.cv) and host.compute_scalar() == dev.compute_scalar()
+    host.close()
+    dev.close()
+    # the same first step through pageable f and with the virial (upload / download path)
+    outs = []
+    for mode in ("pinned", "pageable", "virial"):
+        m = mtd.Metad(args, precision=precision)
+        m.set_box([0, 0, 0], L)
+        f = torch.zeros(xs[0].shape, dtype=torch.float64)
+        f = f.pin_memory() if mode == "pinned" else f
+        vir = m.post_force(0, xs[0], f.numpy(), virial=(mode == "virial"))
+        outs.append(f.numpy().copy())
+        if mode == "virial":
+            assert np.all(np.isfinite(vir))
+        m.close()
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
