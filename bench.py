@@ -926,6 +926,22 @@ def main():
             e2e_s += time.perf_counter() - t0
             step += 1
     clocks = clk.summary()
+    # the three ways f can cross the host link (mtd_set_host_copy_mode), same forces
+    copy_modes = {}
+    for mode in (1, 2, 3):
+        m.set_host_copy_mode(mode)
+        t = 0.0
+        for k in range(max(5, args.steps // 2)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            hf.zero_()
+            t0 = time.perf_counter()
+            m.post_force(step, hx[step % len(hx)].numpy(), hf.numpy())
+            t += time.perf_counter() - t0
+            step += 1
+        copy_modes[{1: "copies", 2: "upload + zero-copy write", 3: "zero copy both ways"}[mode]] = \
+            t * 1e3 / max(5, args.steps // 2)
+    m.set_host_copy_mode(0)
     # where the end-to-end step goes: the library's event marks around the
     # host copies and kernels of a few more calls (a separate, untimed pass)
     m.profile(True)
@@ -991,8 +1007,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps,
                     "split_ms": e2e_split,
-                    "copies": "x uploaded in 3 MB pieces; f (pinned) read and written in place by the force pass "
-                              "over the host link (zero copy), so its bytes cross PCIe inside that kernel"},
+                    "copies": "x uploaded in 3 MB pieces; f (pinned) uploaded on a side stream during the CV "
+                              "passes and written back by the force pass over the host link (zero copy, the "
+                              "library's default host-copy mode)",
+                    "host_copy_modes_ms_per_step": copy_modes},
             "gpu_launches": launches * args.steps,
             "roofline": roof, "clocks": clocks, "cpu_baseline": cpu, "error_vs_fp64": err}
     if rank == 0:

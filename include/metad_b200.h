@@ -206,6 +206,18 @@ mtd_status mtd_neighbor_stats(mtd_ctx *ctx, int64_t *rebuilds, int *skin_active)
  * Extension (the reference has no device-side rebuild). */
 mtd_status mtd_neighbor_set_wait(mtd_ctx *ctx, int limit, int stall);
 
+/* How mtd_post_force / mtd_step move f (n x 3 FP64) over the host link when
+ * f is pinned host memory, the deck has one STEINH L unit and no virial is
+ * asked for (otherwise mode 1 applies):
+ *   1  f uploaded on a side stream during the CV passes, downloaded after;
+ *   2  f uploaded as in 1, written back by the force pass itself (zero copy,
+ *      one thread per caller index so every warp writes one contiguous
+ *      stretch), no download;
+ *   3  f read and written in place by the force pass (zero copy both ways).
+ * 0 (default) is mode 2.  Forces are bitwise identical in every mode; the
+ * fastest depends on the host platform.  Extension (no counterpart). */
+mtd_status mtd_set_host_copy_mode(mtd_ctx *ctx, int mode);
+
 /* Replays a HILLS file into the grid (rows `step cv[D] height sigma`).
  * Replaces GH_t0_uniformGrid::init_hills (src/grids/GH_t0_uniformGrid.cu:101-192). */
 mtd_status mtd_hills_replay(mtd_ctx *ctx, const char *path);

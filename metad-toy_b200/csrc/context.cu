@@ -1318,17 +1318,19 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
     const int *mask = has_mask ? c->d_mask : nullptr;
     mtd_status s = MTD_OK;
     // f in pinned host memory, one STEINH L unit, no virial: the force pass
-    // reads and writes f in place over the host link (zero copy), so no f
-    // upload or download runs beside the step
+    // writes f over the host link in caller order (zero copy, no download),
+    // and with mode 3 also reads it there (no upload)
     double *zf = nullptr;
-    if (!virial && n >= 4096 && single_local_unit(c)) {
+    const int mode = c->host_copy_mode == 0 ? 2 : c->host_copy_mode;
+    if (mode >= 2 && !virial && n >= 4096 && single_local_unit(c)) {
         cudaPointerAttributes pa{};
         if (cudaPointerGetAttributes(&pa, f) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer)
             zf = static_cast<double *>(pa.devicePointer);
         else
             cudaGetLastError();
     }
-    if (!zf) {
+    const bool upload = !zf || mode == 2;
+    if (upload) {
         MTD_CU(cudaEventRecord(c->f_ready, c->st), "force upload");   // the side copies start after the previous step
         MTD_CU(cudaStreamWaitEvent(c->side_st, c->f_ready, 0), "force upload");
         MTD_CU(h2d_pieces(c->d_fin, f, b3, c->side_st), "f upload");
@@ -1340,8 +1342,8 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
     for (int attempt = 0; attempt < 4; ++attempt) {
         MTD_CU(cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->st), "status");
         c->zc_on = zf != nullptr;
-        s = enqueue_step(c, step, n, c->d_x, mask, (image && virial) ? c->d_image : nullptr, zf ? zf : c->d_fin,
-                         zf ? zf : c->d_fout, virial != nullptr, zf ? nullptr : c->f_ready);
+        s = enqueue_step(c, step, n, c->d_x, mask, (image && virial) ? c->d_image : nullptr, upload ? c->d_fin : zf,
+                         zf ? zf : c->d_fout, virial != nullptr, upload ? c->f_ready : nullptr);
         c->zc_on = false;
         if (s != MTD_OK) return s;
         // the forces go back in the same stream pass (a failed attempt's are

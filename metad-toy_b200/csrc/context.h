@@ -178,7 +178,8 @@ struct mtd_ctx {
     SysDev last_sys{};
     cudaStream_t own_st = nullptr;
     cudaStream_t side_st = nullptr;      // host -> device force upload beside the CV passes
-    bool zc_on = false;                  // this step's force pass reads and writes pinned host f in place
+    bool zc_on = false;                  // this step's force pass writes pinned host f in caller order
+    int host_copy_mode = 0;              // mtd_set_host_copy_mode
     // hill-list bias (CV_dim 4 or NN_BIAS 1): hills, exact sum, learned bias
     mtd_nnbias *nb = nullptr;
     double *d_vdv = nullptr;             // V, dV/ds at this step's s

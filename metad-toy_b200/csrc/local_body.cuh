@@ -377,11 +377,19 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
     __shared__ double smem[6 * 32];
     int k, ic = 0;
     bool valid;
+    double fin[3] = {0.0, 0.0, 0.0};
     if constexpr (CALLER) {
         ic = d.i0 + bid * blockDim.x + threadIdx.x;
         valid = ic < d.i1;
         k = valid ? d.iperm[ic] : 0;
         valid = valid && (unsigned)k < (unsigned)d.n;
+        // f_src may be host memory read over the host link: its load is
+        // issued first so its latency passes under the neighbour loop
+        if (valid) {
+            fin[0] = f_src[3 * ic];
+            fin[1] = f_src[3 * ic + 1];
+            fin[2] = f_src[3 * ic + 2];
+        }
     } else {
         k = bid * blockDim.x + threadIdx.x;
         valid = k < d.n;
@@ -448,7 +456,11 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
         }
         const int i = CALLER ? ic : d.perm[k];
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;   // delta f = -dV/dx
-        if ((unsigned)i < (unsigned)d.n) {   // a sorted order left by a rebuild that gave up is not trusted
+        if constexpr (CALLER) {
+            f_dst[3 * i] = fin[0] + fx;
+            f_dst[3 * i + 1] = fin[1] + fy;
+            f_dst[3 * i + 2] = fin[2] + fz;
+        } else if ((unsigned)i < (unsigned)d.n) {   // a sorted order left by a rebuild that gave up is not trusted
             f_dst[3 * i] = f_src[3 * i] + fx;
             f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
             f_dst[3 * i + 2] = f_src[3 * i + 2] + fz;

@@ -105,6 +105,12 @@ mtd_status mtd_neighbor_stats(mtd_ctx *c, int64_t *rebuilds, int *skin_active) {
     return MTD_OK;
 }
 
+mtd_status mtd_set_host_copy_mode(mtd_ctx *c, int mode) {
+    if (!c || mode < 0 || mode > 3) return MTD_ERR_INVALID_ARG;
+    c->host_copy_mode = mode;
+    return MTD_OK;
+}
+
 mtd_status mtd_neighbor_set_wait(mtd_ctx *c, int limit, int stall) {
     if (!c || limit < 0) return MTD_ERR_INVALID_ARG;
     c->rebuild_limit = limit > 0 ? limit : (1 << 22);

@@ -1,10 +1,10 @@
 """mtd_post_force on pinned host f with one STEINH L unit and no virial: the
-force pass reads and writes f in place over the host link (zero copy), one
-thread per caller index so each warp touches one contiguous stretch of f.
-The per-atom arithmetic is the sorted-order pass's, so forces, CVs and bias
-equal the device-buffer path (mtd_post_force_device) bit for bit.  Pageable
-host f, or the virial asked for, take the upload / download path with the
-same forces."""
+force pass writes f over the host link (zero copy; with host-copy mode 3 it
+also reads it there), one thread per caller index so each warp touches one
+contiguous stretch of f.  The per-atom arithmetic is the sorted-order pass's,
+so forces, CVs and bias equal the device-buffer path (mtd_post_force_device)
+bit for bit in every mode.  Pageable host f, or the virial asked for, take
+the upload / download path with the same forces."""
 import numpy as np
 import pytest
 
@@ -46,16 +46,18 @@ def test_zero_copy_host_forces_equal_device_path(precision, skin):
         assert np.array_equal(host.cv, dev.cv) and host.compute_scalar() == dev.compute_scalar()
     host.close()
     dev.close()
-    # the same first step through pageable f and with the virial (upload / download path)
+    # the same first step through every host-copy mode, pageable f and the
+    # virial (upload / download path): the same forces
     outs = []
-    for mode in ("pinned", "pageable", "virial"):
+    for mode in ("copies", "zc_write", "zc_both", "pageable", "virial"):
         m = mtd.Metad(args, precision=precision)
         m.set_box([0, 0, 0], L)
+        m.set_host_copy_mode({"copies": 1, "zc_write": 2, "zc_both": 3}.get(mode, 0))
         f = torch.zeros(xs[0].shape, dtype=torch.float64)
-        f = f.pin_memory() if mode == "pinned" else f
+        f = f.pin_memory() if mode in ("copies", "zc_write", "zc_both") else f
         vir = m.post_force(0, xs[0], f.numpy(), virial=(mode == "virial"))
         outs.append(f.numpy().copy())
         if mode == "virial":
             assert np.all(np.isfinite(vir))
         m.close()
-    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
