@@ -375,21 +375,22 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
     using S = LSet<LA, LB, T>;
     constexpr bool DSIG = !STEP;
     __shared__ double smem[6 * 32];
-    int k, ic = 0;
+    // caller order: the block's stretch of f (3 x blockDim doubles, which
+    // may be host memory over the host link) is read into shared memory and
+    // written back from it with consecutive threads on consecutive doubles,
+    // so every warp access is whole 128-byte lines
+    __shared__ double fstage[CALLER ? 3 * kBlock : 1];
+    int k, ic = 0, ib0 = 0, cnt = 0;
     bool valid;
-    double fin[3] = {0.0, 0.0, 0.0};
     if constexpr (CALLER) {
-        ic = d.i0 + bid * blockDim.x + threadIdx.x;
-        valid = ic < d.i1;
+        ib0 = d.i0 + bid * blockDim.x;
+        cnt = max(0, min((int)blockDim.x, d.i1 - ib0));
+        for (int e = threadIdx.x; e < 3 * cnt; e += blockDim.x) fstage[e] = f_src[3 * (size_t)ib0 + e];
+        __syncthreads();
+        ic = ib0 + threadIdx.x;
+        valid = (int)threadIdx.x < cnt;
         k = valid ? d.iperm[ic] : 0;
         valid = valid && (unsigned)k < (unsigned)d.n;
-        // f_src may be host memory read over the host link: its load is
-        // issued first so its latency passes under the neighbour loop
-        if (valid) {
-            fin[0] = f_src[3 * ic];
-            fin[1] = f_src[3 * ic + 1];
-            fin[2] = f_src[3 * ic + 2];
-        }
     } else {
         k = bid * blockDim.x + threadIdx.x;
         valid = k < d.n;
@@ -457,9 +458,9 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
         const int i = CALLER ? ic : d.perm[k];
         const double fx = -(double)gx, fy = -(double)gy, fz = -(double)gz;   // delta f = -dV/dx
         if constexpr (CALLER) {
-            f_dst[3 * i] = fin[0] + fx;
-            f_dst[3 * i + 1] = fin[1] + fy;
-            f_dst[3 * i + 2] = fin[2] + fz;
+            fstage[3 * threadIdx.x] += fx;
+            fstage[3 * threadIdx.x + 1] += fy;
+            fstage[3 * threadIdx.x + 2] += fz;
         } else if ((unsigned)i < (unsigned)d.n) {   // a sorted order left by a rebuild that gave up is not trusted
             f_dst[3 * i] = f_src[3 * i] + fx;
             f_dst[3 * i + 1] = f_src[3 * i + 1] + fy;
@@ -478,6 +479,10 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
             vir[0] = fx * ux_; vir[1] = fy * uy_; vir[2] = fz * uz_;
             vir[3] = fx * uy_; vir[4] = fx * uz_; vir[5] = fy * uz_;
         }
+    }
+    if constexpr (CALLER) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < 3 * cnt; e += blockDim.x) f_dst[3 * (size_t)ib0 + e] = fstage[e];
     }
     if (vpart) {
         block_sum<6>(vir, smem);
