@@ -995,8 +995,7 @@ def main():
                                                  "library stream; ghost-force reverse communication is the MD "
                                                  "code's and is not timed" % (world, m.ghost_cutoff)}[split],
                        "atoms_per_rank": {"owned": int(nown), "with_ghosts": int(n)},
-                       "autotuned_shapes": {"neighbors": ["fast/256", "fast/128", "flat/128"][tuned[0]],
-                                            "q_block": tuned[1], "lambda_block": tuned[2]},
+                       "autotuned_shapes": dict(m.tuning(), neighbors=["fast/256", "fast/128", "flat/128"][tuned[0]]),
                        "neighbor_lists": {"skin_A": SKIN, "rebuild_every_steps": EVERY,
                                           "rebuild_when_moved_A": SKIN / 2, "skin_active": skin_active,
                                           "rebuilds_in_timed_steps": builds_timed,

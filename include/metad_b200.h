@@ -260,6 +260,11 @@ mtd_status mtd_set_tuning(mtd_ctx *ctx, int neighbor_shape, int q_block, int lam
  * pass's loop over k (1, 2 or 4).  Every k is summed in the same order
  * whatever the shape, so the results are bitwise identical.  Defaults 8, 2. */
 mtd_status mtd_sk_tiles(mtd_ctx *ctx, int *q_values, int *q_force);
+/* Every tuned shape: neighbour search, q block, lambda block (0 = 256),
+ * skin-list q pass with its filter in a separate loop (1) or merged with the
+ * sum (0), S(k) value-pass k-tile and force-pass unroll. */
+mtd_status mtd_get_tuning(mtd_ctx *ctx, int out[6]);
+mtd_status mtd_set_tuning_all(mtd_ctx *ctx, const int in[6]);
 mtd_status mtd_set_sk_tiles(mtd_ctx *ctx, int q_values, int q_force);
 
 /* Atom types (caller order, n values, host array) for `STRU_FACTOR ...

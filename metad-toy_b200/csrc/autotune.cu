@@ -67,19 +67,23 @@ mtd_status autotune_idle(mtd_ctx *c, int n, const double *d_x, const int *d_mask
     }
     const int shapes[2] = {256, 128};
     best = 1e30f;
-    int bq = 256;
-    for (int qb : shapes) {
-        c->tune_q = qb;
-        const float t = timed([&] {
-            if (c->fp64) run_values<double>(c, g, d_x, d_mask);
-            else run_values<float>(c, g, d_x, d_mask);
-        });
-        if (t < best) {
-            best = t;
-            bq = qb;
+    int bq = 256, bs = 0;
+    for (int split = 0; split < (c->skin_last ? 2 : 1); ++split)
+        for (int qb : shapes) {
+            c->tune_q = qb;
+            c->tune_qsplit = split;
+            const float t = timed([&] {
+                if (c->fp64) run_values<double>(c, g, d_x, d_mask);
+                else run_values<float>(c, g, d_x, d_mask);
+            });
+            if (t < best) {
+                best = t;
+                bq = qb;
+                bs = split;
+            }
         }
-    }
     c->tune_q = bq;
+    c->tune_qsplit = bs;
     best = 1e30f;
     int bl = 256;
     for (int lb : shapes) {
@@ -155,6 +159,28 @@ mtd_status mtd_autotune(mtd_ctx *c, int n, const double *d_x, const int *d_mask,
     const mtd_status s = mtd_sync(c);
     if (s != MTD_OK) return s;
     return autotune_idle(c, n, d_x, d_mask, reps, choice);
+}
+
+mtd_status mtd_get_tuning(mtd_ctx *c, int out[6]) {
+    if (!c || !out) return MTD_ERR_INVALID_ARG;
+    out[0] = c->tune_nbr;
+    out[1] = c->tune_q;
+    out[2] = c->tune_l;
+    out[3] = c->tune_qsplit;
+    out[4] = c->tune_skq;
+    out[5] = c->tune_skqf;
+    return MTD_OK;
+}
+
+mtd_status mtd_set_tuning_all(mtd_ctx *c, const int in[6]) {
+    if (!c || !in) return MTD_ERR_INVALID_ARG;
+    mtd_status s = mtd_set_tuning(c, in[0], in[1], in[2]);
+    if (s != MTD_OK) return s;
+    if (in[3] != 0 && in[3] != 1) return MTD_ERR_INVALID_ARG;
+    s = mtd_set_sk_tiles(c, in[4], in[5]);
+    if (s != MTD_OK) return s;
+    c->tune_qsplit = in[3];
+    return MTD_OK;
 }
 
 mtd_status mtd_sk_tiles(mtd_ctx *c, int *q_values, int *q_force) {

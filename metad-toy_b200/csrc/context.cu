@@ -573,6 +573,7 @@ template <typename T> LocalDev<T> local_dev(mtd_ctx *c, Unit &u, const CellGrid 
     d.lam = (T *)u.lam; d.g = (T *)u.g; d.tu = (T *)u.tu; d.partials = u.partials; d.coef = u.coef;
     d.qblock = c->tune_q;
     d.lblock = c->tune_l;
+    d.qsplit = c->tune_qsplit;
     return d;
 }
 

@@ -193,6 +193,7 @@ struct mtd_ctx {
     // kernel shapes chosen by mtd_autotune (every choice gives bitwise-identical results)
     int tune_nbr = 0;                    // neighbour search: 0 fast/256, 1 fast/128, 2 flat/128
     int tune_q = 0, tune_l = 0;          // threads per block of the q and lambda passes (0: 256)
+    int tune_qsplit = 0;                 // skin lists: the q pass's filter in its own loop (1) or merged (0)
     int tune_skq = 8, tune_skqf = 2;     // S(k): k-vectors per pass of the value pass, unroll of the force pass
     // per-atom dCV/dx export (compute metad/atom): last step's inputs, cached result
     const double *last_x = nullptr;

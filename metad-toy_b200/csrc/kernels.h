@@ -209,8 +209,9 @@ template <typename T> struct LocalDev {
     double *partials;           // [nblocks][8]: S1A S0A S1B S0B N
     const double *coef;         // c1A c2A c1B c2B (written by the bias kernel)
     int qblock, lblock;         // threads per block of the q and lambda passes (0: kBlock); same results
-    // skin lists: the q pass first filters this unit's candidates into nb (filter != 0)
-    int filter;
+    // skin lists: the q pass first filters this unit's candidates into nb (filter != 0),
+    // in one loop with the sum (qsplit 0) or in a filter loop before it (qsplit 1)
+    int filter, qsplit;
     GeoF fgf;                   // FP32 cell-relative positions (the exact decision's first test)
     GeoD fgd;                   // FP64 raw positions (the guard band)
     NeighSpec fspec;

@@ -115,7 +115,12 @@ __device__ __forceinline__ int nb_index(const NeighDev &nb, int npad, int t, int
 // Pass 1: q_lm and NF for every atom.  With skin lists (FILTER) the pass
 // first filters the atom's candidates into its exact list (the same
 // decisions as k_filter), then sums over that list.
-template <int LA, int LB, typename T, bool STEP, bool FILTER>
+// With skin lists the pass filters the candidates first: in one loop with the
+// sum (MERGED: the list is never read back) or in a filter loop followed by
+// the sum over the exact list (no lane of a warp waits on another lane's
+// Y_lm work during the filter).  Both sum in list order with the same
+// operations, so they give identical results; the autotuner picks one.
+template <int LA, int LB, typename T, bool STEP, bool FILTER, bool MERGED = true>
 __device__ __forceinline__ void local_q_body(const LocalDev<T> &d, int bid) {
     using S = LSet<LA, LB, T>;
     const int k = bid * blockDim.x + threadIdx.x;
@@ -136,7 +141,43 @@ __device__ __forceinline__ void local_q_body(const LocalDev<T> &d, int bid) {
     for (int t = 0; t < S::SQ; ++t) acc[t] = T(0);
     T nf = T(0);
     int c = 0;
-    if constexpr (FILTER) {
+    if constexpr (FILTER && !MERGED) {
+        constexpr int KIND = STEP ? NK_STEP : NK_SWITCH;
+        const float4 af = __ldg(d.fgf.pf + k);
+        const int nc = min(__ldg(d.cand.count + k), d.cand.M);
+        int jn = nc > 0 ? __ldg(d.cand.list + k) : 0;
+        float4 bn = nc > 0 ? __ldg(d.fgf.pf + jn) : make_float4(0.f, 0.f, 0.f, 0.f);
+        int jn2 = nc > 1 ? __ldg(d.cand.list + (size_t)d.npad + k) : 0;
+        for (int t = 0; t < nc; ++t) {
+            const int j = jn;
+            const float4 b = bn;
+            if (t + 1 < nc) {
+                jn = jn2;
+                bn = __ldg(d.fgf.pf + jn);
+            }
+            if (t + 2 < nc) jn2 = __ldg(d.cand.list + (size_t)(t + 2) * d.npad + k);
+            float fx, fy, fz;
+            disp_f(d.fgf, af, b, fx, fy, fz);
+            if (!decide<KIND>(d.fgd, d.fspec, d.fgd.xs, k, j, fx * fx + fy * fy + fz * fz)) continue;
+            if (c < d.nb.M) d.nb.list[(size_t)c * d.npad + k] = j;
+            ++c;
+        }
+        d.nb.count[k] = c;
+        if (c > d.nb.M) atomicMax(&d.status->overflow, (unsigned)c);
+        c = min(c, d.nb.M);
+        // the sum over the list just written (this thread's own entries,
+        // read back through the coherent path), index one iteration ahead
+        int jl = c > 0 ? d.nb.list[k] : 0;
+        for (int t = 0; t < c; ++t) {
+            T ux, uy, uz, rinv, sg, dsg;
+            const int j = jl;
+            if (t + 1 < c) jl = d.nb.list[(size_t)(t + 1) * d.npad + k];
+            pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
+            nf += sg;
+            ylm_accum<LA, T>(ux, uy, uz, sg, acc);
+            if constexpr (LB > 0) ylm_accum<LB, T>(ux, uy, uz, sg, acc + S::SA);
+        }
+    } else if constexpr (FILTER) {
         // one loop: each candidate is tested (the decisions of filter_atom)
         // and, when kept, written to the exact list and summed at once, so
         // the list is not read back; the sum runs in list order

@@ -27,10 +27,10 @@ namespace mtd {
 namespace {
 
 // The passes as kernels (local_body.cuh).
-template <int LA, int LB, typename T, bool STEP, bool FILTER>
+template <int LA, int LB, typename T, bool STEP, bool FILTER, bool MERGED = true>
 __global__ void __launch_bounds__(kBlock, 4) k_local_q(LocalDev<T> d) {
     pdl_entry();
-    local_q_body<LA, LB, T, STEP, FILTER>(d, blockIdx.x);
+    local_q_body<LA, LB, T, STEP, FILTER, MERGED>(d, blockIdx.x);
 }
 
 template <int LA, int LB, typename T, bool STEP>
@@ -57,13 +57,15 @@ template <int LA, int LB, typename T> void run_values(const LocalDev<T> &d, cuda
     const int nb = (d.n + kBlock - 1) / kBlock;
     const int qb = d.qblock > 0 ? d.qblock : kBlock, qg = (d.n + qb - 1) / qb;   // no block reduction in q
     if (d.sw_r.type == SW_STEP) {
-        if (d.filter) launch_k(k_local_q<LA, LB, T, true, true>, qg, qb, 0, st, d);
+        if (d.filter && d.qsplit) launch_k(k_local_q<LA, LB, T, true, true, false>, qg, qb, 0, st, d);
+        else if (d.filter) launch_k(k_local_q<LA, LB, T, true, true>, qg, qb, 0, st, d);
         else launch_k(k_local_q<LA, LB, T, true, false>, qg, qb, 0, st, d);
         prof_mark("local_q", st);
         launch_k(k_local_lq<LA, LB, T, true>, nb, kBlock, 0, st, d);
         prof_mark("local_lq", st);
     } else {
-        if (d.filter) launch_k(k_local_q<LA, LB, T, false, true>, qg, qb, 0, st, d);
+        if (d.filter && d.qsplit) launch_k(k_local_q<LA, LB, T, false, true, false>, qg, qb, 0, st, d);
+        else if (d.filter) launch_k(k_local_q<LA, LB, T, false, true>, qg, qb, 0, st, d);
         else launch_k(k_local_q<LA, LB, T, false, false>, qg, qb, 0, st, d);
         prof_mark("local_q", st);
         launch_k(k_local_lq<LA, LB, T, false>, nb, kBlock, 0, st, d);

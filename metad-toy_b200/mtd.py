@@ -29,7 +29,7 @@ PREC = {"mixed": 0, "fp64": 1}
 # Every entry point declared in include/metad_b200.h.
 EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args", "mtd_eval_expression", "mtd_set_box", "mtd_init", "mtd_post_force",
            "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
-           "mtd_extract_peratom", "mtd_get_neighbors", "mtd_neighbor_stats", "mtd_neighbor_set_wait", "mtd_set_host_copy_mode", "mtd_sk_tiles", "mtd_set_sk_tiles", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
+           "mtd_extract_peratom", "mtd_get_neighbors", "mtd_neighbor_stats", "mtd_neighbor_set_wait", "mtd_set_host_copy_mode", "mtd_sk_tiles", "mtd_set_sk_tiles", "mtd_get_tuning", "mtd_set_tuning_all", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
            "mtd_set_stream", "mtd_profile_enable", "mtd_profile_report",
            "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc", "mtd_nn_state",
            "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
@@ -111,6 +111,8 @@ def lib():
         L.mtd_neighbor_set_wait.argtypes = [vp, C.c_int, C.c_int]
         L.mtd_set_host_copy_mode.argtypes = [vp, C.c_int]
         L.mtd_sk_tiles.argtypes = [vp, ip, ip]
+        L.mtd_get_tuning.argtypes = [vp, ip]
+        L.mtd_set_tuning_all.argtypes = [vp, ip]
         L.mtd_set_sk_tiles.argtypes = [vp, C.c_int, C.c_int]
         L.mtd_set_types.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.mtd_needs_types.argtypes = [vp]
@@ -340,6 +342,17 @@ class Metad:
         r, a = C.c_int64(), C.c_int()
         self._check(lib().mtd_neighbor_stats(self._h, C.byref(r), C.byref(a)))
         return r.value, bool(a.value)
+
+    def tuning(self):
+        """{name: value} of every tuned shape (results never depend on them)."""
+        a = (C.c_int * 6)()
+        self._check(lib().mtd_get_tuning(self._h, a))
+        keys = ["neighbors", "q_block", "lambda_block", "q_filter_split", "sk_q_values", "sk_force_unroll"]
+        return dict(zip(keys, list(a)))
+
+    def set_tuning_all(self, neighbors, q_block, lambda_block, q_filter_split, sk_q_values, sk_force_unroll):
+        a = (C.c_int * 6)(neighbors, q_block, lambda_block, q_filter_split, sk_q_values, sk_force_unroll)
+        self._check(lib().mtd_set_tuning_all(self._h, a))
 
     def sk_tiles(self):
         """S(k) shapes: (k-vectors per value pass, unroll depth of the force pass)."""

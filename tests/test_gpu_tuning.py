@@ -143,3 +143,30 @@ def test_sk_tiles_give_identical_steps_and_autotune_picks_one():
     qv, qf = m.sk_tiles()
     assert qv in (4, 8, 16) and qf in (1, 2, 4)
     m.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_skin_q_filter_split_and_merged_are_identical(precision):
+    """With skin lists the q pass filters the candidates merged with the sum
+    (split 0) or in a loop of its own before it (split 1): the same steps bit
+    for bit, for both block shapes."""
+    x, L = systems.small_slab(nxy=6, nz_fcc=3, nz_bcc=4, n_liq=300)
+    xs = [np.ascontiguousarray(systems.wrap(systems.jitter(x, 0.04, 70 + s), L)) for s in range(4)]
+    args = H.fix_args_local(pace=2) + ["NEIGH_SKIN", 0.6]
+
+    def run(shape):
+        m = mtd.Metad(args, precision=precision)
+        m.set_box([0, 0, 0], L)
+        m.set_tuning_all(*shape)
+        out = []
+        for step, xv in enumerate(xs):
+            f = np.zeros_like(xv)
+            m.post_force(step, xv, f)
+            out.append((m.cv.copy(), m.compute_scalar(), f))
+        m.close()
+        return out
+
+    ref = run((0, 256, 256, 0, 8, 2))
+    for shape in [(0, 256, 256, 1, 8, 2), (1, 128, 128, 1, 8, 2), (0, 128, 256, 0, 8, 2)]:
+        for (c1, b1, f1), (c2, b2, f2) in zip(ref, run(shape)):
+            assert np.array_equal(c1, c2) and b1 == b2 and np.array_equal(f1, f2), shape
