@@ -377,12 +377,14 @@ __device__ __forceinline__ void local_lambda_body(const LocalDev<T> &d, int bid)
         if (t + 1 < c) jn = nb_index(d.nb, d.npad, t + 1, k);
         T ej[4];
         load_rec(d.e12 + 4 * (size_t)j, ej);
+        // the record is loaded beside the weights, not after the test on them
+        // (a zero weight is rare), so the two loads share one latency
+        T lqj[S::SQ];
+        load_rec32(d.lq + (size_t)j * S::SQ, lqj);
         const T wjA = c1A * ej[0] + c2A * ej[1];
         const T wjB = c1B * ej[2] + c2B * ej[3];
         if (wjA == T(0) && wjB == T(0)) continue;
         const T sg = pair_sigma<T, STEP>(d, a, j);
-        T lqj[S::SQ];
-        load_rec32(d.lq + (size_t)j * S::SQ, lqj);
         add_g<LA, T>(lam, lqj, wjA, sg);
         if constexpr (LB > 0) add_g<LB, T>(lam + S::SA, lqj + S::SA, wjB, sg);
     }
