@@ -771,7 +771,11 @@ mtd_status enqueue_values(mtd_ctx *c, int n, const double *x, const int *mask, c
             // the gated rebuild: cell list and the first environment's
             // candidates as one cooperative launch where it can run, else
             // the separate gated kernels
-            const bool one = c->d_rbar && rebuild_blocks() > 0;
+            // (inside a stream capture, e.g. the walkers' CUDA graph, the
+            // separate gated kernels are captured instead)
+            cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+            cudaStreamIsCapturing(c->st, &cap);
+            const bool one = c->d_rbar && rebuild_blocks() > 0 && cap == cudaStreamCaptureStatusNone;
             if (!one) c->launches += launch_build_cells(g, s, c->st);
             for (size_t ei = 0; ei < c->envs.size(); ++ei) {
                 Env &e = c->envs[ei];

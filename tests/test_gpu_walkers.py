@@ -231,3 +231,18 @@ def test_walkers_sharded_device_allgather_one_rank_nccl():
         W.close()
     finally:
         dist.destroy_process_group()
+
+
+def test_walkers_with_skin_lists_graph_equals_plain():
+    """Skin lists in every walker, the per-walker kernels captured into the
+    group's CUDA graph (the list rebuild is then the separate gated kernels)
+    against plain launches (the one-launch rebuild): identical steps."""
+    syss = _walker_systems()
+    args = H.fix_args_local(pace=2) + ["NEIGH_SKIN", 0.6, "NEIGH_EVERY", 3]
+    steps = list(range(7))
+    plain, g1 = _run(args, syss, steps, graph=False)
+    graph, g2 = _run(args, syss, steps, graph=True)
+    for a, b in zip(plain, graph):
+        for (cv1, b1, f1), (cv2, b2, f2) in zip(a, b):
+            assert np.array_equal(cv1, cv2) and b1 == b2 and np.array_equal(f1, f2)
+    assert np.array_equal(g1, g2)
