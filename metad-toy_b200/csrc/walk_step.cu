@@ -50,7 +50,7 @@ __device__ __forceinline__ int walker_of(const int *pre, int nwalk, int v) {
 }
 
 template <int LA, int LB, typename T, bool STEP>
-__global__ void __launch_bounds__(kWalkBlock, 2) k_walk_step(const WalkDesc<T> *__restrict__ wd, WalkStepArgs a) {
+__global__ void __launch_bounds__(kWalkBlock, 3) k_walk_step(const WalkDesc<T> *__restrict__ wd, WalkStepArgs a) {
     constexpr int KIND = STEP ? NK_STEP : NK_SWITCH;
     __shared__ int pa[kWalkPersistMax + 1], pc[kWalkPersistMax + 1];
     for (int t = threadIdx.x; t <= a.nwalk; t += blockDim.x) {
@@ -64,57 +64,57 @@ __global__ void __launch_bounds__(kWalkBlock, 2) k_walk_step(const WalkDesc<T> *
     // cell list
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const CellGrid g = wd[w].g;
-        const SysDev s = wd[w].s;
+        const CellGrid &g = wd[w].g;
+        const SysDev &s = wd[w].s;
         bin_body(g, s, v - pa[w]);
     }
     if (!grid_barrier(a.bar, a.limit, a.stall && blockIdx.x == 0)) return;
     for (int v = blockIdx.x; v < tc; v += G) {
         const int w = walker_of(pc, nw, v);
-        const SysDev s = wd[w].s;
+        const SysDev &s = wd[w].s;
         const int ncell = wd[w].g.ncell;
         scan_chunk(s, ncell, v - pc[w], s.start + ncell + 1);
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     for (int v = blockIdx.x; v < tc; v += G) {
         const int w = walker_of(pc, nw, v);
-        const SysDev s = wd[w].s;
+        const SysDev &s = wd[w].s;
         const int ncell = wd[w].g.ncell;
         scan_offset(s, ncell, v - pc[w], wd[w].nchunk, s.start + ncell + 1);
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const SysDev s = wd[w].s;
+        const SysDev &s = wd[w].s;
         scatter_body(s, wd[w].g.ncell, v - pa[w], wd[w].nb);
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const CellGrid g = wd[w].g;
-        const SysDev s = wd[w].s;
+        const CellGrid &g = wd[w].g;
+        const SysDev &s = wd[w].s;
         place_body(g, s, v - pa[w]);
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     // neighbour lists and CV values
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const CellGrid g = wd[w].g;
-        const SysDev s = wd[w].s;
-        const NeighSpec ns = wd[w].ns;
-        const NeighDev nd = wd[w].nd;
+        const CellGrid &g = wd[w].g;
+        const SysDev &s = wd[w].s;
+        const NeighSpec &ns = wd[w].ns;
+        const NeighDev &nd = wd[w].nd;
         neighbors_fast_body<KIND>(g, s, ns, nd, s.status, v - pa[w]);
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const LocalDev<T> d = wd[w].ld;
+        const LocalDev<T> &d = wd[w].ld;
         local_q_body<LA, LB, T, STEP, false>(d, v - pa[w]);
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const LocalDev<T> d = wd[w].ld;
+        const LocalDev<T> &d = wd[w].ld;
         local_lq_body<LA, LB, T, STEP>(d, v - pa[w]);
         __syncthreads();
     }
@@ -138,15 +138,15 @@ __global__ void __launch_bounds__(kWalkBlock, 2) k_walk_step(const WalkDesc<T> *
     // forces
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const LocalDev<T> d = wd[w].ld;
+        const LocalDev<T> &d = wd[w].ld;
         local_lambda_body<LA, LB, T, STEP>(d, v - pa[w]);
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     for (int v = blockIdx.x; v < tb; v += G) {
         const int w = walker_of(pa, nw, v);
-        const LocalDev<T> d = wd[w].ld;
-        const SysDev s = wd[w].s;
-        const CellGrid g = wd[w].g;
+        const LocalDev<T> &d = wd[w].ld;
+        const SysDev &s = wd[w].s;
+        const CellGrid &g = wd[w].g;
         local_force_body<LA, LB, T, STEP>(d, wd[w].f_src, wd[w].f_dst, s, g, nullptr, s.status, v - pa[w]);
     }
 }
