@@ -550,29 +550,73 @@ __device__ bool group_failed(const BiasPlan *const *__restrict__ plans, int nwal
     return failed != 0;
 }
 
-// The group's hills in walker order (one block).
+// The group's hills in walker order, spread over every thread of the
+// launch (vblock / nvblocks: this block's place among the blocks taking
+// part): each bin of the bands' bounding box takes, in walker order, the
+// increment of every walker whose band holds it -- per bin the same
+// operations as depositing the hills one after another, so the grid is the
+// same bit for bit.  Block 0's first thread writes the hill records in
+// walker order.
 __device__ void walk_deposit_block(const BiasPlan *const *__restrict__ plans, int nwalk,
-                                   const long long *__restrict__ d_step, const WalkState *ws) {
-    __shared__ __align__(16) unsigned char plan_raw[sizeof(BiasPlan)];
-    stage_plan(plans[0], plan_raw);
-    const BiasPlan &P = *reinterpret_cast<const BiasPlan *>(plan_raw);
+                                   const long long *__restrict__ d_step, const WalkState *ws, int vblock,
+                                   int nvblocks) {
+    const BiasPlan &P = *plans[0];
     const bool failed = group_failed(plans, nwalk);
     const long long step = *(volatile const long long *)d_step;
-    if (!failed && P.pace != 0 && step % P.pace == 0) {   // every walker shares PACE
-        int ix[3] = {1, 1, 1};
-        for (int w = 0; w < nwalk; ++w) {
-            phase_deposit(P, ws[w].s, ws[w].hill_w, ix, nullptr);
-            if (threadIdx.x == 0) record_hill(P, step, ws[w].s, ws[w].hill_w);
-            __syncthreads();
+    if (failed || P.pace == 0 || step % P.pace != 0) return;   // every walker shares PACE
+    __shared__ int bb[6];
+    if (threadIdx.x < 3) {
+        bb[threadIdx.x] = 0x7fffffff;
+        bb[3 + threadIdx.x] = -1;
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < nwalk; w += blockDim.x) {
+        int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        if (!hill_band(P, ws[w].s, lo, hi)) continue;
+        for (int k = 0; k < P.D; ++k) {
+            atomicMin(&bb[k], lo[k]);
+            atomicMax(&bb[3 + k], hi[k]);
         }
     }
     __syncthreads();
+    if (vblock == 0 && threadIdx.x == 0)
+        for (int w = 0; w < nwalk; ++w) record_hill(P, step, ws[w].s, ws[w].hill_w);
+    long long total = 1;
+    int ext[3] = {1, 1, 1};
+    for (int k = 0; k < P.D; ++k) {
+        ext[k] = bb[3 + k] - bb[k] + 1;
+        total = ext[k] > 0 ? total * ext[k] : 0;
+    }
+    for (long long t = (long long)vblock * blockDim.x + threadIdx.x; t < total; t += (long long)nvblocks * blockDim.x) {
+        int idx[3] = {0, 0, 0};
+        long long rem = t;
+        for (int k = P.D - 1; k >= 0; --k) {
+            idx[k] = bb[k] + (int)(rem % ext[k]);
+            rem /= ext[k];
+        }
+        size_t g = idx[0];
+        for (int k = 1; k < P.D; ++k) g = g * P.nbin[k] + idx[k];
+        if (g >= (size_t)P.grid_size) continue;
+        double v = 0.0;
+        bool any = false;
+        for (int w = 0; w < nwalk; ++w) {
+            int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+            if (!hill_band(P, ws[w].s, lo, hi)) continue;
+            bool in = true;
+            for (int k = 0; k < P.D; ++k) in = in && idx[k] >= lo[k] && idx[k] <= hi[k];
+            if (!in) continue;
+            if (!any) v = __ldcg(P.grid + g);
+            any = true;
+            v = v + ws[w].hill_w * hill_gauss(P, ws[w].s, idx, P.sigma);
+        }
+        if (any) P.grid[g] = v;
+    }
 }
 
 __global__ void __launch_bounds__(256) k_walk_deposit(const BiasPlan *const *__restrict__ plans, int nwalk,
                                                       const long long *__restrict__ d_step, const WalkState *ws) {
     pdl_entry();
-    walk_deposit_block(plans, nwalk, d_step, ws);
+    walk_deposit_block(plans, nwalk, d_step, ws, blockIdx.x, gridDim.x);
 }
 
 // Walker w's V, dV/ds on the updated grid and force coefficients (one block).
@@ -722,8 +766,8 @@ __device__ void walk_phase_cvs(const BiasPlan *const *plans, int w, const long l
     walk_cvs_block(plans, w, d_step, ws);
 }
 __device__ void walk_phase_deposit(const BiasPlan *const *plans, int nwalk, const long long *d_step,
-                                   const WalkState *ws) {
-    walk_deposit_block(plans, nwalk, d_step, ws);
+                                   const WalkState *ws, int vblock, int nvblocks) {
+    walk_deposit_block(plans, nwalk, d_step, ws, vblock, nvblocks);
 }
 __device__ void walk_phase_coef(const BiasPlan *const *plans, int nwalk, int w, const WalkState *ws) {
     walk_coef_block(plans, nwalk, w, ws);
@@ -801,7 +845,7 @@ void launch_list_finish(const BiasPlan *d_plan, long long step, const WalkState 
 void launch_walk_bias(const BiasPlan *const *d_plans, int nwalk, const long long *d_step, WalkState *ws,
                       cudaStream_t st) {
     launch_k(k_walk_cvs, nwalk, 256, 0, st, d_plans, d_step, ws);
-    launch_k(k_walk_deposit, 1, 256, 0, st, d_plans, nwalk, d_step, ws);
+    launch_k(k_walk_deposit, 148, 256, 0, st, d_plans, nwalk, d_step, ws);
     launch_k(k_walk_coef, nwalk, 256, 0, st, d_plans, nwalk, ws);
     prof_mark("walk_bias", st);
 }

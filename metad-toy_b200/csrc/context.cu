@@ -927,13 +927,17 @@ mtd_status collect(mtd_ctx *c) {
             write_hill_line(c, r);
             recs.push_back(r);
         } else {
-            for (unsigned long long h = from; h < nh; ++h) {
-                HillRec r;
-                MTD_CU(cudaMemcpy(&r, c->d_hills + (h % kHillCap), sizeof(HillRec), cudaMemcpyDeviceToHost),
-                       "hill record");
-                write_hill_line(c, r);
-                recs.push_back(r);
-            }
+            // the new records in at most two copies (the ring wraps once at most)
+            recs.resize((size_t)(nh - from));
+            const size_t a = (size_t)(from % kHillCap);
+            const size_t first = std::min(recs.size(), (size_t)kHillCap - a);
+            MTD_CU(cudaMemcpy(recs.data(), c->d_hills + a, sizeof(HillRec) * first, cudaMemcpyDeviceToHost),
+                   "hill records");
+            if (first < recs.size())
+                MTD_CU(cudaMemcpy(recs.data() + first, c->d_hills, sizeof(HillRec) * (recs.size() - first),
+                                  cudaMemcpyDeviceToHost),
+                       "hill records");
+            for (const HillRec &r : recs) write_hill_line(c, r);
         }
         c->hills_written = nh;
         if (c->nb) {

@@ -30,7 +30,7 @@ namespace mtd {
 // bias.cu
 __device__ void walk_phase_cvs(const BiasPlan *const *plans, int w, const long long *d_step, WalkState *ws);
 __device__ void walk_phase_deposit(const BiasPlan *const *plans, int nwalk, const long long *d_step,
-                                   const WalkState *ws);
+                                   const WalkState *ws, int vblock, int nvblocks);
 __device__ void walk_phase_coef(const BiasPlan *const *plans, int nwalk, int w, const WalkState *ws);
 
 namespace {
@@ -53,10 +53,14 @@ template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kWalkBlock, 3) k_walk_step(const WalkDesc<T> *__restrict__ wd, WalkStepArgs a) {
     constexpr int KIND = STEP ? NK_STEP : NK_SWITCH;
     __shared__ int pa[kWalkPersistMax + 1], pc[kWalkPersistMax + 1];
+    // the step number lives in pinned host memory: one read per block over
+    // the host link, every later read from shared memory
+    __shared__ long long s_step;
     for (int t = threadIdx.x; t <= a.nwalk; t += blockDim.x) {
         pa[t] = a.pa[t];
         pc[t] = a.pc[t];
     }
+    if (threadIdx.x == 0) s_step = *(volatile const long long *)a.step;
     __syncthreads();
     const int nw = a.nwalk;
     const int G = gridDim.x;
@@ -120,9 +124,10 @@ __global__ void __launch_bounds__(kWalkBlock, 3) k_walk_step(const WalkDesc<T> *
     }
     if (!grid_barrier(a.bar, a.limit, false)) return;
     // bias: every walker's CVs, the deposit in walker order, coefficients
-    for (int w = blockIdx.x; w < nw; w += G) walk_phase_cvs(a.plans, w, a.step, a.ws);
+    for (int w = blockIdx.x; w < nw; w += G) walk_phase_cvs(a.plans, w, &s_step, a.ws);
     if (!grid_barrier(a.bar, a.limit, false)) return;
-    if (blockIdx.x == 0) walk_phase_deposit(a.plans, nw, a.step, a.ws);
+    // one block deposits: spreading the bins over every block measured slower here
+    if (blockIdx.x == 0) walk_phase_deposit(a.plans, nw, &s_step, a.ws, 0, 1);
     if (!grid_barrier(a.bar, a.limit, false)) return;
     for (int w = blockIdx.x; w < nw; w += G) walk_phase_coef(a.plans, nw, w, a.ws);
     if (!grid_barrier(a.bar, a.limit, false)) return;

@@ -518,16 +518,23 @@ mtd_status mtd_walkers_sync(mtd_walkers *W) {
     if (nh > W->hills_written) {
         unsigned long long from = W->hills_written;
         if (nh - from > (unsigned long long)kHillCap) from = nh - kHillCap;
-        for (unsigned long long h = from; h < nh; ++h) {
-            HillRec r;
-            MTD_WCU(cudaMemcpy(&r, c0->d_hills + (h % kHillCap), sizeof(HillRec), cudaMemcpyDeviceToHost), "hill");
-            if (W->f_hills) {
+        if (W->f_hills) {   // the new records in at most two copies (the ring wraps once at most)
+            std::vector<HillRec> recs((size_t)(nh - from));
+            const size_t a = (size_t)(from % kHillCap);
+            const size_t first = std::min(recs.size(), (size_t)kHillCap - a);
+            MTD_WCU(cudaMemcpy(recs.data(), c0->d_hills + a, sizeof(HillRec) * first, cudaMemcpyDeviceToHost),
+                    "hills");
+            if (first < recs.size())
+                MTD_WCU(cudaMemcpy(recs.data() + first, c0->d_hills, sizeof(HillRec) * (recs.size() - first),
+                                   cudaMemcpyDeviceToHost),
+                        "hills");
+            for (const HillRec &r : recs) {
                 std::fprintf(W->f_hills, "%lld", r.step);
                 for (int d = 0; d < c0->cfg.cv_dim; ++d) std::fprintf(W->f_hills, " %.16g", r.s[d]);
                 std::fprintf(W->f_hills, " %.16g %.16g\n", r.w, r.sigma);
             }
+            std::fflush(W->f_hills);
         }
-        if (W->f_hills) std::fflush(W->f_hills);
         W->hills_written = nh;
     }
     for (mtd_ctx *c : W->w) {
