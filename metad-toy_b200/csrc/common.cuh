@@ -131,6 +131,17 @@ __device__ __forceinline__ void pdl_entry() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// The two halves, for a kernel that does work before its wait.  A block of a
+// kernel K starts only after every block of the previous kernel P has let
+// dependents launch; when P let them launch after its own wait, P's
+// predecessor (and everything before it) has completed and is visible.  So
+// before its wait K may read what the kernel two places back (or earlier)
+// wrote, and must not read what P writes.  A kernel that lets dependents
+// launch before its wait gives its successor no such window: that successor
+// must open with its wait.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Deterministic block sum of up to NV doubles per thread (fixed shuffle tree,
 // then warp 0 over the warp partials).  Result valid in thread 0.
 template <int NV>

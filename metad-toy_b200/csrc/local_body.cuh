@@ -335,11 +335,72 @@ __device__ __forceinline__ void add_g(T *acc, const T *lq, T w, T s) {
     }
 }
 
-// Pass 3 (after the bias kernel): lam_k / NF_k, and for smooth switches G_k, t_k, u_k.
+// A CV switch whose derivative is identically zero (e2 = 0 for every atom).
+__device__ __forceinline__ bool sw_flat(const SwParams &p) { return p.type == SW_LINE || p.type == SW_STEP; }
+
+// Pass 3 for a step pair switch and flat CV switches: with e2 = 0 the weight
+// of an order is c1 e1, so lam_k = c1 / NF_k * (e1_k LQ_k + sum_j s_kj e1_j
+// LQ_j), and the sum needs no coefficient.  It is formed before `pdl` waits
+// for the bias kernel (which writes the coefficients; e1 and LQ come from the
+// LQ pass before it), so the gather of the first wave of blocks overlaps the
+// bias kernel's serial phases.
+template <int LA, int LB, typename T>
+__device__ __forceinline__ void local_lambda_e1_body(const LocalDev<T> &d, int bid, bool pdl) {
+    using S = LSet<LA, LB, T>;
+    if (pdl) pdl_release();
+    const int k = bid * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const T nfk = d.nf[k];
+    T acc[S::SQ];
+#pragma unroll
+    for (int s = 0; s < S::SQ; ++s) acc[s] = T(0);
+    if (!(nfk > T(0))) {
+        store_rec(d.lam + (size_t)k * S::SQ, acc);
+        return;
+    }
+    T lqk[S::SQ];
+    load_rec32(d.lq + (size_t)k * S::SQ, lqk);
+    add_g<LA, T>(acc, lqk, d.e12[4 * k], T(1));
+    if constexpr (LB > 0) add_g<LB, T>(acc + S::SA, lqk + S::SA, d.e12[4 * k + 2], T(1));
+    const auto a = d.geo.load(k);
+    const int c = min(d.nb.count[k], d.nb.M);
+    int jn = c > 0 ? nb_index(d.nb, d.npad, 0, k) : 0;
+    for (int t = 0; t < c; ++t) {
+        const int j = jn;
+        if (t + 1 < c) jn = nb_index(d.nb, d.npad, t + 1, k);
+        T ej[4];
+        load_rec(d.e12 + 4 * (size_t)j, ej);
+        T lqj[S::SQ];
+        load_rec32(d.lq + (size_t)j * S::SQ, lqj);
+        if (ej[0] == T(0) && ej[2] == T(0)) continue;
+        const T sg = pair_sigma<T, true>(d, a, j);
+        add_g<LA, T>(acc, lqj, ej[0], sg);
+        if constexpr (LB > 0) add_g<LB, T>(acc + S::SA, lqj + S::SA, ej[2], sg);
+    }
+    if (pdl) pdl_wait();
+    const T inv = T(1) / nfk;
+    const T sA = (T)d.coef[0] * inv, sB = (T)d.coef[2] * inv;
+#pragma unroll
+    for (int s = 0; s < S::SA; ++s) acc[s] *= sA;
+#pragma unroll
+    for (int s = S::SA; s < S::SQ; ++s) acc[s] *= sB;
+    store_rec(d.lam + (size_t)k * S::SQ, acc);
+}
+
+// Pass 3 (after the bias kernel): lam_k / NF_k, and for smooth switches G_k,
+// t_k, u_k.  `pdl`: the kernel was launched as a dependent launch and the
+// body places its wait (the walker kernel passes false).
 template <int LA, int LB, typename T, bool STEP>
-__device__ __forceinline__ void local_lambda_body(const LocalDev<T> &d, int bid) {
+__device__ __forceinline__ void local_lambda_body(const LocalDev<T> &d, int bid, bool pdl = false) {
     using S = LSet<LA, LB, T>;
     constexpr bool DSIG = !STEP;
+    if constexpr (STEP) {
+        if (sw_flat(d.sw_cvA) && (LB == 0 || sw_flat(d.sw_cvB))) {
+            local_lambda_e1_body<LA, LB, T>(d, bid, pdl);
+            return;
+        }
+    }
+    if (pdl) pdl_entry();
     const int k = bid * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
     const T c1A = (T)d.coef[0], c2A = (T)d.coef[1], c1B = (T)d.coef[2], c2B = (T)d.coef[3];

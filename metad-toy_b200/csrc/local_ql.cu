@@ -41,8 +41,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_local_lq(LocalDev<T> d) {
 
 template <int LA, int LB, typename T, bool STEP>
 __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
-    pdl_entry();
-    local_lambda_body<LA, LB, T, STEP>(d, blockIdx.x);
+    local_lambda_body<LA, LB, T, STEP>(d, blockIdx.x, true);   // the body places the wait
 }
 
 template <int LA, int LB, typename T, bool STEP, bool CALLER = false>
