@@ -184,42 +184,60 @@ __device__ __forceinline__ void unpack_image(int img, int &ix, int &iy, int &iz)
     iy = ((img >> 10) & 1023) - 512;
     iz = (img >> 20) - 512;
 }
-// sin and cos of an FP64 phase for the mixed-precision k-vector sums: the
-// phase is reduced in FP64 by the nearest multiple of pi/2 (quadrant q), the
-// remainder |r| <= pi/4 goes to FP32, and sin r, cos r come from their Taylor
-// series to degree 9 and 10 (remainders below 2e-9 and 2e-10 on |r| <= pi/4,
-// under the FP32 rounding of the result), rotated back by the quadrant.
-// The nearest multiple comes from adding 1.5 * 2^52 (an FMA rounds ph * 2/pi
-// to an integer held in the low mantissa bits, read back as q), so the
-// reduction needs no rounding or conversion instruction; |ph| < 2^51.
-__device__ __forceinline__ void quadrant_sincos_f32(float r, int q, float &s, float &c);
+// sin and cos of pi * u for an FP64 phase u in half turns (the mixed-
+// precision k-vector sums scale k by 1 / pi once, so u = (k / pi) . x):
+// u is rounded to the nearest integer n in FP64 (adding 1.5 * 2^52 leaves n
+// in the low mantissa bits, so no rounding or conversion instruction), the
+// remainder f = u - n in [-1/2, 1/2] is exact in FP64 and goes to FP32,
+// sin(pi f) and cos(pi f) come from their Taylor series to degree 13 and 12
+// in pi f (the first omitted terms are below 6.7e-10 and 6.4e-9 for
+// |pi f| <= pi / 2), and (-1)^n flips both signs.  |u| < 2^51.
+constexpr double kPi2 = kPi * kPi;
+constexpr float kSin1 = (float)kPi, kSin3 = (float)(-kPi * kPi2 / 6.0), kSin5 = (float)(kPi * kPi2 * kPi2 / 120.0),
+                kSin7 = (float)(-kPi * kPi2 * kPi2 * kPi2 / 5040.0),
+                kSin9 = (float)(kPi * kPi2 * kPi2 * kPi2 * kPi2 / 362880.0),
+                kSin11 = (float)(-kPi * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 39916800.0),
+                kSin13 = (float)(kPi * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 6227020800.0);
+constexpr float kCos2 = (float)(-kPi2 / 2.0), kCos4 = (float)(kPi2 * kPi2 / 24.0),
+                kCos6 = (float)(-kPi2 * kPi2 * kPi2 / 720.0), kCos8 = (float)(kPi2 * kPi2 * kPi2 * kPi2 / 40320.0),
+                kCos10 = (float)(-kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 3628800.0),
+                kCos12 = (float)(kPi2 * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 479001600.0);
+constexpr double kInvPi = 0.31830988618379067154;
 
-__device__ __forceinline__ void phase_sincos_f32(double ph, float &s, float &c) {
-    constexpr double kRound = 6755399441055744.0;                        // 1.5 * 2^52
-    const double t = fma(ph, 0.63661977236758134308, kRound);            // 2 / pi
-    const double n = t - kRound;
-    const float r = (float)fma(-n, 1.5707963267948966192, ph);          // pi / 2
-    const int q = __double2loint(t) & 3;
-    quadrant_sincos_f32(r, q, s, c);
+// The sign flip of halfturn_sincos_f32 as a bit mask (bit 31 set for odd n),
+// with sin(pi f) and cos(pi f) unsigned: callers that fold the sign into a
+// later product take these three.
+__device__ __forceinline__ unsigned halfturn_sincos_f32_parts(double u, float &s0, float &c0) {
+    constexpr double kRound = 6755399441055744.0;   // 1.5 * 2^52
+    const double t = u + kRound;
+    const double f = u - (t - kRound);
+    const float z = (float)f, z2 = z * z;
+    float p = fmaf(z2, kSin13, kSin11);
+    p = fmaf(p, z2, kSin9);
+    p = fmaf(p, z2, kSin7);
+    p = fmaf(p, z2, kSin5);
+    p = fmaf(p, z2, kSin3);
+    p = fmaf(p, z2, kSin1);
+    s0 = p * z;
+    float q = fmaf(z2, kCos12, kCos10);
+    q = fmaf(q, z2, kCos8);
+    q = fmaf(q, z2, kCos6);
+    q = fmaf(q, z2, kCos4);
+    q = fmaf(q, z2, kCos2);
+    c0 = fmaf(q, z2, 1.0f);
+    return (unsigned)__double2loint(t) << 31;
 }
 
-// sin and cos of r + q pi / 2 for |r| <= pi / 4: Taylor series of sin and cos
-// to degree 9 and 10, then the quadrant rotation.
-__device__ __forceinline__ void quadrant_sincos_f32(float r, int q, float &s, float &c) {
-    const float r2 = r * r;
-    float sp = fmaf(r2, 1.0f / 362880.0f, -1.0f / 5040.0f);
-    sp = fmaf(sp, r2, 1.0f / 120.0f);
-    sp = fmaf(sp, r2, -1.0f / 6.0f);
-    const float s0 = fmaf(sp * r2, r, r);
-    float cp = fmaf(r2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
-    cp = fmaf(cp, r2, -1.0f / 720.0f);
-    cp = fmaf(cp, r2, 1.0f / 24.0f);
-    cp = fmaf(cp, r2, -0.5f);
-    const float c0 = fmaf(cp, r2, 1.0f);
-    const float ss = (q & 1) ? c0 : s0, cc = (q & 1) ? s0 : c0;
-    // rotation by q quarter turns: sign bits from q (bit 1 for sin, bit 1 of q + 1 for cos)
-    s = __int_as_float(__float_as_int(ss) ^ ((q & 2) << 30));
-    c = __int_as_float(__float_as_int(cc) ^ (((q + 1) & 2) << 30));
+__device__ __forceinline__ void halfturn_sincos_f32(double u, float &s, float &c) {
+    float s0, c0;
+    const unsigned sgn = halfturn_sincos_f32_parts(u, s0, c0);
+    s = __uint_as_float(__float_as_uint(s0) ^ sgn);
+    c = __uint_as_float(__float_as_uint(c0) ^ sgn);
+}
+
+// The same for a phase in radians (one FP64 multiply by 1 / pi first).
+__device__ __forceinline__ void phase_sincos_f32(double ph, float &s, float &c) {
+    halfturn_sincos_f32(ph * kInvPi, s, c);
 }
 
 }  // namespace mtd

@@ -156,17 +156,19 @@ constexpr int kSkBlocks = 148 * 4;  // grid for the partial sums (4 blocks per S
 // the atoms in the partial-sum pass (a register tile of 2 QV sums per thread),
 // and the unroll depth U of the force pass's loop over k.  Every k is summed
 // in the same order whatever the shape, so all give bitwise-identical
-// results.  The phase k.x is formed in FP64 (B200 runs FP64 at half the FP32
-// rate) and reduced to [-pi/4, pi/4] before the FP32 polynomials; a
-// per-dimension FP32 phase-table variant (three shared-memory loads and an
-// FP32 reduction per pair) measured 2.2x slower and was removed.
+// results.  In mixed precision the phase (k / pi).x is formed in FP64 (B200
+// runs FP64 at half the FP32 rate), reduced to half a turn in FP64 and
+// finished with FP32 polynomials (halfturn_sincos_f32); a per-dimension FP32
+// phase-table variant (three shared-memory loads and an FP32 reduction per
+// pair) measured 2.2x slower and was removed.
 
 template <bool FP64, int QV> __global__ void __launch_bounds__(256) k_sk_partial(SkDev d) {
     constexpr int kSkChunk = 2 * QV;   // reals per register tile
     pdl_entry();
     __shared__ double smem[kSkChunk * 32];
     extern __shared__ double kk[];   // 3K
-    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
+    // mixed precision: k / pi, so the phases come out in half turns
+    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = FP64 ? d.k[t] : d.k[t] * kInvPi;
     __syncthreads();
     double cnt = 0.0;
     for (int k0 = 0; k0 < d.K; k0 += QV) {
@@ -194,10 +196,13 @@ template <bool FP64, int QV> __global__ void __launch_bounds__(256) k_sk_partial
                         acc[2 * q] += c;
                         acc[2 * q + 1] += s;
                     } else {
-                        float s, c;
-                        phase_sincos_f32(ph, s, c);
-                        facc[2 * q] += c;
-                        facc[2 * q + 1] += s;
+                        // the sign (-1)^n as a factor of exact FMAs: the same
+                        // sums as adding the signed sin and cos
+                        float s0, c0;
+                        const unsigned sgn = halfturn_sincos_f32_parts(ph, s0, c0);
+                        const float sg = __uint_as_float(0x3f800000u | sgn);
+                        facc[2 * q] = fmaf(sg, c0, facc[2 * q]);
+                        facc[2 * q + 1] = fmaf(sg, s0, facc[2 * q + 1]);
                     }
                 }
             }
@@ -234,25 +239,16 @@ __global__ void __launch_bounds__(256) k_sk_reduce(SkDev d) {
     }
 }
 
-template <bool FP64, int U>
+// FP64 force pass: one atom per thread, FP64 sincos of the FP64 phase.
+template <int U>
 __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restrict__ f_src, double *__restrict__ f_dst,
                                                   SysDev s, CellGrid g, double *vpart) {
     pdl_entry();
     __shared__ double smem[6 * 32];
-    extern __shared__ double kk[];   // 3K doubles, then 2K doubles (FP64) or 5K floats (FP32)
-    // FP64: rho as doubles; FP32: rho and k as floats (the per-atom gradient
-    // is accumulated in FP32, the phase stays FP64)
-    float *aux = reinterpret_cast<float *>(kk + 3 * d.K);
+    extern __shared__ double kk[];   // 3K doubles of k, then 2K of rho
     double *rr = kk + 3 * d.K;
-    float *rrf = aux, *kkf = aux + 2 * d.K;
-    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) {
-        kk[t] = d.k[t];
-        if (!FP64) kkf[t] = (float)d.k[t];
-    }
-    for (int t = threadIdx.x; t < 2 * d.K; t += blockDim.x) {
-        if (FP64) rr[t] = d.rho[t];
-        else rrf[t] = (float)d.rho[t];
-    }
+    for (int t = threadIdx.x; t < 3 * d.K; t += blockDim.x) kk[t] = d.k[t];
+    for (int t = threadIdx.x; t < 2 * d.K; t += blockDim.x) rr[t] = d.rho[t];
     __syncthreads();
     const double a = d.coef[0];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -261,32 +257,15 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
         double gx = 0, gy = 0, gz = 0;
         if (i < d.nown && (!d.mask || (d.mask[i] & d.groupbit))) {
             const double x = d.x[3 * i], y = d.x[3 * i + 1], z = d.x[3 * i + 2];
-            if (FP64) {
 #pragma unroll U
-                for (int q = 0; q < d.K; ++q) {
-                    const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
-                    double sn, cs;
-                    sincos(ph, &sn, &cs);
-                    const double w = -rr[2 * q] * sn + rr[2 * q + 1] * cs;
-                    gx += w * kk[3 * q];
-                    gy += w * kk[3 * q + 1];
-                    gz += w * kk[3 * q + 2];
-                }
-            } else {
-                float fx = 0.f, fy = 0.f, fz = 0.f;
-#pragma unroll U
-                for (int q = 0; q < d.K; ++q) {
-                    const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
-                    float sn, cs;
-                    phase_sincos_f32(ph, sn, cs);
-                    const float w = fmaf(rrf[2 * q + 1], cs, -rrf[2 * q] * sn);
-                    fx = fmaf(w, kkf[3 * q], fx);
-                    fy = fmaf(w, kkf[3 * q + 1], fy);
-                    fz = fmaf(w, kkf[3 * q + 2], fz);
-                }
-                gx = fx;
-                gy = fy;
-                gz = fz;
+            for (int q = 0; q < d.K; ++q) {
+                const double ph = kk[3 * q] * x + kk[3 * q + 1] * y + kk[3 * q + 2] * z;
+                double sn, cs;
+                sincos(ph, &sn, &cs);
+                const double w = -rr[2 * q] * sn + rr[2 * q + 1] * cs;
+                gx += w * kk[3 * q];
+                gy += w * kk[3 * q + 1];
+                gz += w * kk[3 * q + 2];
             }
         }
         const double fx = -a * gx, fy = -a * gy, fz = -a * gz;
@@ -304,6 +283,96 @@ __global__ void __launch_bounds__(256) k_sk_force(SkDev d, const double *__restr
             }
             vir[0] = fx * ux; vir[1] = fy * uy; vir[2] = fz * uz;
             vir[3] = fx * uy; vir[4] = fx * uz; vir[5] = fy * uz;
+        }
+    }
+    if (vpart) {
+        block_sum<6>(vir, smem);
+        if (threadIdx.x == 0)
+            for (int t = 0; t < 6; ++t) vpart[blockIdx.x * 8 + t] = vir[t];
+    }
+}
+
+// Mixed-precision force pass: AT atoms per thread (atoms blockIdx.x * 256 *
+// AT + a * 256 + threadIdx.x), so each k's shared-memory loads serve AT
+// atoms; per k one 16-byte load of (k / pi).xy, one of (Re rho, Im rho, kx,
+// ky) in FP32 and two scalars.  Every atom sums its k terms in k order with
+// the same operations whatever U and AT, so the shapes give identical forces.
+template <int U, int AT>
+__global__ void __launch_bounds__(256) k_sk_force_mixed(SkDev d, const double *__restrict__ f_src,
+                                                        double *__restrict__ f_dst, SysDev s, CellGrid g,
+                                                        double *vpart) {
+    pdl_entry();
+    __shared__ double smem[6 * 32];
+    extern __shared__ double4 skf_raw[];   // K double2, K float4, K double, K float (44 K bytes)
+    double2 *kxy = reinterpret_cast<double2 *>(skf_raw);
+    float4 *rk = reinterpret_cast<float4 *>(kxy + d.K);
+    double *kz = reinterpret_cast<double *>(rk + d.K);
+    float *kzf = reinterpret_cast<float *>(kz + d.K);
+    for (int q = threadIdx.x; q < d.K; q += blockDim.x) {
+        kxy[q] = make_double2(d.k[3 * q] * kInvPi, d.k[3 * q + 1] * kInvPi);
+        kz[q] = d.k[3 * q + 2] * kInvPi;
+        rk[q] = make_float4((float)d.rho[2 * q], (float)d.rho[2 * q + 1], (float)d.k[3 * q], (float)d.k[3 * q + 1]);
+        kzf[q] = (float)d.k[3 * q + 2];
+    }
+    __syncthreads();
+    const double a = d.coef[0];
+    double x[AT], y[AT], z[AT];
+    float fx[AT], fy[AT], fz[AT];
+    bool on[AT];
+#pragma unroll
+    for (int t = 0; t < AT; ++t) {
+        const int i = (blockIdx.x * AT + t) * blockDim.x + threadIdx.x;
+        on[t] = i < d.nown && (!d.mask || (d.mask[i] & d.groupbit));
+        x[t] = on[t] ? d.x[3 * i] : 0.0;
+        y[t] = on[t] ? d.x[3 * i + 1] : 0.0;
+        z[t] = on[t] ? d.x[3 * i + 2] : 0.0;
+        fx[t] = fy[t] = fz[t] = 0.f;
+    }
+    bool any = false;
+#pragma unroll
+    for (int t = 0; t < AT; ++t) any = any || on[t];
+    if (any) {
+#pragma unroll U
+        for (int q = 0; q < d.K; ++q) {
+            const double2 kq = kxy[q];
+            const double kzq = kz[q];
+            const float4 r = rk[q];
+            const float kzq_f = kzf[q];
+#pragma unroll
+            for (int t = 0; t < AT; ++t) {
+                const double u = kq.x * x[t] + kq.y * y[t] + kzq * z[t];
+                float s0, c0;
+                const unsigned sgn = halfturn_sincos_f32_parts(u, s0, c0);
+                // Im rho cos - Re rho sin, with the sign (-1)^n applied after
+                // (exact: rounding is symmetric in the sign)
+                const float w = __uint_as_float(__float_as_uint(fmaf(r.y, c0, -r.x * s0)) ^ sgn);
+                fx[t] = fmaf(w, r.z, fx[t]);
+                fy[t] = fmaf(w, r.w, fy[t]);
+                fz[t] = fmaf(w, kzq_f, fz[t]);
+            }
+        }
+    }
+    double vir[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int t = 0; t < AT; ++t) {
+        const int i = (blockIdx.x * AT + t) * blockDim.x + threadIdx.x;
+        if (i >= d.n) continue;
+        const double gx = on[t] ? -a * (double)fx[t] : 0.0, gy = on[t] ? -a * (double)fy[t] : 0.0,
+                     gz = on[t] ? -a * (double)fz[t] : 0.0;
+        f_dst[3 * i] = f_src[3 * i] + gx;
+        f_dst[3 * i + 1] = f_src[3 * i + 1] + gy;
+        f_dst[3 * i + 2] = f_src[3 * i + 2] + gz;
+        if (vpart) {
+            double ux = d.x[3 * i], uy = d.x[3 * i + 1], uz = d.x[3 * i + 2];
+            if (s.image) {
+                int ix, iy, iz;
+                unpack_image(s.image[i], ix, iy, iz);
+                ux += ix * g.L[0];
+                uy += iy * g.L[1];
+                uz += iz * g.L[2];
+            }
+            vir[0] += gx * ux; vir[1] += gy * uy; vir[2] += gz * uz;
+            vir[3] += gx * uy; vir[4] += gx * uz; vir[5] += gy * uz;
         }
     }
     if (vpart) {
@@ -348,8 +417,13 @@ template <int QV> static void launch_sk_partial_q(const SkDev &d, size_t sm, cud
 template <int U>
 static void launch_sk_force_u(const SkDev &d, const double *f_src, double *f_dst, const SysDev &s, const CellGrid &g,
                               double *vpart, size_t sm, int nb, cudaStream_t st) {
-    if (d.fp64) launch_k(k_sk_force<true, U>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
-    else launch_k(k_sk_force<false, U>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
+    if (d.fp64) {
+        launch_k(k_sk_force<U>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
+    } else if (vpart) {   // one atom per thread: one virial partial per 256 atoms, as the other units write
+        launch_k(k_sk_force_mixed<U, 1>, nb, 256, sm, st, d, f_src, f_dst, s, g, vpart);
+    } else {
+        launch_k(k_sk_force_mixed<U, 2>, (d.n + 511) / 512, 256, sm, st, d, f_src, f_dst, s, g, vpart);
+    }
 }
 
 void launch_sk_values(const SkDev &d, cudaStream_t st) {
