@@ -1009,9 +1009,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
                     "d2h_bytes_per_step": 24 * n + 8 * 64, "ms_per_step": e2e_ms / args.steps,
                     "split_ms": e2e_split,
-                    "copies": "x uploaded in 3 MB pieces; f (pinned) uploaded on a side stream during the CV "
-                              "passes and written back by the force pass over the host link (zero copy, the "
-                              "library's default host-copy mode)",
+                    "copies": "x uploaded in 3 MB pieces; f (pinned) read and written in place by the force "
+                              "pass over the host link (zero copy both ways, the library's default host-copy "
+                              "mode)",
                     "host_copy_modes_ms_per_step": copy_modes},
             "gpu_launches": launches * args.steps,
             "roofline": roof, "clocks": clocks, "cpu_baseline": cpu, "error_vs_fp64": err}

@@ -214,7 +214,7 @@ mtd_status mtd_neighbor_set_wait(mtd_ctx *ctx, int limit, int stall);
  *      one thread per caller index so every warp writes one contiguous
  *      stretch), no download;
  *   3  f read and written in place by the force pass (zero copy both ways).
- * 0 (default) is mode 2.  Forces are bitwise identical in every mode; the
+ * 0 (default) is mode 3.  Forces are bitwise identical in every mode; the
  * fastest depends on the host platform.  Extension (no counterpart). */
 mtd_status mtd_set_host_copy_mode(mtd_ctx *ctx, int mode);
 

@@ -1330,7 +1330,7 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
     // writes f over the host link in caller order (zero copy, no download),
     // and with mode 3 also reads it there (no upload)
     double *zf = nullptr;
-    const int mode = c->host_copy_mode == 0 ? 2 : c->host_copy_mode;
+    const int mode = c->host_copy_mode == 0 ? 3 : c->host_copy_mode;
     if (mode >= 2 && !virial && n >= 4096 && single_local_unit(c)) {
         cudaPointerAttributes pa{};
         if (cudaPointerGetAttributes(&pa, f) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer)

@@ -49,11 +49,12 @@ def test_zero_copy_host_forces_equal_device_path(precision, skin):
     # the same first step through every host-copy mode, pageable f and the
     # virial (upload / download path): the same forces
     outs = []
+    f0 = np.random.default_rng(7).normal(size=xs[0].shape)   # f_in not zero: the f read is checked too
     for mode in ("copies", "zc_write", "zc_both", "pageable", "virial"):
         m = mtd.Metad(args, precision=precision)
         m.set_box([0, 0, 0], L)
         m.set_host_copy_mode({"copies": 1, "zc_write": 2, "zc_both": 3}.get(mode, 0))
-        f = torch.zeros(xs[0].shape, dtype=torch.float64)
+        f = torch.from_numpy(f0.copy())
         f = f.pin_memory() if mode in ("copies", "zc_write", "zc_both") else f
         vir = m.post_force(0, xs[0], f.numpy(), virial=(mode == "virial"))
         outs.append(f.numpy().copy())
