@@ -169,6 +169,56 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /* NV * 
     }
 }
 
+// Warp sums of NV = 2^P doubles per lane, spread over the lanes: lane l ends
+// with the sum of value l >> (5 - P).  Lanes 16, 8, ... apart swap the halves
+// of their values each step (NV - 1 shuffles), then the remaining steps add
+// whole sums.  Every value is summed over the same tree of lanes as
+// block_sum's shuffle-down steps (pairs 16, 8, 4, 2, 1 apart; each addition
+// has the same two operands, possibly swapped), so the sums are equal bit
+// for bit.
+template <int NV> struct Log2NV { static constexpr int v = NV <= 1 ? 0 : 1 + Log2NV<NV / 2>::v; };
+template <> struct Log2NV<1> { static constexpr int v = 0; };
+
+template <int NV> __device__ __forceinline__ double warp_sum_spread(double (&v)[NV], int lane) {
+    constexpr int P = Log2NV<NV>::v;
+    static_assert((1 << P) == NV && P <= 5, "NV: a power of two up to 32");
+#pragma unroll
+    for (int st = 0; st < P; ++st) {
+        const int o = 16 >> st, h = (NV >> st) / 2;
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int j = 0; j < h; ++j) {
+            const double send = up ? v[j] : v[j + h];
+            const double keep = up ? v[j + h] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    double r = v[0];
+#pragma unroll
+    for (int st = P; st < 5; ++st) r += __shfl_xor_sync(0xffffffffu, r, 16 >> st);
+    return r;
+}
+
+// block_sum with the totals spread over warp 0 (lane l of warp 0 returns the
+// total of value l >> (5 - P); other warps return 0): the same totals bit
+// for bit, with NV - 1 + 5 - P shuffles per warp instead of 5 NV.
+template <int NV> __device__ __forceinline__ double block_sum_spread(double (&v)[NV], double *smem /* NV * 32 */) {
+    constexpr int P = Log2NV<NV>::v;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    const double r = warp_sum_spread<NV>(v, lane);
+    if ((lane & ((32 >> P) - 1)) == 0) smem[(lane >> (5 - P)) * 32 + warp] = r;
+    __syncthreads();
+    double tot = 0.0;
+    if (warp == 0) {
+        double w[NV];
+#pragma unroll
+        for (int t = 0; t < NV; ++t) w[t] = lane < nw ? smem[t * 32 + lane] : 0.0;
+        tot = warp_sum_spread<NV>(w, lane);
+    }
+    return tot;
+}
+
 }  // namespace mtd
 
 namespace mtd {

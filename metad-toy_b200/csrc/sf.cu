@@ -211,13 +211,14 @@ template <bool FP64, int QV> __global__ void __launch_bounds__(256) k_sk_partial
 #pragma unroll
             for (int t = 0; t < kSkChunk; ++t) acc[t] = facc[t];
         }
-        block_sum<kSkChunk>(acc, smem);
-        if (threadIdx.x == 0)
-            for (int q = 0; q < QV; ++q)
-                if (k0 + q < d.K) {
-                    d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * (k0 + q)] = acc[2 * q];
-                    d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * (k0 + q) + 1] = acc[2 * q + 1];
-                }
+        // the chunk's 2 QV block totals land on the lanes of warp 0 (lane l:
+        // value l >> (5 - log2(2 QV))), which write them side by side
+        const double tot = block_sum_spread<kSkChunk>(acc, smem);
+        constexpr int kSh = 5 - Log2NV<kSkChunk>::v;
+        if (threadIdx.x < 32 && (threadIdx.x & ((1 << kSh) - 1)) == 0) {
+            const int v = threadIdx.x >> kSh;
+            if (k0 + (v >> 1) < d.K) d.partials[(size_t)blockIdx.x * (2 * d.K + 2) + 2 * k0 + v] = tot;
+        }
         __syncthreads();
     }
     double c1[1] = {cnt};
