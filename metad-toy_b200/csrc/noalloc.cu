@@ -76,13 +76,10 @@ __global__ void __launch_bounds__(256) k_na_partial(int n, const double *__restr
                 }
             }
         }
-        block_sum<kNaChunk>(acc, smem);
-        if (threadIdx.x == 0)
-            for (int q = 0; q < kNaChunk / 2; ++q)
-                if (k0 + q < K) {
-                    scratch[row + 2 * (k0 + q)] = acc[2 * q];
-                    scratch[row + 2 * (k0 + q) + 1] = acc[2 * q + 1];
-                }
+        // block totals spread over warp 0 (lane l: value l / 4), as block_sum's
+        const double tot = block_sum_spread<kNaChunk>(acc, smem);
+        if (threadIdx.x < 32 && (threadIdx.x & 3) == 0 && k0 + (threadIdx.x >> 3) < K)
+            scratch[row + 2 * k0 + (threadIdx.x >> 2)] = tot;
         __syncthreads();
     }
     double c1[1] = {cnt};
