@@ -291,10 +291,13 @@ __device__ void phase_deposit(const BiasPlan &P, const double *s, double w, cons
 
 // A step whose neighbour lists overflowed is repeated by the host: it must
 // leave no hill and no bias force behind.
+// The four words are loaded together (no short-circuit between volatile
+// loads, which would wait for each in turn).
 __device__ __forceinline__ bool status_failed(const DevStatus *st) {
-    return st && (*(volatile const unsigned *)&st->overflow != 0u || *(volatile const unsigned *)&st->bad_pos != 0u ||
-                  *(volatile const unsigned *)&st->cand_overflow != 0u ||
-                  *(volatile const unsigned *)&st->timeout != 0u);
+    if (!st) return false;
+    const unsigned a = *(volatile const unsigned *)&st->overflow, b = *(volatile const unsigned *)&st->bad_pos,
+                   c = *(volatile const unsigned *)&st->cand_overflow, d = *(volatile const unsigned *)&st->timeout;
+    return (a | b | c | d) != 0u;
 }
 __device__ __forceinline__ bool step_failed(const BiasPlan &P) { return status_failed(P.status); }
 
