@@ -525,7 +525,7 @@ __device__ __forceinline__ void local_force_body(const LocalDev<T> &d, const dou
             T ux, uy, uz, rinv, sg, dsg;
             pair_geom<T, STEP>(d, a, j, ux, uy, uz, rinv, sg, dsg);
             T lj[S::SQ];
-            load_rec(d.lam + (size_t)j * S::SQ, lj);
+            load_rec32(d.lam + (size_t)j * S::SQ, lj);
             T Lm[S::SQ];
 #pragma unroll
             for (int q = 0; q < S::SA; ++q) Lm[q] = la[q] + sgnA * lj[q];
