@@ -11,14 +11,50 @@
 
 namespace mtd {
 
-// FP64 decision on raw coordinates (the oracle's criterion, operation by operation).
+// What the FP64 decision reads, taken by value by the out-of-line test: a
+// reference into a kernel parameter passed to a non-inlined function makes
+// every thread copy the whole parameter block to its stack at kernel entry.
+struct ExactSpec {
+    double L[3], invL[3];
+    int periodic[3];
+    double rc2, r0, eps;
+    SwParams sw;
+};
+__device__ __forceinline__ ExactSpec exact_spec(const GeoD &gd, const NeighSpec &ns) {
+    ExactSpec e;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        e.L[c] = gd.L[c];
+        e.invL[c] = gd.invL[c];
+        e.periodic[c] = gd.periodic[c];
+    }
+    e.rc2 = ns.rc2;
+    e.r0 = ns.r0;
+    e.eps = ns.eps;
+    e.sw = ns.sw;
+    return e;
+}
+
+// FP64 decision on the raw coordinates of sorted atoms k and j (the oracle's
+// criterion, operation by operation).  Out of line: the guard band is rare,
+// and its FP64 registers stay out of the callers' loops.
 template <int KIND>
-__device__ __noinline__ bool exact_decide(const GeoD &gd, const NeighSpec &ns, const double *xk, const double *xj) {
+__device__ __noinline__ bool exact_decide(const ExactSpec e, const double *__restrict__ xs, int k, int j) {
+    GeoD gd;
+    gd.xs = xs;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        gd.L[c] = e.L[c];
+        gd.invL[c] = e.invL[c];
+        gd.periodic[c] = e.periodic[c];
+    }
+    const double xk[3] = {xs[3 * k], xs[3 * k + 1], xs[3 * k + 2]};
+    const double xj[3] = {xs[3 * j], xs[3 * j + 1], xs[3 * j + 2]};
     double d[3];
     const double r2 = exact_disp(gd, xk, xj, d);
-    if (KIND == NK_RANGE) return (r2 <= ns.rc2) && (r2 >= 1e-12);
-    if (KIND == NK_STEP) return (r2 <= ns.rc2) && (__dsqrt_rn(r2) < ns.r0);
-    return (r2 <= ns.rc2) && (sw_f<double>(ns.sw, __dsqrt_rn(r2)) >= ns.eps);
+    if (KIND == NK_RANGE) return (r2 <= e.rc2) && (r2 >= 1e-12);
+    if (KIND == NK_STEP) return (r2 <= e.rc2) && (__dsqrt_rn(r2) < e.r0);
+    return (r2 <= e.rc2) && (sw_f<double>(e.sw, __dsqrt_rn(r2)) >= e.eps);
 }
 
 // The decision for a candidate at FP32 squared distance r2f.
@@ -27,9 +63,7 @@ __device__ __forceinline__ bool decide(const GeoD &gd, const NeighSpec &ns, cons
                                        float r2f) {
     if (r2f > ns.hi2) return false;
     if (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f) return true;
-    const double xk[3] = {xs[3 * k], xs[3 * k + 1], xs[3 * k + 2]};
-    const double xj[3] = {xs[3 * j], xs[3 * j + 1], xs[3 * j + 2]};
-    return exact_decide<KIND>(gd, ns, xk, xj);
+    return exact_decide<KIND>(exact_spec(gd, ns), xs, k, j);
 }
 
 // Skin-list filter of sorted atom k: the candidates found within cutoff +

@@ -205,9 +205,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbors(CellGrid g, SysDev s, Neig
                     if (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f) {
                         in = true;
                     } else {
-                        const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
-                        const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
-                        in = exact_decide<KIND>(gd, ns, xk, xj);
+                        in = exact_decide<KIND>(exact_spec(gd, ns), s.xs, k, j);
                     }
                     if (!in) continue;
                     if (cnt < nd.M) nd.list[(size_t)cnt * s.npad + k] = j;
@@ -322,9 +320,7 @@ __global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDe
         if (KIND == NK_CAND || (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f)) {
             in = true;
         } else {
-            const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
-            const double xj[3] = {s.xs[3 * jj], s.xs[3 * jj + 1], s.xs[3 * jj + 2]};
-            in = exact_decide<KIND>(gd, ns, xk, xj);
+            in = exact_decide<KIND>(exact_spec(gd, ns), s.xs, k, jj);
         }
         if (!in) continue;
         if (cnt < nd.M) nd.list[(size_t)cnt * s.npad + k] = jj;

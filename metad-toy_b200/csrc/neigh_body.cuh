@@ -134,9 +134,7 @@ __device__ __forceinline__ void neighbors_fast_body(const CellGrid &g, const Sys
                     if (KIND == NK_CAND || (KIND != NK_SWITCH && r2f < ns.lo2 && r2f > 1e-6f)) {
                         in = true;
                     } else {
-                        const double xk[3] = {s.xs[3 * k], s.xs[3 * k + 1], s.xs[3 * k + 2]};
-                        const double xj[3] = {s.xs[3 * j], s.xs[3 * j + 1], s.xs[3 * j + 2]};
-                        in = exact_decide<KIND>(gd, ns, xk, xj);
+                        in = exact_decide<KIND>(exact_spec(gd, ns), s.xs, k, j);
                     }
                     if (!in) continue;
                     if (cnt < nd.M) nd.list[(size_t)cnt * s.npad + k] = j;
