@@ -88,6 +88,18 @@ CellGrid make_grid(const mtd_ctx *c, double extra) {
         g.invLf[d] = 1.0f / (float)L;
         ncell *= nc;
     }
+    // tiles of 4 x 4 x 4 cells where the fast neighbour search applies (every
+    // periodic side with at least three cells)
+    g.tiled = 1;
+    for (int d = 0; d < 3; ++d)
+        if (g.periodic[d] && g.nc[d] < 3) g.tiled = 0;
+    if (g.tiled) {
+        ncell = 64;
+        for (int d = 0; d < 3; ++d) {
+            g.nt[d] = (g.nc[d] + 3) / 4;
+            ncell *= g.nt[d];
+        }
+    }
     g.ncell = (int)ncell;
     return g;
 }

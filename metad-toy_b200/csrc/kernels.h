@@ -24,11 +24,24 @@ namespace mtd {
 
 struct CellGrid {
     int nc[3];
-    int ncell;
+    int ncell;          // cell keys (with tiles: tiles x 64, the cells of partial tiles stay empty)
     int periodic[3];
     double L[3], invL[3], lo[3], h[3], inv_h[3];
     float hf[3], Lf[3], invLf[3];
+    // tiled = 1: cells are keyed (and atoms sorted) by 4 x 4 x 4 tiles of
+    // cells (nt tiles per dimension, tile-major, then x, y, z inside a tile),
+    // so a block of consecutive atoms is a compact piece of space and its
+    // neighbours' records are shared by its own threads; 0: row-major
+    // (x, y, z with z fastest), used where a periodic side has fewer than
+    // three cells (the general search walks runs of z cells)
+    int tiled, nt[3];
 };
+
+// Key of cell (x, y, z): the index of its atom range in the sorted order.
+__host__ __device__ inline int cell_key(const CellGrid &g, int x, int y, int z) {
+    if (!g.tiled) return (x * g.nc[1] + y) * g.nc[2] + z;
+    return ((((x >> 2) * g.nt[1] + (y >> 2)) * g.nt[2] + (z >> 2)) << 6) | ((x & 3) << 4) | ((y & 3) << 2) | (z & 3);
+}
 
 __host__ __device__ inline GeoF geo_f(const CellGrid &g, const float4 *pf) {
     GeoF r;

@@ -271,7 +271,6 @@ __global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDe
                 if (!g.periodic[1]) continue;
                 y += y < 0 ? ny : -ny;
             }
-            const int col = (x * ny + y) * nz;
 #pragma unroll
             for (int oz = 0; oz < 3; ++oz) {
                 int z = cz + oz - 1;
@@ -279,7 +278,8 @@ __global__ void __launch_bounds__(kFlatBlock) k_neighbors_flat(CellGrid g, SysDe
                     if (!g.periodic[2]) continue;
                     z += z < 0 ? nz : -nz;
                 }
-                const int b0 = __ldg(s.start + col + z), b1 = __ldg(s.start + col + z + 1);
+                const int key = cell_key(g, x, y, z);
+                const int b0 = __ldg(s.start + key), b1 = __ldg(s.start + key + 1);
                 // end < 2^26, the stencil offsets (2 bits each) above it
                 const unsigned code = (unsigned)ox | ((unsigned)oy << 2) | ((unsigned)oz << 4);
                 if (b0 < b1) rng[nr++][tid] = make_int2(b0, (int)((unsigned)b1 | (code << 26)));

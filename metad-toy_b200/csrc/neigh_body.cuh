@@ -32,7 +32,7 @@ __device__ __forceinline__ void bin_body(const CellGrid &g, const SysDev &s, int
     const int cx = cell_coord(x0, g, 0, w);
     const int cy = cell_coord(x1, g, 1, w);
     const int cz = cell_coord(x2, g, 2, w);
-    const int cell = (cx * g.nc[1] + cy) * g.nc[2] + cz;
+    const int cell = cell_key(g, cx, cy, cz);
     s.cellof[i] = cell;
     s.slot[i] = atomicAdd(&s.count[cell], 1);
 }
@@ -68,11 +68,11 @@ __device__ __forceinline__ void place_body(const CellGrid &g, const SysDev &s, i
         s.xref[3 * d + 1] = x1;
         s.xref[3 * d + 2] = x2;
     }
-    const int cz = c % g.nc[2], cy = (c / g.nc[2]) % g.nc[1], cx = c / (g.nc[2] * g.nc[1]);
+    // the cell coordinates bin_body keyed this atom by (same operations)
     double w0, w1, w2;
-    cell_coord(x0, g, 0, w0);
-    cell_coord(x1, g, 1, w1);
-    cell_coord(x2, g, 2, w2);
+    const int cx = cell_coord(x0, g, 0, w0);
+    const int cy = cell_coord(x1, g, 1, w1);
+    const int cz = cell_coord(x2, g, 2, w2);
     float4 p;
     p.x = (float)(w0 - cx * g.h[0]);
     p.y = (float)(w1 - cy * g.h[1]);
@@ -113,7 +113,6 @@ __device__ __forceinline__ void neighbors_fast_body(const CellGrid &g, const Sys
                 y += y < 0 ? ny : -ny;
             }
             const float sy = (float)oy * g.hf[1] - a.y;
-            const int col = (x * ny + y) * nz;
 #pragma unroll
             for (int oz = -1; oz <= 1; ++oz) {
                 int z = cz + oz;
@@ -122,7 +121,8 @@ __device__ __forceinline__ void neighbors_fast_body(const CellGrid &g, const Sys
                     z += z < 0 ? nz : -nz;
                 }
                 const float sz = (float)oz * g.hf[2] - a.z;
-                const int jb = __ldg(s.start + col + z), je = __ldg(s.start + col + z + 1);
+                const int key = cell_key(g, x, y, z);
+                const int jb = __ldg(s.start + key), je = __ldg(s.start + key + 1);
                 float4 nxt = jb < je ? __ldg(s.pf + jb) : make_float4(0.f, 0.f, 0.f, 0.f);
                 for (int j = jb; j < je; ++j) {
                     const float4 b = nxt;
