@@ -284,7 +284,6 @@ __device__ __forceinline__ void local_lq_body(const LocalDev<T> &d, int bid) {
 #pragma unroll
             for (int s = 0; s < S::SQ; ++s) A[s] = T(0);
         }
-        store_rec(d.lq + (size_t)k * S::SQ, A);
         d.lqs[2 * k] = lqA;
         d.lqs[2 * k + 1] = lqB;
         T e[4] = {T(0), T(0), T(0), T(0)};
@@ -315,6 +314,12 @@ __device__ __forceinline__ void local_lq_body(const LocalDev<T> &d, int bid) {
         }
 #pragma unroll
         for (int t = 0; t < 4; ++t) d.e12[4 * k + t] = e[t];
+        // the record's m = 0 imaginary slots (zero for LQ_l0, read by no
+        // one as LQ) carry e1 of each order, so the lambda pass gathers one
+        // record per neighbour instead of two
+        A[1] = e[0];
+        if constexpr (LB > 0) A[S::SA + 1] = e[2];
+        store_rec(d.lq + (size_t)k * S::SQ, A);
     }
     // the five totals (padded to eight) spread over warp 0, lane l holding
     // value l / 4: the same sums as block_sum's, with fewer shuffles
@@ -358,24 +363,25 @@ __device__ __forceinline__ void local_lambda_e1_body(const LocalDev<T> &d, int b
         store_rec(d.lam + (size_t)k * S::SQ, acc);
         return;
     }
+    // e1 of each order travels in the LQ record's m = 0 imaginary slot
+    // (written by the LQ pass), so each neighbour costs one record gather
     T lqk[S::SQ];
     load_rec32(d.lq + (size_t)k * S::SQ, lqk);
-    add_g<LA, T>(acc, lqk, d.e12[4 * k], T(1));
-    if constexpr (LB > 0) add_g<LB, T>(acc + S::SA, lqk + S::SA, d.e12[4 * k + 2], T(1));
+    add_g<LA, T>(acc, lqk, lqk[1], T(1));
+    if constexpr (LB > 0) add_g<LB, T>(acc + S::SA, lqk + S::SA, lqk[S::SA + 1], T(1));
     const auto a = d.geo.load(k);
     const int c = min(d.nb.count[k], d.nb.M);
     int jn = c > 0 ? nb_index(d.nb, d.npad, 0, k) : 0;
     for (int t = 0; t < c; ++t) {
         const int j = jn;
         if (t + 1 < c) jn = nb_index(d.nb, d.npad, t + 1, k);
-        T ej[4];
-        load_rec(d.e12 + 4 * (size_t)j, ej);
         T lqj[S::SQ];
         load_rec32(d.lq + (size_t)j * S::SQ, lqj);
-        if (ej[0] == T(0) && ej[2] == T(0)) continue;
+        const T e1A = lqj[1], e1B = LB > 0 ? lqj[S::SA + 1] : T(0);
+        if (e1A == T(0) && e1B == T(0)) continue;
         const T sg = pair_sigma<T, true>(d, a, j);
-        add_g<LA, T>(acc, lqj, ej[0], sg);
-        if constexpr (LB > 0) add_g<LB, T>(acc + S::SA, lqj + S::SA, ej[2], sg);
+        add_g<LA, T>(acc, lqj, e1A, sg);
+        if constexpr (LB > 0) add_g<LB, T>(acc + S::SA, lqj + S::SA, e1B, sg);
     }
     if (pdl) pdl_wait();
     const T inv = T(1) / nfk;
