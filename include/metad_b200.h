@@ -214,9 +214,17 @@ mtd_status mtd_neighbor_set_wait(mtd_ctx *ctx, int limit, int stall);
  *      one thread per caller index so every warp writes one contiguous
  *      stretch), no download;
  *   3  f read and written in place by the force pass (zero copy both ways).
- * 0 (default) is mode 3.  Forces are bitwise identical in every mode; the
- * fastest depends on the host platform.  Extension (no counterpart). */
+ * 0 (default): the fastest depends on the host platform (measured: mode 3 on
+ * some hosts, mode 1 on others), so the first eligible calls of
+ * mtd_post_force run modes 1-3 in turn (three timed calls each, after one
+ * warm-up call) and the mode with the lowest mean wall time is kept; setting
+ * 0 again starts a new trial.  Forces are bitwise identical in every mode.
+ * Extension (no counterpart). */
 mtd_status mtd_set_host_copy_mode(mtd_ctx *ctx, int mode);
+
+/* The host copy mode in use: the caller's, or the one the trial of mode 0
+ * picked (0 while the trial runs).  Extension (no counterpart). */
+mtd_status mtd_host_copy_mode_in_use(mtd_ctx *ctx, int *mode);
 
 /* Replays a HILLS file into the grid (rows `step cv[D] height sigma`).
  * Replaces GH_t0_uniformGrid::init_hills (src/grids/GH_t0_uniformGrid.cu:101-192). */

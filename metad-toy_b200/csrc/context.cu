@@ -11,6 +11,8 @@
 // without its host loops, PCIe round trips and per-call synchronisations.
 #include "context.h"
 
+#include <chrono>
+
 namespace {
 thread_local Prof *g_prof = nullptr;
 thread_local bool g_pdl = false;
@@ -1342,14 +1344,25 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
     // writes f over the host link in caller order (zero copy, no download),
     // and with mode 3 also reads it there (no upload)
     double *zf = nullptr;
-    const int mode = c->host_copy_mode == 0 ? 3 : c->host_copy_mode;
-    if (mode >= 2 && !virial && n >= 4096 && single_local_unit(c)) {
+    c->copy_used = 0;
+    if (!virial && n >= 4096 && single_local_unit(c)) {
         cudaPointerAttributes pa{};
         if (cudaPointerGetAttributes(&pa, f) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer)
             zf = static_cast<double *>(pa.devicePointer);
         else
             cudaGetLastError();
     }
+    // the mode: the caller's, else the one timing picked, else the next to try
+    // (the first eligible call warms up in mode 3 and is not counted)
+    int mode = c->host_copy_mode;
+    if (mode == 0 && zf) {
+        if (c->copy_pick) mode = c->copy_pick;
+        else mode = c->copy_calls == 0 ? 3 : 1 + (c->copy_calls - 1) % 3;
+        c->copy_used = mode;
+    } else if (mode == 0) {
+        mode = 3;
+    }
+    if (mode < 2) zf = nullptr;
     const bool upload = !zf || mode == 2;
     if (upload) {
         MTD_CU(cudaEventRecord(c->f_ready, c->st), "force upload");   // the side copies start after the previous step
@@ -1387,9 +1400,28 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
 }
 }  // namespace
 
+// Host copy mode 0: after the call, the wall time of a trial call counts for
+// its mode; once each of modes 1-3 has three, the fastest mean is kept.
+static void record_copy_trial(mtd_ctx *c, double ms) {
+    if (c->copy_pick || c->copy_used == 0) return;
+    const int m = c->copy_used;
+    if (c->copy_calls > 0) {
+        c->copy_ms[m] += ms;
+        c->copy_cnt[m] += 1;
+    }
+    c->copy_calls += 1;
+    if (c->copy_cnt[1] >= 3 && c->copy_cnt[2] >= 3 && c->copy_cnt[3] >= 3) {
+        int best = 3;
+        for (int k = 1; k <= 3; ++k)
+            if (c->copy_ms[k] / c->copy_cnt[k] < c->copy_ms[best] / c->copy_cnt[best]) best = k;
+        c->copy_pick = best;
+    }
+}
+
 mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, const int *mask, const int *image,
                           double *f, double virial[6]) {
     if (!c || n < 0 || (n > 0 && (!x || !f))) return MTD_ERR_INVALID_ARG;
+    const auto t_call = std::chrono::steady_clock::now();
     if (!c->initialized) {
         mtd_status s = mtd_init(c);
         if (s != MTD_OK) return s;
@@ -1403,7 +1435,10 @@ mtd_status mtd_post_force(mtd_ctx *c, int64_t step, int n, const double *x, cons
     MTD_CU(h2d_pieces(c->d_x, x, b3, c->st), "x upload");
     prof_mark("x_upload", c->st);
     if (mask) MTD_CU(cudaMemcpyAsync(c->d_mask, mask, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st), "mask upload");
-    return step_uploaded(c, step, n, mask != nullptr, image, f, virial);
+    s = step_uploaded(c, step, n, mask != nullptr, image, f, virial);
+    if (s == MTD_OK)
+        record_copy_trial(c, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count());
+    return s;
 }
 
 mtd_status mtd_set_positions_f64(mtd_ctx *c, const double *x, const int *type, const int *mask, int n, int groupbit) {

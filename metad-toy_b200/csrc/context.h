@@ -179,7 +179,14 @@ struct mtd_ctx {
     cudaStream_t own_st = nullptr;
     cudaStream_t side_st = nullptr;      // host -> device force upload beside the CV passes
     bool zc_on = false;                  // this step's force pass writes pinned host f in caller order
-    int host_copy_mode = 0;              // mtd_set_host_copy_mode
+    int host_copy_mode = 0;              // mtd_set_host_copy_mode (0: chosen by timing)
+    // mode 0: the first eligible mtd_post_force calls try modes 1-3 in turn
+    // (wall time of each call), then the fastest is kept
+    int copy_pick = 0;                   // the mode chosen (0: still trying)
+    int copy_calls = 0;                  // eligible calls seen while trying
+    int copy_used = 0;                   // mode of the call in progress (0: not eligible)
+    double copy_ms[4] = {0, 0, 0, 0};
+    int copy_cnt[4] = {0, 0, 0, 0};
     // hill-list bias (CV_dim 4 or NN_BIAS 1): hills, exact sum, learned bias
     mtd_nnbias *nb = nullptr;
     double *d_vdv = nullptr;             // V, dV/ds at this step's s

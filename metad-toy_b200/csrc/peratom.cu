@@ -108,6 +108,20 @@ mtd_status mtd_neighbor_stats(mtd_ctx *c, int64_t *rebuilds, int *skin_active) {
 mtd_status mtd_set_host_copy_mode(mtd_ctx *c, int mode) {
     if (!c || mode < 0 || mode > 3) return MTD_ERR_INVALID_ARG;
     c->host_copy_mode = mode;
+    if (mode == 0) {   // time the modes again
+        c->copy_pick = 0;
+        c->copy_calls = 0;
+        for (int k = 0; k < 4; ++k) {
+            c->copy_ms[k] = 0.0;
+            c->copy_cnt[k] = 0;
+        }
+    }
+    return MTD_OK;
+}
+
+mtd_status mtd_host_copy_mode_in_use(mtd_ctx *c, int *mode) {
+    if (!c || !mode) return MTD_ERR_INVALID_ARG;
+    *mode = c->host_copy_mode ? c->host_copy_mode : c->copy_pick;
     return MTD_OK;
 }
 

@@ -29,7 +29,7 @@ PREC = {"mixed": 0, "fp64": 1}
 # Every entry point declared in include/metad_b200.h.
 EXPORTS = ["mtd_options_default", "mtd_create", "mtd_destroy", "mtd_parse_args", "mtd_eval_expression", "mtd_set_box", "mtd_init", "mtd_post_force",
            "mtd_post_force_device", "mtd_sync", "mtd_compute_scalar", "mtd_compute_vector", "mtd_cv_dim",
-           "mtd_extract_peratom", "mtd_get_neighbors", "mtd_neighbor_stats", "mtd_neighbor_set_wait", "mtd_set_host_copy_mode", "mtd_sk_tiles", "mtd_set_sk_tiles", "mtd_get_tuning", "mtd_set_tuning_all", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
+           "mtd_extract_peratom", "mtd_get_neighbors", "mtd_neighbor_stats", "mtd_neighbor_set_wait", "mtd_set_host_copy_mode", "mtd_host_copy_mode_in_use", "mtd_sk_tiles", "mtd_set_sk_tiles", "mtd_get_tuning", "mtd_set_tuning_all", "mtd_hills_replay", "mtd_get_grid", "mtd_last_launch_count",
            "mtd_set_stream", "mtd_profile_enable", "mtd_profile_report",
            "mtd_max_neighbors", "mtd_last_error", "mtd_abi_version", "mtd_sk_noalloc", "mtd_nn_state",
            "mtd_nnbias_create", "mtd_nnbias_destroy", "mtd_nnbias_last_error", "mtd_nnbias_add_hills",
@@ -110,6 +110,7 @@ def lib():
         L.mtd_neighbor_stats.argtypes = [vp, C.POINTER(C.c_int64), ip]
         L.mtd_neighbor_set_wait.argtypes = [vp, C.c_int, C.c_int]
         L.mtd_set_host_copy_mode.argtypes = [vp, C.c_int]
+        L.mtd_host_copy_mode_in_use.argtypes = [vp, C.POINTER(C.c_int)]
         L.mtd_sk_tiles.argtypes = [vp, ip, ip]
         L.mtd_get_tuning.argtypes = [vp, ip]
         L.mtd_set_tuning_all.argtypes = [vp, ip]
@@ -364,8 +365,15 @@ class Metad:
         self._check(lib().mtd_set_sk_tiles(self._h, int(q_values), int(q_force)))
 
     def set_host_copy_mode(self, mode):
-        """f over the host link for mtd_post_force: 1 copies, 2 upload + zero-copy write (default), 3 zero copy."""
+        """f over the host link for mtd_post_force: 1 copies, 2 upload + zero-copy write, 3 zero copy;
+        0 (default): the first calls time modes 1-3 and the fastest is kept."""
         self._check(lib().mtd_set_host_copy_mode(self._h, int(mode)))
+
+    def host_copy_mode_in_use(self):
+        """The caller's mode, or the one the timing trial of mode 0 picked (0 while it runs)."""
+        m = C.c_int()
+        self._check(lib().mtd_host_copy_mode_in_use(self._h, C.byref(m)))
+        return m.value
 
     def neighbor_set_wait(self, limit=0, stall=False):
         """Grid-barrier wait limit of the one-launch skin-list rebuild (0: default);

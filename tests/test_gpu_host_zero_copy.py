@@ -62,3 +62,38 @@ def test_zero_copy_host_forces_equal_device_path(precision, skin):
             assert np.all(np.isfinite(vir))
         m.close()
     assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+def test_default_mode_times_the_modes_and_keeps_the_forces():
+    """Mode 0: the first eligible calls run modes 1-3 in turn (one warm-up
+    call, then three timed calls each) and the fastest is kept; every call's
+    forces equal the device-buffer path's bit for bit whatever mode ran."""
+    import torch
+
+    x0, L = _system()
+    args = H.fix_args_local(pace=3) + ["NEIGH_SKIN", 0.6]
+    host = mtd.Metad(args, precision="mixed")
+    dev = mtd.Metad(args, precision="mixed")
+    for m in (host, dev):
+        m.set_box([0, 0, 0], L)
+    assert host.host_copy_mode_in_use() == 0
+    for s in range(13):
+        x = np.ascontiguousarray(systems.wrap(systems.jitter(x0, 0.02, 300 + s), L))
+        f_in = np.random.default_rng(40 + s).normal(size=x.shape)
+        fh = torch.from_numpy(f_in.copy()).pin_memory()
+        host.post_force(s, x, fh.numpy())
+        dx = torch.from_numpy(x).cuda()
+        df_in = torch.from_numpy(f_in).cuda()
+        df = torch.empty_like(df_in)
+        dev.post_force_device(s, x.shape[0], dx.data_ptr(), df_in.data_ptr(), df.data_ptr())
+        dev.sync()
+        assert np.array_equal(fh.numpy(), df.cpu().numpy()), s
+        if s < 9:
+            assert host.host_copy_mode_in_use() == 0
+    assert host.host_copy_mode_in_use() in (1, 2, 3)
+    host.set_host_copy_mode(0)   # a new trial
+    assert host.host_copy_mode_in_use() == 0
+    host.set_host_copy_mode(2)
+    assert host.host_copy_mode_in_use() == 2
+    host.close()
+    dev.close()
