@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(kBlock) k_filter(CellGrid g, SysDev s, NeighSp
 // kernels, so the sorted order and the candidate lists are the same.  A
 // barrier wait that runs out marks the step (status->timeout, no deposit, no
 // bias force) and the skin state invalid (the next step rebuilds from scratch).
-__global__ void __launch_bounds__(kPersistBlock, 6) k_rebuild(CellGrid g, SysDev s, NeighSpec ns, NeighDev cd,
+__global__ void __launch_bounds__(kPersistBlock, 8) k_rebuild(CellGrid g, SysDev s, NeighSpec ns, NeighDev cd,
                                                            DevStatus *status, GridBar *bar, int limit, int stall) {
     pdl_entry();
     if (gate_closed(s.skin)) return;
