@@ -444,9 +444,9 @@ def run_secondary(args, local):
 # pass accumulates cos and sin (2) and the force pass projects on rho(k) and
 # k (9).
 # per (atom, k): FP64 phase (k / pi).x (5) and half-turn reduction (3 adds);
-# FP32 z^2, sin(pi z) (6 FMA + 1 mul), cos(pi z) (6 FMA), then the signed
+# FP32 z^2, sin(pi z) (4 FMA + 1 mul), cos(pi z) (5 FMA), then the signed
 # accumulation (2 FMA) or the force weight and gradient (1 mul + 1 FMA + 3 FMA)
-SK_FLOP_PER_PAIR = {"sk_partial": {"fp64": 8, "fp32": 30}, "sk_force": {"fp64": 8, "fp32": 35}}
+SK_FLOP_PER_PAIR = {"sk_partial": {"fp64": 8, "fp32": 24}, "sk_force": {"fp64": 8, "fp32": 29}}
 
 
 def sk_roofline(kernels, n, nk, clocks):

@@ -239,19 +239,20 @@ __device__ __forceinline__ void unpack_image(int img, int &ix, int &iy, int &iz)
 // u is rounded to the nearest integer n in FP64 (adding 1.5 * 2^52 leaves n
 // in the low mantissa bits, so no rounding or conversion instruction), the
 // remainder f = u - n in [-1/2, 1/2] is exact in FP64 and goes to FP32,
-// sin(pi f) and cos(pi f) come from their Taylor series to degree 13 and 12
-// in pi f (the first omitted terms are below 6.7e-10 and 6.4e-9 for
-// |pi f| <= pi / 2), and (-1)^n flips both signs.  |u| < 2^51.
-constexpr double kPi2 = kPi * kPi;
-constexpr float kSin1 = (float)kPi, kSin3 = (float)(-kPi * kPi2 / 6.0), kSin5 = (float)(kPi * kPi2 * kPi2 / 120.0),
-                kSin7 = (float)(-kPi * kPi2 * kPi2 * kPi2 / 5040.0),
-                kSin9 = (float)(kPi * kPi2 * kPi2 * kPi2 * kPi2 / 362880.0),
-                kSin11 = (float)(-kPi * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 39916800.0),
-                kSin13 = (float)(kPi * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 6227020800.0);
-constexpr float kCos2 = (float)(-kPi2 / 2.0), kCos4 = (float)(kPi2 * kPi2 / 24.0),
-                kCos6 = (float)(-kPi2 * kPi2 * kPi2 / 720.0), kCos8 = (float)(kPi2 * kPi2 * kPi2 * kPi2 / 40320.0),
-                kCos10 = (float)(-kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 3628800.0),
-                kCos12 = (float)(kPi2 * kPi2 * kPi2 * kPi2 * kPi2 * kPi2 / 479001600.0);
+// sin(pi f) = f P(f^2) and cos(pi f) = Q(f^2) come from polynomials of
+// degree 4 and 5 in f^2, and (-1)^n flips both signs.  |u| < 2^51.
+// P and Q are near-minimax on f in [0, 1/2]: least squares on Chebyshev
+// nodes, reweighted toward equal error peaks (Lawson's algorithm), with
+// maximum errors 6.7e-9 and 2.2e-10 in exact arithmetic, below the FP32
+// rounding of the result (1.6e-7 with FP32 evaluation, the same as the
+// degree-13 / degree-12 Taylor series they replace, two and one FMA fewer;
+// fit_sincospi.py beside the library regenerates them).
+constexpr float kSinP0 = (float)3.1415926402242746, kSinP1 = (float)-5.167710094404562,
+                kSinP2 = (float)2.5500777409855013, kSinP3 = (float)-0.5982926899608115,
+                kSinP4 = (float)0.07766048988359421;
+constexpr float kCosQ0 = (float)0.9999999997811803, kCosQ1 = (float)-4.934802137317261,
+                kCosQ2 = (float)4.058709167239208, kCosQ3 = (float)-1.3352120902337075,
+                kCosQ4 = (float)0.23493771734282284, kCosQ5 = (float)-0.02439697684324065;
 constexpr double kInvPi = 0.31830988618379067154;
 
 // The sign flip of halfturn_sincos_f32 as a bit mask (bit 31 set for odd n),
@@ -262,19 +263,16 @@ __device__ __forceinline__ unsigned halfturn_sincos_f32_parts(double u, float &s
     const double t = u + kRound;
     const double f = u - (t - kRound);
     const float z = (float)f, z2 = z * z;
-    float p = fmaf(z2, kSin13, kSin11);
-    p = fmaf(p, z2, kSin9);
-    p = fmaf(p, z2, kSin7);
-    p = fmaf(p, z2, kSin5);
-    p = fmaf(p, z2, kSin3);
-    p = fmaf(p, z2, kSin1);
+    float p = fmaf(z2, kSinP4, kSinP3);
+    p = fmaf(p, z2, kSinP2);
+    p = fmaf(p, z2, kSinP1);
+    p = fmaf(p, z2, kSinP0);
     s0 = p * z;
-    float q = fmaf(z2, kCos12, kCos10);
-    q = fmaf(q, z2, kCos8);
-    q = fmaf(q, z2, kCos6);
-    q = fmaf(q, z2, kCos4);
-    q = fmaf(q, z2, kCos2);
-    c0 = fmaf(q, z2, 1.0f);
+    float q = fmaf(z2, kCosQ5, kCosQ4);
+    q = fmaf(q, z2, kCosQ3);
+    q = fmaf(q, z2, kCosQ2);
+    q = fmaf(q, z2, kCosQ1);
+    c0 = fmaf(q, z2, kCosQ0);
     return (unsigned)__double2loint(t) << 31;
 }
 
