@@ -217,7 +217,7 @@ mtd_status mtd_neighbor_set_wait(mtd_ctx *ctx, int limit, int stall);
  * 0 (default): the fastest depends on the host platform (measured: mode 3 on
  * some hosts, mode 1 on others), so the first eligible calls of
  * mtd_post_force run modes 1-3 in turn (three timed calls each, after one
- * warm-up call) and the mode with the lowest mean wall time is kept; setting
+ * warm-up call) and the mode with the fastest call is kept; setting
  * 0 again starts a new trial.  Forces are bitwise identical in every mode.
  * Extension (no counterpart). */
 mtd_status mtd_set_host_copy_mode(mtd_ctx *ctx, int mode);

@@ -11,6 +11,7 @@
 // without its host loops, PCIe round trips and per-call synchronisations.
 #include "context.h"
 
+#include <algorithm>
 #include <chrono>
 
 namespace {
@@ -1401,19 +1402,21 @@ mtd_status step_uploaded(mtd_ctx *c, int64_t step, int n, bool has_mask, const i
 }  // namespace
 
 // Host copy mode 0: after the call, the wall time of a trial call counts for
-// its mode; once each of modes 1-3 has three, the fastest mean is kept.
+// its mode; once each of modes 1-3 has three, the mode with the fastest call
+// is kept (the minimum: a call slowed by something else says nothing about
+// its mode, while the mean of three would carry it).
 static void record_copy_trial(mtd_ctx *c, double ms) {
     if (c->copy_pick || c->copy_used == 0) return;
     const int m = c->copy_used;
     if (c->copy_calls > 0) {
-        c->copy_ms[m] += ms;
+        c->copy_ms[m] = c->copy_cnt[m] ? std::min(c->copy_ms[m], ms) : ms;
         c->copy_cnt[m] += 1;
     }
     c->copy_calls += 1;
     if (c->copy_cnt[1] >= 3 && c->copy_cnt[2] >= 3 && c->copy_cnt[3] >= 3) {
         int best = 3;
         for (int k = 1; k <= 3; ++k)
-            if (c->copy_ms[k] / c->copy_cnt[k] < c->copy_ms[best] / c->copy_cnt[best]) best = k;
+            if (c->copy_ms[k] < c->copy_ms[best]) best = k;
         c->copy_pick = best;
     }
 }

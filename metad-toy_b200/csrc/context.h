@@ -181,7 +181,7 @@ struct mtd_ctx {
     bool zc_on = false;                  // this step's force pass writes pinned host f in caller order
     int host_copy_mode = 0;              // mtd_set_host_copy_mode (0: chosen by timing)
     // mode 0: the first eligible mtd_post_force calls try modes 1-3 in turn
-    // (wall time of each call), then the fastest is kept
+    // (wall time of each call), then the mode with the fastest call is kept
     int copy_pick = 0;                   // the mode chosen (0: still trying)
     int copy_calls = 0;                  // eligible calls seen while trying
     int copy_used = 0;                   // mode of the call in progress (0: not eligible)

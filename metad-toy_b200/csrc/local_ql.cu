@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kBlock) k_local_lambda(LocalDev<T> d) {
 }
 
 template <int LA, int LB, typename T, bool STEP, bool CALLER = false>
-__global__ void __launch_bounds__(kBlock, CALLER ? 3 : 4) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
+__global__ void __launch_bounds__(kBlock, CALLER ? 2 : 4) k_local_force(LocalDev<T> d, const double *__restrict__ f_src,
                                                         double *__restrict__ f_dst, SysDev s, CellGrid g,
                                                         double *vpart, DevStatus *status) {
     pdl_entry();
